@@ -1,0 +1,356 @@
+#!/usr/bin/env python
+"""Benchmark of the ESVO ray-casting path on B200.
+
+Workload (one step = one frame): the 1024^3 cave scene (value noise, spacing
+64, 5 octaves, 50 % fill, depth 10, DXT1 bricks) and 1920x1080 FP32 primary
+rays from a seeded empty voxel in a seeded direction; each rank renders its
+own camera (weak scaling, no data-path collective).  `value` is Mrays/s of the
+device-resident cast kernel (rays and hits in HBM, L2 flushed between steps);
+`e2e` is the same metric through vx_cast_rays_host with pinned host buffers,
+copies included.  `--impl reference` times the CPU restatement of the
+reference castRay on this host's cores instead.
+"""
+import argparse
+import ctypes as C
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "vbvs--vixen_b200")
+METRIC = "Mrays/s on 1 B200, batched vs plain at bit-exact hits; fwd+bwd ms/view"
+
+
+def load_pkg():
+    if "vx_b200" in sys.modules:
+        return sys.modules["vx_b200"]
+    spec = importlib.util.spec_from_file_location("vx_b200", os.path.join(PKG_DIR, "__init__.py"),
+                                                  submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["vx_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import vx_oracle
+    return vx_oracle
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled while work runs."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 7:
+                continue
+            try:
+                sm.append(float(p[0]))
+                mx.append(float(p[1]))
+            except ValueError:
+                continue
+            for k, n in enumerate(names):
+                if p[3 + k].lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_workload(vx, R, seed, rank, use_gpu_gen):
+    from vx_b200 import workloads as W
+    import numpy as np
+    spacing, octaves = 64 * R // 1024, 5 if R >= 1024 else 3
+    if use_gpu_gen:
+        bits = vx.synth_noise_dev(R, spacing, octaves, 0.5, seed, False).cpu().numpy().view(np.uint64)
+    else:
+        bits = vx.synth_noise(R, spacing, octaves, 0.5, seed, False)
+    wl = W.config2(R=R, seed=seed, bits=bits)
+    if rank:
+        wl.camera = W.empty_voxel_camera(bits, R, seed + 7919 * rank, 70.0, wl.width, wl.height)
+    return wl
+
+
+def bytes_per_launch(n, iters, grid_reads, dda_steps, hits, color_kind):
+    """Algorithmic bytes of one cast launch (per-ray terms counted by the traversal):
+    24 ray in + 16 hit record out + colour out (12 B DXT1 texel / 4 B RGBA8) per ray,
+    8 per ESVO iteration (one descriptor), 4 per brick-grid lookup, 4 per DDA step
+    (one occupancy word), plus the colour fetch of every hit (8 B DXT1 block / 4 B RGBA8)."""
+    cout, cin = (12, 8) if color_kind == 2 else ((4, 4) if color_kind == 1 else (0, 0))
+    return n * (24 + 16 + cout) + 8 * iters + 4 * grid_reads + 4 * dda_steps + cin * hits
+
+
+def cpu_baseline(vo, wl, rays, g_hits, budget_s=12.0):
+    """Times the oracle (CPU restatement of castRay) on a bounded prefix of the
+    frame with every host thread, and checks those rays against the GPU."""
+    import numpy as np
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    o = vo.OracleScene.from_dense(wl.bits, wl.R, wl.scene.max_levels)
+    build_s = time.perf_counter() - t0
+    n = min(rays.shape[0], 1 << 16)
+    while True:
+        t0 = time.perf_counter()
+        oh = o.cast_rays(rays[:n], threads=threads)
+        dt = time.perf_counter() - t0
+        if dt >= budget_s / 4 or n >= rays.shape[0]:
+            break
+        n = min(rays.shape[0], n * 4)
+    g = g_hits[:n]
+    hit = (oh["flags"] & 1).astype(bool)
+    mism = int(np.count_nonzero((g["flags"].astype(np.uint32) != oh["flags"]) | (g["brick"] != oh["brick"]) |
+                                (g["node"] != oh["node"]) | (g["voxel"].astype(np.uint32) != oh["voxel"]) |
+                                (hit & (g["t"].view(np.uint32) != oh["t"].view(np.uint32)))))
+    return {"value": n / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
+            "sample": f"first {n} rays of the frame ({n / rays.shape[0]:.1%}), {threads} threads, "
+                      f"{dt:.2f} s; oracle build {build_s:.1f} s"}, {"checked": n, "mismatches": mism}
+
+
+def run_reference(args, rank, world):
+    """CPU restatement of the reference castRay on all host cores."""
+    if rank != 0:
+        return 0
+    import numpy as np
+    vx = load_pkg()
+    vo = load_oracle()
+    use_gpu = False
+    try:
+        import torch
+        use_gpu = torch.cuda.is_available()
+    except Exception:
+        pass
+    wl = make_workload(vx, args.R, args.seed, 0, use_gpu)
+    rays = wl.rays()
+    threads = os.cpu_count() or 1
+    o = vo.OracleScene.from_dense(wl.bits, wl.R, wl.scene.max_levels)
+    n = min(rays.shape[0], 1 << 15)
+    while True:  # size one step at about 3 s
+        t0 = time.perf_counter()
+        o.cast_rays(rays[:n], threads=threads)
+        dt = time.perf_counter() - t0
+        if dt >= 0.75 or n >= rays.shape[0]:
+            break
+        n = min(rays.shape[0], n * 4)
+    n = min(rays.shape[0], max(1024, int(n * 3.0 / max(dt, 1e-3))))
+    for _ in range(args.warmup):
+        o.cast_rays(rays[:n], threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        o.cast_rays(rays[:n], threads=threads)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    v = n * args.steps / total / 1e6
+    line = {"metric": METRIC, "value": v, "unit": "Mrays/s", "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": config_dict(wl, world),
+            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": threads, "kind": "port",
+                             "sample": f"first {n} of {rays.shape[0]} rays per step, {threads} threads"},
+            "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def config_dict(wl, world):
+    return {"workload": f"{wl.name}: cave {wl.R}^3 (depth {wl.scene.max_levels}), value noise spacing "
+                        f"{64 * wl.R // 1024}, 5 octaves, 50% fill, DXT1 bricks, {wl.width}x{wl.height} FP32 "
+                        f"primary rays per rank, plain cast kernel",
+            "rays_per_step_per_gpu": wl.width * wl.height, "bricks": int(wl.scene.brick_count),
+            "nodes": int(wl.scene.node_count), "parallelism": f"replicated scene, {world} camera(s)",
+            "l2": "flushed between timed steps (256 MiB write)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="vx", choices=["vx", "reference"])
+    ap.add_argument("--R", type=int, default=1024)
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    vx = load_pkg()
+    wl = make_workload(vx, args.R, args.seed, rank, True)
+    scene = vx.Scene(wl.scene)
+    rays_np = wl.rays()
+    n = rays_np.shape[0]
+    rays = torch.from_numpy(rays_np).cuda()
+    hits = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+    color = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+    counters = torch.zeros((n,), dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    # Counting pass (untimed): per-ray work for the algorithmic-byte count.
+    scene.cast_rays_dev(rays, hits, color, counters)
+    torch.cuda.synchronize()
+    cnt = counters.cpu().numpy().view(vx.COUNTER_DTYPE).reshape(-1)
+    g_hits = hits.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1).copy()
+    nhit = int(np.count_nonzero(g_hits["flags"] & 1))
+    algo_bytes = bytes_per_launch(n, int(cnt["iters"].astype(np.int64).sum()),
+                                  int(cnt["grid_reads"].astype(np.int64).sum()),
+                                  int(cnt["dda_steps"].astype(np.int64).sum()), nhit, scene.color_kind)
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    sampler = ClockSampler(local)
+    sampler.start()
+    t_soak = time.perf_counter()
+    for _ in range(args.warmup):
+        scene.cast_rays_dev(rays, hits, color)
+    torch.cuda.synchronize()
+    while time.perf_counter() - t_soak < 1.5:  # bring clocks to steady state before timing
+        for _ in range(20):
+            scene.cast_rays_dev(rays, hits, color)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.zero_()
+        ev0[k].record(stream)
+        scene.cast_rays_dev(rays, hits, color)
+        ev1[k].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in zip(ev0, ev1)]
+    total_ms = sum(step_ms)
+
+    # e2e through the host-buffer entry point: pinned rays in, hits + texels out.
+    rays_h = torch.from_numpy(rays_np).pin_memory()
+    hits_h = torch.zeros((n, 4), dtype=torch.int32).pin_memory()
+    col_h = torch.zeros((n, 3), dtype=torch.float32).pin_memory()
+    L = vx.lib()
+
+    def e2e_call():
+        vx.check(L.vx_cast_rays_host(scene.handle, C.c_void_p(rays_h.data_ptr()), n, 0.0, vx.FLT_MAX,
+                                     C.c_void_p(hits_h.data_ptr()), C.c_void_p(col_h.data_ptr()),
+                                     C.c_void_p(stream.cuda_stream)))
+
+    for _ in range(args.warmup):
+        e2e_call()
+    e0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    e1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.zero_()
+        e0[k].record(stream)
+        e2e_call()
+        e1[k].record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in zip(e0, e1))
+    e2e_same = bool(np.array_equal(hits_h.numpy().view(np.uint8), g_hits.view(np.uint8).reshape(n, 16)))
+
+    t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms, e2e_ms = float(t[0]), float(t[1])
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    value = world * n * args.steps / (total_ms / 1e3) / 1e6
+    e2e_value = world * n * args.steps / (e2e_ms / 1e3) / 1e6
+    mean_s = statistics.mean(step_ms) / 1e3
+    peak, peak_kind = measured_peaks()
+    achieved = algo_bytes / mean_s / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "cast_kernel_traffic.json")
+    if os.path.exists(tf):
+        try:
+            with open(tf) as f:
+                d = json.load(f)
+            if d.get("workload") == wl.name:
+                traffic = d.get("dram_bytes_per_launch")
+        except Exception:
+            pass
+    line = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_dict(wl, world),
+            "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": world * n * 24,
+                    "d2h_bytes_per_step": world * n * (16 + 12), "hits_equal_device_path": e2e_same},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": algo_bytes,
+                         "kernel": "vx::cast_kernel", "kernel_ms_mean": mean_s * 1e3},
+            "gpu_launches": args.steps, "hit_rate": nhit / n,
+            "clocks": clocks}
+    if world == 1 and not args.no_cpu_baseline:
+        vo = load_oracle()
+        cb, parity = cpu_baseline(vo, wl, rays_np, g_hits)
+        line["cpu_baseline"] = cb
+        line["parity_sample"] = parity
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

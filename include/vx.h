@@ -1,0 +1,262 @@
+/*
+ * vx.h - C ABI of libvx: B200-native ESVO voxel ray casting.
+ *
+ * Drop-in boundary for the reference's voxel ray-casting hot path
+ * (Lint111/VBVS--VIXEN).  Each entry point names the reference interface it
+ * replaces; paths are relative to the reference project's VIXEN/ directory.
+ *
+ * Conventions
+ *  - Plain C types only.  A stream is passed as `void*` holding a
+ *    cudaStream_t (NULL = legacy default stream).
+ *  - Every call returns VX_OK or a negative vx_status; the message of the
+ *    last error on the calling thread is in vx_last_error_string().  No C++
+ *    exception crosses this boundary (the reference nodes throw
+ *    std::runtime_error, ComputeDispatchNode.cpp:67,78,100,227).
+ *  - A vx_scene is immutable after creation and may be used from any host
+ *    thread; device work is ordered on the stream given to each call.
+ *  - "_dev" pointers are device pointers (cudaMalloc / torch tensors) on the
+ *    scene's device; "_host" pointers are host memory (pinned for best speed).
+ */
+#ifndef VX_H
+#define VX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VX_ABI_VERSION 1
+
+typedef enum vx_status {
+    VX_OK = 0,
+    VX_EINVAL = -1,     /* bad argument or malformed scene buffers */
+    VX_ECUDA = -2,      /* a CUDA runtime call failed */
+    VX_EOVERFLOW = -3,  /* a size is beyond a format limit */
+    VX_ETIMEOUT = -4,   /* a bounded device-side wait gave up */
+    VX_ENOMEM = -5,     /* host or device allocation failed */
+    VX_ENOTFOUND = -6   /* no CUDA device, or the library was built without one */
+} vx_status;
+
+/* ------------------------------------------------------------------------
+ * Device data layout
+ * --------------------------------------------------------------------- */
+
+/* One octree node ("child descriptor"), 8 bytes.
+ * Replaces ChildDescriptor (SVO/include/SVOTypes.h:36-117), whose 15-bit
+ * childPointer is widened to 32 bits so scenes above 32,767 descriptors
+ * keep the indices an unbounded reference would produce.
+ *   child_ptr : index of the first child descriptor (children are stored
+ *               contiguously, non-leaf children first, octant ascending)
+ *   masks     : valid_mask (bits 0-7) | leaf_mask (bits 8-15)        */
+typedef struct vx_node {
+    uint32_t child_ptr;
+    uint32_t masks;
+} vx_node;
+
+/* The OctreeConfig fields the traversal needs
+ * (RenderGraph/src/Nodes/VoxelGridNode.cpp:36-66; filled at
+ * CashSystem/src/VoxelSceneCacher.cpp:592-625). */
+typedef struct vx_octree_config {
+    float world_min[3];     /* rebuild() bounds (SVORebuild.cpp:228) */
+    float world_max[3];
+    int32_t max_levels;     /* userMaxLevels (octree depth), 1..23 */
+    int32_t brick_depth;    /* brickDepthLevels; must be 3 (8^3 bricks) */
+    int32_t bricks_per_axis;/* ceil(int(world size x) / 8) (SVORebuild.cpp:261-262) */
+    int32_t reserved;
+} vx_octree_config;
+
+/* Brick colour payload kinds. */
+typedef enum vx_color_kind {
+    VX_COLOR_NONE = 0,
+    VX_COLOR_RGBA8 = 1,  /* 512 x u32 per brick, voxel z*64+y*8+x (brickData layout,
+                            VoxelSceneCacher.cpp:551-578) */
+    VX_COLOR_DXT1 = 2    /* 32 x u64 BC1 blocks per brick, block = voxel >> 4
+                            (VoxelRayMarch_Compressed.comp:142-158) */
+} vx_color_kind;
+
+/* Host-side description of a scene: the buffers VoxelGridNode publishes
+ * (RenderGraph/include/Data/Nodes/VoxelGridNodeConfig.h:68-125) in this
+ * library's layout.  vx_scene_create copies them to the device. */
+typedef struct vx_scene_desc {
+    vx_octree_config config;
+    const vx_node* nodes;          /* node_count descriptors, root at 0 */
+    uint32_t node_count;
+    uint32_t brick_count;
+    const uint32_t* node_brick;    /* node_count: brick index field of each
+                                      descriptor (leafToBrickView source,
+                                      SVORebuild.cpp:569-574) */
+    const uint32_t* grid_lookup;   /* bricks_per_axis^3, x fastest, brick index
+                                      or 0xFFFFFFFF (brickGridLookup,
+                                      VoxelSceneCacher.cpp:670-713) */
+    const uint32_t* brick_coord;   /* brick_count: grid coordinate
+                                      x | y<<10 | z<<20 */
+    const uint32_t* brick_occ;     /* brick_count x 16 u32: occupancy bit of
+                                      voxel i at word i>>5, bit i&31 */
+    int32_t color_kind;            /* vx_color_kind */
+    const void* brick_color;       /* RGBA8 or DXT1 payload, or NULL */
+} vx_scene_desc;
+
+/* Ray: origin and direction (need not be normalised; the cast normalises
+ * like validateRayInput, SVOTraversal.cpp:238-259). 24 bytes. */
+typedef struct vx_ray {
+    float ox, oy, oz;
+    float dx, dy, dz;
+} vx_ray;
+
+/* Hit flags (vx_hit.flags). */
+#define VX_HIT_HIT          0x01u /* the ray hit a voxel */
+#define VX_HIT_AXIS_MASK    0x06u /* entry-face normal axis (0 x, 1 y, 2 z) << 1 */
+#define VX_HIT_NORMAL_NEG   0x08u /* normal component is -1 (else +1) */
+#define VX_HIT_METHOD_MASK  0x30u /* brick lookup that found the brick (1 position,
+                                     2 ray entry, 3 octant) << 4 */
+#define VX_RAY_ITER_CAP     0x40u /* traversal stopped at the 500-iteration cap */
+#define VX_RAY_INVALID      0x80u /* rejected by input validation */
+
+/* Hit record, 16 bytes.  Replaces ISVOStructure::RayHit
+ * (SVO/include/ISVOStructure.h:101-112): tMin -> t, entity -> (brick, voxel),
+ * normal -> flags; tMax = t + 1, scale = max_levels - 1 and
+ * hitPoint = origin + normalize(dir) * t follow from these. */
+typedef struct vx_hit {
+    float t;          /* hit distance along the normalised direction, world units */
+    uint32_t brick;   /* brick index, 0xFFFFFFFF on a miss */
+    uint32_t node;    /* index of the parent descriptor at the leaf */
+    uint16_t voxel;   /* voxel within the brick, z*64+y*8+x; 0xFFFF on a miss */
+    uint8_t flags;    /* VX_HIT_* / VX_RAY_* */
+    uint8_t reserved;
+} vx_hit;
+
+/* Per-ray work counters (optional output, for algorithmic-byte accounting). */
+typedef struct vx_ray_counters {
+    uint16_t iters;       /* ESVO loop iterations */
+    uint8_t grid_reads;   /* brickGridLookup reads */
+    uint8_t dda_steps;    /* DDA occupancy tests */
+} vx_ray_counters;
+
+/* Camera push constants, 64 bytes: the PushConstants block of
+ * shaders/VoxelRayMarch.comp:85-94 (fov in degrees, vertical). */
+typedef struct vx_camera_pc {
+    float camera_pos[3];  float time;
+    float camera_dir[3];  float fov;
+    float camera_up[3];   float aspect;
+    float camera_right[3]; int32_t debug_mode;
+} vx_camera_pc;
+
+typedef struct vx_scene vx_scene;
+
+/* ------------------------------------------------------------------------
+ * Library
+ * --------------------------------------------------------------------- */
+int32_t vx_abi_version(void);
+/* Message of the last failed call on this thread ("" if none). */
+const char* vx_last_error_string(void);
+
+/* ------------------------------------------------------------------------
+ * Scene lifetime.  Replaces VoxelSceneCacher::UploadToGPU
+ * (CashSystem/src/VoxelSceneCacher.cpp:719-891): one device allocation with
+ * 256-byte aligned sub-buffers, owned by the scene.  The grid lookup entries
+ * and brick coordinates are validated on the host before upload, so every
+ * device read stays in bounds; child pointers are bounds-checked during
+ * traversal exactly as executePushPhase does (SVOTraversal.cpp:352-354).
+ * The scene lives on the device current at creation.
+ * --------------------------------------------------------------------- */
+int vx_scene_create(const vx_scene_desc* desc, vx_scene** out);
+int vx_scene_destroy(vx_scene* scene);
+/* Device bytes held by the scene. */
+int vx_scene_device_bytes(const vx_scene* scene, uint64_t* out);
+
+/* ------------------------------------------------------------------------
+ * Ray casting.  Replaces LaineKarrasOctree::castRay
+ * (SVO/src/SVOTraversal.cpp:189-196, castRayImpl :516-691, brick DDA
+ * SVOBrickDDA.cpp:65-533) for a batch of rays, with identical results.
+ * t_min / t_max clip the ray like castRay's tMin / tMax.
+ * counters_dev and color_dev may be NULL.  color_dev receives, per ray, the
+ * hit voxel's RGBA8 word (u32) for VX_COLOR_RGBA8 scenes or its decoded DXT1
+ * texel (3 floats, DXT1ColorCompressor::decodeColorHead,
+ * VoxelData/src/Compression/DXT1Compressor.cpp:14-36) for VX_COLOR_DXT1 scenes;
+ * misses leave zeros.
+ * --------------------------------------------------------------------- */
+int vx_cast_rays(const vx_scene* scene, const vx_ray* rays_dev, uint32_t n,
+                 float t_min, float t_max, vx_hit* hits_dev, void* color_dev,
+                 vx_ray_counters* counters_dev, void* stream);
+
+/* Same with host buffers: copies rays in, casts, copies hits (and colours)
+ * out, and returns after the results are in host memory. */
+int vx_cast_rays_host(const vx_scene* scene, const vx_ray* rays_host, uint32_t n,
+                      float t_min, float t_max, vx_hit* hits_host, void* color_host,
+                      void* stream);
+
+/* ------------------------------------------------------------------------
+ * Frame render.  Replaces ComputeDispatchNode's
+ * vkCmdDispatch((W+7)/8,(H+7)/8,1) of VoxelRayMarch[_Compressed].comp
+ * (RenderGraph/src/Nodes/ComputeDispatchNode.cpp:249-317) with the
+ * swapchain image replaced by a headless device buffer: one primary ray per
+ * pixel (RayGeneration.glsl:61-71), the cast above, and Lambert shading
+ * (Lighting.glsl:19-28) or the sky colour on a miss.  image_dev: W*H RGBA8
+ * (row-major, row 0 at the top), may be NULL; hits_dev / color_dev optional.
+ * --------------------------------------------------------------------- */
+int vx_render(const vx_scene* scene, const vx_camera_pc* pc, uint32_t width,
+              uint32_t height, uint32_t* image_dev, vx_hit* hits_dev,
+              void* color_dev, void* stream);
+
+/* Primary rays of a camera exactly as vx_render generates them. */
+int vx_camera_rays(const vx_camera_pc* pc, uint32_t width, uint32_t height,
+                   vx_ray* rays_host);
+int vx_camera_rays_dev(const vx_camera_pc* pc, uint32_t width, uint32_t height,
+                       vx_ray* rays_dev, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Host scene builder.  Replaces LaineKarrasOctree::rebuild
+ * (SVO/src/SVORebuild.cpp:228-607) plus VoxelSceneCacher::BuildOctree /
+ * BuildBrickGridLookup (VoxelSceneCacher.cpp:463-713) for a dense occupancy
+ * grid with world bounds [0,R]^3: same brick order (Morton rank), same
+ * descriptor order (BFS, non-leaf children first), same lookup table.
+ * Input: R^3 occupancy bits, x fastest, 64 voxels per u64 word (R a multiple
+ * of 64).  The result owns host arrays exposed through a vx_scene_desc.
+ * --------------------------------------------------------------------- */
+typedef struct vx_build vx_build;
+int vx_build_dense(const uint64_t* occupancy_bits, uint32_t R, int32_t max_levels,
+                   vx_build** out);
+/* Fills desc with pointers into the build (valid until vx_build_free);
+ * colour fields are left empty. */
+int vx_build_desc(const vx_build* build, vx_scene_desc* desc);
+int vx_build_free(vx_build* build);
+
+/* Converts reference-layout descriptors (64-bit ChildDescriptor,
+ * SVOTypes.h:36-47: childPointer:15 far:1 valid:8 leaf:8 | brick:24 flags:8)
+ * into vx_node + node_brick.  Far pointers are rejected (VX_EINVAL). */
+int vx_nodes_from_reference(const uint64_t* ref_nodes, uint32_t n, vx_node* nodes,
+                            uint32_t* node_brick);
+
+/* ------------------------------------------------------------------------
+ * Synthetic inputs (no reference counterpart; seeded, deterministic).
+ * --------------------------------------------------------------------- */
+/* Value-noise occupancy: lattice spacing `spacing` voxels, `octaves`
+ * octaves (persistence 0.5, lacunarity 2), thresholded at the quantile that
+ * leaves `fill` of the voxels solid; `shell` adds the one-voxel box shell.
+ * out_bits: R^3/64 words.  Uses all host threads. */
+int vx_synth_noise(uint32_t R, uint32_t spacing, uint32_t octaves, float fill,
+                   uint64_t seed, int32_t shell, uint64_t* out_bits);
+/* The same bits as vx_synth_noise, generated on the current device into
+ * out_bits_dev (R <= 2048).  Allocates and frees its own scratch (the float
+ * field and the lattice tables) and returns after the bits are written. */
+int vx_synth_noise_dev(uint32_t R, uint32_t spacing, uint32_t octaves, float fill,
+                       uint64_t seed, int32_t shell, uint64_t* out_bits_dev, void* stream);
+/* Urban lattice: 32x32 blocks of pitch R/32 (block + 8-voxel street), each a
+ * solid box of seeded height in [hmin, hmax]. */
+int vx_synth_urban(uint32_t R, uint32_t hmin, uint32_t hmax, uint64_t seed,
+                   uint64_t* out_bits);
+/* Per-brick colour payloads keyed on brick grid coordinates (so they do not
+ * depend on brick order): RGBA8 uniform per voxel, or DXT1 blocks with
+ * uniform u32 head and index words. */
+int vx_synth_rgba8(const uint32_t* brick_coord, uint32_t brick_count, uint64_t seed,
+                   uint32_t* out);
+int vx_synth_dxt1(const uint32_t* brick_coord, uint32_t brick_count, uint64_t seed,
+                  uint64_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VX_H */

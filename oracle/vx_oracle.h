@@ -1,0 +1,110 @@
+/*
+ * vx_oracle.h - C interface of the CPU oracle.
+ *
+ * TEST INFRASTRUCTURE ONLY.  The oracle is a line-by-line CPU restatement of
+ * the reference's octree rebuild (VIXEN/libraries/SVO/src/SVORebuild.cpp),
+ * ray cast (VIXEN/libraries/SVO/src/SVOTraversal.cpp, SVOBrickDDA.cpp) and
+ * DXT1 colour codec (VIXEN/libraries/VoxelData/src/Compression/DXT1Compressor.cpp).
+ * Only tests, the smoke check and the CPU-baseline leg of the benchmark may
+ * load it; the product library never links or calls it.
+ *
+ * Parity status: the reference cannot be compiled here (it needs glm,
+ * gaia-ecs and TBB, none of which is available), and its own tests pin only
+ * tolerances, so bit-level parity with the reference binary is UNPINNED.  The
+ * restatement is pinned to the reference's behavioural tests (ported as KATs
+ * in tests/test_oracle_kat.py) and to golden vectors it generated itself.
+ */
+#ifndef VX_ORACLE_H
+#define VX_ORACLE_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct vxo_scene vxo_scene;
+
+/* Hit record of the oracle (one per ray). */
+typedef struct vxo_hit {
+    float t;          /* RayHit::tMin  (SVOBrickDDA.cpp:506) */
+    float t_exit;     /* RayHit::tMax  (SVOBrickDDA.cpp:507) */
+    float hit_point[3];
+    float normal[3];
+    uint32_t brick;   /* brick-view index (Morton rank), 0xFFFFFFFF on miss */
+    uint32_t node;    /* parent descriptor index at the leaf (SVOBrickDDA.cpp:77) */
+    uint32_t voxel;   /* in-brick voxel index z*64+y*8+x, 0xFFFF on miss */
+    int32_t key[3];   /* integer world position of the hit entity */
+    int32_t scale;    /* RayHit::scale */
+    uint32_t flags;   /* VX_HIT_* bits, same encoding as the product (vx.h) */
+    uint32_t iters;   /* ESVO loop iterations */
+    uint32_t grid_reads; /* brickGridLookup reads (position-based lookups) */
+    uint32_t dda_steps;  /* DDA occupancy tests */
+    uint32_t leaf_visits;
+} vxo_hit;
+
+/* Build from a list of integer voxel keys (world integer positions, as
+ * MortonCode64::fromWorldPos would quantise them).  world_min/max are the
+ * rebuild() bounds.  Returns NULL on error (message in err). */
+vxo_scene* vxo_build_from_keys(const int32_t* keys_xyz, uint64_t n,
+                               const float world_min[3], const float world_max[3],
+                               int max_levels, int brick_depth,
+                               char* err, int errlen);
+
+/* Build from a dense occupancy bit grid of side R (x fastest, 64 voxels per
+ * word, bit b of word w is voxel x = (w % (R/64))*64 + b).  World bounds are
+ * [0,R]^3 as VoxelSceneCacher::BuildOctree uses (VoxelSceneCacher.cpp:521-522).
+ * R must be a multiple of 64. */
+vxo_scene* vxo_build_from_dense(const uint64_t* bits, int R, int max_levels,
+                                int brick_depth, char* err, int errlen);
+
+void vxo_free(vxo_scene* s);
+
+uint32_t vxo_node_count(const vxo_scene* s);
+uint32_t vxo_brick_count(const vxo_scene* s);
+int32_t  vxo_bricks_per_axis(const vxo_scene* s);
+uint32_t vxo_max_child_pointer(const vxo_scene* s);
+
+/* Dump the octree in the product's device format (vx.h):
+ * nodes: 2 u32 per descriptor {child_pointer, valid | leaf << 8};
+ * node_brick: brick index field of every descriptor;
+ * grid_lookup: bricks_per_axis^3 u32 (0xFFFFFFFF empty);
+ * brick_coord: x | y<<10 | z<<20 per brick;
+ * brick_occ: 16 u32 per brick, bit (i & 31) of word (i >> 5) for voxel i.
+ * Any pointer may be NULL. */
+void vxo_export(const vxo_scene* s, uint32_t* nodes, uint32_t* node_brick,
+                uint32_t* grid_lookup, uint32_t* brick_coord, uint32_t* brick_occ);
+
+/* castRay over n rays (6 floats each: origin, direction) with nthreads host
+ * threads (<= 0: all hardware threads). */
+void vxo_cast_rays(const vxo_scene* s, const float* rays, uint64_t n,
+                   float t_min, float t_max, vxo_hit* out, int nthreads);
+
+/* Same as vxo_cast_rays, but replaces the octree with hand-built descriptors
+ * (test_octree_queries.cpp builds such octrees with setOctree()). */
+vxo_scene* vxo_build_from_descriptors(const uint32_t* nodes, const uint32_t* node_brick,
+                                      uint32_t node_count,
+                                      const float world_min[3], const float world_max[3],
+                                      int max_levels, int brick_depth);
+
+/* DXT1 colour codec restatement (DXT1Compressor.cpp:14-130). */
+void     vxo_dxt1_decode_head(uint32_t head, float ref[12]);
+void     vxo_dxt1_decode_block(uint64_t block, float out[48]);
+uint32_t vxo_dxt1_encode_head(const float c0[3], const float c1[3]);
+uint64_t vxo_dxt1_encode_block(const float* colors, uint64_t valid_count,
+                               const int32_t* indices);
+
+/* Colour fetch of a hit, restating the compressed shader's addressing
+ * (VoxelRayMarch_Compressed.comp:142-158): block = voxel >> 4, texel = voxel & 15. */
+void vxo_hit_texel_dxt(const uint64_t* brick_dxt, uint32_t brick, uint32_t voxel, float out[3]);
+
+/* Lambert shading of a hit colour (Lighting.glsl:19-28) and the sky colour on
+ * a miss (VoxelRayMarch.comp:493-499); returns RGBA8 like an UNORM imageStore. */
+uint32_t vxo_shade(const float color[3], int hit, int normal_axis, int normal_neg, float uv_y);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,370 @@
+"""Python binding of libvx (include/vx.h): B200-native ESVO voxel ray casting.
+
+Mirrors the reference's query interface for the ray-casting path:
+`CudaOctree.castRay(origin, direction, tMin, tMax)` returns a `RayHit` with the
+fields of ISVOStructure::RayHit (SVO/include/ISVOStructure.h:101-112), and
+`castRays` casts a whole batch on the GPU.  `render` is the compute-dispatch
+node's frame (RenderGraph/src/Nodes/ComputeDispatchNode.cpp:249-317) with the
+swapchain image replaced by a device buffer.
+
+Every call goes through libvx.so; there is no CPU fallback.  Importing this
+module fails loudly when the library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libvx.so")
+
+VX_OK = 0
+VX_HIT_HIT = 0x01
+VX_HIT_NORMAL_NEG = 0x08
+VX_RAY_ITER_CAP = 0x40
+VX_RAY_INVALID = 0x80
+VX_COLOR_NONE, VX_COLOR_RGBA8, VX_COLOR_DXT1 = 0, 1, 2
+FLT_MAX = 3.4028234663852886e38
+NONE = 0xFFFFFFFF
+
+HIT_DTYPE = np.dtype([("t", "<f4"), ("brick", "<u4"), ("node", "<u4"), ("voxel", "<u2"),
+                      ("flags", "u1"), ("reserved", "u1")])
+RAY_DTYPE = np.dtype([("o", "<f4", 3), ("d", "<f4", 3)])
+COUNTER_DTYPE = np.dtype([("iters", "<u2"), ("grid_reads", "u1"), ("dda_steps", "u1")])
+
+
+class VxError(RuntimeError):
+    """A libvx call returned an error status."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"libvx error {status}: {message}")
+        self.status = status
+
+
+class _Config(C.Structure):
+    _fields_ = [("world_min", C.c_float * 3), ("world_max", C.c_float * 3), ("max_levels", C.c_int32),
+                ("brick_depth", C.c_int32), ("bricks_per_axis", C.c_int32), ("reserved", C.c_int32)]
+
+
+class _SceneDesc(C.Structure):
+    _fields_ = [("config", _Config), ("nodes", C.c_void_p), ("node_count", C.c_uint32),
+                ("brick_count", C.c_uint32), ("node_brick", C.c_void_p), ("grid_lookup", C.c_void_p),
+                ("brick_coord", C.c_void_p), ("brick_occ", C.c_void_p), ("color_kind", C.c_int32),
+                ("brick_color", C.c_void_p)]
+
+
+class CameraPC(C.Structure):
+    """PushConstants of shaders/VoxelRayMarch.comp:85-94 (64 bytes)."""
+    _fields_ = [("camera_pos", C.c_float * 3), ("time", C.c_float), ("camera_dir", C.c_float * 3),
+                ("fov", C.c_float), ("camera_up", C.c_float * 3), ("aspect", C.c_float),
+                ("camera_right", C.c_float * 3), ("debug_mode", C.c_int32)]
+
+    @classmethod
+    def make(cls, pos, direction, up, right, fov_deg, aspect):
+        pc = cls()
+        pc.camera_pos[:] = [float(v) for v in pos]
+        pc.camera_dir[:] = [float(v) for v in direction]
+        pc.camera_up[:] = [float(v) for v in up]
+        pc.camera_right[:] = [float(v) for v in right]
+        pc.fov = float(fov_deg)
+        pc.aspect = float(aspect)
+        return pc
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"libvx.so is not built ({LIB_PATH}); run __graft_entry__.build() or make -C vbvs--vixen_b200")
+    L = C.CDLL(LIB_PATH)
+    vp, u32, i32, u64, f32 = C.c_void_p, C.c_uint32, C.c_int32, C.c_uint64, C.c_float
+    sig = {
+        "vx_abi_version": (i32, []),
+        "vx_last_error_string": (C.c_char_p, []),
+        "vx_scene_create": (C.c_int, [vp, vp]),
+        "vx_scene_destroy": (C.c_int, [vp]),
+        "vx_scene_device_bytes": (C.c_int, [vp, vp]),
+        "vx_cast_rays": (C.c_int, [vp, vp, u32, f32, f32, vp, vp, vp, vp]),
+        "vx_cast_rays_host": (C.c_int, [vp, vp, u32, f32, f32, vp, vp, vp]),
+        "vx_render": (C.c_int, [vp, vp, u32, u32, vp, vp, vp, vp]),
+        "vx_camera_rays": (C.c_int, [vp, u32, u32, vp]),
+        "vx_camera_rays_dev": (C.c_int, [vp, u32, u32, vp, vp]),
+        "vx_build_dense": (C.c_int, [vp, u32, i32, vp]),
+        "vx_build_desc": (C.c_int, [vp, vp]),
+        "vx_build_free": (C.c_int, [vp]),
+        "vx_nodes_from_reference": (C.c_int, [vp, u32, vp, vp]),
+        "vx_synth_noise": (C.c_int, [u32, u32, u32, f32, u64, i32, vp]),
+        "vx_synth_noise_dev": (C.c_int, [u32, u32, u32, f32, u64, i32, vp, vp]),
+        "vx_synth_urban": (C.c_int, [u32, u32, u32, u64, vp]),
+        "vx_synth_rgba8": (C.c_int, [vp, u32, u64, vp]),
+        "vx_synth_dxt1": (C.c_int, [vp, u32, u64, vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def check(status: int) -> None:
+    if status != VX_OK:
+        raise VxError(status, lib().vx_last_error_string().decode(errors="replace"))
+
+
+def _p(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data_as(C.c_void_p)
+    return C.c_void_p(int(a.data_ptr()))  # torch tensor
+
+
+# ---------------------------------------------------------------------------
+# Synthetic inputs and the host builder
+# ---------------------------------------------------------------------------
+
+def synth_noise(R: int, spacing: int, octaves: int, fill: float, seed: int, shell: bool) -> np.ndarray:
+    bits = np.zeros(R * R * (R // 64), np.uint64)
+    check(lib().vx_synth_noise(R, spacing, octaves, float(fill), seed, int(shell), _p(bits)))
+    return bits
+
+
+def synth_noise_dev(R: int, spacing: int, octaves: int, fill: float, seed: int, shell: bool, out=None):
+    """vx_synth_noise on the current CUDA device; returns a uint64 CUDA tensor (as int64)."""
+    import torch
+    if out is None:
+        out = torch.empty(R * R * (R // 64), dtype=torch.int64, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    check(lib().vx_synth_noise_dev(R, spacing, octaves, float(fill), seed, int(shell), _p(out), C.c_void_p(s)))
+    return out
+
+
+def synth_urban(R: int, hmin: int, hmax: int, seed: int) -> np.ndarray:
+    bits = np.zeros(R * R * (R // 64), np.uint64)
+    check(lib().vx_synth_urban(R, hmin, hmax, seed, _p(bits)))
+    return bits
+
+
+def synth_rgba8(brick_coord: np.ndarray, seed: int) -> np.ndarray:
+    bc = np.ascontiguousarray(brick_coord, np.uint32)
+    out = np.zeros(bc.size * 512, np.uint32)
+    check(lib().vx_synth_rgba8(_p(bc), bc.size, seed, _p(out)))
+    return out
+
+
+def synth_dxt1(brick_coord: np.ndarray, seed: int) -> np.ndarray:
+    bc = np.ascontiguousarray(brick_coord, np.uint32)
+    out = np.zeros(bc.size * 32, np.uint64)
+    check(lib().vx_synth_dxt1(_p(bc), bc.size, seed, _p(out)))
+    return out
+
+
+@dataclass
+class SceneArrays:
+    """Host copy of a scene in the device layout of vx.h."""
+    world_min: tuple
+    world_max: tuple
+    max_levels: int
+    bricks_per_axis: int
+    nodes: np.ndarray        # u32 pairs {child_ptr, valid | leaf << 8}
+    node_brick: np.ndarray
+    grid_lookup: np.ndarray
+    brick_coord: np.ndarray
+    brick_occ: np.ndarray    # 16 u32 per brick
+    color_kind: int = VX_COLOR_NONE
+    brick_color: np.ndarray | None = None
+
+    @property
+    def node_count(self) -> int:
+        return self.nodes.size // 2
+
+    @property
+    def brick_count(self) -> int:
+        return self.brick_coord.size
+
+
+def build_dense(bits: np.ndarray, R: int, max_levels: int) -> SceneArrays:
+    """LaineKarrasOctree::rebuild + VoxelSceneCacher packing for a dense grid
+    with world bounds [0,R]^3 (vx_build_dense)."""
+    bits = np.ascontiguousarray(bits, np.uint64)
+    assert bits.size == R * R * (R // 64)
+    h = C.c_void_p()
+    check(lib().vx_build_dense(_p(bits), R, max_levels, C.byref(h)))
+    try:
+        d = _SceneDesc()
+        check(lib().vx_build_desc(h, C.byref(d)))
+        bpa = d.config.bricks_per_axis
+
+        def take(ptr, n, dt):
+            if n == 0 or not ptr:
+                return np.zeros(0, dt)
+            buf = (C.c_char * (n * np.dtype(dt).itemsize)).from_address(ptr)
+            return np.frombuffer(buf, dtype=dt, count=n).copy()
+
+        return SceneArrays(tuple(d.config.world_min), tuple(d.config.world_max), d.config.max_levels, bpa,
+                           take(d.nodes, 2 * d.node_count, np.uint32), take(d.node_brick, d.node_count, np.uint32),
+                           take(d.grid_lookup, bpa ** 3, np.uint32), take(d.brick_coord, d.brick_count, np.uint32),
+                           take(d.brick_occ, 16 * d.brick_count, np.uint32))
+    finally:
+        lib().vx_build_free(h)
+
+
+def nodes_from_reference(ref_nodes: np.ndarray):
+    ref = np.ascontiguousarray(ref_nodes, np.uint64)
+    nodes = np.zeros(2 * ref.size, np.uint32)
+    nb = np.zeros(ref.size, np.uint32)
+    check(lib().vx_nodes_from_reference(_p(ref), ref.size, _p(nodes), _p(nb)))
+    return nodes, nb
+
+
+def camera_rays(pc: CameraPC, width: int, height: int) -> np.ndarray:
+    """Primary rays exactly as vx_render generates them (N x 6 float32)."""
+    out = np.zeros((width * height, 6), np.float32)
+    check(lib().vx_camera_rays(C.byref(pc), width, height, _p(out)))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Device scene
+# ---------------------------------------------------------------------------
+
+class Scene:
+    """A scene resident in device memory (vx_scene)."""
+
+    def __init__(self, arrays: SceneArrays):
+        self.arrays = arrays
+        a = arrays
+        d = _SceneDesc()
+        d.config.world_min[:] = [float(v) for v in a.world_min]
+        d.config.world_max[:] = [float(v) for v in a.world_max]
+        d.config.max_levels = a.max_levels
+        d.config.brick_depth = 3
+        d.config.bricks_per_axis = a.bricks_per_axis
+        self._keep = [np.ascontiguousarray(x) for x in (a.nodes, a.node_brick, a.grid_lookup, a.brick_coord,
+                                                         a.brick_occ)]
+        d.nodes, d.node_brick, d.grid_lookup, d.brick_coord, d.brick_occ = [_p(x) for x in self._keep]
+        d.node_count = a.node_count
+        d.brick_count = a.brick_count
+        d.color_kind = a.color_kind
+        if a.brick_color is not None:
+            self._keep.append(np.ascontiguousarray(a.brick_color))
+            d.brick_color = _p(self._keep[-1])
+        self._h = C.c_void_p()
+        check(lib().vx_scene_create(C.byref(d), C.byref(self._h)))
+        self._keep = None  # the scene holds device copies
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def color_kind(self) -> int:
+        return self.arrays.color_kind
+
+    def device_bytes(self) -> int:
+        v = C.c_uint64()
+        check(lib().vx_scene_device_bytes(self._h, C.byref(v)))
+        return v.value
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            check(lib().vx_scene_destroy(self._h))
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- device-buffer calls (torch tensors) --------------------------------
+    def color_width(self) -> int:
+        return {VX_COLOR_NONE: 0, VX_COLOR_RGBA8: 1, VX_COLOR_DXT1: 3}[self.color_kind]
+
+    def cast_rays_dev(self, rays, hits, color=None, counters=None, t_min=0.0, t_max=FLT_MAX, stream=None):
+        """rays: (n,6) float32 CUDA tensor; hits: (n,4) int32/uint32 CUDA tensor (16 B per ray)."""
+        import torch
+        n = rays.shape[0]
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        check(lib().vx_cast_rays(self._h, _p(rays), n, float(t_min), float(t_max), _p(hits), _p(color),
+                                 _p(counters), C.c_void_p(s)))
+
+    def render_dev(self, pc: CameraPC, width: int, height: int, image=None, hits=None, color=None, stream=None):
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        check(lib().vx_render(self._h, C.byref(pc), width, height, _p(image), _p(hits), _p(color), C.c_void_p(s)))
+
+    # -- host-buffer calls ---------------------------------------------------
+    def cast_rays_host(self, rays: np.ndarray, t_min=0.0, t_max=FLT_MAX, with_color=True):
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
+        hits = np.zeros(rays.shape[0], HIT_DTYPE)
+        cw = self.color_width()
+        color = None
+        if with_color and cw:
+            color = np.zeros((rays.shape[0], cw), np.uint32 if cw == 1 else np.float32)
+        check(lib().vx_cast_rays_host(self._h, _p(rays), rays.shape[0], float(t_min), float(t_max), _p(hits),
+                                      _p(color), None))
+        return hits, color
+
+
+# ---------------------------------------------------------------------------
+# ISVOStructure-shaped facade
+# ---------------------------------------------------------------------------
+
+@dataclass
+class RayHit:
+    """ISVOStructure::RayHit (SVO/include/ISVOStructure.h:101-112)."""
+    hit: bool
+    tMin: float
+    tMax: float
+    hitPoint: tuple
+    normal: tuple
+    scale: int
+    brick: int
+    voxel: int
+    node: int
+    entity: tuple | None  # integer voxel position of the hit (the entity's MortonKey position)
+
+
+class CudaOctree:
+    """Drop-in for LaineKarrasOctree::castRay on a device-resident scene."""
+
+    def __init__(self, scene: Scene):
+        self.scene = scene
+        a = scene.arrays
+        self.world_min = np.array(a.world_min, np.float32)
+        self.max_levels = a.max_levels
+
+    def castRays(self, origins, directions, tMin=0.0, tMax=FLT_MAX):
+        o = np.asarray(origins, np.float32).reshape(-1, 3)
+        d = np.asarray(directions, np.float32).reshape(-1, 3)
+        hits, _ = self.scene.cast_rays_host(np.concatenate([o, d], axis=1), tMin, tMax, with_color=False)
+        return hits
+
+    def castRay(self, origin, direction, tMin=0.0, tMax=FLT_MAX) -> RayHit:
+        h = self.castRays([origin], [direction], tMin, tMax)[0]
+        if not (h["flags"] & VX_HIT_HIT):
+            return RayHit(False, 0.0, 0.0, (0.0, 0.0, 0.0), (0.0, 0.0, 0.0), 0, NONE, 0xFFFF, NONE, None)
+        o = np.asarray(origin, np.float32)
+        d = np.asarray(direction, np.float32)
+        dn = d * (np.float32(1.0) / np.sqrt((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]))
+        t = np.float32(h["t"])
+        hp = tuple(float(v) for v in (o + dn * t))
+        axis = (int(h["flags"]) >> 1) & 3
+        n = [0.0, 0.0, 0.0]
+        n[axis] = -1.0 if h["flags"] & VX_HIT_NORMAL_NEG else 1.0
+        bc = int(self.scene.arrays.brick_coord[h["brick"]])
+        v = int(h["voxel"])
+        q = np.floor(self.world_min).astype(np.int64)
+        ent = ((bc & 0x3FF) * 8 + (v & 7) + int(q[0]), ((bc >> 10) & 0x3FF) * 8 + ((v >> 3) & 7) + int(q[1]),
+               ((bc >> 20) & 0x3FF) * 8 + (v >> 6) + int(q[2]))
+        return RayHit(True, float(t), float(t + np.float32(1.0)), hp, tuple(n), self.max_levels - 1,
+                      int(h["brick"]), v, int(h["node"]), ent)

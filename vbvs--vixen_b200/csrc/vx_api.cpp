@@ -1,0 +1,283 @@
+// vx_api.cpp - host side of the C ABI (include/vx.h): validation, the scene's
+// device allocation, error reporting and launches.
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "vx_internal.h"
+#include "vx_raygen.h"
+
+namespace vx {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+const char* last_error_c_str() { return g_last_error.c_str(); }
+
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(VX_ECUDA, std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+CameraDev camera_from_pc(const vx_camera_pc& pc) {
+    CameraDev c{};
+    for (int i = 0; i < 3; ++i) {
+        c.pos[i] = pc.camera_pos[i];
+        c.dir[i] = pc.camera_dir[i];
+        c.up[i] = pc.camera_up[i];
+        c.right[i] = pc.camera_right[i];
+    }
+    c.aspect = pc.aspect;
+    // tan(radians(fov * 0.5)) (RayGeneration.glsl:62), once, in binary32.
+    const float half = pc.fov * 0.5f;
+    const float rad = half * 0.01745329251994329577f;
+    c.tan_half_fov = std::tan(rad);
+    return c;
+}
+
+}  // namespace vx
+
+struct vx_scene {
+    int device = 0;
+    void* pool = nullptr;  // single device allocation, 256-byte aligned slices
+    uint64_t pool_bytes = 0;
+    vx::DevScene dev{};
+    // staging buffer for vx_cast_rays_host, grown on demand
+    std::mutex stage_mu;
+    void* stage = nullptr;
+    uint64_t stage_bytes = 0;
+};
+
+namespace {
+
+using vx::fail;
+
+uint64_t align256(uint64_t x) { return (x + 255) & ~uint64_t(255); }
+
+// Host-side checks that make every device read in bounds: grid entries and
+// node brick fields are brick indices or 0xFFFFFFFF, coordinates lie in the
+// grid.  Child pointers are not rejected: the traversal bounds-checks them
+// exactly as executePushPhase does (SVOTraversal.cpp:352-354).
+int validate(const vx_scene_desc* d) {
+    const vx_octree_config& c = d->config;
+    if (c.brick_depth != 3) return fail(VX_EINVAL, "vx_scene_create: brick_depth must be 3 (8^3 bricks)");
+    if (c.max_levels < 1 || c.max_levels > 23) return fail(VX_EINVAL, "vx_scene_create: max_levels must be in [1, 23]");
+    if (c.bricks_per_axis < 1 || c.bricks_per_axis > 1024)
+        return fail(VX_EINVAL, "vx_scene_create: bricks_per_axis must be in [1, 1024]");
+    for (int i = 0; i < 3; ++i)
+        if (!std::isfinite(c.world_min[i]) || !std::isfinite(c.world_max[i]) || !(c.world_max[i] > c.world_min[i]))
+            return fail(VX_EINVAL, "vx_scene_create: world bounds must be finite with max > min");
+    const float wsx = c.world_max[0] - c.world_min[0];
+    const int vpa = (wsx < 2147483648.0f) ? int(wsx) : -1;
+    if (vpa < 0 || (vpa + 7) / 8 != c.bricks_per_axis)
+        return fail(VX_EINVAL, "vx_scene_create: bricks_per_axis must be ceil(int(world_max.x - world_min.x) / 8)");
+    if (d->node_count && (!d->nodes || !d->node_brick)) return fail(VX_EINVAL, "vx_scene_create: nodes missing");
+    if (!d->grid_lookup) return fail(VX_EINVAL, "vx_scene_create: grid_lookup missing");
+    if (d->brick_count && (!d->brick_coord || !d->brick_occ))
+        return fail(VX_EINVAL, "vx_scene_create: brick buffers missing");
+    if (d->color_kind != VX_COLOR_NONE && d->color_kind != VX_COLOR_RGBA8 && d->color_kind != VX_COLOR_DXT1)
+        return fail(VX_EINVAL, "vx_scene_create: unknown color_kind");
+    if (d->color_kind != VX_COLOR_NONE && d->brick_count && !d->brick_color)
+        return fail(VX_EINVAL, "vx_scene_create: brick_color missing");
+    const uint64_t slots = uint64_t(c.bricks_per_axis) * c.bricks_per_axis * c.bricks_per_axis;
+    for (uint64_t i = 0; i < slots; ++i)
+        if (d->grid_lookup[i] != 0xFFFFFFFFu && d->grid_lookup[i] >= d->brick_count)
+            return fail(VX_EINVAL, "vx_scene_create: grid_lookup[" + std::to_string(i) + "] is not a brick index");
+    const uint32_t bpa = uint32_t(c.bricks_per_axis);
+    for (uint32_t b = 0; b < d->brick_count; ++b) {
+        const uint32_t v = d->brick_coord[b];
+        if ((v & 0x3FF) >= bpa || ((v >> 10) & 0x3FF) >= bpa || ((v >> 20) & 0x3FF) >= bpa || (v >> 30))
+            return fail(VX_EINVAL, "vx_scene_create: brick_coord[" + std::to_string(b) + "] outside the grid");
+    }
+    return VX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t vx_abi_version(void) { return VX_ABI_VERSION; }
+
+const char* vx_last_error_string(void) { return vx::last_error_c_str(); }
+
+int vx_scene_create(const vx_scene_desc* d, vx_scene** out) {
+    if (!d || !out) return fail(VX_EINVAL, "vx_scene_create: null argument");
+    *out = nullptr;
+    if (int r = validate(d)) return r;
+    const vx_octree_config& c = d->config;
+    const uint64_t bpa = uint64_t(c.bricks_per_axis);
+    const uint64_t sz_nodes = uint64_t(d->node_count) * sizeof(vx_node);
+    const uint64_t sz_nb = uint64_t(d->node_count) * 4;
+    const uint64_t sz_grid = bpa * bpa * bpa * 4;
+    const uint64_t sz_coord = uint64_t(d->brick_count) * 4;
+    const uint64_t sz_occ = uint64_t(d->brick_count) * 64;
+    uint64_t sz_color = 0;
+    if (d->color_kind == VX_COLOR_RGBA8) sz_color = uint64_t(d->brick_count) * 512 * 4;
+    if (d->color_kind == VX_COLOR_DXT1) sz_color = uint64_t(d->brick_count) * 32 * 8;
+    const uint64_t o_nodes = 0;
+    const uint64_t o_nb = o_nodes + align256(sz_nodes);
+    const uint64_t o_grid = o_nb + align256(sz_nb);
+    const uint64_t o_coord = o_grid + align256(sz_grid);
+    const uint64_t o_occ = o_coord + align256(sz_coord);
+    const uint64_t o_color = o_occ + align256(sz_occ);
+    const uint64_t total = o_color + align256(sz_color) + 256;
+
+    auto* s = new (std::nothrow) vx_scene();
+    if (!s) return fail(VX_ENOMEM, "vx_scene_create: out of host memory");
+    cudaError_t e = cudaGetDevice(&s->device);
+    if (e != cudaSuccess) { delete s; return vx::cuda_fail(e, "vx_scene_create: cudaGetDevice"); }
+    e = cudaMalloc(&s->pool, total);
+    if (e != cudaSuccess) { delete s; return vx::cuda_fail(e, "vx_scene_create: cudaMalloc"); }
+    s->pool_bytes = total;
+    char* base = static_cast<char*>(s->pool);
+    struct Copy { uint64_t off; const void* src; uint64_t n; };
+    const Copy copies[] = {{o_nodes, d->nodes, sz_nodes}, {o_nb, d->node_brick, sz_nb},
+                           {o_grid, d->grid_lookup, sz_grid}, {o_coord, d->brick_coord, sz_coord},
+                           {o_occ, d->brick_occ, sz_occ}, {o_color, d->brick_color, sz_color}};
+    for (const Copy& cp : copies) {
+        if (!cp.n) continue;
+        e = cudaMemcpy(base + cp.off, cp.src, cp.n, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(s->pool);
+            delete s;
+            return vx::cuda_fail(e, "vx_scene_create: cudaMemcpy");
+        }
+    }
+    vx::DevScene& ds = s->dev;
+    for (int i = 0; i < 3; ++i) {
+        ds.wmin[i] = c.world_min[i];
+        ds.wmax[i] = c.world_max[i];
+        ds.wsize[i] = c.world_max[i] - c.world_min[i];
+        ds.qwm[i] = int32_t(std::floor(c.world_min[i]));
+    }
+    ds.max_levels = c.max_levels;
+    ds.min_scale = 22 - c.max_levels + 1;
+    ds.brick_user_scale = c.max_levels - c.brick_depth;
+    ds.bpa = c.bricks_per_axis;
+    ds.node_count = d->node_count;
+    ds.brick_count = d->brick_count;
+    ds.nodes = reinterpret_cast<const uint2*>(base + o_nodes);
+    ds.node_brick = reinterpret_cast<const uint32_t*>(base + o_nb);
+    ds.grid = reinterpret_cast<const uint32_t*>(base + o_grid);
+    ds.coord = reinterpret_cast<const uint32_t*>(base + o_coord);
+    ds.occ = reinterpret_cast<const uint4*>(base + o_occ);
+    ds.color_kind = d->color_kind;
+    ds.rgba = d->color_kind == VX_COLOR_RGBA8 ? reinterpret_cast<const uint32_t*>(base + o_color) : nullptr;
+    ds.dxt = d->color_kind == VX_COLOR_DXT1 ? reinterpret_cast<const uint2*>(base + o_color) : nullptr;
+    *out = s;
+    return VX_OK;
+}
+
+int vx_scene_destroy(vx_scene* s) {
+    if (!s) return VX_OK;
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (dev != s->device) cudaSetDevice(s->device);
+    cudaError_t e1 = cudaFree(s->pool);
+    cudaError_t e2 = s->stage ? cudaFree(s->stage) : cudaSuccess;
+    if (dev >= 0 && dev != s->device) cudaSetDevice(dev);
+    delete s;
+    if (e1 != cudaSuccess) return vx::cuda_fail(e1, "vx_scene_destroy: cudaFree");
+    if (e2 != cudaSuccess) return vx::cuda_fail(e2, "vx_scene_destroy: cudaFree");
+    return VX_OK;
+}
+
+int vx_scene_device_bytes(const vx_scene* s, uint64_t* out) {
+    if (!s || !out) return fail(VX_EINVAL, "vx_scene_device_bytes: null argument");
+    *out = s->pool_bytes;
+    return VX_OK;
+}
+
+int vx_cast_rays(const vx_scene* s, const vx_ray* rays, uint32_t n, float tmin, float tmax, vx_hit* hits,
+                 void* color, vx_ray_counters* counters, void* stream) {
+    if (!s || (n && (!rays || !hits))) return fail(VX_EINVAL, "vx_cast_rays: null argument");
+    if (std::isnan(tmin) || std::isnan(tmax)) return fail(VX_EINVAL, "vx_cast_rays: t_min / t_max is NaN");
+    if (reinterpret_cast<uintptr_t>(rays) % 8 || reinterpret_cast<uintptr_t>(hits) % 16 ||
+        reinterpret_cast<uintptr_t>(color) % 4 || reinterpret_cast<uintptr_t>(counters) % 4)
+        return fail(VX_EINVAL, "vx_cast_rays: rays need 8-byte, hits 16-byte, colour/counters 4-byte alignment");
+    int r = vx::launch_cast(s->dev, rays, n, tmin, tmax, hits, color, counters, stream);
+    if (r != 0) return vx::cuda_fail(cudaError_t(r), "vx_cast_rays: launch");
+    return VX_OK;
+}
+
+int vx_cast_rays_host(const vx_scene* cs, const vx_ray* rays_host, uint32_t n, float tmin, float tmax,
+                      vx_hit* hits_host, void* color_host, void* stream) {
+    if (!cs || (n && (!rays_host || !hits_host))) return fail(VX_EINVAL, "vx_cast_rays_host: null argument");
+    if (n == 0) return VX_OK;
+    vx_scene* s = const_cast<vx_scene*>(cs);
+    std::lock_guard<std::mutex> lk(s->stage_mu);
+    const uint64_t colw = s->dev.color_kind == VX_COLOR_DXT1 ? 12 : 4;
+    const uint64_t sz_r = align256(uint64_t(n) * sizeof(vx_ray));
+    const uint64_t sz_h = align256(uint64_t(n) * sizeof(vx_hit));
+    const uint64_t sz_c = color_host && s->dev.color_kind != VX_COLOR_NONE ? align256(uint64_t(n) * colw) : 0;
+    const uint64_t need = sz_r + sz_h + sz_c;
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (dev != s->device) return fail(VX_EINVAL, "vx_cast_rays_host: the scene belongs to another device");
+    if (need > s->stage_bytes) {
+        if (s->stage) cudaFree(s->stage);
+        s->stage = nullptr;
+        s->stage_bytes = 0;
+        cudaError_t e = cudaMalloc(&s->stage, need);
+        if (e != cudaSuccess) return vx::cuda_fail(e, "vx_cast_rays_host: cudaMalloc");
+        s->stage_bytes = need;
+    }
+    char* base = static_cast<char*>(s->stage);
+    vx_ray* dr = reinterpret_cast<vx_ray*>(base);
+    vx_hit* dh = reinterpret_cast<vx_hit*>(base + sz_r);
+    void* dc = sz_c ? base + sz_r + sz_h : nullptr;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemcpyAsync(dr, rays_host, uint64_t(n) * sizeof(vx_ray), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return vx::cuda_fail(e, "vx_cast_rays_host: copy in");
+    int r = vx::launch_cast(s->dev, dr, n, tmin, tmax, dh, dc, nullptr, stream);
+    if (r != 0) return vx::cuda_fail(cudaError_t(r), "vx_cast_rays_host: launch");
+    e = cudaMemcpyAsync(hits_host, dh, uint64_t(n) * sizeof(vx_hit), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && dc) e = cudaMemcpyAsync(color_host, dc, uint64_t(n) * colw, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return vx::cuda_fail(e, "vx_cast_rays_host: copy out");
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return vx::cuda_fail(e, "vx_cast_rays_host: synchronize");
+    return VX_OK;
+}
+
+int vx_render(const vx_scene* s, const vx_camera_pc* pc, uint32_t w, uint32_t h, uint32_t* image, vx_hit* hits,
+              void* color, void* stream) {
+    if (!s || !pc) return fail(VX_EINVAL, "vx_render: null argument");
+    if (uint64_t(w) * h > 0xFFFFFFFFull) return fail(VX_EOVERFLOW, "vx_render: width * height exceeds 2^32");
+    if (reinterpret_cast<uintptr_t>(hits) % 16 || reinterpret_cast<uintptr_t>(image) % 4 ||
+        reinterpret_cast<uintptr_t>(color) % 4)
+        return fail(VX_EINVAL, "vx_render: misaligned output");
+    const vx::CameraDev cam = vx::camera_from_pc(*pc);
+    int r = vx::launch_render(s->dev, cam, w, h, image, hits, color, stream);
+    if (r != 0) return vx::cuda_fail(cudaError_t(r), "vx_render: launch");
+    return VX_OK;
+}
+
+int vx_camera_rays(const vx_camera_pc* pc, uint32_t w, uint32_t h, vx_ray* rays) {
+    if (!pc || (uint64_t(w) * h != 0 && !rays)) return fail(VX_EINVAL, "vx_camera_rays: null argument");
+    if (uint64_t(w) * h > 0xFFFFFFFFull) return fail(VX_EOVERFLOW, "vx_camera_rays: width * height exceeds 2^32");
+    const vx::CameraDev cam = vx::camera_from_pc(*pc);
+    for (uint32_t y = 0; y < h; ++y)
+        for (uint32_t x = 0; x < w; ++x) vx::camera_ray(cam, x, y, w, h, rays[uint64_t(y) * w + x], nullptr);
+    return VX_OK;
+}
+
+int vx_camera_rays_dev(const vx_camera_pc* pc, uint32_t w, uint32_t h, vx_ray* rays, void* stream) {
+    if (!pc || (uint64_t(w) * h != 0 && !rays)) return fail(VX_EINVAL, "vx_camera_rays_dev: null argument");
+    if (uint64_t(w) * h > 0xFFFFFFFFull) return fail(VX_EOVERFLOW, "vx_camera_rays_dev: width * height exceeds 2^32");
+    const vx::CameraDev cam = vx::camera_from_pc(*pc);
+    int r = vx::launch_camera_rays(cam, w, h, rays, stream);
+    if (r != 0) return vx::cuda_fail(cudaError_t(r), "vx_camera_rays_dev: launch");
+    return VX_OK;
+}
+
+}  // extern "C"

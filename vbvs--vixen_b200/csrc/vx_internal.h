@@ -1,0 +1,52 @@
+// vx_internal.h - shared between the host API (vx_api.cpp, vx_build.cpp)
+// and the CUDA kernels (vx_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/vx.h"
+
+namespace vx {
+
+// Scene as the kernels see it (passed by value as a kernel parameter).
+struct DevScene {
+    float wmin[3], wmax[3], wsize[3];  // wsize = wmax - wmin (float subtract)
+    int32_t qwm[3];                    // floor(world_min), VoxelComponents.h:373-379
+    int32_t max_levels;
+    int32_t min_scale;                 // 22 - max_levels + 1
+    int32_t brick_user_scale;          // max_levels - brick_depth (SVOTraversal.cpp:305)
+    int32_t bpa;                       // bricks per axis
+    uint32_t node_count, brick_count;
+    const uint2* nodes;                // {child_ptr, valid | leaf << 8}
+    const uint32_t* node_brick;
+    const uint32_t* grid;              // bpa^3
+    const uint32_t* coord;             // brick grid coordinate, 10:10:10
+    const uint4* occ;                  // 4 x uint4 (16 words) per brick
+    int32_t color_kind;
+    const uint32_t* rgba;              // 512 per brick
+    const uint2* dxt;                  // 32 per brick
+};
+
+// Per-thread-local error string.
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+
+// Kernel launchers (vx_kernels.cu).  Return cudaError_t as int.
+int launch_cast(const DevScene& s, const vx_ray* rays, uint32_t n, float tmin, float tmax,
+                vx_hit* hits, void* color, vx_ray_counters* counters, void* stream);
+struct CameraDev {
+    float pos[3], dir[3], up[3], right[3];
+    float aspect, tan_half_fov;
+};
+int launch_render(const DevScene& s, const CameraDev& cam, uint32_t w, uint32_t h, uint32_t* image,
+                  vx_hit* hits, void* color, void* stream);
+int launch_camera_rays(const CameraDev& cam, uint32_t w, uint32_t h, vx_ray* rays, void* stream);
+
+// Host camera setup shared by vx_render and vx_camera_rays: tan(radians(fov/2))
+// is evaluated once on the host (RayGeneration.glsl:62).
+CameraDev camera_from_pc(const vx_camera_pc& pc);
+
+}  // namespace vx

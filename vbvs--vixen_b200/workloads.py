@@ -1,0 +1,159 @@
+"""Seeded synthetic workloads for the ESVO ray-casting path.
+
+The reference measures on procedural scenes only (application/benchmark/
+benchmark_config.json:49-80, RenderGraph/src/Data/SceneGenerator.cpp); the
+scenes here have the shapes, sizes and fill fractions of the benchmark
+configurations this library is measured on:
+
+  cfg1  256^3 (octree depth 8), value noise (spacing 32, 4 octaves) at 10 %
+        fill plus a one-voxel box shell; RGBA8 colour per voxel; 512x512
+        pinhole camera, 60 deg, at the centre of the -Z face looking +Z.
+        The face itself is shell, so the camera sits at (128, 128, 1.5), just
+        inside it.
+  cfg2  1024^3 (depth 10), value noise (spacing 64, 5 octaves) at 50 % fill;
+        DXT1 bricks with uniform random heads and index words; 1920x1080,
+        70 deg, at a seeded empty voxel looking in a uniform random direction.
+  cfg3  2048^3 (depth 11) urban lattice: 32x32 blocks, 8-voxel streets,
+        heights uniform in [64, 1800]; DXT1 bricks; 3840x2160 primary rays
+        plus one shadow ray per hit toward a seeded directional light.
+
+Every input is produced on the host in binary32 so the oracle and the GPU see
+the same bits.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import (VX_COLOR_DXT1, VX_COLOR_NONE, VX_COLOR_RGBA8, CameraPC, SceneArrays, build_dense, camera_rays,
+               synth_dxt1, synth_noise, synth_rgba8, synth_urban)
+
+
+def levels_for(R: int) -> int:
+    """ceil(log2(R)) as VoxelSceneCacher::BuildOctree picks maxLevels (VoxelSceneCacher.cpp:525-528)."""
+    return int(math.ceil(math.log2(R)))
+
+
+def splitmix64(z: int) -> int:
+    z = (z + 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+    return z ^ (z >> 31)
+
+
+def _f32(v):
+    return np.asarray(v, np.float32)
+
+
+def _normalize(v):
+    v = _f32(v)
+    d = np.float32((v[0] * v[0] + v[1] * v[1]) + v[2] * v[2])
+    return (v * (np.float32(1.0) / np.sqrt(d))).astype(np.float32)
+
+
+def _cross(a, b):
+    a, b = _f32(a), _f32(b)
+    return _f32([a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]])
+
+
+def look_camera(pos, direction, fov_deg, width, height) -> CameraPC:
+    d = _normalize(direction)
+    up0 = _f32([0, 1, 0]) if abs(float(d[1])) < 0.99 else _f32([1, 0, 0])
+    right = _normalize(_cross(d, up0))
+    up = _cross(right, d)
+    return CameraPC.make(pos, d, up, right, fov_deg, float(np.float32(width) / np.float32(height)))
+
+
+@dataclass
+class Workload:
+    name: str
+    R: int
+    scene: SceneArrays
+    bits: np.ndarray
+    camera: CameraPC
+    width: int
+    height: int
+
+    def rays(self) -> np.ndarray:
+        return camera_rays(self.camera, self.width, self.height)
+
+
+def noise_scene(R, spacing, octaves, fill, seed, shell, color, max_levels=None):
+    bits = synth_noise(R, spacing, octaves, fill, seed, shell)
+    return scene_from_bits(bits, R, color, seed, max_levels), bits
+
+
+def scene_from_bits(bits, R, color, seed, max_levels=None) -> SceneArrays:
+    a = build_dense(bits, R, max_levels or levels_for(R))
+    if color == "rgba8":
+        a.color_kind, a.brick_color = VX_COLOR_RGBA8, synth_rgba8(a.brick_coord, seed ^ 0xC0105)
+    elif color == "dxt1":
+        a.color_kind, a.brick_color = VX_COLOR_DXT1, synth_dxt1(a.brick_coord, seed ^ 0xD7C1)
+    else:
+        a.color_kind, a.brick_color = VX_COLOR_NONE, None
+    return a
+
+
+def config1(R: int = 256, width: int = 512, height: int = 512, seed: int = 1) -> Workload:
+    """cfg1; R, width and height shrink it for fast parity tests."""
+    spacing = max(4, 32 * R // 256)
+    scene, bits = noise_scene(R, spacing, 4 if spacing >= 32 else 3, 0.10, seed, True, "rgba8")
+    cam = look_camera([R / 2, R / 2, 1.5], [0, 0, 1], 60.0, width, height)
+    return Workload(f"cfg1_noise{R}_rgba8_{width}x{height}", R, scene, bits, cam, width, height)
+
+
+def empty_voxel_camera(bits, R, seed, fov, width, height) -> CameraPC:
+    wpr = R // 64
+    k = 0
+    while True:
+        h = splitmix64(seed * 1000003 + k)
+        x, y, z = h % R, (h >> 20) % R, (h >> 40) % R
+        w = int(bits[(z * R + y) * wpr + (x >> 6)])
+        if not (w >> (x & 63)) & 1:
+            break
+        k += 1
+    h1, h2 = splitmix64(seed ^ 0xA5A5A5A5), splitmix64(seed ^ 0x5A5A5A5A)
+    u, v = (h1 >> 11) / float(1 << 53), (h2 >> 11) / float(1 << 53)
+    cz = 1.0 - 2.0 * u
+    r = math.sqrt(max(0.0, 1.0 - cz * cz))
+    phi = 2.0 * math.pi * v
+    d = [r * math.cos(phi), r * math.sin(phi), cz]
+    return look_camera([x + 0.5, y + 0.5, z + 0.5], d, fov, width, height)
+
+
+def config2(R: int = 1024, width: int = 1920, height: int = 1080, seed: int = 2, bits=None) -> Workload:
+    """cfg2; bits may be supplied (e.g. generated on the GPU with the same definition)."""
+    spacing = max(4, 64 * R // 1024)
+    if bits is None:
+        bits = synth_noise(R, spacing, 5 if spacing >= 64 else 3, 0.50, seed, False)
+    scene = scene_from_bits(bits, R, "dxt1", seed)
+    cam = empty_voxel_camera(bits, R, seed, 70.0, width, height)
+    return Workload(f"cfg2_cave{R}_dxt1_{width}x{height}", R, scene, bits, cam, width, height)
+
+
+def config3(R: int = 2048, width: int = 3840, height: int = 2160, seed: int = 3) -> Workload:
+    hmin, hmax = (64, 1800) if R == 2048 else (max(1, R // 32), max(2, R * 1800 // 2048))
+    bits = synth_urban(R, hmin, hmax, seed)
+    scene = scene_from_bits(bits, R, "dxt1", seed)
+    cam = look_camera([R * 0.5, R * 0.9, -R * 0.25], [0.05, -0.45, 1.0], 60.0, width, height)
+    return Workload(f"cfg3_urban{R}_dxt1_{width}x{height}", R, scene, bits, cam, width, height)
+
+
+def random_rays(n: int, R: float, seed: int, lo=-0.25, hi=1.25) -> np.ndarray:
+    """Origins uniform in [lo*R, hi*R]^3, directions uniform on the sphere,
+    plus axis-aligned and near-axis directions (every 7th / 11th ray)."""
+    rng = np.random.default_rng(seed)
+    o = rng.uniform(lo * R, hi * R, size=(n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    axis = rng.integers(0, 3, size=n)
+    sign = rng.choice(np.array([-1.0, 1.0], np.float32), size=n)
+    k = np.arange(n)
+    aa = (k % 7) == 3
+    d[aa] = 0.0
+    d[aa, axis[aa]] = sign[aa]
+    na = (k % 11) == 5
+    d[na] = np.float32(1e-6) * d[na]
+    d[na, axis[na]] = sign[na]
+    return np.concatenate([o, d], axis=1).astype(np.float32)
