@@ -219,6 +219,8 @@ def main():
     ap.add_argument("--R", type=int, default=1024)
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--soak-seconds", type=float, default=1.5,
+                    help="untimed launches before timing so clocks reach steady state")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -241,7 +243,7 @@ def main():
     rays = torch.from_numpy(rays_np).cuda()
     hits = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
     color = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
-    counters = torch.zeros((n,), dtype=torch.int32, device="cuda")
+    counters = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
     stream = torch.cuda.current_stream()
 
     # Counting pass (untimed): per-ray work for the algorithmic-byte count.
@@ -261,7 +263,7 @@ def main():
     for _ in range(args.warmup):
         scene.cast_rays_dev(rays, hits, color)
     torch.cuda.synchronize()
-    while time.perf_counter() - t_soak < 1.5:  # bring clocks to steady state before timing
+    while time.perf_counter() - t_soak < args.soak_seconds:  # clocks to steady state before timing
         for _ in range(20):
             scene.cast_rays_dev(rays, hits, color)
         torch.cuda.synchronize()

@@ -127,11 +127,18 @@ typedef struct vx_hit {
     uint8_t reserved;
 } vx_hit;
 
-/* Per-ray work counters (optional output, for algorithmic-byte accounting). */
+/* Per-ray work counters (optional output, for algorithmic-byte accounting),
+ * 16 bytes.  The first three are the reference traversal's counts (bounds:
+ * iters <= 500, grid_reads <= 2 and dda_steps <= 24 per iteration); the
+ * run_* fields are what the kernel executed, which is less when a ray is
+ * caught in a repeating cycle before the iteration cap. */
 typedef struct vx_ray_counters {
-    uint16_t iters;       /* ESVO loop iterations */
-    uint8_t grid_reads;   /* brickGridLookup reads */
-    uint8_t dda_steps;    /* DDA occupancy tests */
+    uint16_t iters;           /* ESVO loop iterations */
+    uint16_t grid_reads;      /* brickGridLookup reads */
+    uint32_t dda_steps;       /* DDA occupancy tests */
+    uint16_t run_iters;
+    uint16_t run_grid_reads;
+    uint32_t run_dda_steps;
 } vx_ray_counters;
 
 /* Camera push constants, 64 bytes: the PushConstants block of

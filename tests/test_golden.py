@@ -65,7 +65,7 @@ def test_kernel_reproduces_dense_golden(vx, golden, cuda):
     n = rays.shape[0]
     r = torch.from_numpy(np.ascontiguousarray(rays)).cuda()
     hits = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
-    cnt = torch.zeros((n,), dtype=torch.int32, device="cuda")
+    cnt = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
     s.cast_rays_dev(r, hits, None, cnt)
     torch.cuda.synchronize()
     g = hits.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1)

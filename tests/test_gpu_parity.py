@@ -31,7 +31,7 @@ def gpu_cast(vx, scene, rays, tmin=0.0, tmax=FLT_MAX, with_counters=True):
     color = None
     if cw:
         color = torch.zeros((n, cw), dtype=torch.int32 if cw == 1 else torch.float32, device="cuda")
-    counters = torch.zeros((n,), dtype=torch.int32, device="cuda") if with_counters else None
+    counters = torch.zeros((n, 4), dtype=torch.int32, device="cuda") if with_counters else None
     s.cast_rays_dev(r, hits, color, counters, tmin, tmax)
     torch.cuda.synchronize()
     h = hits.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1)

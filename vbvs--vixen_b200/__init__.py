@@ -33,7 +33,8 @@ NONE = 0xFFFFFFFF
 HIT_DTYPE = np.dtype([("t", "<f4"), ("brick", "<u4"), ("node", "<u4"), ("voxel", "<u2"),
                       ("flags", "u1"), ("reserved", "u1")])
 RAY_DTYPE = np.dtype([("o", "<f4", 3), ("d", "<f4", 3)])
-COUNTER_DTYPE = np.dtype([("iters", "<u2"), ("grid_reads", "u1"), ("dda_steps", "u1")])
+COUNTER_DTYPE = np.dtype([("iters", "<u2"), ("grid_reads", "<u2"), ("dda_steps", "<u4"), ("run_iters", "<u2"),
+                          ("run_grid_reads", "<u2"), ("run_dda_steps", "<u4")])
 
 
 class VxError(RuntimeError):

@@ -203,8 +203,8 @@ int vx_cast_rays(const vx_scene* s, const vx_ray* rays, uint32_t n, float tmin, 
     if (!s || (n && (!rays || !hits))) return fail(VX_EINVAL, "vx_cast_rays: null argument");
     if (std::isnan(tmin) || std::isnan(tmax)) return fail(VX_EINVAL, "vx_cast_rays: t_min / t_max is NaN");
     if (reinterpret_cast<uintptr_t>(rays) % 8 || reinterpret_cast<uintptr_t>(hits) % 16 ||
-        reinterpret_cast<uintptr_t>(color) % 4 || reinterpret_cast<uintptr_t>(counters) % 4)
-        return fail(VX_EINVAL, "vx_cast_rays: rays need 8-byte, hits 16-byte, colour/counters 4-byte alignment");
+        reinterpret_cast<uintptr_t>(color) % 4 || reinterpret_cast<uintptr_t>(counters) % 16)
+        return fail(VX_EINVAL, "vx_cast_rays: rays need 8-byte, hits and counters 16-byte, colour 4-byte alignment");
     int r = vx::launch_cast(s->dev, rays, n, tmin, tmax, hits, color, counters, stream);
     if (r != 0) return vx::cuda_fail(cudaError_t(r), "vx_cast_rays: launch");
     return VX_OK;

@@ -61,7 +61,8 @@ __device__ __forceinline__ uint32_t mirror_mask(uint32_t m, int octant_mask) {
 struct Hit {
     float t;
     uint32_t brick, node, voxel, flags;
-    uint32_t iters, grid_reads, dda_steps;
+    uint32_t iters, grid_reads, dda_steps;            // the reference traversal's counts
+    uint32_t run_iters, run_grid_reads, run_dda_steps;  // what this kernel executed
 };
 
 // traverseBrickView (SVOBrickDDA.cpp:390-533) with brickVoxelSize = 1 and
@@ -169,7 +170,8 @@ __device__ __forceinline__ float corrected_tc_max(float tx, float ty, float tz, 
 
 // castRayImpl without LOD (SVOTraversal.cpp:516-691).
 __device__ void cast_ray(const DevScene& s, float ox, float oy, float oz, float ddx, float ddy, float ddz,
-                         float tMinArg, float tMaxArg, uint32_t* stkN, float* stkT, int stride, Hit& h) {
+                         float tMinArg, float tMaxArg, uint32_t* stkN, float* stkT, uint32_t* cyc, int stride,
+                         Hit& h) {
     h.t = 0.0f;
     h.brick = NONE;
     h.node = NONE;
@@ -178,6 +180,9 @@ __device__ void cast_ray(const DevScene& s, float ox, float oy, float oz, float 
     h.iters = 0;
     h.grid_reads = 0;
     h.dda_steps = 0;
+    h.run_iters = 0;
+    h.run_grid_reads = 0;
+    h.run_dda_steps = 0;
     // validateRayInput (:238-259)
     if (s.node_count == 0) { h.flags = F_INVALID; return; }
     float dx, dy, dz;
@@ -287,8 +292,27 @@ __device__ void cast_ray(const DevScene& s, float ox, float oy, float oz, float 
     uint32_t mValid = 0, mLeaf = 0, pChild = 0, pValid = 0, pLeaf = 0;
     float tx_center = 0.0f, ty_center = 0.0f, tz_center = 0.0f;
     int iter = 0;
+    // Cycle detection.  The loop state below (with the stack, which a cycle
+    // only rewrites with the values it already holds) determines every later
+    // iteration, so once it repeats after one or two iterations the ray can
+    // neither hit nor leave before the 500-iteration cap: the result is the
+    // capped miss and the remaining iterations' counters repeat the cycle's.
+    // The two previous states live in shared memory (cyc[k * stride] for
+    // k < 8: one iteration back, k >= 8: two back).
+    uint32_t d1g = 0, d1d = 0;
+    bool have2 = false;
+    cyc[0] = uint32_t(scale) | (uint32_t(idx) << 8) | (uint32_t(fetched) << 16);
+    cyc[1 * stride] = parent;
+    cyc[2 * stride] = __float_as_uint(px);
+    cyc[3 * stride] = __float_as_uint(py);
+    cyc[4 * stride] = __float_as_uint(pz);
+    cyc[5 * stride] = __float_as_uint(t_min);
+    cyc[6 * stride] = __float_as_uint(t_max);
+    cyc[7 * stride] = __float_as_uint(hh);
     while (scale >= minScale && scale <= ESVO_MAX_SCALE && iter < MAX_ITER) {
         ++iter;
+        const uint32_t g0 = h.grid_reads, dd0 = h.dda_steps;
+        {  // one iteration; `goto next_iter` is the reference's `continue`
         // fetchChildDescriptor (:282-293)
         if (!fetched) {
             const uint2 nd = __ldg(s.nodes + parent);
@@ -401,6 +425,9 @@ __device__ void cast_ray(const DevScene& s, float ox, float oy, float oz, float 
                         h.node = parent;
                         h.flags |= method << 4;
                         h.iters = uint32_t(iter);
+                        h.run_iters = h.iters;
+                        h.run_grid_reads = h.grid_reads;
+                        h.run_dda_steps = h.dda_steps;
                         return;
                     }
                 }
@@ -420,7 +447,7 @@ __device__ void cast_ray(const DevScene& s, float ox, float oy, float oz, float 
                 const int worldIdx = idx ^ (~c.octant_mask & 7);
                 const uint32_t nonLeafMask = ~pLeaf & pValid & 0xFFu;
                 const uint32_t child_index = pChild + __popc(nonLeafMask & ((1u << worldIdx) - 1u));
-                if (child_index >= s.node_count) continue;
+                if (child_index >= s.node_count) goto next_iter;
                 parent = child_index;
                 idx = 0;
                 scale--;
@@ -430,7 +457,7 @@ __device__ void cast_ray(const DevScene& s, float ox, float oy, float oz, float 
                 if (tz_center > t_min) { idx ^= 4; pz += scale_exp2; }
                 t_max = tv_max;
                 fetched = false;
-                continue;
+                goto next_iter;
             }
         }
         // executeAdvancePhase (:380-416)
@@ -446,7 +473,7 @@ __device__ void cast_ray(const DevScene& s, float ox, float oy, float oz, float 
             if (csz && tz <= tcc) { step_mask ^= 4; pz -= scale_exp2; }
             t_min = gmax(tcc, 0.0f);
             idx ^= step_mask;
-            if ((idx & step_mask) == 0) continue;
+            if ((idx & step_mask) == 0) goto next_iter;
         }
         // POP: step mask recomputed at the new position (:672-681)
         int step_mask = 0;
@@ -464,7 +491,7 @@ __device__ void cast_ray(const DevScene& s, float ox, float oy, float oz, float 
             if (t_min > t_max || px < 1.0f || px >= 2.0f || py < 1.0f || py >= 2.0f || pz < 1.0f || pz >= 2.0f)
                 break;
             fetched = false;
-            continue;
+            goto next_iter;
         }
         {
             // floatToInt: clamp to [0,1], scale by 2^22, clamp to 2^22-1, truncate.
@@ -503,8 +530,50 @@ __device__ void cast_ray(const DevScene& s, float ox, float oy, float oz, float 
             hh = 0.0f;
             fetched = false;
         }
+        }
+    next_iter:
+        {
+            uint32_t cur[8];
+            cur[0] = uint32_t(scale) | (uint32_t(idx) << 8) | (uint32_t(fetched) << 16);
+            cur[1] = parent;
+            cur[2] = __float_as_uint(px); cur[3] = __float_as_uint(py); cur[4] = __float_as_uint(pz);
+            cur[5] = __float_as_uint(t_min); cur[6] = __float_as_uint(t_max); cur[7] = __float_as_uint(hh);
+            const uint32_t dg = h.grid_reads - g0, ddd = h.dda_steps - dd0;
+            bool eq1 = true, eq2 = have2;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const uint32_t a = cyc[k * stride], b = cyc[(k + 8) * stride];
+                eq1 = eq1 && (cur[k] == a);
+                eq2 = eq2 && (cur[k] == b);
+                cyc[(k + 8) * stride] = a;
+                cyc[k * stride] = cur[k];
+            }
+            if (eq1 || eq2) {
+                const uint32_t rem = uint32_t(MAX_ITER - iter);
+                h.run_iters = uint32_t(iter);
+                h.run_grid_reads = h.grid_reads;
+                h.run_dda_steps = h.dda_steps;
+                if (eq1) {
+                    h.grid_reads += rem * dg;
+                    h.dda_steps += rem * ddd;
+                } else {
+                    h.grid_reads += ((rem + 1) / 2) * d1g + (rem / 2) * dg;
+                    h.dda_steps += ((rem + 1) / 2) * d1d + (rem / 2) * ddd;
+                }
+                iter = MAX_ITER;
+                h.iters = uint32_t(iter);
+                h.flags |= F_ITER_CAP;
+                return;
+            }
+            have2 = true;
+            d1g = dg;
+            d1d = ddd;
+        }
     }
     h.iters = uint32_t(iter);
+    h.run_iters = h.iters;
+    h.run_grid_reads = h.grid_reads;
+    h.run_dda_steps = h.dda_steps;
     if (iter >= MAX_ITER) h.flags |= F_ITER_CAP;
 }
 
@@ -554,27 +623,29 @@ __device__ __forceinline__ void store_color(const DevScene& s, void* color, uint
 
 constexpr int BLOCK = 256;
 
-__global__ void __launch_bounds__(BLOCK) cast_kernel(DevScene s, const vx_ray* __restrict__ rays, uint32_t n,
+__global__ void __launch_bounds__(BLOCK, 3) cast_kernel(DevScene s, const vx_ray* __restrict__ rays, uint32_t n,
                                                       float tmin, float tmax, vx_hit* __restrict__ hits,
                                                       void* __restrict__ color,
                                                       vx_ray_counters* __restrict__ counters) {
     extern __shared__ uint32_t smem[];
     uint32_t* stkN = smem + threadIdx.x;
     float* stkT = reinterpret_cast<float*>(smem + s.max_levels * blockDim.x) + threadIdx.x;
+    uint32_t* cyc = smem + 2 * s.max_levels * blockDim.x + threadIdx.x;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float2* r2 = reinterpret_cast<const float2*>(rays + i);
     const float2 a = __ldg(r2), b = __ldg(r2 + 1), c = __ldg(r2 + 2);
     Hit h;
-    cast_ray(s, a.x, a.y, b.x, b.y, c.x, c.y, tmin, tmax, stkN, stkT, blockDim.x, h);
+    cast_ray(s, a.x, a.y, b.x, b.y, c.x, c.y, tmin, tmax, stkN, stkT, cyc, blockDim.x, h);
     store_hit(hits, i, h);
     if (color) store_color(s, color, i, h);
     if (counters) {
-        vx_ray_counters rc;
-        rc.iters = uint16_t(h.iters);
-        rc.grid_reads = uint8_t(h.grid_reads);
-        rc.dda_steps = uint8_t(h.dda_steps);
-        counters[i] = rc;
+        uint4 rc;
+        rc.x = (h.iters & 0xFFFFu) | (h.grid_reads << 16);
+        rc.y = h.dda_steps;
+        rc.z = (h.run_iters & 0xFFFFu) | (h.run_grid_reads << 16);
+        rc.w = h.run_dda_steps;
+        reinterpret_cast<uint4*>(counters)[i] = rc;
     }
 }
 
@@ -584,6 +655,7 @@ __global__ void __launch_bounds__(BLOCK) render_kernel(DevScene s, CameraDev cam
     extern __shared__ uint32_t smem[];
     uint32_t* stkN = smem + threadIdx.x;
     float* stkT = reinterpret_cast<float*>(smem + s.max_levels * blockDim.x) + threadIdx.x;
+    uint32_t* cyc = smem + 2 * s.max_levels * blockDim.x + threadIdx.x;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= w * hgt) return;
     const uint32_t px = i % w, py = i / w;
@@ -591,7 +663,7 @@ __global__ void __launch_bounds__(BLOCK) render_kernel(DevScene s, CameraDev cam
     float uv_y;
     camera_ray(cam, px, py, w, hgt, r, &uv_y);
     Hit h;
-    cast_ray(s, r.ox, r.oy, r.oz, r.dx, r.dy, r.dz, 0.0f, FLT_MAX_, stkN, stkT, blockDim.x, h);
+    cast_ray(s, r.ox, r.oy, r.oz, r.dx, r.dy, r.dz, 0.0f, FLT_MAX_, stkN, stkT, cyc, blockDim.x, h);
     if (hits) store_hit(hits, i, h);
     if (color) store_color(s, color, i, h);
     if (image) {
@@ -635,7 +707,7 @@ __global__ void camera_rays_kernel(CameraDev cam, uint32_t w, uint32_t hgt, vx_r
     rays[i] = r;
 }
 
-size_t stack_bytes(const DevScene& s) { return size_t(2) * size_t(s.max_levels) * BLOCK * sizeof(uint32_t); }
+size_t stack_bytes(const DevScene& s) { return (size_t(2) * size_t(s.max_levels) + 16) * BLOCK * sizeof(uint32_t); }
 
 }  // namespace
 
