@@ -252,9 +252,13 @@ def main():
     cnt = counters.cpu().numpy().view(vx.COUNTER_DTYPE).reshape(-1)
     g_hits = hits.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1).copy()
     nhit = int(np.count_nonzero(g_hits["flags"] & 1))
-    algo_bytes = bytes_per_launch(n, int(cnt["iters"].astype(np.int64).sum()),
-                                  int(cnt["grid_reads"].astype(np.int64).sum()),
-                                  int(cnt["dda_steps"].astype(np.int64).sum()), nhit, scene.color_kind)
+    tot = {k: int(cnt[k].astype(np.int64).sum()) for k in cnt.dtype.names}
+    # Bytes the kernel has to move (iterations after a detected cycle repeat
+    # data already read and are not counted) and, for reference, the bytes of
+    # the full 500-iteration reference loop.
+    algo_bytes = bytes_per_launch(n, tot["run_iters"], tot["run_grid_reads"], tot["run_dda_steps"], nhit,
+                                  scene.color_kind)
+    ref_bytes = bytes_per_launch(n, tot["iters"], tot["grid_reads"], tot["dda_steps"], nhit, scene.color_kind)
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     sampler = ClockSampler(local)
@@ -342,6 +346,8 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": algo_bytes,
+                         "reference_loop_bytes_per_launch": ref_bytes,
+                         "per_ray": {k: v / n for k, v in tot.items()},
                          "kernel": "vx::cast_kernel", "kernel_ms_mean": mean_s * 1e3},
             "gpu_launches": args.steps, "hit_rate": nhit / n,
             "clocks": clocks}

@@ -93,7 +93,7 @@ def test_noise_scene_rgba8_bit_exact(vx, vo, cuda, R):
     oh = o.cast_rays(rays)
     assert_hits_equal(g, oh, cnt, wl.name)
     hit = (oh["flags"] & 1).astype(bool)
-    assert hit.mean() > 0.3
+    assert hit.mean() > 0.1
     want = np.zeros(rays.shape[0], np.uint32)
     want[hit] = wl.scene.brick_color[oh["brick"][hit].astype(np.int64) * 512 + oh["voxel"][hit]]
     np.testing.assert_array_equal(col[:, 0].view(np.uint32), want)
@@ -124,7 +124,7 @@ def test_config1_full_size_bit_exact(vx, vo, cuda):
     g, col, cnt = gpu_cast(vx, wl.scene, rays)
     oh = o.cast_rays(rays)
     assert_hits_equal(g, oh, cnt, wl.name)
-    assert (oh["flags"] & 1).mean() > 0.5
+    assert (oh["flags"] & 1).mean() > 0.2
 
 
 def test_t_range_clipping(vx, vo, cuda):

@@ -158,6 +158,7 @@ int vx_scene_create(const vx_scene_desc* d, vx_scene** out) {
         ds.wmin[i] = c.world_min[i];
         ds.wmax[i] = c.world_max[i];
         ds.wsize[i] = c.world_max[i] - c.world_min[i];
+        ds.wsm[i] = ds.wsize[i] - 0.001f;
         ds.qwm[i] = int32_t(std::floor(c.world_min[i]));
     }
     ds.max_levels = c.max_levels;

@@ -14,6 +14,7 @@ namespace vx {
 // Scene as the kernels see it (passed by value as a kernel parameter).
 struct DevScene {
     float wmin[3], wmax[3], wsize[3];  // wsize = wmax - wmin (float subtract)
+    float wsm[3];                      // wsize - 0.001 (SVOBrickDDA.cpp:128, 143)
     int32_t qwm[3];                    // floor(world_min), VoxelComponents.h:373-379
     int32_t max_levels;
     int32_t min_scale;                 // 22 - max_levels + 1

@@ -8,8 +8,10 @@ configurations this library is measured on:
   cfg1  256^3 (octree depth 8), value noise (spacing 32, 4 octaves) at 10 %
         fill plus a one-voxel box shell; RGBA8 colour per voxel; 512x512
         pinhole camera, 60 deg, at the centre of the -Z face looking +Z.
-        The face itself is shell, so the camera sits at (128, 128, 1.5), just
-        inside it.
+        The face itself is shell, so the camera sits just inside it, at the
+        centre of the face's middle voxel, (128.5, 128.5, 1.5).  (At exactly
+        x = y = 128 every ray starts on an ESVO cell boundary and the
+        reference traversal exits before reaching any voxel.)
   cfg2  1024^3 (depth 10), value noise (spacing 64, 5 octaves) at 50 % fill;
         DXT1 bricks with uniform random heads and index words; 1920x1080,
         70 deg, at a seeded empty voxel looking in a uniform random direction.
@@ -100,7 +102,7 @@ def config1(R: int = 256, width: int = 512, height: int = 512, seed: int = 1) ->
     """cfg1; R, width and height shrink it for fast parity tests."""
     spacing = max(4, 32 * R // 256)
     scene, bits = noise_scene(R, spacing, 4 if spacing >= 32 else 3, 0.10, seed, True, "rgba8")
-    cam = look_camera([R / 2, R / 2, 1.5], [0, 0, 1], 60.0, width, height)
+    cam = look_camera([R / 2 + 0.5, R / 2 + 0.5, 1.5], [0, 0, 1], 60.0, width, height)
     return Workload(f"cfg1_noise{R}_rgba8_{width}x{height}", R, scene, bits, cam, width, height)
 
 
