@@ -214,6 +214,57 @@ int vx_camera_rays_dev(const vx_camera_pc* pc, uint32_t width, uint32_t height,
                        vx_ray* rays_dev, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Batched form (no reference counterpart).  One persistent launch casts the
+ * rays of many scenes: rays of scene i are rays[begin[i] .. begin[i+1]) of
+ * one buffer (begin: count + 1 device u32, begin[0] = 0, begin[count] = n).
+ * Hits are identical to vx_cast_rays on each scene.  Warps take tasks of
+ * `rays_per_task` consecutive rays from a work counter the batch owns, so
+ * calls on one batch must not overlap on the GPU.
+ * --------------------------------------------------------------------- */
+typedef struct vx_batch vx_batch;
+typedef struct vx_batch_tuning {
+    int32_t block;            /* 128 or 256 threads */
+    int32_t rays_per_task;    /* multiple of 32 */
+    int32_t stack_in_shared;  /* 1: traversal stack in shared memory, 0: in local memory */
+    int32_t reserved;
+} vx_batch_tuning;
+
+int vx_batch_create(const vx_scene* const* scenes, uint32_t count, vx_batch** out);
+int vx_batch_destroy(vx_batch* batch);
+int vx_batch_set_tuning(vx_batch* batch, const vx_batch_tuning* tuning);
+int vx_batch_get_tuning(const vx_batch* batch, vx_batch_tuning* tuning);
+int vx_cast_batch(vx_batch* batch, const vx_ray* rays_dev, const uint32_t* begin_dev, uint32_t n,
+                  float t_min, float t_max, vx_hit* hits_dev, vx_ray_counters* counters_dev,
+                  void* stream);
+/* Times every (block, rays_per_task, stack placement) candidate on the given
+ * rays (3 launches each, best of the last 2), keeps the fastest in the batch
+ * and returns it.  Writes hits_dev. */
+int vx_batch_autotune(vx_batch* batch, const vx_ray* rays_dev, const uint32_t* begin_dev, uint32_t n,
+                      vx_hit* hits_dev, void* stream, vx_batch_tuning* best, float* best_ms);
+
+/* Secondary rays from primary hits.  Bounce: 2 rays per primary ray (out:
+ * 2n), origin = hit point + 1e-3 * normal (hit point = origin +
+ * normalize(dir) * t), direction = a cosine-weighted hemisphere sample about
+ * the normal from a fixed 4096-entry table (vx_bounce_table), chosen by a
+ * hash of (seed, ray index, k).  Shadow: 1 ray per primary ray toward
+ * light_dir.  Misses produce zero-direction rays, which a cast reports as
+ * VX_RAY_INVALID. */
+int vx_spawn_bounce_rays(const vx_ray* rays_dev, const vx_hit* hits_dev, uint32_t n, uint64_t seed,
+                         vx_ray* out_dev, void* stream);
+int vx_spawn_shadow_rays(const vx_ray* rays_dev, const vx_hit* hits_dev, uint32_t n,
+                         const float light_dir[3], vx_ray* out_dev, void* stream);
+int vx_bounce_table(float* out /* 4096 x 3 */);
+
+/* One frame as a CUDA graph: batched primary cast, bounce spawn, batched
+ * bounce cast (bounce_begin = 2 x primary begin).  Capture needs a
+ * non-default stream; launch replays it on any stream. */
+int vx_batch_capture_frame(vx_batch* batch, const vx_ray* primary_dev, const uint32_t* primary_begin_dev,
+                           uint32_t n, vx_hit* primary_hits_dev, vx_ray* bounce_dev,
+                           const uint32_t* bounce_begin_dev, vx_hit* bounce_hits_dev, uint64_t seed,
+                           void* stream);
+int vx_batch_launch_frame(vx_batch* batch, void* stream);
+
+/* ------------------------------------------------------------------------
  * Host scene builder.  Replaces LaineKarrasOctree::rebuild
  * (SVO/src/SVORebuild.cpp:228-607) plus VoxelSceneCacher::BuildOctree /
  * BuildBrickGridLookup (VoxelSceneCacher.cpp:463-713) for a dense occupancy
@@ -250,8 +301,8 @@ int vx_synth_noise(uint32_t R, uint32_t spacing, uint32_t octaves, float fill,
  * field and the lattice tables) and returns after the bits are written. */
 int vx_synth_noise_dev(uint32_t R, uint32_t spacing, uint32_t octaves, float fill,
                        uint64_t seed, int32_t shell, uint64_t* out_bits_dev, void* stream);
-/* Urban lattice: 32x32 blocks of pitch R/32 (block + 8-voxel street), each a
- * solid box of seeded height in [hmin, hmax]. */
+/* Urban lattice: 32x32 blocks of pitch R/32 (block + street of max(1, R/256)
+ * voxels: 8 at R = 2048), each a solid box of seeded height in [hmin, hmax]. */
 int vx_synth_urban(uint32_t R, uint32_t hmin, uint32_t hmax, uint64_t seed,
                    uint64_t* out_bits);
 /* Per-brick colour payloads keyed on brick grid coordinates (so they do not

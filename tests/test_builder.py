@@ -107,8 +107,8 @@ def test_synth_urban_shape(vx):
     R = 512
     bits = vx.synth_urban(R, 16, 400, 3)
     dense = np.unpackbits(bits.view(np.uint8), bitorder="little").reshape(R, R, R)  # [z, y, x]
-    pitch = R // 32
-    assert not dense[:, :, pitch - 8:pitch].any()          # street in x
-    assert not dense[pitch - 8:pitch, :, :].any()          # street in z
-    col = dense[:pitch - 8, :, :pitch - 8]
+    pitch, street = R // 32, max(1, R // 256)
+    assert not dense[:, :, pitch - street:pitch].any()          # street in x
+    assert not dense[pitch - street:pitch, :, :].any()          # street in z
+    col = dense[:pitch - street, :, :pitch - street]
     assert col.any()

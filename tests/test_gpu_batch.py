@@ -1,0 +1,154 @@
+"""Batched persistent kernel, secondary-ray spawn and the frame CUDA graph
+(needs a B200).  The batched cast must return exactly the plain kernel's hits
+for every scene, and the plain kernel's are checked against the oracle."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _small_specs(W, n=10, seed=11):
+    return W.config4_specs(n, seed=seed, r_range=(6, 7.4), res_lo=(48, 40), res_hi=(160, 96))
+
+
+def _setup(vx, W, n=10, seed=11):
+    import torch
+    wls = [W.build_spec(s) for s in _small_specs(W, n, seed)]
+    scenes = [vx.Scene(w.scene) for w in wls]
+    rays = [w.rays() for w in wls]
+    begin = np.concatenate([[0], np.cumsum([r.shape[0] for r in rays])]).astype(np.uint32)
+    allr = np.concatenate(rays).astype(np.float32)
+    return wls, scenes, rays, begin, allr, torch.from_numpy(allr).cuda(), torch.from_numpy(begin.astype(np.int32)).cuda()
+
+
+def _plain(vx, scenes, rays, begin, d_rays):
+    import torch
+    n = d_rays.shape[0]
+    hits = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+    for i, s in enumerate(scenes):
+        a, b = int(begin[i]), int(begin[i + 1])
+        s.cast_rays_dev(d_rays[a:b], hits[a:b])
+    torch.cuda.synchronize()
+    return hits
+
+
+@pytest.mark.parametrize("block,k,smem", [(256, 128, 1), (128, 32, 1), (256, 64, 0), (128, 512, 0)])
+def test_batch_equals_plain_and_oracle(vx, vo, cuda, block, k, smem):
+    import torch
+    from vx_b200 import workloads as W
+    wls, scenes, rays, begin, allr, d_rays, d_begin = _setup(vx, W)
+    plain = _plain(vx, scenes, rays, begin, d_rays)
+    batch = vx.Batch(scenes)
+    batch.set_tuning(block, k, smem)
+    hits = torch.full_like(plain, -1)
+    cnt = torch.zeros((allr.shape[0], 4), dtype=torch.int32, device="cuda")
+    batch.cast(d_rays, d_begin, hits, cnt)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(hits.cpu().numpy(), plain.cpu().numpy())
+    g = hits.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1)
+    c = cnt.cpu().numpy().view(vx.COUNTER_DTYPE).reshape(-1)
+    for i, w in enumerate(wls[:4]):
+        a, b = int(begin[i]), int(begin[i + 1])
+        oh = vo.OracleScene.from_dense(w.bits, w.R, w.scene.max_levels).cast_rays(rays[i])
+        assert np.array_equal(g["brick"][a:b], oh["brick"]) and np.array_equal(g["node"][a:b], oh["node"])
+        assert np.array_equal(g["flags"][a:b].astype(np.uint32), oh["flags"])
+        assert np.array_equal(c["iters"][a:b].astype(np.uint32), oh["iters"])
+
+
+def test_bounce_spawn_matches_reference_and_casts_exactly(vx, vo, cuda):
+    import torch
+    from vx_b200 import workloads as W
+    wls, scenes, rays, begin, allr, d_rays, d_begin = _setup(vx, W, n=6, seed=12)
+    hits = _plain(vx, scenes, rays, begin, d_rays)
+    n = allr.shape[0]
+    bounce = torch.zeros((2 * n, 6), dtype=torch.float32, device="cuda")
+    vx.spawn_bounce_rays(d_rays, hits, 99, bounce)
+    torch.cuda.synchronize()
+    h = hits.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1)
+    want = W.bounce_rays_reference(allr, h, 99, vx.bounce_table())
+    np.testing.assert_array_equal(bounce.cpu().numpy().view(np.uint32), want.view(np.uint32))
+    # bounce rays through the batched kernel vs the oracle, per scene
+    bbegin = (2 * begin).astype(np.uint32)
+    batch = vx.Batch(scenes)
+    bh = torch.zeros((2 * n, 4), dtype=torch.int32, device="cuda")
+    batch.cast(bounce, torch.from_numpy(bbegin.astype(np.int32)).cuda(), bh)
+    torch.cuda.synchronize()
+    g = bh.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1)
+    for i, w in enumerate(wls):
+        a, b = int(bbegin[i]), int(bbegin[i + 1])
+        oh = vo.OracleScene.from_dense(w.bits, w.R, w.scene.max_levels).cast_rays(want[a:b])
+        hit = (oh["flags"] & 1).astype(bool)
+        assert np.array_equal(g["flags"][a:b].astype(np.uint32), oh["flags"])
+        assert np.array_equal(g["brick"][a:b], oh["brick"]) and np.array_equal(g["voxel"][a:b].astype(np.uint32),
+                                                                               oh["voxel"])
+        assert np.array_equal(g["t"][a:b][hit].view(np.uint32), oh["t"][hit].view(np.uint32))
+
+
+def test_shadow_spawn_matches_reference(vx, cuda):
+    import torch
+    from vx_b200 import workloads as W
+    wls, scenes, rays, begin, allr, d_rays, d_begin = _setup(vx, W, n=3, seed=13)
+    hits = _plain(vx, scenes, rays, begin, d_rays)
+    n = allr.shape[0]
+    L = np.array([0.3, 0.8, -0.52], np.float32)
+    out = torch.zeros((n, 6), dtype=torch.float32, device="cuda")
+    vx.spawn_shadow_rays(d_rays, hits, L, out)
+    torch.cuda.synchronize()
+    h = hits.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1)
+    b = W.bounce_rays_reference(allr, h, 0, vx.bounce_table())[0::2]  # same origins
+    hit = (h["flags"] & 1).astype(bool)
+    got = out.cpu().numpy()
+    np.testing.assert_array_equal(got[hit, :3].view(np.uint32), b[hit, :3].view(np.uint32))
+    assert np.all(got[hit, 3:] == L) and np.all(got[~hit, 3:] == 0)
+
+
+def test_frame_graph_equals_eager(vx, cuda):
+    import torch
+    from vx_b200 import workloads as W
+    wls, scenes, rays, begin, allr, d_rays, d_begin = _setup(vx, W, n=8, seed=14)
+    n = allr.shape[0]
+    batch = vx.Batch(scenes)
+    bb = torch.from_numpy((2 * begin).astype(np.int32)).cuda()
+    ph, bh = torch.zeros((n, 4), dtype=torch.int32, device="cuda"), torch.zeros((2 * n, 4), dtype=torch.int32,
+                                                                               device="cuda")
+    bounce = torch.zeros((2 * n, 6), dtype=torch.float32, device="cuda")
+    # eager frame
+    batch.cast(d_rays, d_begin, ph)
+    vx.spawn_bounce_rays(d_rays, ph, 7, bounce)
+    batch.cast(bounce, bb, bh)
+    torch.cuda.synchronize()
+    eager = (ph.cpu().numpy().copy(), bh.cpu().numpy().copy())
+    ph.zero_(), bh.zero_(), bounce.zero_()
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        batch.capture_frame(d_rays, d_begin, ph, bounce, bb, bh, 7, s.cuda_stream)
+        batch.launch_frame(s.cuda_stream)
+        batch.launch_frame(s.cuda_stream)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(ph.cpu().numpy(), eager[0])
+    np.testing.assert_array_equal(bh.cpu().numpy(), eager[1])
+
+
+def test_autotune_keeps_results(vx, cuda):
+    import torch
+    from vx_b200 import workloads as W
+    wls, scenes, rays, begin, allr, d_rays, d_begin = _setup(vx, W, n=6, seed=15)
+    plain = _plain(vx, scenes, rays, begin, d_rays)
+    batch = vx.Batch(scenes)
+    hits = torch.zeros_like(plain)
+    t, ms = batch.autotune(d_rays, d_begin, hits)
+    assert t.block in (128, 256) and t.rays_per_task % 32 == 0 and ms > 0
+    hits.zero_()
+    batch.cast(d_rays, d_begin, hits)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(hits.cpu().numpy(), plain.cpu().numpy())
+
+
+def test_batch_rejects_bad_tuning(vx, cuda):
+    from vx_b200 import workloads as W
+    wl = W.config1(R=64, width=8, height=8)
+    b = vx.Batch([vx.Scene(wl.scene)])
+    with pytest.raises(vx.VxError):
+        b.set_tuning(block=96)
+    with pytest.raises(vx.VxError):
+        b.set_tuning(rays_per_task=40)

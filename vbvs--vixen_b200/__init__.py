@@ -106,6 +106,17 @@ def lib():
         "vx_synth_urban": (C.c_int, [u32, u32, u32, u64, vp]),
         "vx_synth_rgba8": (C.c_int, [vp, u32, u64, vp]),
         "vx_synth_dxt1": (C.c_int, [vp, u32, u64, vp]),
+        "vx_batch_create": (C.c_int, [vp, u32, vp]),
+        "vx_batch_destroy": (C.c_int, [vp]),
+        "vx_batch_set_tuning": (C.c_int, [vp, vp]),
+        "vx_batch_get_tuning": (C.c_int, [vp, vp]),
+        "vx_cast_batch": (C.c_int, [vp, vp, vp, u32, f32, f32, vp, vp, vp]),
+        "vx_batch_autotune": (C.c_int, [vp, vp, vp, u32, vp, vp, vp, vp]),
+        "vx_spawn_bounce_rays": (C.c_int, [vp, vp, u32, u64, vp, vp]),
+        "vx_spawn_shadow_rays": (C.c_int, [vp, vp, u32, vp, vp, vp]),
+        "vx_bounce_table": (C.c_int, [vp]),
+        "vx_batch_capture_frame": (C.c_int, [vp, vp, vp, u32, vp, vp, vp, vp, u64, vp]),
+        "vx_batch_launch_frame": (C.c_int, [vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -369,3 +380,85 @@ class CudaOctree:
                ((bc >> 20) & 0x3FF) * 8 + (v >> 6) + int(q[2]))
         return RayHit(True, float(t), float(t + np.float32(1.0)), hp, tuple(n), self.max_levels - 1,
                       int(h["brick"]), v, int(h["node"]), ent)
+
+
+# ---------------------------------------------------------------------------
+# Batched form
+# ---------------------------------------------------------------------------
+
+class BatchTuning(C.Structure):
+    _fields_ = [("block", C.c_int32), ("rays_per_task", C.c_int32), ("stack_in_shared", C.c_int32),
+                ("reserved", C.c_int32)]
+
+    def as_dict(self):
+        return {"block": self.block, "rays_per_task": self.rays_per_task, "stack_in_shared": self.stack_in_shared}
+
+
+def _stream(stream):
+    import torch
+    return C.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+
+
+class Batch:
+    """Scenes cast together by the persistent batched kernel (vx_batch)."""
+
+    def __init__(self, scenes):
+        self.scenes = list(scenes)
+        arr = (C.c_void_p * len(self.scenes))(*[sc.handle.value for sc in self.scenes])
+        self._h = C.c_void_p()
+        check(lib().vx_batch_create(arr, len(self.scenes), C.byref(self._h)))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            check(lib().vx_batch_destroy(self._h))
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def tuning(self) -> BatchTuning:
+        t = BatchTuning()
+        check(lib().vx_batch_get_tuning(self._h, C.byref(t)))
+        return t
+
+    def set_tuning(self, block=256, rays_per_task=128, stack_in_shared=1):
+        t = BatchTuning(block, rays_per_task, stack_in_shared, 0)
+        check(lib().vx_batch_set_tuning(self._h, C.byref(t)))
+
+    def cast(self, rays, begin, hits, counters=None, t_min=0.0, t_max=FLT_MAX, stream=None):
+        check(lib().vx_cast_batch(self._h, _p(rays), _p(begin), rays.shape[0], float(t_min), float(t_max), _p(hits),
+                                  _p(counters), _stream(stream)))
+
+    def autotune(self, rays, begin, hits, stream=None):
+        t = BatchTuning()
+        ms = C.c_float()
+        check(lib().vx_batch_autotune(self._h, _p(rays), _p(begin), rays.shape[0], _p(hits), _stream(stream),
+                                      C.byref(t), C.byref(ms)))
+        return t, ms.value
+
+    def capture_frame(self, primary, primary_begin, primary_hits, bounce, bounce_begin, bounce_hits, seed, stream):
+        check(lib().vx_batch_capture_frame(self._h, _p(primary), _p(primary_begin), primary.shape[0],
+                                           _p(primary_hits), _p(bounce), _p(bounce_begin), _p(bounce_hits), seed,
+                                           C.c_void_p(stream)))
+
+    def launch_frame(self, stream=None):
+        check(lib().vx_batch_launch_frame(self._h, _stream(stream)))
+
+
+def spawn_bounce_rays(rays, hits, seed, out, stream=None):
+    check(lib().vx_spawn_bounce_rays(_p(rays), _p(hits), rays.shape[0], seed, _p(out), _stream(stream)))
+
+
+def spawn_shadow_rays(rays, hits, light_dir, out, stream=None):
+    ld = (C.c_float * 3)(*[float(v) for v in light_dir])
+    check(lib().vx_spawn_shadow_rays(_p(rays), _p(hits), rays.shape[0], ld, _p(out), _stream(stream)))
+
+
+def bounce_table() -> np.ndarray:
+    out = np.zeros(4096 * 3, np.float32)
+    check(lib().vx_bounce_table(_p(out)))
+    return out.reshape(4096, 3)

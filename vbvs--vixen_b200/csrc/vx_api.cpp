@@ -58,6 +58,11 @@ struct vx_scene {
     uint64_t stage_bytes = 0;
 };
 
+namespace vx {
+const DevScene& scene_dev(const vx_scene* s) { return s->dev; }
+int scene_device(const vx_scene* s) { return s->device; }
+}  // namespace vx
+
 namespace {
 
 using vx::fail;

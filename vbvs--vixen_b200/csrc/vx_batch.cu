@@ -1,0 +1,471 @@
+// vx_batch.cu - batched form: rays of many scenes in one persistent launch,
+// bounce / shadow ray generation, the frame CUDA graph and the autotuner.
+//
+// The batched kernel is persistent: one grid of (SM count x resident blocks)
+// whose warps take tasks of K consecutive rays from a global work counter
+// (atomicAdd by lane 0, broadcast with __shfl_sync).  The rays of all scenes
+// sit in one buffer; ray r belongs to the scene i with begin[i] <= r <
+// begin[i+1], found by binary search over a copy of begin[] and of the scene
+// table in shared memory, so a task may span two scenes.  Each lane walks its
+// rays of the task independently (independent thread scheduling lets lanes
+// that finish early take their next ray while others are still traversing);
+// the warp re-converges at the next task fetch.  The per-ray traversal is the
+// one of the plain kernel (vx_cast.cuh), so hits are identical bit for bit.
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "vx_cast.cuh"
+
+namespace vx {
+namespace {
+
+constexpr int MAX_LEVELS_ALL = 23;
+constexpr uint32_t NUM_BOUNCE_DIRS = 4096;
+
+// Cosine-weighted hemisphere directions about +z (device copy of bounce_table()).
+__device__ float g_bounce_dirs[NUM_BOUNCE_DIRS * 3];
+
+struct BatchArgs {
+    const DevScene* scenes;
+    uint32_t S;
+    const uint32_t* begin;  // S + 1 prefix offsets
+    const vx_ray* rays;
+    uint32_t n;
+    float tmin, tmax;
+    vx_hit* hits;
+    vx_ray_counters* counters;
+    uint32_t* work;  // task counter, zero before the launch
+    uint32_t K;      // rays per warp task
+    int maxL;        // largest max_levels in the batch
+};
+
+template <int BLOCK, int MINB, bool SMEM_STACK>
+__global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
+    extern __shared__ uint32_t smem[];
+    DevScene* sc = reinterpret_cast<DevScene*>(smem);
+    uint32_t* beg = reinterpret_cast<uint32_t*>(sc + a.S);
+    {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(a.scenes);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(sc);
+        const uint32_t words = a.S * uint32_t(sizeof(DevScene) / 4);
+        for (uint32_t i = threadIdx.x; i < words; i += BLOCK) dst[i] = src[i];
+        for (uint32_t i = threadIdx.x; i <= a.S; i += BLOCK) beg[i] = a.begin[i];
+    }
+    __syncthreads();
+    uint32_t* stk_base = beg + ((a.S + 1 + 3) & ~3u);
+    uint32_t lnode[SMEM_STACK ? 1 : MAX_LEVELS_ALL];
+    float ltmax[SMEM_STACK ? 1 : MAX_LEVELS_ALL];
+    uint32_t lcyc[SMEM_STACK ? 1 : 16];
+    uint32_t* stkN;
+    float* stkT;
+    uint32_t* cyc;
+    int stride;
+    if (SMEM_STACK) {
+        stkN = stk_base + threadIdx.x;
+        stkT = reinterpret_cast<float*>(stk_base + a.maxL * BLOCK) + threadIdx.x;
+        cyc = stk_base + 2 * a.maxL * BLOCK + threadIdx.x;
+        stride = BLOCK;
+    } else {
+        stkN = lnode;
+        stkT = ltmax;
+        cyc = lcyc;
+        stride = 1;
+    }
+    const uint32_t lane = threadIdx.x & 31u;
+    for (;;) {
+        uint32_t t = 0;
+        if (lane == 0) t = atomicAdd(a.work, 1u);
+        t = __shfl_sync(0xFFFFFFFFu, t, 0);
+        const uint64_t r0 = uint64_t(t) * a.K;
+        if (r0 >= a.n) break;
+        const uint32_t r1 = uint32_t(min(r0 + a.K, uint64_t(a.n)));
+        for (uint32_t r = uint32_t(r0) + lane; r < r1; r += 32) {
+            int lo = 0, hi = int(a.S);
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (beg[mid] <= r) lo = mid;
+                else hi = mid;
+            }
+            const float2* r2 = reinterpret_cast<const float2*>(a.rays + r);
+            const float2 p = __ldg(r2), q = __ldg(r2 + 1), w = __ldg(r2 + 2);
+            Hit h;
+            cast_ray(sc[lo], p.x, p.y, q.x, q.y, w.x, w.y, a.tmin, a.tmax, stkN, stkT, cyc, stride, h);
+            store_hit(a.hits, r, h);
+            if (a.counters) {
+                uint4 rc;
+                rc.x = (h.iters & 0xFFFFu) | (h.grid_reads << 16);
+                rc.y = h.dda_steps;
+                rc.z = (h.run_iters & 0xFFFFu) | (h.run_grid_reads << 16);
+                rc.w = h.run_dda_steps;
+                reinterpret_cast<uint4*>(a.counters)[r] = rc;
+            }
+        }
+    }
+}
+
+__host__ __device__ inline uint64_t mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+// Hit point and offset origin of a secondary ray: hp = o + normalize(d) * t
+// (normalised exactly as the cast does), then hp + 1e-3 * n on the normal axis.
+__device__ __forceinline__ bool secondary_origin(const vx_ray& r, const vx_hit& h, float org[3], int& axis,
+                                                 float& sgn) {
+    if (!(h.flags & VX_HIT_HIT)) return false;
+    const float dd = (r.dx * r.dx + r.dy * r.dy) + r.dz * r.dz;
+    const float inv = 1.0f / sqrtf(dd);
+    org[0] = r.ox + (r.dx * inv) * h.t;
+    org[1] = r.oy + (r.dy * inv) * h.t;
+    org[2] = r.oz + (r.dz * inv) * h.t;
+    axis = (h.flags >> 1) & 3;
+    sgn = (h.flags & VX_HIT_NORMAL_NEG) ? -1.0f : 1.0f;
+    org[axis] = org[axis] + sgn * 0.001f;
+    return true;
+}
+
+__global__ void spawn_bounce_kernel(const vx_ray* __restrict__ rays, const vx_hit* __restrict__ hits, uint32_t n,
+                                    uint64_t seed, vx_ray* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const vx_ray r = rays[i];
+    const vx_hit h = hits[i];
+    float org[3];
+    int axis;
+    float sgn;
+    if (!secondary_origin(r, h, org, axis, sgn)) {
+        const vx_ray z{r.ox, r.oy, r.oz, 0.0f, 0.0f, 0.0f};
+        out[2 * size_t(i)] = z;
+        out[2 * size_t(i) + 1] = z;
+        return;
+    }
+    for (uint32_t k = 0; k < 2; ++k) {
+        const uint32_t j = uint32_t(mix64(seed ^ mix64((uint64_t(i) << 1) | k)) & (NUM_BOUNCE_DIRS - 1));
+        const float u = g_bounce_dirs[3 * j], v = g_bounce_dirs[3 * j + 1], w = g_bounce_dirs[3 * j + 2] * sgn;
+        vx_ray b;
+        b.ox = org[0];
+        b.oy = org[1];
+        b.oz = org[2];
+        if (axis == 0) { b.dx = w; b.dy = u; b.dz = v; }
+        else if (axis == 1) { b.dx = v; b.dy = w; b.dz = u; }
+        else { b.dx = u; b.dy = v; b.dz = w; }
+        out[2 * size_t(i) + k] = b;
+    }
+}
+
+__global__ void spawn_shadow_kernel(const vx_ray* __restrict__ rays, const vx_hit* __restrict__ hits, uint32_t n,
+                                    float lx, float ly, float lz, vx_ray* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const vx_ray r = rays[i];
+    const vx_hit h = hits[i];
+    float org[3];
+    int axis;
+    float sgn;
+    if (!secondary_origin(r, h, org, axis, sgn)) {
+        out[i] = vx_ray{r.ox, r.oy, r.oz, 0.0f, 0.0f, 0.0f};
+        return;
+    }
+    out[i] = vx_ray{org[0], org[1], org[2], lx, ly, lz};
+}
+
+// The direction table (host), generated once: stratum-free cosine-weighted
+// samples from a counter hash, evaluated in double and rounded to binary32.
+const std::vector<float>& bounce_table() {
+    static std::vector<float> tab = [] {
+        std::vector<float> t(NUM_BOUNCE_DIRS * 3);
+        for (uint32_t k = 0; k < NUM_BOUNCE_DIRS; ++k) {
+            const uint64_t h1 = mix64(0xB0C0E5EEDULL + k), h2 = mix64(h1);
+            const double u1 = double(h1 >> 11) * (1.0 / 9007199254740992.0);
+            const double u2 = double(h2 >> 11) * (1.0 / 9007199254740992.0);
+            const double rr = std::sqrt(u1), phi = 6.283185307179586476925 * u2;
+            t[3 * k] = float(rr * std::cos(phi));
+            t[3 * k + 1] = float(rr * std::sin(phi));
+            t[3 * k + 2] = float(std::sqrt(std::max(0.0, 1.0 - u1)));
+        }
+        return t;
+    }();
+    return tab;
+}
+
+std::mutex g_table_mu;
+bool g_table_ready[64] = {};
+
+int ensure_bounce_table() {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(VX_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (dev < 0 || dev >= 64) return fail(VX_EINVAL, "device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_table_mu);
+    if (g_table_ready[dev]) return VX_OK;
+    const auto& t = bounce_table();
+    e = cudaMemcpyToSymbol(g_bounce_dirs, t.data(), t.size() * sizeof(float));
+    if (e != cudaSuccess) return fail(VX_ECUDA, std::string("bounce table upload: ") + cudaGetErrorString(e));
+    g_table_ready[dev] = true;
+    return VX_OK;
+}
+
+struct Variant {
+    int block;
+    bool smem;
+};
+
+}  // namespace
+}  // namespace vx
+
+struct vx_batch {
+    int device = 0;
+    int per_sm[4] = {0, 0, 0, 0};    // resident blocks per SM of each kernel variant (0 = not resolved)
+    uint32_t S = 0;
+    int maxL = 1;
+    vx::DevScene* scenes = nullptr;  // device copy of the scene table
+    uint32_t* work = nullptr;        // task counter (device scratch)
+    vx_batch_tuning tuning{256, 128, 1, 0};
+    int num_sms = 148;
+    cudaGraphExec_t frame = nullptr;
+    cudaGraph_t frame_graph = nullptr;
+};
+
+namespace {
+
+using vx::fail;
+
+int cuda_err(cudaError_t e, const char* what) {
+    return fail(VX_ECUDA, std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+size_t batch_smem(const vx_batch* b, bool smem_stack, int block) {
+    size_t bytes = size_t(b->S) * sizeof(vx::DevScene) + ((size_t(b->S) + 1 + 3) & ~size_t(3)) * 4;
+    if (smem_stack) bytes += (size_t(2) * size_t(b->maxL) + 16) * size_t(block) * 4;
+    return bytes;
+}
+
+// Resolves (once per batch and variant, outside any stream capture) the
+// dynamic shared-memory attribute and the resident blocks per SM.
+template <int BLOCK, int MINB, bool SMEM>
+int prepare_variant(vx_batch* b, int slot) {
+    if (b->per_sm[slot]) return VX_OK;
+    auto kern = vx::batch_kernel<BLOCK, MINB, SMEM>;
+    const size_t smem = batch_smem(b, SMEM, BLOCK);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch: shared memory attribute");
+    }
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BLOCK, smem);
+    if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch: occupancy");
+    if (per_sm < 1) return fail(VX_EINVAL, "vx_cast_batch: kernel does not fit on an SM (too many scenes?)");
+    b->per_sm[slot] = per_sm;
+    return VX_OK;
+}
+
+template <int BLOCK, int MINB, bool SMEM>
+int launch_variant(vx_batch* b, int slot, const vx::BatchArgs& a, cudaStream_t st) {
+    if (int r = prepare_variant<BLOCK, MINB, SMEM>(b, slot)) return r;
+    vx::batch_kernel<BLOCK, MINB, SMEM><<<b->num_sms * b->per_sm[slot], BLOCK, batch_smem(b, SMEM, BLOCK), st>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch: launch");
+    return VX_OK;
+}
+
+int launch_batch(vx_batch* b, const vx_batch_tuning& t, const vx::BatchArgs& a, cudaStream_t st) {
+    if (t.block == 128)
+        return t.stack_in_shared ? launch_variant<128, 6, true>(b, 0, a, st) : launch_variant<128, 6, false>(b, 1, a, st);
+    return t.stack_in_shared ? launch_variant<256, 3, true>(b, 2, a, st) : launch_variant<256, 3, false>(b, 3, a, st);
+}
+
+int prepare_batch(vx_batch* b, const vx_batch_tuning& t) {
+    if (t.block == 128)
+        return t.stack_in_shared ? prepare_variant<128, 6, true>(b, 0) : prepare_variant<128, 6, false>(b, 1);
+    return t.stack_in_shared ? prepare_variant<256, 3, true>(b, 2) : prepare_variant<256, 3, false>(b, 3);
+}
+
+int check_tuning(const vx_batch_tuning* t) {
+    if (!t || (t->block != 128 && t->block != 256) || t->rays_per_task < 32 || t->rays_per_task > 65536 ||
+        (t->rays_per_task % 32) != 0)
+        return fail(VX_EINVAL, "batch tuning: block must be 128 or 256, rays_per_task a multiple of 32 in [32, 65536]");
+    return VX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vx_batch_create(const vx_scene* const* scenes, uint32_t count, vx_batch** out) {
+    if (!out || (!scenes && count) || count == 0 || count > 256)
+        return fail(VX_EINVAL, "vx_batch_create: need 1..256 scenes");
+    *out = nullptr;
+    auto* b = new (std::nothrow) vx_batch();
+    if (!b) return fail(VX_ENOMEM, "vx_batch_create: out of host memory");
+    cudaGetDevice(&b->device);
+    std::vector<vx::DevScene> host(count);
+    for (uint32_t i = 0; i < count; ++i) {
+        if (!scenes[i]) { delete b; return fail(VX_EINVAL, "vx_batch_create: null scene"); }
+        if (vx::scene_device(scenes[i]) != b->device) {
+            delete b;
+            return fail(VX_EINVAL, "vx_batch_create: every scene must live on the current device");
+        }
+        host[i] = vx::scene_dev(scenes[i]);
+        b->maxL = std::max(b->maxL, host[i].max_levels);
+    }
+    b->S = count;
+    cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device);
+    cudaError_t e = cudaMalloc(&b->scenes, sizeof(vx::DevScene) * count);
+    if (e == cudaSuccess) e = cudaMalloc(&b->work, 256);
+    if (e == cudaSuccess) e = cudaMemcpy(b->scenes, host.data(), sizeof(vx::DevScene) * count, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(b->scenes);
+        cudaFree(b->work);
+        delete b;
+        return cuda_err(e, "vx_batch_create");
+    }
+    *out = b;
+    return VX_OK;
+}
+
+int vx_batch_destroy(vx_batch* b) {
+    if (!b) return VX_OK;
+    if (b->frame) cudaGraphExecDestroy(b->frame);
+    if (b->frame_graph) cudaGraphDestroy(b->frame_graph);
+    cudaFree(b->scenes);
+    cudaFree(b->work);
+    delete b;
+    return VX_OK;
+}
+
+int vx_batch_set_tuning(vx_batch* b, const vx_batch_tuning* t) {
+    if (!b) return fail(VX_EINVAL, "vx_batch_set_tuning: null batch");
+    if (int r = check_tuning(t)) return r;
+    b->tuning = *t;
+    return VX_OK;
+}
+
+int vx_batch_get_tuning(const vx_batch* b, vx_batch_tuning* t) {
+    if (!b || !t) return fail(VX_EINVAL, "vx_batch_get_tuning: null argument");
+    *t = b->tuning;
+    return VX_OK;
+}
+
+int vx_cast_batch(vx_batch* b, const vx_ray* rays, const uint32_t* begin, uint32_t n, float tmin, float tmax,
+                  vx_hit* hits, vx_ray_counters* counters, void* stream) {
+    if (!b || !begin || (n && (!rays || !hits))) return fail(VX_EINVAL, "vx_cast_batch: null argument");
+    if (reinterpret_cast<uintptr_t>(rays) % 8 || reinterpret_cast<uintptr_t>(hits) % 16 ||
+        reinterpret_cast<uintptr_t>(counters) % 16 || reinterpret_cast<uintptr_t>(begin) % 4)
+        return fail(VX_EINVAL, "vx_cast_batch: misaligned buffer");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(b->work, 0, 4, st);
+    if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch: reset work counter");
+    if (n == 0) return VX_OK;
+    vx::BatchArgs a{b->scenes, b->S, begin, rays, n, tmin, tmax, hits, counters, b->work,
+                    uint32_t(b->tuning.rays_per_task), b->maxL};
+    return launch_batch(b, b->tuning, a, st);
+}
+
+int vx_batch_autotune(vx_batch* b, const vx_ray* rays, const uint32_t* begin, uint32_t n, vx_hit* hits, void* stream,
+                      vx_batch_tuning* best_out, float* best_ms_out) {
+    if (!b || !begin || !rays || !hits || n == 0) return fail(VX_EINVAL, "vx_batch_autotune: bad argument");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    vx_batch_tuning bt = b->tuning;
+    const int blocks[] = {128, 256};
+    const int ks[] = {32, 64, 128, 256, 512, 1024};
+    for (int blk : blocks)
+        for (int sm = 1; sm >= 0; --sm)
+            for (int k : ks) {
+                vx_batch_tuning t{blk, k, sm, 0};
+                vx::BatchArgs a{b->scenes, b->S, begin, rays, n, 0.0f, 3.402823466e+38f, hits, nullptr, b->work,
+                                uint32_t(k), b->maxL};
+                float ms_min = 1e30f;
+                for (int rep = 0; rep < 3; ++rep) {
+                    cudaMemsetAsync(b->work, 0, 4, st);
+                    cudaEventRecord(e0, st);
+                    int r = launch_batch(b, t, a, st);
+                    cudaEventRecord(e1, st);
+                    if (r != VX_OK) { cudaEventDestroy(e0); cudaEventDestroy(e1); return r; }
+                    cudaError_t e = cudaEventSynchronize(e1);
+                    if (e != cudaSuccess) { cudaEventDestroy(e0); cudaEventDestroy(e1); return cuda_err(e, "autotune"); }
+                    float ms = 0;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    if (rep > 0) ms_min = std::min(ms_min, ms);
+                }
+                if (ms_min < best) { best = ms_min; bt = t; }
+            }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->tuning = bt;
+    if (best_out) *best_out = bt;
+    if (best_ms_out) *best_ms_out = best;
+    return VX_OK;
+}
+
+int vx_bounce_table(float* out) {
+    if (!out) return fail(VX_EINVAL, "vx_bounce_table: null argument");
+    const auto& t = vx::bounce_table();
+    std::copy(t.begin(), t.end(), out);
+    return VX_OK;
+}
+
+int vx_spawn_bounce_rays(const vx_ray* rays, const vx_hit* hits, uint32_t n, uint64_t seed, vx_ray* out,
+                         void* stream) {
+    if (n && (!rays || !hits || !out)) return fail(VX_EINVAL, "vx_spawn_bounce_rays: null argument");
+    if (int r = vx::ensure_bounce_table()) return r;
+    if (n == 0) return VX_OK;
+    vx::spawn_bounce_kernel<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(rays, hits, n, seed, out);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_spawn_bounce_rays");
+}
+
+int vx_spawn_shadow_rays(const vx_ray* rays, const vx_hit* hits, uint32_t n, const float light_dir[3], vx_ray* out,
+                         void* stream) {
+    if (!light_dir || (n && (!rays || !hits || !out))) return fail(VX_EINVAL, "vx_spawn_shadow_rays: null argument");
+    if (n == 0) return VX_OK;
+    vx::spawn_shadow_kernel<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        rays, hits, n, light_dir[0], light_dir[1], light_dir[2], out);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_spawn_shadow_rays");
+}
+
+int vx_batch_capture_frame(vx_batch* b, const vx_ray* primary, const uint32_t* primary_begin, uint32_t n,
+                           vx_hit* primary_hits, vx_ray* bounce, const uint32_t* bounce_begin, vx_hit* bounce_hits,
+                           uint64_t seed, void* stream) {
+    if (!b || !primary || !primary_begin || !primary_hits || !bounce || !bounce_begin || !bounce_hits || n == 0 ||
+        n > 0x7FFFFFFFu)
+        return fail(VX_EINVAL, "vx_batch_capture_frame: bad argument");
+    if (int r = vx::ensure_bounce_table()) return r;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (!st) return fail(VX_EINVAL, "vx_batch_capture_frame: capture needs a non-default stream");
+    if (b->frame) { cudaGraphExecDestroy(b->frame); b->frame = nullptr; }
+    if (b->frame_graph) { cudaGraphDestroy(b->frame_graph); b->frame_graph = nullptr; }
+    // Resolve shared-memory attributes and occupancy outside the capture.
+    if (int r = prepare_batch(b, b->tuning)) return r;
+    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_err(e, "vx_batch_capture_frame: begin capture");
+    int r = vx_cast_batch(b, primary, primary_begin, n, 0.0f, 3.402823466e+38f, primary_hits, nullptr, stream);
+    if (r == VX_OK) r = vx_spawn_bounce_rays(primary, primary_hits, n, seed, bounce, stream);
+    if (r == VX_OK)
+        r = vx_cast_batch(b, bounce, bounce_begin, 2 * n, 0.0f, 3.402823466e+38f, bounce_hits, nullptr, stream);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(st, &g);
+    if (r != VX_OK) { if (g) cudaGraphDestroy(g); return r; }
+    if (e != cudaSuccess) return cuda_err(e, "vx_batch_capture_frame: end capture");
+    e = cudaGraphInstantiate(&b->frame, g, 0);
+    if (e != cudaSuccess) { cudaGraphDestroy(g); return cuda_err(e, "vx_batch_capture_frame: instantiate"); }
+    b->frame_graph = g;
+    return VX_OK;
+}
+
+int vx_batch_launch_frame(vx_batch* b, void* stream) {
+    if (!b || !b->frame) return fail(VX_EINVAL, "vx_batch_launch_frame: no captured frame");
+    cudaError_t e = cudaGraphLaunch(b->frame, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_batch_launch_frame");
+}
+
+}  // extern "C"

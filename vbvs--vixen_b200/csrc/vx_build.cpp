@@ -107,7 +107,6 @@ int vx_build_dense(const uint64_t* bits, uint32_t R, int32_t max_levels, vx_buil
     // 1. per-slot occupancy masks (16 words) and populated flags, slab-parallel.
     const uint64_t slots = uint64_t(bpa) * bpa * bpa;
     std::vector<uint8_t> populated(slots, 0);
-    std::vector<uint32_t> slot_mask;  // only for populated slots, filled in pass 2
     parallel_for(int64_t(bpa), [&](int64_t bz) {
         for (uint32_t by = 0; by < bpa; ++by)
             for (uint32_t bx = 0; bx < bpa; ++bx) {
@@ -152,7 +151,6 @@ int vx_build_dense(const uint64_t* bits, uint32_t R, int32_t max_levels, vx_buil
     std::vector<Level> lv(1);
     lv[0].coord = b->coord;
     const int brickDepth = 3;
-    bool rooted = false;
     for (int depth = brickDepth + 1; depth <= max_levels; ++depth) {
         const Level& ch = lv.back();
         Level par;
@@ -169,9 +167,8 @@ int vx_build_dense(const uint64_t* bits, uint32_t R, int32_t max_levels, vx_buil
         }
         bool isRoot = par.coord.size() == 1 && par.coord[0] == 0;
         lv.push_back(std::move(par));
-        if (isRoot) { rooted = true; break; }
+        if (isRoot) break;
     }
-    (void)rooted;
     if (lv.back().coord.size() != 1) {
         delete b;
         return fail(VX_EINVAL, "vx_build_dense: several nodes at the top level (max_levels too small for R)");
@@ -388,9 +385,10 @@ int vx_synth_noise(uint32_t R, uint32_t spacing, uint32_t octaves, float fill, u
 
 int vx_synth_urban(uint32_t R, uint32_t hmin, uint32_t hmax, uint64_t seed, uint64_t* out_bits) {
     using namespace vx;
-    if (!out_bits || R < 64 || R % 64 != 0 || R > 8192 || (R / 32) <= 8 || hmin > hmax)
+    if (!out_bits || R < 64 || R % 64 != 0 || R > 8192 || hmin > hmax)
         return fail(VX_EINVAL, "vx_synth_urban: bad arguments");
-    const uint32_t pitch = R / 32, block = pitch - 8, wpr = R / 64;
+    // 32 x 32 blocks; streets 8 voxels wide at R = 2048, scaled with R (at least 1).
+    const uint32_t pitch = R / 32, street = std::max(1u, R / 256), block = pitch - street, wpr = R / 64;
     uint32_t height[32][32];
     for (uint32_t bz = 0; bz < 32; ++bz)
         for (uint32_t bx = 0; bx < 32; ++bx) {

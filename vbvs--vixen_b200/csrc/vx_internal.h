@@ -31,6 +31,10 @@ struct DevScene {
     const uint2* dxt;                  // 32 per brick
 };
 
+// Accessors of an opaque vx_scene (vx_api.cpp).
+const DevScene& scene_dev(const vx_scene* s);
+int scene_device(const vx_scene* s);
+
 // Per-thread-local error string.
 void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);

@@ -1,609 +1,8 @@
-// vx_kernels.cu - ESVO ray casting kernels for sm_100a.
-//
-// One thread per ray.  The traversal restates LaineKarrasOctree::castRayImpl
-// (SVO/src/SVOTraversal.cpp:516-691), handleLeafHit and the brick DDA
-// (SVO/src/SVOBrickDDA.cpp:65-533) in IEEE binary32, compiled with
-// --fmad=false and IEEE division / square root, so hit indices and t match
-// the host code bit for bit.  Paths are relative to the reference project's
-// VIXEN/ directory.
-//
-// Every floating-point value the reference computes is computed here by the
-// same operations on the same operands.  What changes is only where it is
-// computed: quantities that depend on the ray alone (the clamped ray-entry
-// position, the slab reciprocals, the DDA step lengths, the ray-entry brick
-// of the second lookup) are evaluated once per ray instead of at every leaf,
-// voxel-corner t values are shared by the phases of one iteration that read
-// them at the same position, and divisions by 8 and by 1 become the exact
-// multiplications / identities they equal.
-//
-// Device layout (vx.h):
-//   nodes      8 B per descriptor {child_ptr, valid | leaf << 8}; one 8-byte
-//              load per parent change (the reference's fetchChildDescriptor)
-//   grid       u32 per brick slot; read by the position-based brick lookups
-//   occ        16 u32 per brick; one word per DDA step
-//   rgba / dxt colour payload; one word / one 8-byte block per hit
-// The per-ray ESVO stack (node, t_max per scale) lives in shared memory,
-// [scale][thread] so neighbouring threads hit different banks.
-#include <climits>
-#include <cstdint>
-
-#include "vx_internal.h"
-#include "vx_raygen.h"
+// vx_kernels.cu - plain (one launch per scene) cast and render kernels.
+#include "vx_cast.cuh"
 
 namespace vx {
 namespace {
-
-constexpr int ESVO_MAX_SCALE = 22;  // LaineKarrasOctree.h:337
-constexpr int MAX_ITER = 500;       // SVOTraversal.cpp:588
-constexpr int CYCLE_START = 4;      // iteration from which loop states are recorded
-constexpr float FLT_MAX_ = 3.402823466e+38f;
-constexpr uint32_t NONE = 0xFFFFFFFFu;
-
-constexpr uint32_t F_HIT = 1u;
-constexpr uint32_t F_NEG = 1u << 3;
-constexpr uint32_t F_ITER_CAP = 1u << 6;
-constexpr uint32_t F_INVALID = 1u << 7;
-
-// glm scalar min/max (func_common.inl): min = (y < x) ? y : x, max = (x < y) ? y : x.
-__device__ __forceinline__ float gmin(float x, float y) { return (y < x) ? y : x; }
-__device__ __forceinline__ float gmax(float x, float y) { return (x < y) ? y : x; }
-__device__ __forceinline__ int imin(int x, int y) { return (y < x) ? y : x; }
-__device__ __forceinline__ int imax(int x, int y) { return (x < y) ? y : x; }
-__device__ __forceinline__ int iclamp(int v, int lo, int hi) { return imin(imax(v, lo), hi); }
-__device__ __forceinline__ float fclamp(float v, float lo, float hi) { return gmin(gmax(v, lo), hi); }
-__device__ __forceinline__ float min3(float a, float b, float c) { return gmin(gmin(a, b), c); }
-__device__ __forceinline__ float max3(float a, float b, float c) { return gmax(gmax(a, b), c); }
-// static_cast<int>(float) as x86-64 evaluates it (cvttss2si: INT_MIN when
-// the value is outside the int range or NaN).
-__device__ __forceinline__ int f2i(float f) {
-    return (f >= -2147483648.0f && f < 2147483648.0f) ? __float2int_rz(f) : INT_MIN;
-}
-
-// mirrorMask (SVOTypes.h:343-364): bit i moves to i ^ flip.
-__device__ __forceinline__ uint32_t mirror_mask(uint32_t m, int octant_mask) {
-    const int flip = (~octant_mask) & 7;
-    if (flip & 1) m = ((m & 0x55u) << 1) | ((m & 0xAAu) >> 1);
-    if (flip & 2) m = ((m & 0x33u) << 2) | ((m & 0xCCu) >> 2);
-    if (flip & 4) m = ((m & 0x0Fu) << 4) | ((m & 0xF0u) >> 4);
-    return m;
-}
-
-__device__ __forceinline__ uint32_t grid_lookup(const DevScene& s, int bx, int by, int bz) {
-    // getBrickViewByGrid (SVOBuilder.h:107-116) over the dense table
-    // (VoxelSceneCacher.cpp:670-713).
-    const size_t li = size_t(bx) + size_t(by) * size_t(s.bpa) + size_t(bz) * size_t(s.bpa) * size_t(s.bpa);
-    return __ldg(s.grid + li);
-}
-
-struct Hit {
-    float t;
-    uint32_t brick, node, voxel, flags;
-    uint32_t iters, grid_reads, dda_steps;            // the reference traversal's counts
-    uint32_t run_iters, run_grid_reads, run_dda_steps;  // what this kernel executed
-};
-
-// Per-ray constants of the brick stage.
-struct RayB {
-    float lo[3];     // ray origin in grid-local space: origin + (0 - worldMin)
-    float d[3];      // normalised direction
-    float inv[3];    // brick slab reciprocal, +-1e8 when |d| < 1e-8 (SVOBrickDDA.cpp:202-209)
-    float tdel[3];   // DDA step length 1/|d|, FLT_MAX when |d| < 1e-8 (:424-430)
-    int step[3];     // DDA step, 0 when |d| < 1e-8
-};
-
-// traverseBrickView (SVOBrickDDA.cpp:390-533) with brickVoxelSize = 1 and
-// brickN = 8; occupancy from the brick's 512-bit mask.
-__device__ __forceinline__ bool brick_dda(const DevScene& s, uint32_t brick, const float bmn[3], const RayB& rb,
-                                          float tMin, float tMax, Hit& h) {
-    int cur[3];
-    float tNext[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const float ep = rb.lo[a] + rb.d[a] * tMin;          // entryPoint
-        cur[a] = iclamp(f2i(floorf(ep - bmn[a])), 0, 7);     // (entry - min) / 1
-        if (fabsf(rb.d[a]) < 1e-8f) {
-            tNext[a] = FLT_MAX_;
-        } else if (rb.d[a] > 0.0f) {
-            tNext[a] = tMin + ((bmn[a] + float(cur[a] + 1)) - ep) / rb.d[a];
-        } else {
-            tNext[a] = tMin + (ep - (bmn[a] + float(cur[a]))) / fabsf(rb.d[a]);
-        }
-    }
-    const uint32_t* occ = reinterpret_cast<const uint32_t*>(s.occ) + size_t(brick) * 16;
-    for (int stepCount = 0; stepCount < 24; ++stepCount) {
-        if (uint32_t(cur[0]) >= 8u || uint32_t(cur[1]) >= 8u || uint32_t(cur[2]) >= 8u) return false;
-        ++h.dda_steps;
-        const int vi = cur[2] * 64 + cur[1] * 8 + cur[0];
-        const uint32_t word = __ldg(occ + (vi >> 5));
-        if ((word >> (vi & 31)) & 1u) {
-            float tn[3];
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                if (fabsf(rb.d[a]) < 1e-8f) {
-                    tn[a] = -__int_as_float(0x7f800000);
-                } else {
-                    const float vmn = bmn[a] + float(cur[a]);
-                    const float t0 = (vmn - rb.lo[a]) / rb.d[a];
-                    const float t1 = ((vmn + 1.0f) - rb.lo[a]) / rb.d[a];
-                    tn[a] = gmin(t0, t1);
-                }
-            }
-            float hitT = gmax(gmax(tn[0], tn[1]), tn[2]);
-            hitT = gmax(hitT, 0.0f);
-            int axis;
-            if (tn[0] >= tn[1] && tn[0] >= tn[2]) axis = 0;
-            else if (tn[1] >= tn[2]) axis = 1;
-            else axis = 2;
-            h.t = hitT;
-            h.voxel = uint32_t(vi);
-            const float dax = axis == 0 ? rb.d[0] : (axis == 1 ? rb.d[1] : rb.d[2]);
-            h.flags |= F_HIT | (uint32_t(axis) << 1) | (dax > 0.0f ? F_NEG : 0u);
-            return true;
-        }
-        if (tNext[0] < tNext[1] && tNext[0] < tNext[2]) {
-            if (tNext[0] > tMax) return false;
-            cur[0] += rb.step[0];
-            tNext[0] += rb.tdel[0];
-        } else if (tNext[1] < tNext[2]) {
-            if (tNext[1] > tMax) return false;
-            cur[1] += rb.step[1];
-            tNext[1] += rb.tdel[1];
-        } else {
-            if (tNext[2] > tMax) return false;
-            cur[2] += rb.step[2];
-            tNext[2] += rb.tdel[2];
-        }
-    }
-    return false;
-}
-
-struct Coef {
-    float tx_coef, ty_coef, tz_coef, tx_bias, ty_bias, tz_bias;
-    int octant_mask;
-};
-
-// castRayImpl without LOD (SVOTraversal.cpp:516-691).
-__device__ void cast_ray(const DevScene& s, float ox, float oy, float oz, float ddx, float ddy, float ddz,
-                         float tMinArg, float tMaxArg, uint32_t* stkN, float* stkT, uint32_t* cyc, int stride,
-                         Hit& h) {
-    h.t = 0.0f;
-    h.brick = NONE;
-    h.node = NONE;
-    h.voxel = 0xFFFFu;
-    h.flags = 0;
-    h.iters = 0;
-    h.grid_reads = 0;
-    h.dda_steps = 0;
-    h.run_iters = 0;
-    h.run_grid_reads = 0;
-    h.run_dda_steps = 0;
-    // validateRayInput (:238-259)
-    if (s.node_count == 0) { h.flags = F_INVALID; return; }
-    float dx, dy, dz;
-    {
-        const float dd = (ddx * ddx + ddy * ddy) + ddz * ddz;
-        const float inv = 1.0f / sqrtf(dd);
-        dx = ddx * inv; dy = ddy * inv; dz = ddz * inv;
-        const float len = sqrtf((dx * dx + dy * dy) + dz * dz);
-        if (len < 1e-6f) { h.flags = F_INVALID; return; }
-        if (isnan(ox) || isnan(oy) || isnan(oz) || isnan(dx) || isnan(dy) || isnan(dz) || isinf(ox) ||
-            isinf(oy) || isinf(oz) || isinf(dx) || isinf(dy) || isinf(dz)) {
-            h.flags = F_INVALID;
-            return;
-        }
-    }
-    const float wminx = s.wmin[0], wminy = s.wmin[1], wminz = s.wmin[2];
-    const bool inside = ox >= wminx && ox <= s.wmax[0] && oy >= wminy && oy <= s.wmax[1] && oz >= wminz &&
-                        oz <= s.wmax[2];
-    // intersectAABB (:117-149)
-    float tEntry, tExit;
-    {
-        const float o[3] = {ox, oy, oz}, d[3] = {dx, dy, dz};
-        float tnear[3], tfar[3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            float inv;
-            if (fabsf(d[i]) < 1e-8f) {
-                if (o[i] < s.wmin[i] || o[i] > s.wmax[i]) return;
-                inv = (d[i] >= 0.0f) ? 1e20f : -1e20f;
-            } else {
-                inv = 1.0f / d[i];
-            }
-            const float t0 = (s.wmin[i] - o[i]) * inv;
-            const float t1 = (s.wmax[i] - o[i]) * inv;
-            tnear[i] = gmin(t0, t1);
-            tfar[i] = gmax(t0, t1);
-        }
-        tEntry = max3(tnear[0], tnear[1], tnear[2]);
-        tExit = min3(tfar[0], tfar[1], tfar[2]);
-        if (!(tEntry <= tExit && tExit >= 0.0f)) return;
-    }
-    tEntry = gmax(tEntry, tMinArg);
-    tExit = gmin(tExit, tMaxArg);
-    if (tEntry >= tExit || tExit < 0.0f) return;
-    const float tRayStart = inside ? 0.0f : gmax(0.0f, tEntry);
-    const float wsx = s.wsize[0], wsy = s.wsize[1], wsz = s.wsize[2];
-    const float nox = (ox + dx * tRayStart - wminx) / wsx + 1.0f;
-    const float noy = (oy + dy * tRayStart - wminy) / wsy + 1.0f;
-    const float noz = (oz + dz * tRayStart - wminz) / wsz + 1.0f;
-    // computeRayCoefficients (:699-728)
-    Coef c;
-    {
-        float sx = dx, sy = dy, sz = dz;
-        if (fabsf(sx) < 1e-5f) sx = copysignf(1e-5f, sx);
-        if (fabsf(sy) < 1e-5f) sy = copysignf(1e-5f, sy);
-        if (fabsf(sz) < 1e-5f) sz = copysignf(1e-5f, sz);
-        c.tx_coef = 1.0f / -fabsf(sx);
-        c.ty_coef = 1.0f / -fabsf(sy);
-        c.tz_coef = 1.0f / -fabsf(sz);
-        c.tx_bias = c.tx_coef * nox;
-        c.ty_bias = c.ty_coef * noy;
-        c.tz_bias = c.tz_coef * noz;
-        c.octant_mask = 7;
-        if (dx > 0.0f) { c.octant_mask ^= 1; c.tx_bias = 3.0f * c.tx_coef - c.tx_bias; }
-        if (dy > 0.0f) { c.octant_mask ^= 2; c.ty_bias = 3.0f * c.ty_coef - c.ty_bias; }
-        if (dz > 0.0f) { c.octant_mask ^= 4; c.tz_bias = 3.0f * c.tz_coef - c.tz_bias; }
-    }
-    float t_min, t_max;
-    if (inside) {
-        t_min = 0.0f;
-        t_max = min3(c.tx_coef - c.tx_bias, c.ty_coef - c.ty_bias, c.tz_coef - c.tz_bias);
-        t_max = gmin(t_max, 1.0f);
-    } else {
-        t_min = max3(2.0f * c.tx_coef - c.tx_bias, 2.0f * c.ty_coef - c.ty_bias, 2.0f * c.tz_coef - c.tz_bias);
-        t_max = min3(c.tx_coef - c.tx_bias, c.ty_coef - c.ty_bias, c.tz_coef - c.tz_bias);
-        t_min = gmax(t_min, 0.0f);
-        t_max = gmin(t_max, 1.0f);
-    }
-    float hh = t_max;
-    // initializeTraversalState (:261-280): stack[minScale..22] = root
-    const int minScale = s.min_scale;
-    for (int sc = minScale; sc <= ESVO_MAX_SCALE; ++sc) {
-        stkN[(sc - minScale) * stride] = 0;
-        stkT[(sc - minScale) * stride] = t_max;
-    }
-    int scale = ESVO_MAX_SCALE;
-    uint32_t parent = 0;
-    bool fetched = false;
-    int idx = 0;
-    float px = 1.0f, py = 1.0f, pz = 1.0f;
-    float scale_exp2 = 0.5f;
-    const bool csx = fabsf(dx) >= 1e-5f, csy = fabsf(dy) >= 1e-5f, csz = fabsf(dz) >= 1e-5f;
-    // selectInitialOctant (:730-766)
-    {
-        const bool usePos = (t_min < 0.01f);
-        const float mx = (c.octant_mask & 1) ? nox : (3.0f - nox);
-        const float my = (c.octant_mask & 2) ? noy : (3.0f - noy);
-        const float mz = (c.octant_mask & 4) ? noz : (3.0f - noz);
-        if (!csx || usePos) { if (mx >= 1.5f) { idx |= 1; px = 1.5f; } }
-        else if (1.5f * c.tx_coef - c.tx_bias > t_min) { idx ^= 1; px = 1.5f; }
-        if (!csy || usePos) { if (my >= 1.5f) { idx |= 2; py = 1.5f; } }
-        else if (1.5f * c.ty_coef - c.ty_bias > t_min) { idx ^= 2; py = 1.5f; }
-        if (!csz || usePos) { if (mz >= 1.5f) { idx |= 4; pz = 1.5f; } }
-        else if (1.5f * c.tz_coef - c.tz_bias > t_min) { idx ^= 4; pz = 1.5f; }
-    }
-    // handleLeafHit quantities that depend on the ray only (SVOBrickDDA.cpp:98-121, 140-143, 165-166)
-    const float offx = (dx > 0) ? 0.001f : -0.001f;
-    const float offy = (dy > 0) ? 0.001f : -0.001f;
-    const float offz = (dz > 0) ? 0.001f : -0.001f;
-    const float te0 = gmax(tEntry, 0.0f);
-    const float rwx = ox + dx * te0, rwy = oy + dy * te0, rwz = oz + dz * te0;
-    const float rlx = fclamp((rwx - wminx) / wsx, 0.001f, 0.999f);
-    const float rly = fclamp((rwy - wminy) / wsy, 0.001f, 0.999f);
-    const float rlz = fclamp((rwz - wminz) / wsz, 0.001f, 0.999f);
-    const int bmax = s.bpa - 1;
-    uint32_t brick2 = 0;      // ray-entry brick of the second lookup, read on first use
-    bool have_brick2 = false;
-    RayB rb;
-    rb.lo[0] = ox + (0.0f - wminx);
-    rb.lo[1] = oy + (0.0f - wminy);
-    rb.lo[2] = oz + (0.0f - wminz);
-    rb.d[0] = dx; rb.d[1] = dy; rb.d[2] = dz;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        rb.inv[i] = (fabsf(rb.d[i]) < 1e-8f) ? ((rb.d[i] >= 0) ? 1e8f : -1e8f) : 1.0f / rb.d[i];
-        rb.tdel[i] = (fabsf(rb.d[i]) < 1e-8f) ? FLT_MAX_ : 1.0f / fabsf(rb.d[i]);
-        rb.step[i] = (fabsf(rb.d[i]) < 1e-8f) ? 0 : ((rb.d[i] > 0.0f) ? 1 : -1);
-    }
-
-    uint32_t mValid = 0, mLeaf = 0, pChild = 0, pValid = 0, pLeaf = 0;
-    int iter = 0;
-    // Cycle detection.  The loop state (scale, idx, fetched, parent, pos,
-    // t_min, t_max, h) with the stack determines every later iteration, and a
-    // cycle only rewrites stack slots with the values they already hold.  So
-    // once the state repeats after one or two iterations the ray can neither
-    // hit nor leave before the 500-iteration cap: the result is the capped
-    // miss and the remaining iterations' counters repeat the cycle's.  The two
-    // previous states are kept in shared memory (cyc[k * stride], k < 8: one
-    // iteration back, k >= 8: two back) from iteration CYCLE_START on.
-    uint32_t d1g = 0, d1d = 0;
-    int nrec = 0;
-    while (scale >= minScale && scale <= ESVO_MAX_SCALE && iter < MAX_ITER) {
-        ++iter;
-        const uint32_t g0 = h.grid_reads, dd0 = h.dda_steps;
-        {  // one iteration; `goto next_iter` is the reference's `continue`
-            // fetchChildDescriptor (:282-293)
-            if (!fetched) {
-                const uint2 nd = __ldg(s.nodes + parent);
-                pChild = nd.x;
-                pValid = nd.y & 0xFFu;
-                pLeaf = (nd.y >> 8) & 0xFFu;
-                mValid = mirror_mask(pValid, c.octant_mask);
-                mLeaf = mirror_mask(pLeaf, c.octant_mask);
-                const uint32_t nonLeaf = ~mLeaf & 0xFFu;
-                fetched = (nonLeaf | (mValid << 8) | pChild) != 0u;
-            }
-            // Voxel corners at the iteration's position (computeVoxelCorners,
-            // :786-794) and the corrected tc_max (:768-784); checkChildValidity,
-            // PUSH and ADVANCE all evaluate them at this position and t_max.
-            const float tx = px * c.tx_coef - c.tx_bias;
-            const float ty = py * c.ty_coef - c.ty_bias;
-            const float tz = pz * c.tz_coef - c.tz_bias;
-            const float tcc = min3((csx && fabsf(tx) < 1000.0f) ? tx : t_max, (csy && fabsf(ty) < 1000.0f) ? ty : t_max,
-                                   (csz && fabsf(tz) < 1000.0f) ? tz : t_max);
-            // checkChildValidity (:295-326)
-            const bool child_valid = (mValid >> idx) & 1u;
-            bool isLeaf = (mLeaf >> idx) & 1u;
-            if (scale - minScale == s.brick_user_scale && child_valid) isLeaf = true;
-            float tv_max = 0.0f;
-            if (child_valid && !(t_min > t_max) && t_min <= (tv_max = gmin(t_max, tcc))) {
-                if (isLeaf) {
-                    // handleLeafHit (SVOBrickDDA.cpp:65-181)
-                    float lx = px, ly = py, lz = pz;
-                    if ((c.octant_mask & 1) == 0) lx = 3.0f - scale_exp2 - lx;
-                    if ((c.octant_mask & 2) == 0) ly = 3.0f - scale_exp2 - ly;
-                    if ((c.octant_mask & 4) == 0) lz = 3.0f - scale_exp2 - lz;
-                    const float ix = fclamp(csx ? (lx - 1.0f) + offx : rlx, 0.001f, 0.999f);
-                    const float iy = fclamp(csy ? (ly - 1.0f) + offy : rly, 0.001f, 0.999f);
-                    const float iz = fclamp(csz ? (lz - 1.0f) + offz : rlz, 0.001f, 0.999f);
-                    // Method 1: ESVO state position (x / 8 == x * 0.125 exactly)
-                    const float hx = fclamp(ix * wsx, 0.0f, s.wsm[0]);
-                    const float hy = fclamp(iy * wsy, 0.0f, s.wsm[1]);
-                    const float hz = fclamp(iz * wsz, 0.0f, s.wsm[2]);
-                    uint32_t brick = grid_lookup(s, iclamp(f2i(hx * 0.125f), 0, bmax),
-                                                 iclamp(f2i(hy * 0.125f), 0, bmax), iclamp(f2i(hz * 0.125f), 0, bmax));
-                    ++h.grid_reads;
-                    uint32_t method = 1;
-                    if (brick == NONE) {
-                        // Method 2: ray entry position (the same brick for the whole ray)
-                        if (!have_brick2) {
-                            const float ex = fclamp((rwx - wminx) + dx * 0.01f, 0.0f, s.wsm[0]);
-                            const float ey = fclamp((rwy - wminy) + dy * 0.01f, 0.0f, s.wsm[1]);
-                            const float ez = fclamp((rwz - wminz) + dz * 0.01f, 0.0f, s.wsm[2]);
-                            brick2 = grid_lookup(s, iclamp(f2i(ex * 0.125f), 0, bmax),
-                                                 iclamp(f2i(ey * 0.125f), 0, bmax), iclamp(f2i(ez * 0.125f), 0, bmax));
-                            have_brick2 = true;
-                        }
-                        brick = brick2;
-                        ++h.grid_reads;
-                        method = 2;
-                    }
-                    if (brick == NONE) {
-                        // Fallback 3: leaf child of the parent at the local octant
-                        // (leafToBrickView, SVORebuild.cpp:569-574)
-                        method = 3;
-                        const uint32_t lo = uint32_t(idx ^ (~c.octant_mask & 7));
-                        const uint32_t leafs = pValid & pLeaf;
-                        if ((leafs >> lo) & 1u) {
-                            const uint32_t ci = pChild + __popc(pValid & ~pLeaf & 0xFFu) +
-                                                __popc(leafs & ((1u << lo) - 1u));
-                            if (ci < s.node_count) {
-                                const uint32_t b = __ldg(s.node_brick + ci);
-                                if (b < s.brick_count) brick = b;
-                            }
-                        }
-                    }
-                    if (brick != NONE) {
-                        // traverseBrickAndReturnHit (SVOBrickDDA.cpp:187-225)
-                        const uint32_t bc = __ldg(s.coord + brick);
-                        const float bmn[3] = {float(int(bc & 0x3FFu) * 8), float(int((bc >> 10) & 0x3FFu) * 8),
-                                              float(int((bc >> 20) & 0x3FFu) * 8)};
-                        float tn[3], tf[3];
-#pragma unroll
-                        for (int i = 0; i < 3; ++i) {
-                            const float t0 = (bmn[i] - rb.lo[i]) * rb.inv[i];
-                            const float t1 = ((bmn[i] + 8.0f) - rb.lo[i]) * rb.inv[i];
-                            tn[i] = gmin(t0, t1);
-                            tf[i] = gmax(t0, t1);
-                        }
-                        const float btmin = gmax(gmax(gmax(tn[0], tn[1]), tn[2]), tEntry);
-                        const float btmax = gmin(gmin(tf[0], tf[1]), tf[2]);
-                        if (brick_dda(s, brick, bmn, rb, btmin, btmax, h)) {
-                            h.brick = brick;
-                            h.node = parent;
-                            h.flags |= method << 4;
-                            h.iters = uint32_t(iter);
-                            h.run_iters = h.iters;
-                            h.run_grid_reads = h.grid_reads;
-                            h.run_dda_steps = h.dda_steps;
-                            return;
-                        }
-                    }
-                    t_min = tv_max;
-                    // fall through to ADVANCE
-                } else {
-                    // executePushPhase (:328-378); tx_center etc. of checkChildValidity
-                    const float half = scale_exp2 * 0.5f;
-                    const float tx_center = half * c.tx_coef + tx;
-                    const float ty_center = half * c.ty_coef + ty;
-                    const float tz_center = half * c.tz_coef + tz;
-                    const float tc_max = min3(tx, ty, tz);
-                    if (tc_max < hh) {
-                        stkN[(scale - minScale) * stride] = parent;
-                        stkT[(scale - minScale) * stride] = t_max;
-                    }
-                    hh = tc_max;
-                    const int worldIdx = idx ^ (~c.octant_mask & 7);
-                    const uint32_t nonLeafMask = ~pLeaf & pValid & 0xFFu;
-                    const uint32_t child_index = pChild + __popc(nonLeafMask & ((1u << worldIdx) - 1u));
-                    if (child_index >= s.node_count) goto next_iter;
-                    parent = child_index;
-                    idx = 0;
-                    scale--;
-                    scale_exp2 = half;
-                    if (tx_center > t_min) { idx ^= 1; px += scale_exp2; }
-                    if (ty_center > t_min) { idx ^= 2; py += scale_exp2; }
-                    if (tz_center > t_min) { idx ^= 4; pz += scale_exp2; }
-                    t_max = tv_max;
-                    fetched = false;
-                    goto next_iter;
-                }
-            }
-            // executeAdvancePhase (:380-416)
-            {
-                float tca = tcc;
-                if (tca == FLT_MAX_) tca = max3(csx ? tx : -FLT_MAX_, csy ? ty : -FLT_MAX_, csz ? tz : -FLT_MAX_);
-                int step_mask = 0;
-                if (csx && tx <= tca) { step_mask ^= 1; px -= scale_exp2; }
-                if (csy && ty <= tca) { step_mask ^= 2; py -= scale_exp2; }
-                if (csz && tz <= tca) { step_mask ^= 4; pz -= scale_exp2; }
-                t_min = gmax(tca, 0.0f);
-                idx ^= step_mask;
-                if ((idx & step_mask) == 0) goto next_iter;
-            }
-            // POP: step mask recomputed at the new position (:672-681)
-            int step_mask = 0;
-            {
-                const float ux = px * c.tx_coef - c.tx_bias;
-                const float uy = py * c.ty_coef - c.ty_bias;
-                const float uz = pz * c.tz_coef - c.tz_bias;
-                const float ucc = min3((csx && fabsf(ux) < 1000.0f) ? ux : t_max,
-                                       (csy && fabsf(uy) < 1000.0f) ? uy : t_max,
-                                       (csz && fabsf(uz) < 1000.0f) ? uz : t_max);
-                if (csx && ux <= ucc) step_mask ^= 1;
-                if (csy && uy <= ucc) step_mask ^= 2;
-                if (csz && uz <= ucc) step_mask ^= 4;
-            }
-            // executePopPhase (:418-510)
-            if (scale == ESVO_MAX_SCALE) {
-                if (t_min > t_max || px < 1.0f || px >= 2.0f || py < 1.0f || py >= 2.0f || pz < 1.0f || pz >= 2.0f)
-                    break;
-                fetched = false;
-                goto next_iter;
-            }
-            {
-                // floatToInt: std::max(0, std::min(f, 1)), * 2^22, std::min(., 2^22-1),
-                // std::max(0, .), truncate (SVOTraversal.cpp:439-442)
-                auto f2q = [](float f) -> uint32_t {
-                    const float m1 = (1.0f < f) ? 1.0f : f;
-                    const float cl = (0.0f < m1) ? m1 : 0.0f;
-                    const float sc = cl * 4194304.0f;
-                    const float m2 = (4194303.0f < sc) ? 4194303.0f : sc;
-                    return uint32_t((0.0f < m2) ? m2 : 0.0f);
-                };
-                uint32_t qx = f2q(gmax(0.0f, px - 1.0f));
-                uint32_t qy = f2q(gmax(0.0f, py - 1.0f));
-                uint32_t qz = f2q(gmax(0.0f, pz - 1.0f));
-                uint32_t diff = 0;
-                if (step_mask & 1) diff |= qx ^ f2q(gmax(0.0f, px + scale_exp2 - 1.0f));
-                if (step_mask & 2) diff |= qy ^ f2q(gmax(0.0f, py + scale_exp2 - 1.0f));
-                if (step_mask & 4) diff |= qz ^ f2q(gmax(0.0f, pz + scale_exp2 - 1.0f));
-                if (diff == 0) break;
-                scale = 31 - __clz(diff);
-                if (scale < minScale || scale > ESVO_MAX_SCALE) break;
-                scale_exp2 = __int_as_float((scale - ESVO_MAX_SCALE + 127) << 23);
-                parent = stkN[(scale - minScale) * stride];
-                t_max = stkT[(scale - minScale) * stride];
-                const uint32_t mask = ~((1u << (ESVO_MAX_SCALE - scale)) - 1u);
-                qx &= mask; qy &= mask; qz &= mask;
-                px = 1.0f + float(qx) / 4194304.0f;
-                py = 1.0f + float(qy) / 4194304.0f;
-                pz = 1.0f + float(qz) / 4194304.0f;
-                const int sh = ESVO_MAX_SCALE - scale - 1;
-                if (sh < 0 || sh >= 32) idx = 0;
-                else idx = int(((qx >> sh) & 1u) | (((qy >> sh) & 1u) << 1) | (((qz >> sh) & 1u) << 2));
-                hh = 0.0f;
-                fetched = false;
-            }
-        }
-    next_iter:
-        if (iter >= CYCLE_START) {
-            uint32_t cur[8];
-            cur[0] = uint32_t(scale) | (uint32_t(idx) << 8) | (uint32_t(fetched) << 16);
-            cur[1] = parent;
-            cur[2] = __float_as_uint(px); cur[3] = __float_as_uint(py); cur[4] = __float_as_uint(pz);
-            cur[5] = __float_as_uint(t_min); cur[6] = __float_as_uint(t_max); cur[7] = __float_as_uint(hh);
-            const uint32_t dg = h.grid_reads - g0, ddd = h.dda_steps - dd0;
-            bool eq1 = nrec >= 1, eq2 = nrec >= 2;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const uint32_t a = cyc[k * stride], b = cyc[(k + 8) * stride];
-                eq1 = eq1 && (cur[k] == a);
-                eq2 = eq2 && (cur[k] == b);
-                cyc[(k + 8) * stride] = a;
-                cyc[k * stride] = cur[k];
-            }
-            if (eq1 || eq2) {
-                const uint32_t rem = uint32_t(MAX_ITER - iter);
-                h.run_iters = uint32_t(iter);
-                h.run_grid_reads = h.grid_reads;
-                h.run_dda_steps = h.dda_steps;
-                if (eq1) {
-                    h.grid_reads += rem * dg;
-                    h.dda_steps += rem * ddd;
-                } else {
-                    h.grid_reads += ((rem + 1) / 2) * d1g + (rem / 2) * dg;
-                    h.dda_steps += ((rem + 1) / 2) * d1d + (rem / 2) * ddd;
-                }
-                h.iters = uint32_t(MAX_ITER);
-                h.flags |= F_ITER_CAP;
-                return;
-            }
-            ++nrec;
-            d1g = dg;
-            d1d = ddd;
-        }
-    }
-    h.iters = uint32_t(iter);
-    h.run_iters = h.iters;
-    h.run_grid_reads = h.grid_reads;
-    h.run_dda_steps = h.dda_steps;
-    if (iter >= MAX_ITER) h.flags |= F_ITER_CAP;
-}
-
-// DXT1 texel of the hit voxel: decodeColorHead (DXT1Compressor.cpp:14-36)
-// and the compressed shader's addressing (VoxelRayMarch_Compressed.comp:142-158).
-__device__ __forceinline__ void dxt_texel(const uint2* dxt, uint32_t brick, uint32_t voxel, float& r, float& g,
-                                          float& b) {
-    const uint2 blk = __ldg(dxt + size_t(brick) * 32 + (voxel >> 4));
-    const uint32_t head = blk.x;
-    const uint32_t sel = (blk.y >> ((voxel & 15u) * 2u)) & 3u;
-    const float scale = 1.0f / 4294967296.0f;
-    const float r0x = float(head << 16) * scale, r0y = float(head << 21) * scale, r0z = float(head << 27) * scale;
-    const float r1x = float(head) * scale, r1y = float(head << 5) * scale, r1z = float(head << 11) * scale;
-    if (sel == 0) { r = r0x; g = r0y; b = r0z; }
-    else if (sel == 1) { r = r1x; g = r1y; b = r1z; }
-    else if (sel == 2) {
-        r = r0x * (2.0f / 3.0f) + r1x * (1.0f / 3.0f);
-        g = r0y * (2.0f / 3.0f) + r1y * (1.0f / 3.0f);
-        b = r0z * (2.0f / 3.0f) + r1z * (1.0f / 3.0f);
-    } else {
-        r = r0x * (1.0f / 3.0f) + r1x * (2.0f / 3.0f);
-        g = r0y * (1.0f / 3.0f) + r1y * (2.0f / 3.0f);
-        b = r0z * (1.0f / 3.0f) + r1z * (2.0f / 3.0f);
-    }
-}
-
-__device__ __forceinline__ void store_hit(vx_hit* hits, uint32_t i, const Hit& h) {
-    uint4 v;
-    v.x = __float_as_uint(h.t);
-    v.y = h.brick;
-    v.z = h.node;
-    v.w = (h.voxel & 0xFFFFu) | ((h.flags & 0xFFu) << 16);
-    reinterpret_cast<uint4*>(hits)[i] = v;
-}
-
-__device__ __forceinline__ void store_color(const DevScene& s, void* color, uint32_t i, const Hit& h) {
-    const bool hit = h.flags & F_HIT;
-    if (s.color_kind == VX_COLOR_RGBA8) {
-        reinterpret_cast<uint32_t*>(color)[i] = hit ? __ldg(s.rgba + size_t(h.brick) * 512 + h.voxel) : 0u;
-    } else if (s.color_kind == VX_COLOR_DXT1) {
-        float r = 0.0f, g = 0.0f, b = 0.0f;
-        if (hit) dxt_texel(s.dxt, h.brick, h.voxel, r, g, b);
-        float* c = reinterpret_cast<float*>(color) + size_t(i) * 3;
-        c[0] = r; c[1] = g; c[2] = b;
-    }
-}
 
 constexpr int BLOCK = 256;
 

@@ -159,3 +159,75 @@ def random_rays(n: int, R: float, seed: int, lo=-0.25, hi=1.25) -> np.ndarray:
     d[na] = np.float32(1e-6) * d[na]
     d[na, axis[na]] = sign[na]
     return np.concatenate([o, d], axis=1).astype(np.float32)
+
+
+@dataclass
+class SceneSpec:
+    R: int
+    kind: str      # "noise" or "urban"
+    fill: float    # noise fill fraction (urban: 0.9 nominal)
+    color: str     # "dxt1" or "rgba8"
+    width: int
+    height: int
+    seed: int
+
+
+def config4_specs(n_scenes: int = 64, seed: int = 4, r_range=(6, 10), res_lo=(256, 256), res_hi=(1920, 1080)):
+    """cfg4 scene draws: R = 2^round(U[6,10]), density in {10,50,90} % (noise for 10/50,
+    urban for 90), DXT1 for every other scene, resolution log-uniform between 256x256 and
+    1920x1080 (one uniform draw t: w = 256*(1920/256)^t, h = 256*(1080/256)^t)."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n_scenes):
+        R = 2 ** int(round(rng.uniform(*r_range)))
+        fill = float(rng.choice([0.1, 0.5, 0.9]))
+        t = rng.uniform(0.0, 1.0)
+        w = int(round(res_lo[0] * (res_hi[0] / res_lo[0]) ** t))
+        h = int(round(res_lo[1] * (res_hi[1] / res_lo[1]) ** t))
+        specs.append(SceneSpec(R, "urban" if fill > 0.8 else "noise", fill, "dxt1" if i % 2 else "rgba8", w, h,
+                               seed * 1000 + i))
+    return specs
+
+
+def build_spec(spec: SceneSpec, bits=None) -> Workload:
+    R = spec.R
+    if bits is None:
+        if spec.kind == "noise":
+            spacing = max(4, 64 * R // 1024)
+            bits = synth_noise(R, spacing, 5 if spacing >= 64 else 3, spec.fill, spec.seed, False)
+        else:
+            bits = synth_urban(R, max(1, R // 32), max(2, R * 1800 // 2048), spec.seed)
+    scene = scene_from_bits(bits, R, spec.color, spec.seed)
+    if spec.kind == "noise":
+        cam = empty_voxel_camera(bits, R, spec.seed, 70.0, spec.width, spec.height)
+    else:
+        cam = look_camera([R * 0.5, R * 0.9, -R * 0.25], [0.05, -0.45, 1.0], 60.0, spec.width, spec.height)
+    return Workload(f"cfg4_{spec.kind}{R}_{spec.color}_{spec.width}x{spec.height}", R, scene, bits, cam,
+                    spec.width, spec.height)
+
+
+def bounce_rays_reference(rays: np.ndarray, hits: np.ndarray, seed: int, table: np.ndarray) -> np.ndarray:
+    """vx_spawn_bounce_rays restated in numpy binary32 (used by the tests)."""
+    n = rays.shape[0]
+    out = np.zeros((2 * n, 6), np.float32)
+    out[0::2, :3] = rays[:, :3]
+    out[1::2, :3] = rays[:, :3]
+    hit = (hits["flags"] & 1).astype(bool)
+    o, d = rays[:, :3], rays[:, 3:]
+    dd = (d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2]
+    inv = np.float32(1.0) / np.sqrt(dd)
+    org = (o + (d * inv[:, None]) * hits["t"][:, None]).astype(np.float32)
+    axis = (hits["flags"].astype(np.int64) >> 1) & 3
+    sgn = np.where(hits["flags"] & 8, np.float32(-1.0), np.float32(1.0)).astype(np.float32)
+    rows = np.arange(n)
+    org[rows, axis] = org[rows, axis] + sgn * np.float32(0.001)
+    for k in range(2):
+        j = np.array([splitmix64(seed ^ splitmix64((i << 1) | k)) & 4095 for i in range(n)], np.int64)
+        u, v, w = table[j, 0], table[j, 1], table[j, 2] * sgn
+        dirs = np.stack([u, v, w], 1)
+        dirs[axis == 0] = np.stack([w, u, v], 1)[axis == 0]
+        dirs[axis == 1] = np.stack([v, w, u], 1)[axis == 1]
+        sel = hit
+        out[2 * rows[sel] + k, :3] = org[sel]
+        out[2 * rows[sel] + k, 3:] = dirs[sel]
+    return out
