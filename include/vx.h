@@ -242,6 +242,25 @@ int vx_cast_batch(vx_batch* batch, const vx_ray* rays_dev, const uint32_t* begin
 int vx_batch_autotune(vx_batch* batch, const vx_ray* rays_dev, const uint32_t* begin_dev, uint32_t n,
                       vx_hit* hits_dev, void* stream, vx_batch_tuning* best, float* best_ms);
 
+/* The batched cast without any device allocation.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory: an application
+ * that owns a fixed device-memory budget, or a frame loop where cudaMalloc's
+ * implicit device synchronisation is not acceptable.  Takes the scenes
+ * directly (no vx_batch) and keeps its scratch -- the task counter and a copy
+ * of the scene table -- in a static device array of VX_NOALLOC_SCRATCH_BYTES
+ * that every device loading the library holds until exit; count above
+ * VX_NOALLOC_MAX_SCENES is rejected (VX_EOVERFLOW).  The first call on a
+ * device resolves the array's address and the launch shape; make that first
+ * call before any stream capture.  Every call shares the one array: the call
+ * rewrites the table and clears the counter on its stream, and calls that
+ * overlap on the GPU race.  Uses block 256, 32 rays per task, stack in shared
+ * memory; hits are identical to vx_cast_batch. */
+#define VX_NOALLOC_MAX_SCENES 64
+#define VX_NOALLOC_SCRATCH_BYTES 16384
+int vx_cast_batch_noalloc(const vx_scene* const* scenes, uint32_t count, const vx_ray* rays_dev,
+                          const uint32_t* begin_dev, uint32_t n, float t_min, float t_max,
+                          vx_hit* hits_dev, void* stream);
+
 /* Secondary rays from primary hits.  Bounce: 2 rays per primary ray (out:
  * 2n), origin = hit point + 1e-3 * normal (hit point = origin +
  * normalize(dir) * t), direction = a cosine-weighted hemisphere sample about

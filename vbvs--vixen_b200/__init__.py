@@ -117,6 +117,7 @@ def lib():
         "vx_bounce_table": (C.c_int, [vp]),
         "vx_batch_capture_frame": (C.c_int, [vp, vp, vp, u32, vp, vp, vp, vp, u64, vp]),
         "vx_batch_launch_frame": (C.c_int, [vp, vp]),
+        "vx_cast_batch_noalloc": (C.c_int, [vp, u32, vp, vp, u32, f32, f32, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -462,3 +463,17 @@ def bounce_table() -> np.ndarray:
     out = np.zeros(4096 * 3, np.float32)
     check(lib().vx_bounce_table(_p(out)))
     return out.reshape(4096, 3)
+
+
+VX_NOALLOC_MAX_SCENES = 64
+
+
+def cast_batch_noalloc(scenes, rays, begin, hits, t_min=0.0, t_max=FLT_MAX, stream=None):
+    """vx_cast_batch_noalloc: the batched cast without any device allocation, for
+    callers that cannot allocate device memory (a fixed device-memory budget owned by
+    the host application, or a frame loop that cannot take cudaMalloc's implicit
+    synchronisation).  At most VX_NOALLOC_MAX_SCENES scenes; calls must not overlap
+    on the GPU (they share one static scratch array)."""
+    arr = (C.c_void_p * len(scenes))(*[sc.handle.value for sc in scenes])
+    check(lib().vx_cast_batch_noalloc(arr, len(scenes), _p(rays), _p(begin), rays.shape[0], float(t_min),
+                                      float(t_max), _p(hits), _stream(stream)))

@@ -469,3 +469,103 @@ int vx_batch_launch_frame(vx_batch* b, void* stream) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// vx_cast_batch_noalloc: the batched cast for callers that cannot allocate
+// device memory, e.g. code running under a fixed device-memory budget owned by
+// a host application, or on a frame path where cudaMalloc's implicit device
+// synchronisation is not acceptable.  Its scratch (the task counter and the
+// scene table) is the file-scope array below, VX_NOALLOC_SCRATCH_BYTES on
+// every device that loads the library, held until the process exits.
+// ---------------------------------------------------------------------------
+namespace vx {
+namespace {
+
+constexpr uint32_t NOALLOC_TABLE_OFFSET = 256;  // the counter sits at offset 0
+static_assert(NOALLOC_TABLE_OFFSET + VX_NOALLOC_MAX_SCENES * sizeof(DevScene) <= VX_NOALLOC_SCRATCH_BYTES,
+              "no-alloc scratch too small for its scene table");
+static __device__ __align__(256) unsigned char g_noalloc_scratch[VX_NOALLOC_SCRATCH_BYTES];
+
+struct NoallocDevice {
+    bool ready = false;
+    unsigned char* scratch = nullptr;  // device address of g_noalloc_scratch on this device
+    int blocks = 0;                    // persistent grid size
+};
+std::mutex g_noalloc_mu;
+NoallocDevice g_noalloc[64];
+
+// Once per device, with that device current: resolve the scratch array's
+// device address and the launch shape of the kernel variant used here.
+int noalloc_setup(int dev, NoallocDevice*& out) {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    NoallocDevice& d = g_noalloc[dev];
+    if (!d.ready) {
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch_noalloc: cudaGetSymbolAddress");
+        auto kern = batch_kernel<256, 3, true>;
+        const size_t smem_max = size_t(VX_NOALLOC_MAX_SCENES) * sizeof(DevScene) +
+                                ((size_t(VX_NOALLOC_MAX_SCENES) + 1 + 3) & ~size_t(3)) * 4 +
+                                (size_t(2) * MAX_LEVELS_ALL + 16) * 256 * 4;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_max));
+        if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch_noalloc: shared memory attribute");
+        int per_sm = 0, sms = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem_max);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch_noalloc: occupancy");
+        if (per_sm < 1) return fail(VX_EINVAL, "vx_cast_batch_noalloc: kernel does not fit on an SM");
+        d.scratch = static_cast<unsigned char*>(ptr);
+        d.blocks = per_sm * sms;
+        d.ready = true;
+    }
+    out = &d;
+    return VX_OK;
+}
+
+}  // namespace
+}  // namespace vx
+
+extern "C" int vx_cast_batch_noalloc(const vx_scene* const* scenes, uint32_t count, const vx_ray* rays,
+                                     const uint32_t* begin, uint32_t n, float tmin, float tmax, vx_hit* hits,
+                                     void* stream) {
+    using namespace vx;
+    if (!scenes || !begin || (n && (!rays || !hits))) return fail(VX_EINVAL, "vx_cast_batch_noalloc: null argument");
+    if (count == 0 || count > VX_NOALLOC_MAX_SCENES)
+        return fail(VX_EOVERFLOW, "vx_cast_batch_noalloc: scene count " + std::to_string(count) +
+                                      " is outside 1.." + std::to_string(VX_NOALLOC_MAX_SCENES) +
+                                      " (the size of its static scratch table)");
+    if (reinterpret_cast<uintptr_t>(rays) % 8 || reinterpret_cast<uintptr_t>(hits) % 16 ||
+        reinterpret_cast<uintptr_t>(begin) % 4)
+        return fail(VX_EINVAL, "vx_cast_batch_noalloc: misaligned buffer");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch_noalloc: cudaGetDevice");
+    if (dev < 0 || dev >= 64) return fail(VX_EINVAL, "vx_cast_batch_noalloc: device ordinal out of range");
+    DevScene table[VX_NOALLOC_MAX_SCENES];
+    int maxL = 1;
+    for (uint32_t i = 0; i < count; ++i) {
+        if (!scenes[i]) return fail(VX_EINVAL, "vx_cast_batch_noalloc: null scene");
+        if (scene_device(scenes[i]) != dev)
+            return fail(VX_EINVAL, "vx_cast_batch_noalloc: every scene must live on the current device");
+        table[i] = scene_dev(scenes[i]);
+        maxL = std::max(maxL, table[i].max_levels);
+    }
+    NoallocDevice* d = nullptr;
+    if (int r = noalloc_setup(dev, d)) return r;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // The scratch keeps the previous call's contents: rewrite the scene table
+    // and clear the task counter on this call's stream.
+    e = cudaMemcpyAsync(d->scratch + NOALLOC_TABLE_OFFSET, table, count * sizeof(DevScene), cudaMemcpyHostToDevice,
+                        st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d->scratch, 0, 4, st);
+    if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch_noalloc: scratch upload");
+    if (n == 0) return VX_OK;
+    BatchArgs a{reinterpret_cast<const DevScene*>(d->scratch + NOALLOC_TABLE_OFFSET), count, begin, rays, n, tmin,
+                tmax, hits, nullptr, reinterpret_cast<uint32_t*>(d->scratch), 32u, maxL};
+    const size_t smem = size_t(count) * sizeof(DevScene) + ((size_t(count) + 1 + 3) & ~size_t(3)) * 4 +
+                        (size_t(2) * size_t(maxL) + 16) * 256 * 4;
+    batch_kernel<256, 3, true><<<d->blocks, 256, smem, st>>>(a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch_noalloc: launch");
+    return VX_OK;
+}
