@@ -202,11 +202,7 @@ def run_reference(args, rank, world):
 
 
 def run_cfg4(args, rank, world):
-    """cfg4: 64 scenes (64^3..1024^3; noise 10/50 %, urban 90 %; half DXT1) with one camera
-    each (256x256..1920x1080) and 2 cosine-weighted bounce rays per hit.  One frame = primary
-    pass, bounce spawn, bounce pass.  Batched: the persistent kernel (autotuned) in a CUDA
-    graph; plain: one cast launch per scene and pass.  Both produce identical hits."""
-    import numpy as np
+    """Prints the cfg4 line (see measure_cfg4)."""
     import torch
     import torch.distributed as dist
     from datetime import timedelta
@@ -214,6 +210,28 @@ def run_cfg4(args, rank, world):
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    res = measure_cfg4(args, rank, world, args.steps, args.warmup)
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        line = {"metric": METRIC, "value": res["batched"]["value"], "unit": "Mrays/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["batched"]["ms_per_frame"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": res.pop("config"), "gpu_launches": args.steps * 3}
+        line.update(res)
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def measure_cfg4(args, rank, world, steps, warmup):
+    """cfg4: 64 scenes (64^3..1024^3; noise 10/50 %, urban 90 %; half DXT1) with one camera
+    each (256x256..1920x1080) and 2 cosine-weighted bounce rays per hit.  One frame = primary
+    pass, bounce spawn, bounce pass.  Batched: the persistent kernel (autotuned) in a CUDA
+    graph; plain: one cast launch per scene and pass.  Both produce identical hits."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    local = int(os.environ.get("LOCAL_RANK", "0"))
     vx = load_pkg()
     from vx_b200 import workloads as W
     t_setup = time.perf_counter()
@@ -272,12 +290,12 @@ def run_cfg4(args, rank, world):
 
     def timed(frame_fn, s):
         with torch.cuda.stream(s):
-            for _ in range(args.warmup):
+            for _ in range(warmup):
                 frame_fn()
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
         with torch.cuda.stream(s):
             for a, b in ev:
                 flush.zero_()
@@ -293,30 +311,116 @@ def run_cfg4(args, rank, world):
     t = torch.tensor([sum(plain_ms), sum(batched_ms)], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.destroy_process_group()
-    if rank != 0:
-        return 0
     plain_total, batched_total = float(t[0]), float(t[1])
-    value = world * rays_per_frame * args.steps / (batched_total / 1e3) / 1e6
-    plain_value = world * rays_per_frame * args.steps / (plain_total / 1e3) / 1e6
-    line = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": batched_total / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"cfg4: {len(specs)} scenes 64^3..1024^3 (noise 10/50%, urban 90%, half DXT1), "
+    value = world * rays_per_frame * steps / (batched_total / 1e3) / 1e6
+    plain_value = world * rays_per_frame * steps / (plain_total / 1e3) / 1e6
+    return {"config": {"workload": f"cfg4: {len(specs)} scenes 64^3..1024^3 (noise 10/50%, urban 90%, half DXT1), "
                                    f"one camera each 256x256..1920x1080, 2 bounce rays per hit; batched "
                                    f"persistent kernel in a CUDA graph vs {2 * len(specs)} plain launches",
                        "primary_rays": n, "rays_per_frame": rays_per_frame, "hits": nhit,
                        "scene_R": [sp.R for sp in specs], "setup_s": setup_s,
                        "l2": "flushed before every timed frame (256 MiB write)"},
-            "batched": {"value": value, "ms_per_frame": batched_total / args.steps, "tuning": tuning.as_dict(),
-                        "autotune_best_ms_primary": tune_ms},
-            "plain": {"value": plain_value, "ms_per_frame": plain_total / args.steps,
+            "batched": {"value": value, "unit": "Mrays/s", "ms_per_frame": batched_total / steps,
+                        "tuning": tuning.as_dict(), "autotune_best_ms_primary": tune_ms},
+            "plain": {"value": plain_value, "unit": "Mrays/s", "ms_per_frame": plain_total / steps,
                       "launches_per_frame": 2 * len(specs) + 1},
             "speedup_batched_vs_plain": plain_total / batched_total,
-            "hits_identical_batched_vs_plain": identical,
-            "gpu_launches": args.steps * 3, "clocks": clocks}
-    print(json.dumps(line), flush=True)
-    return 0
+            "hits_identical_batched_vs_plain": identical, "clocks": clocks}
+
+
+def measure_cfg5(args, rank, world, steps, warmup):
+    """cfg5: the 512^3 noise scene (30 % fill), 16 views of 512x512; per variant (per-voxel
+    FP32 RGB, FP32 DXT1 endpoints) the forward-with-record time and the forward+adjoint time per
+    view, the FP64 CPU gradient check and central finite differences (h = 1e-3) on 1000 entries."""
+    import numpy as np
+    import torch
+    vx = load_pkg()
+    from vx_b200 import workloads as W
+    R = 512
+    bits = vx.synth_noise_dev(R, 32, 4, 0.30, 5, False).cpu().numpy().view(np.uint64)
+    out = {}
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for kind, name in ((0, "voxel_rgb"), (1, "dxt1_endpoints")):
+        dw = W.config5(R=R, views=16, width=512, height=512, kind=kind, seed=5, bits=bits)
+        scene = vx.Scene(dw.wl.scene)
+        n = 512 * 512
+        attr_d = torch.from_numpy(dw.attr).cuda()
+        idx_d = None if dw.dxt_idx is None else torch.from_numpy(dw.dxt_idx.view(np.int32)).cuda()
+        tgt_attr = torch.from_numpy(dw.target_attr).cuda()
+        imgs = [torch.zeros((n, 3), dtype=torch.float32, device="cuda") for _ in dw.views]
+        recs = [torch.zeros((n, 4), dtype=torch.int32, device="cuda") for _ in dw.views]
+        tgts = [torch.zeros((n, 3), dtype=torch.float32, device="cuda") for _ in dw.views]
+        for v, pc in enumerate(dw.views):
+            vx.diff_forward(scene, pc, 512, 512, kind, tgt_attr, idx_d, tgts[v], recs[v])
+        grad = torch.zeros_like(attr_d)
+        loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+
+        def fwd():
+            for v, pc in enumerate(dw.views):
+                vx.diff_forward(scene, pc, 512, 512, kind, attr_d, idx_d, imgs[v], recs[v])
+
+        def fwdbwd():
+            grad.zero_()
+            loss.zero_()
+            for v, pc in enumerate(dw.views):
+                vx.diff_forward(scene, pc, 512, 512, kind, attr_d, idx_d, imgs[v], recs[v])
+                vx.diff_backward(kind, idx_d, recs[v], imgs[v], tgts[v], grad, loss)
+
+        def timed(fn):
+            for _ in range(warmup):
+                fn()
+            torch.cuda.synchronize()
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+            for a, b in ev:
+                flush.zero_()
+                a.record()
+                fn()
+                b.record()
+            torch.cuda.synchronize()
+            return sum(a.elapsed_time(b) for a, b in ev) / steps
+
+        f_ms = timed(fwd)
+        fb_ms = timed(fwdbwd)
+        g = grad.cpu().numpy().astype(np.float64)
+        rec_np = [r.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1) for r in recs]
+        tgt_np = [t.cpu().numpy() for t in tgts]
+        ref = W.adjoint_reference64(dw, rec_np, tgt_np)
+        rel64 = float(np.linalg.norm(g - ref) / np.linalg.norm(ref))
+        # central finite differences of the GPU forward on 1000 touched entries
+        rng = np.random.default_rng(11)
+        stride = 3 if kind == 0 else 6
+        touched = np.flatnonzero(np.abs(ref) > 1e-4 * np.abs(ref).max())
+        fd_err = 0.0
+        checked = 0
+        for ch in range(stride):
+            cand = touched[touched % stride == ch]
+            sel = rng.choice(cand, size=min(-(-1000 // stride), cand.size), replace=False)
+            h = np.float32(1e-3)
+            res = []
+            for sgn in (1, -1):
+                pert = dw.attr.copy()
+                pert[sel] += sgn * h
+                pd = torch.from_numpy(pert).cuda()
+                dl = np.zeros(dw.attr.shape[0], np.float64)
+                for v, pc in enumerate(dw.views):
+                    vx.diff_forward(scene, pc, 512, 512, kind, pd, idx_d, imgs[v], recs[v])
+                    p64 = imgs[v].cpu().numpy().astype(np.float64)
+                    r = rec_np[v]
+                    hit = (r["flags"] & 1).astype(bool)
+                    key = (r["brick"].astype(np.int64) * 512 + r["voxel"]) if kind == 0 else \
+                        (r["brick"].astype(np.int64) * 32 + (r["voxel"].astype(np.int64) >> 4))
+                    np.add.at(dl, key[hit] * stride + ch, ((p64 - tgt_np[v].astype(np.float64)) ** 2).sum(1)[hit])
+                res.append(dl)
+            fd = (res[0] - res[1]) / (2.0 * float(h))
+            fd_err = max(fd_err, float(np.max(np.abs(fd[sel] - g[sel]) / np.maximum(np.abs(g[sel]), 1e-6))))
+            checked += sel.size
+        out[name] = {"fwd_ms_per_view": f_ms / 16, "fwd_bwd_ms_per_view": fb_ms / 16, "ratio": fb_ms / f_ms,
+                     "fp64_grad_rel_err": rel64, "fd_max_rel_err": fd_err, "fd_entries": checked,
+                     "hit_rate": float(np.mean([(r["flags"] & 1).mean() for r in rec_np])),
+                     "attributes": int(dw.attr.shape[0])}
+        del scene
+    return {"workload": "cfg5: 512^3 noise 30% fill, 16 views 512x512 on an orbit, L2 loss vs targets rendered "
+                        "from colours + N(0, 0.05)", **out}
 
 
 def config_dict(wl, world):
@@ -337,8 +441,11 @@ def main():
     ap.add_argument("--R", type=int, default=1024)
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg4"],
-                    help="cfg2: plain cast of the 1024^3 cave frame; cfg4: 64-scene batched frame vs plain")
+    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg4", "cfg5"],
+                    help="cfg2: plain cast of the 1024^3 cave frame (with the cfg4 and cfg5 results attached "
+                         "at N=1); cfg4: 64-scene batched frame vs plain; cfg5: forward / adjoint ms per view")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="cfg2 only: skip the attached batched (cfg4) and adjoint (cfg5) measurements")
     ap.add_argument("--scenes", type=int, default=64, help="cfg4: number of scenes")
     ap.add_argument("--soak-seconds", type=float, default=1.5,
                     help="untimed launches before timing so clocks reach steady state")
@@ -350,6 +457,19 @@ def main():
         return run_reference(args, rank, world)
     if args.workload == "cfg4":
         return run_cfg4(args, rank, world)
+    if args.workload == "cfg5":
+        import torch
+        torch.cuda.set_device(local)
+        res = measure_cfg5(args, rank, world, args.steps, args.warmup)
+        if rank == 0:
+            a = res["voxel_rgb"]
+            print(json.dumps({"metric": METRIC, "value": a["fwd_bwd_ms_per_view"], "unit": "ms/view", "n_gpus": 1,
+                              "steps": args.steps, "warmup": args.warmup,
+                              "ms_per_step": a["fwd_bwd_ms_per_view"] * 16, "higher_is_better": False,
+                              "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                              "config": {"workload": res.pop("workload")}, "adjoint": res,
+                              "gpu_launches": args.steps * 32}), flush=True)
+        return 0
 
     import numpy as np
     import torch
@@ -479,6 +599,18 @@ def main():
         cb, parity = cpu_baseline(vo, wl, rays_np, g_hits)
         line["cpu_baseline"] = cb
         line["parity_sample"] = parity
+    if world == 1 and not args.no_extra:
+        del scene
+        torch.cuda.empty_cache()
+        extra_steps, extra_warmup = max(3, min(args.steps, 5)), max(2, min(args.warmup, 3))
+        b = measure_cfg4(args, rank, world, extra_steps, extra_warmup)
+        line["batched"] = {"workload": b["config"]["workload"], "rays_per_frame": b["config"]["rays_per_frame"],
+                           "batched_mrays_s": b["batched"]["value"], "plain_mrays_s": b["plain"]["value"],
+                           "speedup_batched_vs_plain": b["speedup_batched_vs_plain"],
+                           "hits_identical": b["hits_identical_batched_vs_plain"], "tuning": b["batched"]["tuning"],
+                           "steps": extra_steps}
+        torch.cuda.empty_cache()
+        line["adjoint"] = measure_cfg5(args, rank, world, extra_steps, extra_warmup)
     print(json.dumps(line), flush=True)
     return 0
 

@@ -284,6 +284,30 @@ int vx_batch_capture_frame(vx_batch* batch, const vx_ray* primary_dev, const uin
 int vx_batch_launch_frame(vx_batch* batch, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Differentiable form (no reference counterpart).  The traversal is discrete
+ * and not differentiated: the forward pass records each pixel's hit (the
+ * vx_hit of the cast) and the backward pass replays it.  Attributes are FP32:
+ *   VX_DIFF_VOXEL_RGB:      attr[(brick*512 + voxel)*3 + c], 3 floats per voxel
+ *   VX_DIFF_DXT1_ENDPOINTS: attr[block*6 + 0..2] = e0, [block*6 + 3..5] = e1
+ *                           per DXT1 block (block = brick*32 + voxel/16), with
+ *                           the fixed 2-bit selectors idx[block]; texel =
+ *                           w0*e0 + w1*e1, (w0,w1) = (1,0),(0,1),(2/3,1/3),(1/3,2/3)
+ * Pixel of a hit = texel * (0.3 + max(n.L, 0) * 0.7) (Lighting.glsl:19-28);
+ * a miss shows the sky colour.  image: W*H*3 floats, record: W*H vx_hit.
+ * Backward: loss = sum (image - target)^2 over pixels and channels (added to
+ * *loss_dev if not NULL); dL/dattr is ADDED to grad_dev (same layout as attr;
+ * zero it first) with warp-aggregated atomics.
+ * --------------------------------------------------------------------- */
+#define VX_DIFF_VOXEL_RGB 0
+#define VX_DIFF_DXT1_ENDPOINTS 1
+int vx_diff_forward(const vx_scene* scene, const vx_camera_pc* pc, uint32_t width, uint32_t height,
+                    int32_t kind, const float* attr_dev, const uint32_t* dxt_idx_dev, float* image_dev,
+                    vx_hit* record_dev, void* stream);
+int vx_diff_backward(uint32_t n, int32_t kind, const uint32_t* dxt_idx_dev, const vx_hit* record_dev,
+                     const float* image_dev, const float* target_dev, float* grad_dev, float* loss_dev,
+                     void* stream);
+
+/* ------------------------------------------------------------------------
  * Host scene builder.  Replaces LaineKarrasOctree::rebuild
  * (SVO/src/SVORebuild.cpp:228-607) plus VoxelSceneCacher::BuildOctree /
  * BuildBrickGridLookup (VoxelSceneCacher.cpp:463-713) for a dense occupancy

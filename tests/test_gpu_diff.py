@@ -1,0 +1,82 @@
+"""Differentiable form (needs a B200): forward records equal the plain cast,
+the adjoint equals an FP64 CPU gradient (rel err <= 1e-5) and central finite
+differences of the GPU forward (h = 1e-3, rel err <= 1e-2)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _render(vx, scene, dw, attr_d, idx_d, views):
+    import torch
+    n = dw.wl.width * dw.wl.height
+    imgs, recs = [], []
+    for pc in views:
+        img = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+        rec = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+        vx.diff_forward(scene, pc, dw.wl.width, dw.wl.height, dw.kind, attr_d, idx_d, img, rec)
+        imgs.append(img)
+        recs.append(rec)
+    return imgs, recs
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_adjoint_matches_fp64_and_finite_differences(vx, vo, cuda, kind):
+    import torch
+    from vx_b200 import workloads as W
+    dw = W.config5(R=128, views=4, width=128, height=96, kind=kind, seed=7)
+    scene = vx.Scene(dw.wl.scene)
+    attr_d = torch.from_numpy(dw.attr).cuda()
+    idx_d = None if dw.dxt_idx is None else torch.from_numpy(dw.dxt_idx.view(np.int32)).cuda()
+    tgt_d = torch.from_numpy(dw.target_attr).cuda()
+    targets, _ = _render(vx, scene, dw, tgt_d, idx_d, dw.views)
+    imgs, recs = _render(vx, scene, dw, attr_d, idx_d, dw.views)
+    grad = torch.zeros_like(attr_d)
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    for img, rec, tgt in zip(imgs, recs, targets):
+        vx.diff_backward(dw.kind, idx_d, rec, img, tgt, grad, loss)
+    torch.cuda.synchronize()
+    g = grad.cpu().numpy().astype(np.float64)
+    rec_np = [r.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1) for r in recs]
+    tgt_np = [t.cpu().numpy() for t in targets]
+    # records equal the plain cast of the same camera rays, checked by the oracle
+    o = vo.OracleScene.from_dense(dw.wl.bits, dw.wl.R, dw.wl.scene.max_levels)
+    for pc, r in zip(dw.views[:2], rec_np):
+        oh = o.cast_rays(vx.camera_rays(pc, dw.wl.width, dw.wl.height))
+        assert np.array_equal(r["brick"], oh["brick"]) and np.array_equal(r["flags"].astype(np.uint32), oh["flags"])
+    # loss
+    want_loss = sum(float(((i.cpu().numpy().astype(np.float64) - t.astype(np.float64)) ** 2).sum())
+                    for i, t in zip(imgs, tgt_np))
+    assert abs(float(loss.item()) - want_loss) <= 1e-4 * want_loss
+    # FP64 reference gradient
+    ref = W.adjoint_reference64(dw, rec_np, tgt_np)
+    assert np.count_nonzero(ref) > 1000
+    rel = np.linalg.norm(g - ref) / np.linalg.norm(ref)
+    assert rel <= 1e-5, rel
+    big = np.abs(ref) > 1e-3 * np.abs(ref).max()
+    assert np.max(np.abs(g - ref)[big] / np.abs(ref)[big]) <= 1e-4
+    # central finite differences of the GPU forward, h = 1e-3, on up to 1000 touched entries
+    rng = np.random.default_rng(3)
+    touched = np.flatnonzero(np.abs(ref) > 1e-4 * np.abs(ref).max())
+    stride = 3 if kind == 0 else 6
+    for ch in range(stride if kind == 1 else 3):
+        cand = touched[touched % stride == ch]
+        # one entry per voxel / block so perturbations do not interact
+        sel = rng.choice(cand, size=min(1000 // stride + 1, cand.size), replace=False)
+        h = np.float32(1e-3)
+        plus, minus = dw.attr.copy(), dw.attr.copy()
+        plus[sel] += h
+        minus[sel] -= h
+        ip, _ = _render(vx, scene, dw, torch.from_numpy(plus).cuda(), idx_d, dw.views)
+        im, _ = _render(vx, scene, dw, torch.from_numpy(minus).cuda(), idx_d, dw.views)
+        fd = np.zeros(dw.attr.shape[0], np.float64)
+        for p_, m_, r, t in zip(ip, im, rec_np, tgt_np):
+            p64, m64, t64 = p_.cpu().numpy().astype(np.float64), m_.cpu().numpy().astype(np.float64), t.astype(np.float64)
+            dl = ((p64 - t64) ** 2 - (m64 - t64) ** 2).sum(1)  # per pixel
+            hit = (r["flags"] & 1).astype(bool)
+            key = (r["brick"].astype(np.int64) * 512 + r["voxel"]) if kind == 0 else \
+                (r["brick"].astype(np.int64) * 32 + (r["voxel"].astype(np.int64) >> 4))
+            np.add.at(fd, key[hit] * stride + ch, dl[hit])
+        fd /= 2.0 * float(h)
+        err = np.abs(fd[sel] - g[sel]) / np.maximum(np.abs(g[sel]), 1e-6)
+        assert np.max(err) <= 1e-2, (ch, np.max(err))

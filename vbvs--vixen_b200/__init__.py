@@ -118,6 +118,8 @@ def lib():
         "vx_batch_capture_frame": (C.c_int, [vp, vp, vp, u32, vp, vp, vp, vp, u64, vp]),
         "vx_batch_launch_frame": (C.c_int, [vp, vp]),
         "vx_cast_batch_noalloc": (C.c_int, [vp, u32, vp, vp, u32, f32, f32, vp, vp]),
+        "vx_diff_forward": (C.c_int, [vp, vp, u32, u32, i32, vp, vp, vp, vp, vp]),
+        "vx_diff_backward": (C.c_int, [u32, i32, vp, vp, vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -477,3 +479,20 @@ def cast_batch_noalloc(scenes, rays, begin, hits, t_min=0.0, t_max=FLT_MAX, stre
     arr = (C.c_void_p * len(scenes))(*[sc.handle.value for sc in scenes])
     check(lib().vx_cast_batch_noalloc(arr, len(scenes), _p(rays), _p(begin), rays.shape[0], float(t_min),
                                       float(t_max), _p(hits), _stream(stream)))
+
+
+# ---------------------------------------------------------------------------
+# Differentiable form
+# ---------------------------------------------------------------------------
+VX_DIFF_VOXEL_RGB, VX_DIFF_DXT1_ENDPOINTS = 0, 1
+
+
+def diff_forward(scene: "Scene", pc: CameraPC, width: int, height: int, kind: int, attr, dxt_idx, image, record,
+                 stream=None):
+    check(lib().vx_diff_forward(scene.handle, C.byref(pc), width, height, kind, _p(attr), _p(dxt_idx), _p(image),
+                                _p(record), _stream(stream)))
+
+
+def diff_backward(kind: int, dxt_idx, record, image, target, grad, loss=None, stream=None):
+    check(lib().vx_diff_backward(record.shape[0], kind, _p(dxt_idx), _p(record), _p(image), _p(target), _p(grad),
+                                 _p(loss), _stream(stream)))

@@ -231,3 +231,85 @@ def bounce_rays_reference(rays: np.ndarray, hits: np.ndarray, seed: int, table: 
         out[2 * rows[sel] + k, :3] = org[sel]
         out[2 * rows[sel] + k, 3:] = dirs[sel]
     return out
+
+
+@dataclass
+class DiffWorkload:
+    wl: Workload
+    kind: int
+    attr: np.ndarray          # FP32 attributes (VX_DIFF_* layout)
+    target_attr: np.ndarray   # attr + N(0, 0.05): the colours the target images are rendered from
+    dxt_idx: np.ndarray | None
+    views: list
+
+
+def config5(R: int = 512, views: int = 16, width: int = 512, height: int = 512, kind: int = 0, seed: int = 5,
+            bits=None) -> DiffWorkload:
+    """cfg5: 512^3 value-noise scene at 30 % fill (spacing 32, 4 octaves); FP32 per-voxel RGB
+    (kind 0) or FP32 DXT1 endpoints with fixed selectors (kind 1); `views` pinhole views on a
+    seeded orbit around the grid centre, looking at it; targets rendered from the attributes
+    plus N(0, 0.05)."""
+    spacing = max(4, 32 * R // 512)
+    if bits is None:
+        bits = synth_noise(R, spacing, 4 if spacing >= 32 else 3, 0.30, seed, False)
+    scene = scene_from_bits(bits, R, None, seed)
+    rng = np.random.default_rng(seed)
+    B = scene.brick_count
+    if kind == 0:
+        attr = rng.random(B * 512 * 3, dtype=np.float32)
+        idx = None
+    else:
+        attr = rng.random(B * 32 * 6, dtype=np.float32)
+        idx = rng.integers(0, 2 ** 32, size=B * 32, dtype=np.uint64).astype(np.uint32)
+    target = (attr + rng.normal(0.0, 0.05, size=attr.shape).astype(np.float32)).astype(np.float32)
+    c = np.float32(R / 2)
+    cams = []
+    phase = rng.uniform(0, 2 * np.pi)
+    for v in range(views):
+        th = phase + 2 * np.pi * v / views
+        pos = [c + 0.95 * R * np.cos(th), c + R * rng.uniform(-0.3, 0.3), c + 0.95 * R * np.sin(th)]
+        cams.append(look_camera(pos, [c - pos[0], c - pos[1], c - pos[2]], 60.0, width, height))
+    wl = Workload(f"cfg5_noise{R}_{'rgb' if kind == 0 else 'dxt1ep'}_{views}x{width}x{height}", R, scene, bits,
+                  cams[0], width, height)
+    return DiffWorkload(wl, kind, attr, target, idx, cams)
+
+
+def lambert_k64(flags: np.ndarray) -> np.ndarray:
+    """Lambert factor of Lighting.glsl:19-28 per hit flag, in double."""
+    L = np.array([1.0, 1.0, -1.0]) / np.sqrt(3.0)
+    axis = (flags.astype(np.int64) >> 1) & 3
+    sgn = np.where(flags & 8, -1.0, 1.0)
+    return 0.3 + np.maximum(sgn * L[axis], 0.0) * 0.7
+
+
+def dxt_weights64(idx: np.ndarray, block: np.ndarray, voxel: np.ndarray):
+    sel = (idx[block].astype(np.int64) >> (2 * (voxel.astype(np.int64) & 15))) & 3
+    w0 = np.array([1.0, 0.0, 2.0 / 3.0, 1.0 / 3.0])[sel]
+    w1 = np.array([0.0, 1.0, 1.0 / 3.0, 2.0 / 3.0])[sel]
+    return w0, w1
+
+
+def adjoint_reference64(dw: DiffWorkload, records, targets) -> np.ndarray:
+    """FP64 gradient of the L2 loss, replaying the forward records (brick, voxel, normal) with
+    the colour math in double."""
+    grad = np.zeros(dw.attr.shape[0], np.float64)
+    attr = dw.attr.astype(np.float64)
+    for rec, tgt in zip(records, targets):
+        hit = (rec["flags"] & 1).astype(bool)
+        br, vx_, fl = rec["brick"][hit].astype(np.int64), rec["voxel"][hit].astype(np.int64), rec["flags"][hit]
+        k = lambert_k64(fl)
+        t = tgt.reshape(-1, 3)[hit].astype(np.float64)
+        if dw.kind == 0:
+            base = (br * 512 + vx_) * 3
+            for ch in range(3):
+                pix = attr[base + ch] * k
+                np.add.at(grad, base + ch, 2.0 * (pix - t[:, ch]) * k)
+        else:
+            blk = br * 32 + (vx_ >> 4)
+            w0, w1 = dxt_weights64(dw.dxt_idx, blk, vx_)
+            for ch in range(3):
+                pix = (w0 * attr[blk * 6 + ch] + w1 * attr[blk * 6 + 3 + ch]) * k
+                g = 2.0 * (pix - t[:, ch]) * k
+                np.add.at(grad, blk * 6 + ch, w0 * g)
+                np.add.at(grad, blk * 6 + 3 + ch, w1 * g)
+    return grad
