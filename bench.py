@@ -328,6 +328,59 @@ def measure_cfg4(args, rank, world, steps, warmup):
             "hits_identical_batched_vs_plain": identical, "clocks": clocks}
 
 
+def measure_cfg3(args, steps, warmup):
+    """cfg3: 2048^3 urban lattice (32x32 blocks, 8-voxel streets, heights U[64,1800]), DXT1
+    bricks, 3840x2160 primary rays plus one shadow ray per hit toward a seeded light.  One frame =
+    primary cast, shadow spawn, shadow cast (plain kernel)."""
+    import numpy as np
+    import torch
+    vx = load_pkg()
+    from vx_b200 import workloads as W
+    t0 = time.perf_counter()
+    wl = W.config3(R=args.R if args.R != 1024 else 2048)
+    scene = vx.Scene(wl.scene)
+    setup_s = time.perf_counter() - t0
+    bricks, nodes, dev_bytes = wl.scene.brick_count, wl.scene.node_count, scene.device_bytes()
+    wl.scene.brick_color = None
+    rays_np = wl.rays()
+    n = rays_np.shape[0]
+    rays = torch.from_numpy(rays_np).cuda()
+    hits = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+    col = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+    shadow = torch.zeros((n, 6), dtype=torch.float32, device="cuda")
+    sh = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+    L = W.light_dir(3)
+
+    def frame():
+        scene.cast_rays_dev(rays, hits, col)
+        vx.spawn_shadow_rays(rays, hits, L, shadow)
+        scene.cast_rays_dev(shadow, sh)
+
+    frame()
+    torch.cuda.synchronize()
+    g = hits.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1)
+    nhit = int(np.count_nonzero(g["flags"] & 1))
+    shit = int(np.count_nonzero(sh.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1)["flags"] & 1))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(warmup):
+        frame()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for a, b in ev:
+        flush.zero_()
+        a.record()
+        frame()
+        b.record()
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / steps
+    rays_per_frame = n + nhit
+    return {"workload": f"{wl.name}: urban {wl.R}^3 (depth {wl.scene.max_levels}), 32x32 blocks, heights "
+                        f"U[64,1800], DXT1; {wl.width}x{wl.height} primary + 1 shadow ray per hit",
+            "mrays_s": rays_per_frame / (ms / 1e3) / 1e6, "ms_per_frame": ms, "primary_rays": n,
+            "shadow_rays": nhit, "primary_hit_rate": nhit / n, "shadowed_fraction": shit / max(nhit, 1),
+            "bricks": bricks, "nodes": nodes, "scene_device_bytes": dev_bytes, "setup_s": setup_s}
+
+
 def measure_cfg5(args, rank, world, steps, warmup):
     """cfg5: the 512^3 noise scene (30 % fill), 16 views of 512x512; per variant (per-voxel
     FP32 RGB, FP32 DXT1 endpoints) the forward-with-record time and the forward+adjoint time per
@@ -441,7 +494,7 @@ def main():
     ap.add_argument("--R", type=int, default=1024)
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg4", "cfg5"],
+    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg3", "cfg4", "cfg5"],
                     help="cfg2: plain cast of the 1024^3 cave frame (with the cfg4 and cfg5 results attached "
                          "at N=1); cfg4: 64-scene batched frame vs plain; cfg5: forward / adjoint ms per view")
     ap.add_argument("--no-extra", action="store_true",
@@ -457,6 +510,18 @@ def main():
         return run_reference(args, rank, world)
     if args.workload == "cfg4":
         return run_cfg4(args, rank, world)
+    if args.workload == "cfg3":
+        import torch
+        torch.cuda.set_device(local)
+        res = measure_cfg3(args, args.steps, args.warmup)
+        if rank == 0:
+            line = {"metric": METRIC, "value": res["mrays_s"], "unit": "Mrays/s", "n_gpus": 1, "steps": args.steps,
+                    "warmup": args.warmup, "ms_per_step": res["ms_per_frame"], "higher_is_better": True,
+                    "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                    "config": {"workload": res.pop("workload")}, "gpu_launches": args.steps * 3}
+            line.update(res)
+            print(json.dumps(line), flush=True)
+        return 0
     if args.workload == "cfg5":
         import torch
         torch.cuda.set_device(local)

@@ -313,3 +313,12 @@ def adjoint_reference64(dw: DiffWorkload, records, targets) -> np.ndarray:
                 np.add.at(grad, blk * 6 + ch, w0 * g)
                 np.add.at(grad, blk * 6 + 3 + ch, w1 * g)
     return grad
+
+
+def light_dir(seed: int) -> np.ndarray:
+    """Seeded directional light for cfg3 shadow rays: above the horizon (y > 0.3), normalised
+    in binary32."""
+    rng = np.random.default_rng(seed ^ 0x116)
+    v = rng.normal(size=3)
+    v[1] = abs(v[1]) + 0.3 * np.linalg.norm(v)
+    return _normalize(v.astype(np.float32))
