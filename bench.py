@@ -114,9 +114,10 @@ def make_workload(vx, R, seed, rank, use_gpu_gen):
         bits = vx.synth_noise_dev(R, spacing, octaves, 0.5, seed, False).cpu().numpy().view(np.uint64)
     else:
         bits = vx.synth_noise(R, spacing, octaves, 0.5, seed, False)
+    from vx_b200 import multigpu as M
     wl = W.config2(R=R, seed=seed, bits=bits)
     if rank:
-        wl.camera = W.empty_voxel_camera(bits, R, seed + 7919 * rank, 70.0, wl.width, wl.height)
+        wl.camera = W.empty_voxel_camera(bits, R, M.rank_seed(seed, rank), 70.0, wl.width, wl.height)
     return wl
 
 
@@ -235,7 +236,8 @@ def measure_cfg4(args, rank, world, steps, warmup):
     vx = load_pkg()
     from vx_b200 import workloads as W
     t_setup = time.perf_counter()
-    specs = W.config4_specs(args.scenes, seed=4 + 1000 * rank)
+    from vx_b200 import multigpu as M
+    specs = W.config4_specs(args.scenes, seed=M.rank_seed(4, rank))
     wls, scenes, rays = [], [], []
     for sp in specs:
         bits = None
@@ -308,10 +310,8 @@ def measure_cfg4(args, rank, world, steps, warmup):
     plain_ms = timed(plain_frame, stream)
     batched_ms = timed(lambda: batch.launch_frame(stream.cuda_stream), stream)
     clocks = sampler.stop()
-    t = torch.tensor([sum(plain_ms), sum(batched_ms)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    plain_total, batched_total = float(t[0]), float(t[1])
+    from vx_b200 import multigpu as M
+    plain_total, batched_total = M.max_over_ranks([sum(plain_ms), sum(batched_ms)])
     value = world * rays_per_frame * steps / (batched_total / 1e3) / 1e6
     plain_value = world * rays_per_frame * steps / (plain_total / 1e3) / 1e6
     return {"config": {"workload": f"cfg4: {len(specs)} scenes 64^3..1024^3 (noise 10/50%, urban 90%, half DXT1), "
@@ -621,17 +621,15 @@ def main():
     e2e_ms = sum(a.elapsed_time(b) for a, b in zip(e0, e1))
     e2e_same = bool(np.array_equal(hits_h.numpy().view(np.uint8), g_hits.view(np.uint8).reshape(n, 16)))
 
-    t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms, e2e_ms = float(t[0]), float(t[1])
+    from vx_b200 import multigpu as M
+    total_ms, e2e_ms = M.max_over_ranks([total_ms, e2e_ms])
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
         return 0
 
-    value = world * n * args.steps / (total_ms / 1e3) / 1e6
-    e2e_value = world * n * args.steps / (e2e_ms / 1e3) / 1e6
+    value = M.aggregate_throughput(n * args.steps, world, total_ms / 1e3) / 1e6
+    e2e_value = M.aggregate_throughput(n * args.steps, world, e2e_ms / 1e3) / 1e6
     mean_s = statistics.mean(step_ms) / 1e3
     peak, peak_kind = measured_peaks()
     achieved = algo_bytes / mean_s / 1e9

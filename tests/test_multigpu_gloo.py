@@ -1,0 +1,82 @@
+"""Multi-GPU host logic on CPU with world_size 2 (gloo): the ray split covers
+every ray exactly once, per-rank casts concatenate to the single-process
+result, and the timing reduction is the max over ranks."""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def test_ray_range_partition():
+    import importlib.util
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from conftest import load_vx
+    load_vx()
+    from vx_b200 import multigpu as M
+    for n in (0, 1, 7, 1000, 2073600):
+        for world in (1, 2, 3, 8):
+            ranges = [M.ray_range(n, r, world) for r in range(world)]
+            assert ranges[0][0] == 0 and ranges[-1][1] == n
+            assert all(a[1] == b[0] for a, b in zip(ranges, ranges[1:]))
+            sizes = [e - b for b, e in ranges]
+            assert max(sizes) - min(sizes) <= 1
+    assert M.rank_seed(2, 0) == 2 and M.rank_seed(2, 1) != M.rank_seed(2, 0)
+    with pytest.raises(ValueError):
+        M.ray_range(10, 2, 2)
+
+
+def _worker(rank, world, port, out_dir):
+    import sys
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import torch.distributed as dist
+    from conftest import load_vx
+    import vx_oracle as vo
+    load_vx()
+    from vx_b200 import multigpu as M
+    from vx_b200 import workloads as W
+    from datetime import timedelta
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    wl = W.config1(R=64, width=48, height=40, seed=5)
+    rays = wl.rays()
+    b, e = M.ray_range(rays.shape[0], rank, world)
+    hits = vo.OracleScene.from_dense(wl.bits, 64, wl.scene.max_levels).cast_rays(rays[b:e], threads=1)
+    parts = [None] * world
+    dist.all_gather_object(parts, hits.tobytes())
+    tmax = M.max_over_ranks([1.0 + rank, 5.0 - rank])
+    if rank == 0:
+        np.save(os.path.join(out_dir, "gathered.npy"), np.frombuffer(b"".join(parts), dtype=hits.dtype))
+        np.save(os.path.join(out_dir, "tmax.npy"), np.array(tmax))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_gloo_split_matches_single_process(vo, tmp_path):
+    import multiprocessing as mp
+    from vx_b200 import workloads as W
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, str(tmp_path))) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=180)
+        assert p.exitcode == 0
+    gathered = np.load(tmp_path / "gathered.npy")
+    wl = W.config1(R=64, width=48, height=40, seed=5)
+    whole = vo.OracleScene.from_dense(wl.bits, 64, wl.scene.max_levels).cast_rays(wl.rays(), threads=1)
+    assert np.array_equal(gathered.view(np.uint8), whole.view(np.uint8))
+    assert list(np.load(tmp_path / "tmax.npy")) == [2.0, 5.0]
