@@ -226,7 +226,9 @@ typedef struct vx_batch_tuning {
     int32_t block;            /* 128 or 256 threads */
     int32_t rays_per_task;    /* multiple of 32 */
     int32_t stack_in_shared;  /* 1: traversal stack in shared memory, 0: in local memory */
-    int32_t reserved;
+    int32_t refill;           /* 0: each lane casts its rays of a task start to end;
+                                 1..32: lanes advance one ESVO iteration per round and the
+                                 warp deals new rays to idle lanes once this many are idle */
 } vx_batch_tuning;
 
 int vx_batch_create(const vx_scene* const* scenes, uint32_t count, vx_batch** out);
@@ -236,9 +238,9 @@ int vx_batch_get_tuning(const vx_batch* batch, vx_batch_tuning* tuning);
 int vx_cast_batch(vx_batch* batch, const vx_ray* rays_dev, const uint32_t* begin_dev, uint32_t n,
                   float t_min, float t_max, vx_hit* hits_dev, vx_ray_counters* counters_dev,
                   void* stream);
-/* Times every (block, rays_per_task, stack placement) candidate on the given
- * rays (3 launches each, best of the last 2), keeps the fastest in the batch
- * and returns it.  Writes hits_dev. */
+/* Times every (block, rays_per_task, stack placement, refill) candidate on
+ * the given rays (3 launches each, best of the last 2), keeps the fastest in
+ * the batch and returns it.  Writes hits_dev. */
 int vx_batch_autotune(vx_batch* batch, const vx_ray* rays_dev, const uint32_t* begin_dev, uint32_t n,
                       vx_hit* hits_dev, void* stream, vx_batch_tuning* best, float* best_ms);
 

@@ -32,14 +32,16 @@ def _plain(vx, scenes, rays, begin, d_rays):
     return hits
 
 
-@pytest.mark.parametrize("block,k,smem", [(256, 128, 1), (128, 32, 1), (256, 64, 0), (128, 512, 0)])
-def test_batch_equals_plain_and_oracle(vx, vo, cuda, block, k, smem):
+@pytest.mark.parametrize("block,k,smem,refill", [(256, 128, 1, 0), (128, 32, 1, 0), (256, 64, 0, 0), (128, 512, 0, 0),
+                                                 (256, 32, 1, 16), (128, 64, 1, 8), (256, 128, 0, 24),
+                                                 (256, 32, 1, 32), (128, 32, 0, 1)])
+def test_batch_equals_plain_and_oracle(vx, vo, cuda, block, k, smem, refill):
     import torch
     from vx_b200 import workloads as W
     wls, scenes, rays, begin, allr, d_rays, d_begin = _setup(vx, W)
     plain = _plain(vx, scenes, rays, begin, d_rays)
     batch = vx.Batch(scenes)
-    batch.set_tuning(block, k, smem)
+    batch.set_tuning(block, k, smem, refill)
     hits = torch.full_like(plain, -1)
     cnt = torch.zeros((allr.shape[0], 4), dtype=torch.int32, device="cuda")
     batch.cast(d_rays, d_begin, hits, cnt)
@@ -152,3 +154,5 @@ def test_batch_rejects_bad_tuning(vx, cuda):
         b.set_tuning(block=96)
     with pytest.raises(vx.VxError):
         b.set_tuning(rays_per_task=40)
+    with pytest.raises(vx.VxError):
+        b.set_tuning(refill=33)

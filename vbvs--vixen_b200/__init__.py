@@ -391,10 +391,11 @@ class CudaOctree:
 
 class BatchTuning(C.Structure):
     _fields_ = [("block", C.c_int32), ("rays_per_task", C.c_int32), ("stack_in_shared", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("refill", C.c_int32)]
 
     def as_dict(self):
-        return {"block": self.block, "rays_per_task": self.rays_per_task, "stack_in_shared": self.stack_in_shared}
+        return {"block": self.block, "rays_per_task": self.rays_per_task, "stack_in_shared": self.stack_in_shared,
+                "refill": self.refill}
 
 
 def _stream(stream):
@@ -428,8 +429,8 @@ class Batch:
         check(lib().vx_batch_get_tuning(self._h, C.byref(t)))
         return t
 
-    def set_tuning(self, block=256, rays_per_task=128, stack_in_shared=1):
-        t = BatchTuning(block, rays_per_task, stack_in_shared, 0)
+    def set_tuning(self, block=256, rays_per_task=32, stack_in_shared=1, refill=0):
+        t = BatchTuning(block, rays_per_task, stack_in_shared, refill)
         check(lib().vx_batch_set_tuning(self._h, C.byref(t)))
 
     def cast(self, rays, begin, hits, counters=None, t_min=0.0, t_max=FLT_MAX, stream=None):

@@ -40,7 +40,121 @@ struct BatchArgs {
     uint32_t* work;  // task counter, zero before the launch
     uint32_t K;      // rays per warp task
     int maxL;        // largest max_levels in the batch
+    int refill;      // refill idle lanes once this many are idle (refilling kernels)
 };
+
+__device__ __forceinline__ int scene_of(const uint32_t* beg, uint32_t S, uint32_t r) {
+    int lo = 0, hi = int(S);
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (beg[mid] <= r) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void store_counters(vx_ray_counters* counters, uint32_t r, const Hit& h) {
+    if (!counters) return;
+    uint4 rc;
+    rc.x = (h.iters & 0xFFFFu) | (h.grid_reads << 16);
+    rc.y = h.dda_steps;
+    rc.z = (h.run_iters & 0xFFFFu) | (h.run_grid_reads << 16);
+    rc.w = h.run_dda_steps;
+    reinterpret_cast<uint4*>(counters)[r] = rc;
+}
+
+// Refilling variant: a lane keeps its ray's traversal state in registers and
+// advances it one ESVO iteration per round; when at least `refill` lanes of
+// the warp are idle, the warp deals the next rays of its task to them (rank
+// among the idle lanes by __ballot_sync / __popc) and takes a new task from
+// the work counter when the current one is used up.  Every warp-wide
+// primitive runs with all 32 lanes converged; the traversal between them is
+// per lane.
+template <int BLOCK, int MINB, bool SMEM_STACK>
+__global__ void __launch_bounds__(BLOCK, MINB) batch_refill_kernel(BatchArgs a) {
+    extern __shared__ uint32_t smem[];
+    DevScene* sc = reinterpret_cast<DevScene*>(smem);
+    uint32_t* beg = reinterpret_cast<uint32_t*>(sc + a.S);
+    {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(a.scenes);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(sc);
+        const uint32_t words = a.S * uint32_t(sizeof(DevScene) / 4);
+        for (uint32_t i = threadIdx.x; i < words; i += BLOCK) dst[i] = src[i];
+        for (uint32_t i = threadIdx.x; i <= a.S; i += BLOCK) beg[i] = a.begin[i];
+    }
+    __syncthreads();
+    uint32_t* stk_base = beg + ((a.S + 1 + 3) & ~3u);
+    uint32_t lnode[SMEM_STACK ? 1 : MAX_LEVELS_ALL];
+    float ltmax[SMEM_STACK ? 1 : MAX_LEVELS_ALL];
+    uint32_t lcyc[SMEM_STACK ? 1 : 16];
+    uint32_t* stkN;
+    float* stkT;
+    uint32_t* cyc;
+    int stride;
+    if (SMEM_STACK) {
+        stkN = stk_base + threadIdx.x;
+        stkT = reinterpret_cast<float*>(stk_base + a.maxL * BLOCK) + threadIdx.x;
+        cyc = stk_base + 2 * a.maxL * BLOCK + threadIdx.x;
+        stride = BLOCK;
+    } else {
+        stkN = lnode;
+        stkT = ltmax;
+        cyc = lcyc;
+        stride = 1;
+    }
+    const uint32_t FULL = 0xFFFFFFFFu;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t below = (1u << lane) - 1u;
+    uint64_t next = 0, end = 0;  // warp-uniform cursor into the current task
+    bool tasks_left = true;
+    bool active = false;
+    uint32_t ray = 0;
+    int sid = 0;
+    CastState st;
+    for (;;) {
+        uint32_t idle = __ballot_sync(FULL, !active);
+        if (__popc(idle) >= a.refill || idle == FULL) {
+            while (idle) {
+                if (next >= end) {
+                    if (!tasks_left) break;
+                    uint32_t t = 0;
+                    if (lane == 0) t = atomicAdd(a.work, 1u);
+                    t = __shfl_sync(FULL, t, 0);
+                    next = uint64_t(t) * a.K;
+                    if (next >= a.n) { tasks_left = false; next = end = 0; break; }
+                    end = min(next + a.K, uint64_t(a.n));
+                }
+                const uint32_t avail = uint32_t(end - next);
+                const uint32_t rank = __popc(idle & below);
+                const bool got = ((idle >> lane) & 1u) && rank < avail;
+                const uint32_t taken = min(avail, uint32_t(__popc(idle)));
+                if (got) {
+                    ray = uint32_t(next) + rank;
+                    sid = scene_of(beg, a.S, ray);
+                    const float2* r2 = reinterpret_cast<const float2*>(a.rays + ray);
+                    const float2 p = __ldg(r2), q = __ldg(r2 + 1), w = __ldg(r2 + 2);
+                    if (cast_init(sc[sid], p.x, p.y, q.x, q.y, w.x, w.y, a.tmin, a.tmax, stkN, stkT, stride, st)) {
+                        store_hit(a.hits, ray, st.h);
+                        store_counters(a.counters, ray, st.h);
+                    } else {
+                        active = true;
+                    }
+                }
+                next += taken;
+                idle = __ballot_sync(FULL, !active);
+            }
+        }
+        if (__ballot_sync(FULL, active) == 0) {
+            if (!tasks_left && next >= end) break;
+            continue;
+        }
+        if (active && cast_step(sc[sid], st, stkN, stkT, cyc, stride)) {
+            store_hit(a.hits, ray, st.h);
+            store_counters(a.counters, ray, st.h);
+            active = false;
+        }
+    }
+}
 
 template <int BLOCK, int MINB, bool SMEM_STACK>
 __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
@@ -83,25 +197,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
         if (r0 >= a.n) break;
         const uint32_t r1 = uint32_t(min(r0 + a.K, uint64_t(a.n)));
         for (uint32_t r = uint32_t(r0) + lane; r < r1; r += 32) {
-            int lo = 0, hi = int(a.S);
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (beg[mid] <= r) lo = mid;
-                else hi = mid;
-            }
+            const int lo = scene_of(beg, a.S, r);
             const float2* r2 = reinterpret_cast<const float2*>(a.rays + r);
             const float2 p = __ldg(r2), q = __ldg(r2 + 1), w = __ldg(r2 + 2);
             Hit h;
             cast_ray(sc[lo], p.x, p.y, q.x, q.y, w.x, w.y, a.tmin, a.tmax, stkN, stkT, cyc, stride, h);
             store_hit(a.hits, r, h);
-            if (a.counters) {
-                uint4 rc;
-                rc.x = (h.iters & 0xFFFFu) | (h.grid_reads << 16);
-                rc.y = h.dda_steps;
-                rc.z = (h.run_iters & 0xFFFFu) | (h.run_grid_reads << 16);
-                rc.w = h.run_dda_steps;
-                reinterpret_cast<uint4*>(a.counters)[r] = rc;
-            }
+            store_counters(a.counters, r, h);
         }
     }
 }
@@ -220,12 +322,12 @@ struct Variant {
 
 struct vx_batch {
     int device = 0;
-    int per_sm[4] = {0, 0, 0, 0};    // resident blocks per SM of each kernel variant (0 = not resolved)
+    int per_sm[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // resident blocks per SM of each kernel variant (0 = unresolved)
     uint32_t S = 0;
     int maxL = 1;
     vx::DevScene* scenes = nullptr;  // device copy of the scene table
     uint32_t* work = nullptr;        // task counter (device scratch)
-    vx_batch_tuning tuning{256, 128, 1, 0};
+    vx_batch_tuning tuning{256, 32, 1, 0};
     int num_sms = 148;
     cudaGraphExec_t frame = nullptr;
     cudaGraph_t frame_graph = nullptr;
@@ -245,12 +347,18 @@ size_t batch_smem(const vx_batch* b, bool smem_stack, int block) {
     return bytes;
 }
 
+template <int BLOCK, int MINB, bool SMEM, bool REFILL>
+constexpr void (*batch_kernel_ptr())(vx::BatchArgs) {
+    if constexpr (REFILL) return vx::batch_refill_kernel<BLOCK, MINB, SMEM>;
+    else return vx::batch_kernel<BLOCK, MINB, SMEM>;
+}
+
 // Resolves (once per batch and variant, outside any stream capture) the
 // dynamic shared-memory attribute and the resident blocks per SM.
-template <int BLOCK, int MINB, bool SMEM>
+template <int BLOCK, int MINB, bool SMEM, bool REFILL>
 int prepare_variant(vx_batch* b, int slot) {
     if (b->per_sm[slot]) return VX_OK;
-    auto kern = vx::batch_kernel<BLOCK, MINB, SMEM>;
+    auto kern = batch_kernel_ptr<BLOCK, MINB, SMEM, REFILL>();
     const size_t smem = batch_smem(b, SMEM, BLOCK);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
@@ -264,31 +372,48 @@ int prepare_variant(vx_batch* b, int slot) {
     return VX_OK;
 }
 
-template <int BLOCK, int MINB, bool SMEM>
+template <int BLOCK, int MINB, bool SMEM, bool REFILL>
 int launch_variant(vx_batch* b, int slot, const vx::BatchArgs& a, cudaStream_t st) {
-    if (int r = prepare_variant<BLOCK, MINB, SMEM>(b, slot)) return r;
-    vx::batch_kernel<BLOCK, MINB, SMEM><<<b->num_sms * b->per_sm[slot], BLOCK, batch_smem(b, SMEM, BLOCK), st>>>(a);
+    if (int r = prepare_variant<BLOCK, MINB, SMEM, REFILL>(b, slot)) return r;
+    auto kern = batch_kernel_ptr<BLOCK, MINB, SMEM, REFILL>();
+    kern<<<b->num_sms * b->per_sm[slot], BLOCK, batch_smem(b, SMEM, BLOCK), st>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch: launch");
     return VX_OK;
 }
 
-int launch_batch(vx_batch* b, const vx_batch_tuning& t, const vx::BatchArgs& a, cudaStream_t st) {
-    if (t.block == 128)
-        return t.stack_in_shared ? launch_variant<128, 6, true>(b, 0, a, st) : launch_variant<128, 6, false>(b, 1, a, st);
-    return t.stack_in_shared ? launch_variant<256, 3, true>(b, 2, a, st) : launch_variant<256, 3, false>(b, 3, a, st);
+template <bool PREPARE_ONLY>
+int dispatch_batch(vx_batch* b, const vx_batch_tuning& t, const vx::BatchArgs* a, cudaStream_t st) {
+    const int slot = (t.block == 128 ? 0 : 4) + (t.stack_in_shared ? 0 : 2) + (t.refill ? 1 : 0);
+#define VX_BATCH_CASE(SLOT, BLK, MINB, SMEM, REF)                                                      \
+    case SLOT:                                                                                          \
+        return PREPARE_ONLY ? prepare_variant<BLK, MINB, SMEM, REF>(b, SLOT)                            \
+                            : launch_variant<BLK, MINB, SMEM, REF>(b, SLOT, *a, st);
+    switch (slot) {
+        VX_BATCH_CASE(0, 128, 6, true, false)
+        VX_BATCH_CASE(1, 128, 4, true, true)
+        VX_BATCH_CASE(2, 128, 6, false, false)
+        VX_BATCH_CASE(3, 128, 4, false, true)
+        VX_BATCH_CASE(4, 256, 3, true, false)
+        VX_BATCH_CASE(5, 256, 2, true, true)
+        VX_BATCH_CASE(6, 256, 3, false, false)
+        VX_BATCH_CASE(7, 256, 2, false, true)
+    }
+#undef VX_BATCH_CASE
+    return fail(VX_EINVAL, "vx_cast_batch: no kernel variant for this tuning");
 }
 
-int prepare_batch(vx_batch* b, const vx_batch_tuning& t) {
-    if (t.block == 128)
-        return t.stack_in_shared ? prepare_variant<128, 6, true>(b, 0) : prepare_variant<128, 6, false>(b, 1);
-    return t.stack_in_shared ? prepare_variant<256, 3, true>(b, 2) : prepare_variant<256, 3, false>(b, 3);
+int launch_batch(vx_batch* b, const vx_batch_tuning& t, const vx::BatchArgs& a, cudaStream_t st) {
+    return dispatch_batch<false>(b, t, &a, st);
 }
+
+int prepare_batch(vx_batch* b, const vx_batch_tuning& t) { return dispatch_batch<true>(b, t, nullptr, nullptr); }
 
 int check_tuning(const vx_batch_tuning* t) {
     if (!t || (t->block != 128 && t->block != 256) || t->rays_per_task < 32 || t->rays_per_task > 65536 ||
-        (t->rays_per_task % 32) != 0)
-        return fail(VX_EINVAL, "batch tuning: block must be 128 or 256, rays_per_task a multiple of 32 in [32, 65536]");
+        (t->rays_per_task % 32) != 0 || t->refill < 0 || t->refill > 32)
+        return fail(VX_EINVAL, "batch tuning: block must be 128 or 256, rays_per_task a multiple of 32 in "
+                               "[32, 65536], refill in [0, 32]");
     return VX_OK;
 }
 
@@ -362,7 +487,7 @@ int vx_cast_batch(vx_batch* b, const vx_ray* rays, const uint32_t* begin, uint32
     if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch: reset work counter");
     if (n == 0) return VX_OK;
     vx::BatchArgs a{b->scenes, b->S, begin, rays, n, tmin, tmax, hits, counters, b->work,
-                    uint32_t(b->tuning.rays_per_task), b->maxL};
+                    uint32_t(b->tuning.rays_per_task), b->maxL, b->tuning.refill};
     return launch_batch(b, b->tuning, a, st);
 }
 
@@ -377,27 +502,34 @@ int vx_batch_autotune(vx_batch* b, const vx_ray* rays, const uint32_t* begin, ui
     vx_batch_tuning bt = b->tuning;
     const int blocks[] = {128, 256};
     const int ks[] = {32, 64, 128, 256, 512, 1024};
+    const int refills[] = {0, 8, 16, 24};
     for (int blk : blocks)
         for (int sm = 1; sm >= 0; --sm)
-            for (int k : ks) {
-                vx_batch_tuning t{blk, k, sm, 0};
-                vx::BatchArgs a{b->scenes, b->S, begin, rays, n, 0.0f, 3.402823466e+38f, hits, nullptr, b->work,
-                                uint32_t(k), b->maxL};
-                float ms_min = 1e30f;
-                for (int rep = 0; rep < 3; ++rep) {
-                    cudaMemsetAsync(b->work, 0, 4, st);
-                    cudaEventRecord(e0, st);
-                    int r = launch_batch(b, t, a, st);
-                    cudaEventRecord(e1, st);
-                    if (r != VX_OK) { cudaEventDestroy(e0); cudaEventDestroy(e1); return r; }
-                    cudaError_t e = cudaEventSynchronize(e1);
-                    if (e != cudaSuccess) { cudaEventDestroy(e0); cudaEventDestroy(e1); return cuda_err(e, "autotune"); }
-                    float ms = 0;
-                    cudaEventElapsedTime(&ms, e0, e1);
-                    if (rep > 0) ms_min = std::min(ms_min, ms);
+            for (int rf : refills)
+                for (int k : ks) {
+                    if (rf && k > 256) continue;  // refilling warps draw rays one round at a time
+                    vx_batch_tuning t{blk, k, sm, rf};
+                    vx::BatchArgs a{b->scenes, b->S, begin, rays, n, 0.0f, 3.402823466e+38f, hits, nullptr, b->work,
+                                    uint32_t(k), b->maxL, rf};
+                    float ms_min = 1e30f;
+                    for (int rep = 0; rep < 3; ++rep) {
+                        cudaMemsetAsync(b->work, 0, 4, st);
+                        cudaEventRecord(e0, st);
+                        int r = launch_batch(b, t, a, st);
+                        cudaEventRecord(e1, st);
+                        if (r != VX_OK) { cudaEventDestroy(e0); cudaEventDestroy(e1); return r; }
+                        cudaError_t e = cudaEventSynchronize(e1);
+                        if (e != cudaSuccess) {
+                            cudaEventDestroy(e0);
+                            cudaEventDestroy(e1);
+                            return cuda_err(e, "autotune");
+                        }
+                        float ms = 0;
+                        cudaEventElapsedTime(&ms, e0, e1);
+                        if (rep > 0) ms_min = std::min(ms_min, ms);
+                    }
+                    if (ms_min < best) { best = ms_min; bt = t; }
                 }
-                if (ms_min < best) { best = ms_min; bt = t; }
-            }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     b->tuning = bt;

@@ -164,10 +164,43 @@ struct Coef {
     int octant_mask;
 };
 
-// castRayImpl without LOD (SVOTraversal.cpp:516-691).
-__device__ void cast_ray(const DevScene& s, float ox, float oy, float oz, float ddx, float ddy, float ddz,
-                         float tMinArg, float tMaxArg, uint32_t* stkN, float* stkT, uint32_t* cyc, int stride,
-                         Hit& h) {
+// Everything castRayImpl carries from one loop iteration to the next, plus the
+// per-ray constants the iterations read.  cast_init fills it (the part of
+// castRayImpl before the loop); every cast_step runs one loop iteration.
+struct CastState {
+    Hit h;
+    // per-ray constants
+    float ox, oy, oz, dx, dy, dz, tEntry;
+    Coef c;
+    float rlx, rly, rlz;   // clamped ray-entry position in [0,1] (SVOBrickDDA.cpp:107-109)
+    RayB rb;
+    uint32_t brick2;       // ray-entry brick of the second lookup, read on first use
+    bool have_brick2;
+    // loop state (ESVOTraversalState, LaineKarrasOctree.h:229-257)
+    int scale, idx, iter;
+    uint32_t parent;
+    bool fetched;
+    float px, py, pz, scale_exp2, t_min, t_max, hh;
+    uint32_t mValid, mLeaf, pChild, pValid, pLeaf;
+    // cycle detection
+    uint32_t d1g, d1d;
+    int nrec;
+};
+
+__device__ __forceinline__ void cast_finish(CastState& st) {
+    st.h.iters = uint32_t(st.iter);
+    st.h.run_iters = st.h.iters;
+    st.h.run_grid_reads = st.h.grid_reads;
+    st.h.run_dda_steps = st.h.dda_steps;
+    if (st.iter >= MAX_ITER) st.h.flags |= F_ITER_CAP;
+}
+
+// castRayImpl up to its loop (SVOTraversal.cpp:516-586).  Returns true when the
+// ray is already finished (invalid input or no overlap with the world box).
+__device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy, float oz, float ddx, float ddy,
+                                          float ddz, float tMinArg, float tMaxArg, uint32_t* stkN, float* stkT,
+                                          int stride, CastState& st) {
+    Hit& h = st.h;
     h.t = 0.0f;
     h.brick = NONE;
     h.node = NONE;
@@ -180,18 +213,18 @@ __device__ void cast_ray(const DevScene& s, float ox, float oy, float oz, float 
     h.run_grid_reads = 0;
     h.run_dda_steps = 0;
     // validateRayInput (:238-259)
-    if (s.node_count == 0) { h.flags = F_INVALID; return; }
+    if (s.node_count == 0) { h.flags = F_INVALID; return true; }
     float dx, dy, dz;
     {
         const float dd = (ddx * ddx + ddy * ddy) + ddz * ddz;
         const float inv = 1.0f / sqrtf(dd);
         dx = ddx * inv; dy = ddy * inv; dz = ddz * inv;
         const float len = sqrtf((dx * dx + dy * dy) + dz * dz);
-        if (len < 1e-6f) { h.flags = F_INVALID; return; }
+        if (len < 1e-6f) { h.flags = F_INVALID; return true; }
         if (isnan(ox) || isnan(oy) || isnan(oz) || isnan(dx) || isnan(dy) || isnan(dz) || isinf(ox) ||
             isinf(oy) || isinf(oz) || isinf(dx) || isinf(dy) || isinf(dz)) {
             h.flags = F_INVALID;
-            return;
+            return true;
         }
     }
     const float wminx = s.wmin[0], wminy = s.wmin[1], wminz = s.wmin[2];
@@ -206,7 +239,7 @@ __device__ void cast_ray(const DevScene& s, float ox, float oy, float oz, float 
         for (int i = 0; i < 3; ++i) {
             float inv;
             if (fabsf(d[i]) < 1e-8f) {
-                if (o[i] < s.wmin[i] || o[i] > s.wmax[i]) return;
+                if (o[i] < s.wmin[i] || o[i] > s.wmax[i]) return true;
                 inv = (d[i] >= 0.0f) ? 1e20f : -1e20f;
             } else {
                 inv = 1.0f / d[i];
@@ -218,18 +251,18 @@ __device__ void cast_ray(const DevScene& s, float ox, float oy, float oz, float 
         }
         tEntry = max3(tnear[0], tnear[1], tnear[2]);
         tExit = min3(tfar[0], tfar[1], tfar[2]);
-        if (!(tEntry <= tExit && tExit >= 0.0f)) return;
+        if (!(tEntry <= tExit && tExit >= 0.0f)) return true;
     }
     tEntry = gmax(tEntry, tMinArg);
     tExit = gmin(tExit, tMaxArg);
-    if (tEntry >= tExit || tExit < 0.0f) return;
+    if (tEntry >= tExit || tExit < 0.0f) return true;
     const float tRayStart = inside ? 0.0f : gmax(0.0f, tEntry);
     const float wsx = s.wsize[0], wsy = s.wsize[1], wsz = s.wsize[2];
     const float nox = (ox + dx * tRayStart - wminx) / wsx + 1.0f;
     const float noy = (oy + dy * tRayStart - wminy) / wsy + 1.0f;
     const float noz = (oz + dz * tRayStart - wminz) / wsz + 1.0f;
     // computeRayCoefficients (:699-728)
-    Coef c;
+    Coef& c = st.c;
     {
         float sx = dx, sy = dy, sz = dz;
         if (fabsf(sx) < 1e-5f) sx = copysignf(1e-5f, sx);
@@ -257,19 +290,14 @@ __device__ void cast_ray(const DevScene& s, float ox, float oy, float oz, float 
         t_min = gmax(t_min, 0.0f);
         t_max = gmin(t_max, 1.0f);
     }
-    float hh = t_max;
     // initializeTraversalState (:261-280): stack[minScale..22] = root
     const int minScale = s.min_scale;
     for (int sc = minScale; sc <= ESVO_MAX_SCALE; ++sc) {
         stkN[(sc - minScale) * stride] = 0;
         stkT[(sc - minScale) * stride] = t_max;
     }
-    int scale = ESVO_MAX_SCALE;
-    uint32_t parent = 0;
-    bool fetched = false;
     int idx = 0;
     float px = 1.0f, py = 1.0f, pz = 1.0f;
-    float scale_exp2 = 0.5f;
     const bool csx = fabsf(dx) >= 1e-5f, csy = fabsf(dy) >= 1e-5f, csz = fabsf(dz) >= 1e-5f;
     // selectInitialOctant (:730-766)
     {
@@ -285,18 +313,11 @@ __device__ void cast_ray(const DevScene& s, float ox, float oy, float oz, float 
         else if (1.5f * c.tz_coef - c.tz_bias > t_min) { idx ^= 4; pz = 1.5f; }
     }
     // handleLeafHit quantities that depend on the ray only (SVOBrickDDA.cpp:98-121, 140-143, 165-166)
-    const float offx = (dx > 0) ? 0.001f : -0.001f;
-    const float offy = (dy > 0) ? 0.001f : -0.001f;
-    const float offz = (dz > 0) ? 0.001f : -0.001f;
     const float te0 = gmax(tEntry, 0.0f);
-    const float rwx = ox + dx * te0, rwy = oy + dy * te0, rwz = oz + dz * te0;
-    const float rlx = fclamp((rwx - wminx) / wsx, 0.001f, 0.999f);
-    const float rly = fclamp((rwy - wminy) / wsy, 0.001f, 0.999f);
-    const float rlz = fclamp((rwz - wminz) / wsz, 0.001f, 0.999f);
-    const int bmax = s.bpa - 1;
-    uint32_t brick2 = 0;      // ray-entry brick of the second lookup, read on first use
-    bool have_brick2 = false;
-    RayB rb;
+    st.rlx = fclamp(((ox + dx * te0) - wminx) / wsx, 0.001f, 0.999f);
+    st.rly = fclamp(((oy + dy * te0) - wminy) / wsy, 0.001f, 0.999f);
+    st.rlz = fclamp(((oz + dz * te0) - wminz) / wsz, 0.001f, 0.999f);
+    RayB& rb = st.rb;
     rb.lo[0] = ox + (0.0f - wminx);
     rb.lo[1] = oy + (0.0f - wminy);
     rb.lo[2] = oz + (0.0f - wminz);
@@ -307,260 +328,300 @@ __device__ void cast_ray(const DevScene& s, float ox, float oy, float oz, float 
         rb.tdel[i] = (fabsf(rb.d[i]) < 1e-8f) ? FLT_MAX_ : 1.0f / fabsf(rb.d[i]);
         rb.step[i] = (fabsf(rb.d[i]) < 1e-8f) ? 0 : ((rb.d[i] > 0.0f) ? 1 : -1);
     }
+    st.ox = ox; st.oy = oy; st.oz = oz;
+    st.dx = dx; st.dy = dy; st.dz = dz;
+    st.tEntry = tEntry;
+    st.brick2 = 0;
+    st.have_brick2 = false;
+    st.scale = ESVO_MAX_SCALE;
+    st.idx = idx;
+    st.iter = 0;
+    st.parent = 0;
+    st.fetched = false;
+    st.px = px; st.py = py; st.pz = pz;
+    st.scale_exp2 = 0.5f;
+    st.t_min = t_min;
+    st.t_max = t_max;
+    st.hh = t_max;
+    st.mValid = st.mLeaf = st.pChild = st.pValid = st.pLeaf = 0;
+    st.d1g = st.d1d = 0;
+    st.nrec = 0;
+    return false;
+}
 
-    uint32_t mValid = 0, mLeaf = 0, pChild = 0, pValid = 0, pLeaf = 0;
-    int iter = 0;
-    // Cycle detection.  The loop state (scale, idx, fetched, parent, pos,
-    // t_min, t_max, h) with the stack determines every later iteration, and a
-    // cycle only rewrites stack slots with the values they already hold.  So
-    // once the state repeats after one or two iterations the ray can neither
-    // hit nor leave before the 500-iteration cap: the result is the capped
-    // miss and the remaining iterations' counters repeat the cycle's.  The two
-    // previous states are kept in shared memory (cyc[k * stride], k < 8: one
-    // iteration back, k >= 8: two back) from iteration CYCLE_START on.
-    uint32_t d1g = 0, d1d = 0;
-    int nrec = 0;
-    while (scale >= minScale && scale <= ESVO_MAX_SCALE && iter < MAX_ITER) {
-        ++iter;
-        const uint32_t g0 = h.grid_reads, dd0 = h.dda_steps;
-        {  // one iteration; `goto next_iter` is the reference's `continue`
-            // fetchChildDescriptor (:282-293)
-            if (!fetched) {
-                const uint2 nd = __ldg(s.nodes + parent);
-                pChild = nd.x;
-                pValid = nd.y & 0xFFu;
-                pLeaf = (nd.y >> 8) & 0xFFu;
-                mValid = mirror_mask(pValid, c.octant_mask);
-                mLeaf = mirror_mask(pLeaf, c.octant_mask);
-                const uint32_t nonLeaf = ~mLeaf & 0xFFu;
-                fetched = (nonLeaf | (mValid << 8) | pChild) != 0u;
-            }
-            // Voxel corners at the iteration's position (computeVoxelCorners,
-            // :786-794) and the corrected tc_max (:768-784); checkChildValidity,
-            // PUSH and ADVANCE all evaluate them at this position and t_max.
-            const float tx = px * c.tx_coef - c.tx_bias;
-            const float ty = py * c.ty_coef - c.ty_bias;
-            const float tz = pz * c.tz_coef - c.tz_bias;
-            const float tcc = min3((csx && fabsf(tx) < 1000.0f) ? tx : t_max, (csy && fabsf(ty) < 1000.0f) ? ty : t_max,
-                                   (csz && fabsf(tz) < 1000.0f) ? tz : t_max);
-            // checkChildValidity (:295-326)
-            const bool child_valid = (mValid >> idx) & 1u;
-            bool isLeaf = (mLeaf >> idx) & 1u;
-            if (scale - minScale == s.brick_user_scale && child_valid) isLeaf = true;
-            float tv_max = 0.0f;
-            if (child_valid && !(t_min > t_max) && t_min <= (tv_max = gmin(t_max, tcc))) {
-                if (isLeaf) {
-                    // handleLeafHit (SVOBrickDDA.cpp:65-181)
-                    float lx = px, ly = py, lz = pz;
-                    if ((c.octant_mask & 1) == 0) lx = 3.0f - scale_exp2 - lx;
-                    if ((c.octant_mask & 2) == 0) ly = 3.0f - scale_exp2 - ly;
-                    if ((c.octant_mask & 4) == 0) lz = 3.0f - scale_exp2 - lz;
-                    const float ix = fclamp(csx ? (lx - 1.0f) + offx : rlx, 0.001f, 0.999f);
-                    const float iy = fclamp(csy ? (ly - 1.0f) + offy : rly, 0.001f, 0.999f);
-                    const float iz = fclamp(csz ? (lz - 1.0f) + offz : rlz, 0.001f, 0.999f);
-                    // Method 1: ESVO state position (x / 8 == x * 0.125 exactly)
-                    const float hx = fclamp(ix * wsx, 0.0f, s.wsm[0]);
-                    const float hy = fclamp(iy * wsy, 0.0f, s.wsm[1]);
-                    const float hz = fclamp(iz * wsz, 0.0f, s.wsm[2]);
-                    uint32_t brick = grid_lookup(s, iclamp(f2i(hx * 0.125f), 0, bmax),
-                                                 iclamp(f2i(hy * 0.125f), 0, bmax), iclamp(f2i(hz * 0.125f), 0, bmax));
+// One iteration of castRayImpl's loop (SVOTraversal.cpp:597-688), its loop
+// condition first.  Returns true when the ray is finished (hit, exit, cap).
+//
+// Cycle detection: the loop state (scale, idx, fetched, parent, pos, t_min,
+// t_max, h) with the stack determines every later iteration, and a cycle only
+// rewrites stack slots with the values they already hold.  So once the state
+// repeats after one or two iterations the ray can neither hit nor leave before
+// the 500-iteration cap: the result is the capped miss and the remaining
+// iterations' counters repeat the cycle's.  The two previous states are kept
+// in shared memory (cyc[k * stride], k < 8: one iteration back, k >= 8: two
+// back) from iteration CYCLE_START on.
+__device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint32_t* stkN, float* stkT,
+                                          uint32_t* cyc, int stride) {
+    Hit& h = st.h;
+    const Coef& c = st.c;
+    const int minScale = s.min_scale;
+    if (!(st.scale >= minScale && st.scale <= ESVO_MAX_SCALE && st.iter < MAX_ITER)) {
+        cast_finish(st);
+        return true;
+    }
+    const bool csx = fabsf(st.dx) >= 1e-5f, csy = fabsf(st.dy) >= 1e-5f, csz = fabsf(st.dz) >= 1e-5f;
+    ++st.iter;
+    const uint32_t g0 = h.grid_reads, dd0 = h.dda_steps;
+    {  // one iteration; `goto next_iter` is the reference's `continue`
+        // fetchChildDescriptor (:282-293)
+        if (!st.fetched) {
+            const uint2 nd = __ldg(s.nodes + st.parent);
+            st.pChild = nd.x;
+            st.pValid = nd.y & 0xFFu;
+            st.pLeaf = (nd.y >> 8) & 0xFFu;
+            st.mValid = mirror_mask(st.pValid, c.octant_mask);
+            st.mLeaf = mirror_mask(st.pLeaf, c.octant_mask);
+            const uint32_t nonLeaf = ~st.mLeaf & 0xFFu;
+            st.fetched = (nonLeaf | (st.mValid << 8) | st.pChild) != 0u;
+        }
+        // Voxel corners at the iteration's position (computeVoxelCorners,
+        // :786-794) and the corrected tc_max (:768-784); checkChildValidity,
+        // PUSH and ADVANCE all evaluate them at this position and t_max.
+        const float tx = st.px * c.tx_coef - c.tx_bias;
+        const float ty = st.py * c.ty_coef - c.ty_bias;
+        const float tz = st.pz * c.tz_coef - c.tz_bias;
+        const float tcc = min3((csx && fabsf(tx) < 1000.0f) ? tx : st.t_max,
+                               (csy && fabsf(ty) < 1000.0f) ? ty : st.t_max,
+                               (csz && fabsf(tz) < 1000.0f) ? tz : st.t_max);
+        // checkChildValidity (:295-326)
+        const bool child_valid = (st.mValid >> st.idx) & 1u;
+        bool isLeaf = (st.mLeaf >> st.idx) & 1u;
+        if (st.scale - minScale == s.brick_user_scale && child_valid) isLeaf = true;
+        float tv_max = 0.0f;
+        if (child_valid && !(st.t_min > st.t_max) && st.t_min <= (tv_max = gmin(st.t_max, tcc))) {
+            if (isLeaf) {
+                // handleLeafHit (SVOBrickDDA.cpp:65-181)
+                float lx = st.px, ly = st.py, lz = st.pz;
+                if ((c.octant_mask & 1) == 0) lx = 3.0f - st.scale_exp2 - lx;
+                if ((c.octant_mask & 2) == 0) ly = 3.0f - st.scale_exp2 - ly;
+                if ((c.octant_mask & 4) == 0) lz = 3.0f - st.scale_exp2 - lz;
+                const float ix = fclamp(csx ? (lx - 1.0f) + ((st.dx > 0) ? 0.001f : -0.001f) : st.rlx, 0.001f, 0.999f);
+                const float iy = fclamp(csy ? (ly - 1.0f) + ((st.dy > 0) ? 0.001f : -0.001f) : st.rly, 0.001f, 0.999f);
+                const float iz = fclamp(csz ? (lz - 1.0f) + ((st.dz > 0) ? 0.001f : -0.001f) : st.rlz, 0.001f, 0.999f);
+                const int bmax = s.bpa - 1;
+                // Method 1: ESVO state position (x / 8 == x * 0.125 exactly)
+                const float hx = fclamp(ix * s.wsize[0], 0.0f, s.wsm[0]);
+                const float hy = fclamp(iy * s.wsize[1], 0.0f, s.wsm[1]);
+                const float hz = fclamp(iz * s.wsize[2], 0.0f, s.wsm[2]);
+                uint32_t brick = grid_lookup(s, iclamp(f2i(hx * 0.125f), 0, bmax), iclamp(f2i(hy * 0.125f), 0, bmax),
+                                             iclamp(f2i(hz * 0.125f), 0, bmax));
+                ++h.grid_reads;
+                uint32_t method = 1;
+                if (brick == NONE) {
+                    // Method 2: ray entry position (the same brick for the whole ray)
+                    if (!st.have_brick2) {
+                        const float te0 = gmax(st.tEntry, 0.0f);
+                        const float ex = fclamp(((st.ox + st.dx * te0) - s.wmin[0]) + st.dx * 0.01f, 0.0f, s.wsm[0]);
+                        const float ey = fclamp(((st.oy + st.dy * te0) - s.wmin[1]) + st.dy * 0.01f, 0.0f, s.wsm[1]);
+                        const float ez = fclamp(((st.oz + st.dz * te0) - s.wmin[2]) + st.dz * 0.01f, 0.0f, s.wsm[2]);
+                        st.brick2 = grid_lookup(s, iclamp(f2i(ex * 0.125f), 0, bmax), iclamp(f2i(ey * 0.125f), 0, bmax),
+                                                iclamp(f2i(ez * 0.125f), 0, bmax));
+                        st.have_brick2 = true;
+                    }
+                    brick = st.brick2;
                     ++h.grid_reads;
-                    uint32_t method = 1;
-                    if (brick == NONE) {
-                        // Method 2: ray entry position (the same brick for the whole ray)
-                        if (!have_brick2) {
-                            const float ex = fclamp((rwx - wminx) + dx * 0.01f, 0.0f, s.wsm[0]);
-                            const float ey = fclamp((rwy - wminy) + dy * 0.01f, 0.0f, s.wsm[1]);
-                            const float ez = fclamp((rwz - wminz) + dz * 0.01f, 0.0f, s.wsm[2]);
-                            brick2 = grid_lookup(s, iclamp(f2i(ex * 0.125f), 0, bmax),
-                                                 iclamp(f2i(ey * 0.125f), 0, bmax), iclamp(f2i(ez * 0.125f), 0, bmax));
-                            have_brick2 = true;
-                        }
-                        brick = brick2;
-                        ++h.grid_reads;
-                        method = 2;
-                    }
-                    if (brick == NONE) {
-                        // Fallback 3: leaf child of the parent at the local octant
-                        // (leafToBrickView, SVORebuild.cpp:569-574)
-                        method = 3;
-                        const uint32_t lo = uint32_t(idx ^ (~c.octant_mask & 7));
-                        const uint32_t leafs = pValid & pLeaf;
-                        if ((leafs >> lo) & 1u) {
-                            const uint32_t ci = pChild + __popc(pValid & ~pLeaf & 0xFFu) +
-                                                __popc(leafs & ((1u << lo) - 1u));
-                            if (ci < s.node_count) {
-                                const uint32_t b = __ldg(s.node_brick + ci);
-                                if (b < s.brick_count) brick = b;
-                            }
-                        }
-                    }
-                    if (brick != NONE) {
-                        // traverseBrickAndReturnHit (SVOBrickDDA.cpp:187-225)
-                        const uint32_t bc = __ldg(s.coord + brick);
-                        const float bmn[3] = {float(int(bc & 0x3FFu) * 8), float(int((bc >> 10) & 0x3FFu) * 8),
-                                              float(int((bc >> 20) & 0x3FFu) * 8)};
-                        float tn[3], tf[3];
-#pragma unroll
-                        for (int i = 0; i < 3; ++i) {
-                            const float t0 = (bmn[i] - rb.lo[i]) * rb.inv[i];
-                            const float t1 = ((bmn[i] + 8.0f) - rb.lo[i]) * rb.inv[i];
-                            tn[i] = gmin(t0, t1);
-                            tf[i] = gmax(t0, t1);
-                        }
-                        const float btmin = gmax(gmax(gmax(tn[0], tn[1]), tn[2]), tEntry);
-                        const float btmax = gmin(gmin(tf[0], tf[1]), tf[2]);
-                        if (brick_dda(s, brick, bmn, rb, btmin, btmax, h)) {
-                            h.brick = brick;
-                            h.node = parent;
-                            h.flags |= method << 4;
-                            h.iters = uint32_t(iter);
-                            h.run_iters = h.iters;
-                            h.run_grid_reads = h.grid_reads;
-                            h.run_dda_steps = h.dda_steps;
-                            return;
-                        }
-                    }
-                    t_min = tv_max;
-                    // fall through to ADVANCE
-                } else {
-                    // executePushPhase (:328-378); tx_center etc. of checkChildValidity
-                    const float half = scale_exp2 * 0.5f;
-                    const float tx_center = half * c.tx_coef + tx;
-                    const float ty_center = half * c.ty_coef + ty;
-                    const float tz_center = half * c.tz_coef + tz;
-                    const float tc_max = min3(tx, ty, tz);
-                    if (tc_max < hh) {
-                        stkN[(scale - minScale) * stride] = parent;
-                        stkT[(scale - minScale) * stride] = t_max;
-                    }
-                    hh = tc_max;
-                    const int worldIdx = idx ^ (~c.octant_mask & 7);
-                    const uint32_t nonLeafMask = ~pLeaf & pValid & 0xFFu;
-                    const uint32_t child_index = pChild + __popc(nonLeafMask & ((1u << worldIdx) - 1u));
-                    if (child_index >= s.node_count) goto next_iter;
-                    parent = child_index;
-                    idx = 0;
-                    scale--;
-                    scale_exp2 = half;
-                    if (tx_center > t_min) { idx ^= 1; px += scale_exp2; }
-                    if (ty_center > t_min) { idx ^= 2; py += scale_exp2; }
-                    if (tz_center > t_min) { idx ^= 4; pz += scale_exp2; }
-                    t_max = tv_max;
-                    fetched = false;
-                    goto next_iter;
+                    method = 2;
                 }
-            }
-            // executeAdvancePhase (:380-416)
-            {
-                float tca = tcc;
-                if (tca == FLT_MAX_) tca = max3(csx ? tx : -FLT_MAX_, csy ? ty : -FLT_MAX_, csz ? tz : -FLT_MAX_);
-                int step_mask = 0;
-                if (csx && tx <= tca) { step_mask ^= 1; px -= scale_exp2; }
-                if (csy && ty <= tca) { step_mask ^= 2; py -= scale_exp2; }
-                if (csz && tz <= tca) { step_mask ^= 4; pz -= scale_exp2; }
-                t_min = gmax(tca, 0.0f);
-                idx ^= step_mask;
-                if ((idx & step_mask) == 0) goto next_iter;
-            }
-            // POP: step mask recomputed at the new position (:672-681)
-            int step_mask = 0;
-            {
-                const float ux = px * c.tx_coef - c.tx_bias;
-                const float uy = py * c.ty_coef - c.ty_bias;
-                const float uz = pz * c.tz_coef - c.tz_bias;
-                const float ucc = min3((csx && fabsf(ux) < 1000.0f) ? ux : t_max,
-                                       (csy && fabsf(uy) < 1000.0f) ? uy : t_max,
-                                       (csz && fabsf(uz) < 1000.0f) ? uz : t_max);
-                if (csx && ux <= ucc) step_mask ^= 1;
-                if (csy && uy <= ucc) step_mask ^= 2;
-                if (csz && uz <= ucc) step_mask ^= 4;
-            }
-            // executePopPhase (:418-510)
-            if (scale == ESVO_MAX_SCALE) {
-                if (t_min > t_max || px < 1.0f || px >= 2.0f || py < 1.0f || py >= 2.0f || pz < 1.0f || pz >= 2.0f)
-                    break;
-                fetched = false;
+                if (brick == NONE) {
+                    // Fallback 3: leaf child of the parent at the local octant
+                    // (leafToBrickView, SVORebuild.cpp:569-574)
+                    method = 3;
+                    const uint32_t lo = uint32_t(st.idx ^ (~c.octant_mask & 7));
+                    const uint32_t leafs = st.pValid & st.pLeaf;
+                    if ((leafs >> lo) & 1u) {
+                        const uint32_t ci = st.pChild + __popc(st.pValid & ~st.pLeaf & 0xFFu) +
+                                            __popc(leafs & ((1u << lo) - 1u));
+                        if (ci < s.node_count) {
+                            const uint32_t b = __ldg(s.node_brick + ci);
+                            if (b < s.brick_count) brick = b;
+                        }
+                    }
+                }
+                if (brick != NONE) {
+                    // traverseBrickAndReturnHit (SVOBrickDDA.cpp:187-225)
+                    const uint32_t bc = __ldg(s.coord + brick);
+                    const float bmn[3] = {float(int(bc & 0x3FFu) * 8), float(int((bc >> 10) & 0x3FFu) * 8),
+                                          float(int((bc >> 20) & 0x3FFu) * 8)};
+                    float tn[3], tf[3];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        const float t0 = (bmn[i] - st.rb.lo[i]) * st.rb.inv[i];
+                        const float t1 = ((bmn[i] + 8.0f) - st.rb.lo[i]) * st.rb.inv[i];
+                        tn[i] = gmin(t0, t1);
+                        tf[i] = gmax(t0, t1);
+                    }
+                    const float btmin = gmax(gmax(gmax(tn[0], tn[1]), tn[2]), st.tEntry);
+                    const float btmax = gmin(gmin(tf[0], tf[1]), tf[2]);
+                    if (brick_dda(s, brick, bmn, st.rb, btmin, btmax, h)) {
+                        h.brick = brick;
+                        h.node = st.parent;
+                        h.flags |= method << 4;
+                        h.iters = uint32_t(st.iter);
+                        h.run_iters = h.iters;
+                        h.run_grid_reads = h.grid_reads;
+                        h.run_dda_steps = h.dda_steps;
+                        return true;
+                    }
+                }
+                st.t_min = tv_max;
+                // fall through to ADVANCE
+            } else {
+                // executePushPhase (:328-378); tx_center etc. of checkChildValidity
+                const float half = st.scale_exp2 * 0.5f;
+                const float tx_center = half * c.tx_coef + tx;
+                const float ty_center = half * c.ty_coef + ty;
+                const float tz_center = half * c.tz_coef + tz;
+                const float tc_max = min3(tx, ty, tz);
+                if (tc_max < st.hh) {
+                    stkN[(st.scale - minScale) * stride] = st.parent;
+                    stkT[(st.scale - minScale) * stride] = st.t_max;
+                }
+                st.hh = tc_max;
+                const int worldIdx = st.idx ^ (~c.octant_mask & 7);
+                const uint32_t nonLeafMask = ~st.pLeaf & st.pValid & 0xFFu;
+                const uint32_t child_index = st.pChild + __popc(nonLeafMask & ((1u << worldIdx) - 1u));
+                if (child_index >= s.node_count) goto next_iter;
+                st.parent = child_index;
+                st.idx = 0;
+                st.scale--;
+                st.scale_exp2 = half;
+                if (tx_center > st.t_min) { st.idx ^= 1; st.px += st.scale_exp2; }
+                if (ty_center > st.t_min) { st.idx ^= 2; st.py += st.scale_exp2; }
+                if (tz_center > st.t_min) { st.idx ^= 4; st.pz += st.scale_exp2; }
+                st.t_max = tv_max;
+                st.fetched = false;
                 goto next_iter;
             }
-            {
-                // floatToInt: std::max(0, std::min(f, 1)), * 2^22, std::min(., 2^22-1),
-                // std::max(0, .), truncate (SVOTraversal.cpp:439-442)
-                auto f2q = [](float f) -> uint32_t {
-                    const float m1 = (1.0f < f) ? 1.0f : f;
-                    const float cl = (0.0f < m1) ? m1 : 0.0f;
-                    const float sc = cl * 4194304.0f;
-                    const float m2 = (4194303.0f < sc) ? 4194303.0f : sc;
-                    return uint32_t((0.0f < m2) ? m2 : 0.0f);
-                };
-                uint32_t qx = f2q(gmax(0.0f, px - 1.0f));
-                uint32_t qy = f2q(gmax(0.0f, py - 1.0f));
-                uint32_t qz = f2q(gmax(0.0f, pz - 1.0f));
-                uint32_t diff = 0;
-                if (step_mask & 1) diff |= qx ^ f2q(gmax(0.0f, px + scale_exp2 - 1.0f));
-                if (step_mask & 2) diff |= qy ^ f2q(gmax(0.0f, py + scale_exp2 - 1.0f));
-                if (step_mask & 4) diff |= qz ^ f2q(gmax(0.0f, pz + scale_exp2 - 1.0f));
-                if (diff == 0) break;
-                scale = 31 - __clz(diff);
-                if (scale < minScale || scale > ESVO_MAX_SCALE) break;
-                scale_exp2 = __int_as_float((scale - ESVO_MAX_SCALE + 127) << 23);
-                parent = stkN[(scale - minScale) * stride];
-                t_max = stkT[(scale - minScale) * stride];
-                const uint32_t mask = ~((1u << (ESVO_MAX_SCALE - scale)) - 1u);
-                qx &= mask; qy &= mask; qz &= mask;
-                px = 1.0f + float(qx) / 4194304.0f;
-                py = 1.0f + float(qy) / 4194304.0f;
-                pz = 1.0f + float(qz) / 4194304.0f;
-                const int sh = ESVO_MAX_SCALE - scale - 1;
-                if (sh < 0 || sh >= 32) idx = 0;
-                else idx = int(((qx >> sh) & 1u) | (((qy >> sh) & 1u) << 1) | (((qz >> sh) & 1u) << 2));
-                hh = 0.0f;
-                fetched = false;
-            }
         }
-    next_iter:
-        if (iter >= CYCLE_START) {
-            uint32_t cur[8];
-            cur[0] = uint32_t(scale) | (uint32_t(idx) << 8) | (uint32_t(fetched) << 16);
-            cur[1] = parent;
-            cur[2] = __float_as_uint(px); cur[3] = __float_as_uint(py); cur[4] = __float_as_uint(pz);
-            cur[5] = __float_as_uint(t_min); cur[6] = __float_as_uint(t_max); cur[7] = __float_as_uint(hh);
-            const uint32_t dg = h.grid_reads - g0, ddd = h.dda_steps - dd0;
-            bool eq1 = nrec >= 1, eq2 = nrec >= 2;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const uint32_t a = cyc[k * stride], b = cyc[(k + 8) * stride];
-                eq1 = eq1 && (cur[k] == a);
-                eq2 = eq2 && (cur[k] == b);
-                cyc[(k + 8) * stride] = a;
-                cyc[k * stride] = cur[k];
+        // executeAdvancePhase (:380-416)
+        {
+            float tca = tcc;
+            if (tca == FLT_MAX_) tca = max3(csx ? tx : -FLT_MAX_, csy ? ty : -FLT_MAX_, csz ? tz : -FLT_MAX_);
+            int step_mask = 0;
+            if (csx && tx <= tca) { step_mask ^= 1; st.px -= st.scale_exp2; }
+            if (csy && ty <= tca) { step_mask ^= 2; st.py -= st.scale_exp2; }
+            if (csz && tz <= tca) { step_mask ^= 4; st.pz -= st.scale_exp2; }
+            st.t_min = gmax(tca, 0.0f);
+            st.idx ^= step_mask;
+            if ((st.idx & step_mask) == 0) goto next_iter;
+        }
+        // POP: step mask recomputed at the new position (:672-681)
+        int step_mask = 0;
+        {
+            const float ux = st.px * c.tx_coef - c.tx_bias;
+            const float uy = st.py * c.ty_coef - c.ty_bias;
+            const float uz = st.pz * c.tz_coef - c.tz_bias;
+            const float ucc = min3((csx && fabsf(ux) < 1000.0f) ? ux : st.t_max,
+                                   (csy && fabsf(uy) < 1000.0f) ? uy : st.t_max,
+                                   (csz && fabsf(uz) < 1000.0f) ? uz : st.t_max);
+            if (csx && ux <= ucc) step_mask ^= 1;
+            if (csy && uy <= ucc) step_mask ^= 2;
+            if (csz && uz <= ucc) step_mask ^= 4;
+        }
+        // executePopPhase (:418-510)
+        if (st.scale == ESVO_MAX_SCALE) {
+            if (st.t_min > st.t_max || st.px < 1.0f || st.px >= 2.0f || st.py < 1.0f || st.py >= 2.0f ||
+                st.pz < 1.0f || st.pz >= 2.0f) {
+                cast_finish(st);
+                return true;
             }
-            if (eq1 || eq2) {
-                const uint32_t rem = uint32_t(MAX_ITER - iter);
-                h.run_iters = uint32_t(iter);
-                h.run_grid_reads = h.grid_reads;
-                h.run_dda_steps = h.dda_steps;
-                if (eq1) {
-                    h.grid_reads += rem * dg;
-                    h.dda_steps += rem * ddd;
-                } else {
-                    h.grid_reads += ((rem + 1) / 2) * d1g + (rem / 2) * dg;
-                    h.dda_steps += ((rem + 1) / 2) * d1d + (rem / 2) * ddd;
-                }
-                h.iters = uint32_t(MAX_ITER);
-                h.flags |= F_ITER_CAP;
-                return;
-            }
-            ++nrec;
-            d1g = dg;
-            d1d = ddd;
+            st.fetched = false;
+            goto next_iter;
+        }
+        {
+            // floatToInt: std::max(0, std::min(f, 1)), * 2^22, std::min(., 2^22-1),
+            // std::max(0, .), truncate (SVOTraversal.cpp:439-442)
+            auto f2q = [](float f) -> uint32_t {
+                const float m1 = (1.0f < f) ? 1.0f : f;
+                const float cl = (0.0f < m1) ? m1 : 0.0f;
+                const float sc = cl * 4194304.0f;
+                const float m2 = (4194303.0f < sc) ? 4194303.0f : sc;
+                return uint32_t((0.0f < m2) ? m2 : 0.0f);
+            };
+            uint32_t qx = f2q(gmax(0.0f, st.px - 1.0f));
+            uint32_t qy = f2q(gmax(0.0f, st.py - 1.0f));
+            uint32_t qz = f2q(gmax(0.0f, st.pz - 1.0f));
+            uint32_t diff = 0;
+            if (step_mask & 1) diff |= qx ^ f2q(gmax(0.0f, st.px + st.scale_exp2 - 1.0f));
+            if (step_mask & 2) diff |= qy ^ f2q(gmax(0.0f, st.py + st.scale_exp2 - 1.0f));
+            if (step_mask & 4) diff |= qz ^ f2q(gmax(0.0f, st.pz + st.scale_exp2 - 1.0f));
+            if (diff == 0) { cast_finish(st); return true; }
+            st.scale = 31 - __clz(diff);
+            if (st.scale < minScale || st.scale > ESVO_MAX_SCALE) { cast_finish(st); return true; }
+            st.scale_exp2 = __int_as_float((st.scale - ESVO_MAX_SCALE + 127) << 23);
+            st.parent = stkN[(st.scale - minScale) * stride];
+            st.t_max = stkT[(st.scale - minScale) * stride];
+            const uint32_t mask = ~((1u << (ESVO_MAX_SCALE - st.scale)) - 1u);
+            qx &= mask; qy &= mask; qz &= mask;
+            st.px = 1.0f + float(qx) / 4194304.0f;
+            st.py = 1.0f + float(qy) / 4194304.0f;
+            st.pz = 1.0f + float(qz) / 4194304.0f;
+            const int sh = ESVO_MAX_SCALE - st.scale - 1;
+            if (sh < 0 || sh >= 32) st.idx = 0;
+            else st.idx = int(((qx >> sh) & 1u) | (((qy >> sh) & 1u) << 1) | (((qz >> sh) & 1u) << 2));
+            st.hh = 0.0f;
+            st.fetched = false;
         }
     }
-    h.iters = uint32_t(iter);
-    h.run_iters = h.iters;
-    h.run_grid_reads = h.grid_reads;
-    h.run_dda_steps = h.dda_steps;
-    if (iter >= MAX_ITER) h.flags |= F_ITER_CAP;
+next_iter:
+    if (st.iter >= CYCLE_START) {
+        uint32_t cur[8];
+        cur[0] = uint32_t(st.scale) | (uint32_t(st.idx) << 8) | (uint32_t(st.fetched) << 16);
+        cur[1] = st.parent;
+        cur[2] = __float_as_uint(st.px); cur[3] = __float_as_uint(st.py); cur[4] = __float_as_uint(st.pz);
+        cur[5] = __float_as_uint(st.t_min); cur[6] = __float_as_uint(st.t_max); cur[7] = __float_as_uint(st.hh);
+        const uint32_t dg = h.grid_reads - g0, ddd = h.dda_steps - dd0;
+        bool eq1 = st.nrec >= 1, eq2 = st.nrec >= 2;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t a = cyc[k * stride], b = cyc[(k + 8) * stride];
+            eq1 = eq1 && (cur[k] == a);
+            eq2 = eq2 && (cur[k] == b);
+            cyc[(k + 8) * stride] = a;
+            cyc[k * stride] = cur[k];
+        }
+        if (eq1 || eq2) {
+            const uint32_t rem = uint32_t(MAX_ITER - st.iter);
+            h.run_iters = uint32_t(st.iter);
+            h.run_grid_reads = h.grid_reads;
+            h.run_dda_steps = h.dda_steps;
+            if (eq1) {
+                h.grid_reads += rem * dg;
+                h.dda_steps += rem * ddd;
+            } else {
+                h.grid_reads += ((rem + 1) / 2) * st.d1g + (rem / 2) * dg;
+                h.dda_steps += ((rem + 1) / 2) * st.d1d + (rem / 2) * ddd;
+            }
+            h.iters = uint32_t(MAX_ITER);
+            h.flags |= F_ITER_CAP;
+            return true;
+        }
+        ++st.nrec;
+        st.d1g = dg;
+        st.d1d = ddd;
+    }
+    return false;
+}
+
+// castRayImpl without LOD (SVOTraversal.cpp:516-691): setup, then the loop.
+__device__ __forceinline__ void cast_ray(const DevScene& s, float ox, float oy, float oz, float ddx, float ddy,
+                                         float ddz, float tMinArg, float tMaxArg, uint32_t* stkN, float* stkT,
+                                         uint32_t* cyc, int stride, Hit& h) {
+    CastState st;
+    if (!cast_init(s, ox, oy, oz, ddx, ddy, ddz, tMinArg, tMaxArg, stkN, stkT, stride, st))
+        while (!cast_step(s, st, stkN, stkT, cyc, stride)) {
+        }
+    h = st.h;
 }
 
 // DXT1 texel of the hit voxel: decodeColorHead (DXT1Compressor.cpp:14-36)
