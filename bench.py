@@ -260,8 +260,13 @@ def measure_cfg4(args, rank, world, steps, warmup):
     bh = torch.zeros((2 * n, 4), dtype=torch.int32, device="cuda")
     bounce = torch.zeros((2 * n, 6), dtype=torch.float32, device="cuda")
     batch = vx.Batch(scenes)
-    tuning, tune_ms = batch.autotune(d_rays, d_begin, ph)
     seed = 77
+    # Tune each pass on its own rays: the bounce pass is tuned on the bounce rays of this frame.
+    tuning, tune_ms = batch.autotune(d_rays, d_begin, ph)
+    vx.spawn_bounce_rays(d_rays, ph, seed, bounce)
+    btuning, btune_ms = batch.autotune(bounce, d_bbegin, bh)
+    batch.set_tuning(tuning.block, tuning.rays_per_task, tuning.stack_in_shared, tuning.refill)
+    batch.set_bounce_tuning(btuning)
 
     def plain_frame():
         for i, sc in enumerate(scenes):
@@ -321,7 +326,8 @@ def measure_cfg4(args, rank, world, steps, warmup):
                        "scene_R": [sp.R for sp in specs], "setup_s": setup_s,
                        "l2": "flushed before every timed frame (256 MiB write)"},
             "batched": {"value": value, "unit": "Mrays/s", "ms_per_frame": batched_total / steps,
-                        "tuning": tuning.as_dict(), "autotune_best_ms_primary": tune_ms},
+                        "tuning": tuning.as_dict(), "autotune_best_ms_primary": tune_ms,
+                        "bounce_tuning": btuning.as_dict(), "autotune_best_ms_bounce": btune_ms},
             "plain": {"value": plain_value, "unit": "Mrays/s", "ms_per_frame": plain_total / steps,
                       "launches_per_frame": 2 * len(specs) + 1},
             "speedup_batched_vs_plain": plain_total / batched_total,

@@ -116,15 +116,17 @@ typedef struct vx_ray {
 
 /* Hit record, 16 bytes.  Replaces ISVOStructure::RayHit
  * (SVO/include/ISVOStructure.h:101-112): tMin -> t, entity -> (brick, voxel),
- * normal -> flags; tMax = t + 1, scale = max_levels - 1 and
- * hitPoint = origin + normalize(dir) * t follow from these. */
+ * normal -> flags; tMax = t + 1 and hitPoint = origin + normalize(dir) * t
+ * follow from these. */
 typedef struct vx_hit {
     float t;          /* hit distance along the normalised direction, world units */
-    uint32_t brick;   /* brick index, 0xFFFFFFFF on a miss */
+    uint32_t brick;   /* brick index, 0xFFFFFFFF on a miss (and on an LOD hit) */
     uint32_t node;    /* index of the parent descriptor at the leaf */
     uint16_t voxel;   /* voxel within the brick, z*64+y*8+x; 0xFFFF on a miss */
     uint8_t flags;    /* VX_HIT_* / VX_RAY_* */
-    uint8_t reserved;
+    uint8_t scale;    /* RayHit::scale: max_levels - 1 for a voxel hit
+                         (SVOBrickDDA.cpp:509), the cell's user scale for an
+                         LOD hit, 0 on a miss */
 } vx_hit;
 
 /* Per-ray work counters (optional output, for algorithmic-byte accounting),
@@ -193,6 +195,38 @@ int vx_cast_rays(const vx_scene* scene, const vx_ray* rays_dev, uint32_t n,
 int vx_cast_rays_host(const vx_scene* scene, const vx_ray* rays_host, uint32_t n,
                       float t_min, float t_max, vx_hit* hits_host, void* color_host,
                       void* stream);
+
+/* ------------------------------------------------------------------------
+ * Screen-space LOD cut.  Replaces LaineKarrasOctree::castRayWithLOD /
+ * castRayScreenSpaceLOD / castRayLOD (SVO/src/SVOTraversal.cpp:198-232, the
+ * termination test :613-651) and LODParameters (SVO/include/SVOLOD.h:50-177).
+ * Every processed child cell whose entry distance d satisfies
+ * d * ray_dir_size + ray_orig_size >= cell size ends the ray with an LOD hit:
+ * t = d, flags = VX_HIT_HIT with the +y normal, brick 0xFFFFFFFF, voxel
+ * 0xFFFF, node = the parent descriptor of the cell, scale = the cell's user
+ * scale (esvoToUserScale, LaineKarrasOctree.h:381-383); colour zeros.
+ * ray_dir_size <= 0 disables the cut (results equal vx_cast_rays).
+ * castRayLOD(bias) is {0, bias}; castRayScreenSpaceLOD(fovY, H) is
+ * vx_lod_from_camera(fovY, H, 0).
+ * --------------------------------------------------------------------- */
+typedef struct vx_lod_params {
+    float ray_orig_size;  /* cone diameter at the ray origin, world units */
+    float ray_dir_size;   /* cone diameter growth per unit distance */
+} vx_lod_params;
+
+/* LODParameters::fromCameraWithNearPlane (near_plane = 0: fromCamera),
+ * SVOLOD.h:83-119: ray_dir_size = 2 tan(fov_y / screen_height / 2),
+ * ray_orig_size = near_plane * ray_dir_size.  Host arithmetic. */
+int vx_lod_from_camera(float fov_y, int32_t screen_height, float near_plane, vx_lod_params* out);
+/* LODParameters::withBias (SVOLOD.h:169-176): both sizes times 2^bias. */
+int vx_lod_with_bias(const vx_lod_params* in, float bias, vx_lod_params* out);
+
+int vx_cast_rays_lod(const vx_scene* scene, const vx_ray* rays_dev, uint32_t n,
+                     float t_min, float t_max, const vx_lod_params* lod, vx_hit* hits_dev,
+                     void* color_dev, vx_ray_counters* counters_dev, void* stream);
+int vx_cast_rays_host_lod(const vx_scene* scene, const vx_ray* rays_host, uint32_t n,
+                          float t_min, float t_max, const vx_lod_params* lod, vx_hit* hits_host,
+                          void* color_host, void* stream);
 
 /* ------------------------------------------------------------------------
  * Frame render.  Replaces ComputeDispatchNode's
@@ -284,6 +318,10 @@ int vx_batch_capture_frame(vx_batch* batch, const vx_ray* primary_dev, const uin
                            const uint32_t* bounce_begin_dev, vx_hit* bounce_hits_dev, uint64_t seed,
                            void* stream);
 int vx_batch_launch_frame(vx_batch* batch, void* stream);
+/* Tuning of the bounce pass of a captured frame (default, or after a null
+ * tuning: the batch's own).  Incoherent bounce rays favour other shapes than
+ * camera rays: autotune each pass on its own rays.  Applies to later captures. */
+int vx_batch_set_bounce_tuning(vx_batch* batch, const vx_batch_tuning* tuning);
 
 /* ------------------------------------------------------------------------
  * Differentiable form (no reference counterpart).  The traversal is discrete

@@ -4,6 +4,8 @@
 // (SVO/src/SVOTraversal.cpp:189-196): a single ray returns a RayHit with
 // hit / tMin / tMax / hitPoint / normal / scale and the hit voxel's integer
 // position in place of the ECS entity.  castRays() casts a batch in one call.
+// castRayWithLOD / castRayLOD / castRayScreenSpaceLOD and LODParameters follow
+// SVOTraversal.cpp:198-232 and SVO/include/SVOLOD.h:50-177.
 //
 // Header-only; link with libvx.so.  No glm dependency: positions are float[3].
 #pragma once
@@ -26,15 +28,42 @@ struct Vec3 {
 struct RayHit {
     bool hit = false;
     float tMin = 0.0f;       // distance along the normalised direction
-    float tMax = 0.0f;       // tMin + voxel size (1)
+    float tMax = 0.0f;       // tMin + voxel size (1; the cell size for an LOD hit)
     Vec3 hitPoint;           // origin + normalize(direction) * tMin
-    Vec3 normal;             // entry face, +-1 on one axis
-    int scale = 0;           // maxLevels - 1
-    uint32_t brick = 0xFFFFFFFFu;
+    Vec3 normal;             // entry face, +-1 on one axis; +y for an LOD hit
+    int scale = 0;           // maxLevels - 1; the cell's user scale for an LOD hit
+    uint32_t brick = 0xFFFFFFFFu;  // 0xFFFFFFFF for an LOD hit (no entity)
     uint32_t voxel = 0xFFFFu;  // z*64 + y*8 + x within the brick
     uint32_t node = 0xFFFFFFFFu;
     int32_t voxelPos[3] = {0, 0, 0};  // integer position of the hit voxel (the entity's key)
     uint8_t flags = 0;
+};
+
+// LODParameters (SVOLOD.h:50-177).
+struct LODParameters {
+    float rayOrigSize = 0.0f;  // cone diameter at the origin
+    float rayDirSize = 0.0f;   // cone growth per unit distance; 0 disables the cut
+
+    static LODParameters fromCamera(float fovY, int screenHeight) {
+        return fromCameraWithNearPlane(fovY, screenHeight, 0.0f);
+    }
+    static LODParameters fromCameraWithNearPlane(float fovY, int screenHeight, float nearPlane) {
+        vx_lod_params p{};
+        if (vx_lod_from_camera(fovY, screenHeight, nearPlane, &p) != VX_OK)
+            throw std::invalid_argument(vx_last_error_string());
+        return {p.ray_orig_size, p.ray_dir_size};
+    }
+    float getProjectedPixelSize(float voxelDistance) const { return voxelDistance * rayDirSize + rayOrigSize; }
+    bool shouldTerminate(float voxelDistance, float voxelSize) const {
+        return getProjectedPixelSize(voxelDistance) >= voxelSize;
+    }
+    bool isEnabled() const { return rayDirSize > 0.0f; }
+    LODParameters withBias(float bias) const {
+        const vx_lod_params in{rayOrigSize, rayDirSize};
+        vx_lod_params p{};
+        vx_lod_with_bias(&in, bias, &p);
+        return {p.ray_orig_size, p.ray_dir_size};
+    }
 };
 
 class Error : public std::runtime_error {
@@ -71,13 +100,40 @@ public:
         return toRayHit(r, h);
     }
 
+    // LaineKarrasOctree::castRayWithLOD(origin, direction, lodParams, tMin, tMax).
+    RayHit castRayWithLOD(const Vec3& origin, const Vec3& direction, const LODParameters& lod,
+                          float tMin = 0.0f, float tMax = 3.402823466e+38f) const {
+        vx_ray r{origin.x, origin.y, origin.z, direction.x, direction.y, direction.z};
+        vx_hit h{};
+        const vx_lod_params p{lod.rayOrigSize, lod.rayDirSize};
+        check(vx_cast_rays_host_lod(scene_, &r, 1, tMin, tMax, &p, &h, nullptr, nullptr));
+        return toRayHit(r, h);
+    }
+    // castRayLOD(origin, direction, lodBias, ...): the bias is the cone spread.
+    RayHit castRayLOD(const Vec3& origin, const Vec3& direction, float lodBias, float tMin = 0.0f,
+                      float tMax = 3.402823466e+38f) const {
+        return castRayWithLOD(origin, direction, LODParameters{0.0f, lodBias}, tMin, tMax);
+    }
+    // castRayScreenSpaceLOD(origin, direction, fovY, screenHeight, ...).
+    RayHit castRayScreenSpaceLOD(const Vec3& origin, const Vec3& direction, float fovY, int screenHeight,
+                                 float tMin = 0.0f, float tMax = 3.402823466e+38f) const {
+        return castRayWithLOD(origin, direction, LODParameters::fromCamera(fovY, screenHeight), tMin, tMax);
+    }
+
     // Batch form: one host->device copy, one launch, one copy back.
     std::vector<RayHit> castRays(const std::vector<vx_ray>& rays, float tMin = 0.0f,
-                                 float tMax = 3.402823466e+38f) const {
+                                 float tMax = 3.402823466e+38f, const LODParameters* lod = nullptr) const {
         std::vector<vx_hit> hits(rays.size());
-        if (!rays.empty())
-            check(vx_cast_rays_host(scene_, rays.data(), uint32_t(rays.size()), tMin, tMax, hits.data(),
-                                    nullptr, nullptr));
+        if (!rays.empty()) {
+            if (lod) {
+                const vx_lod_params p{lod->rayOrigSize, lod->rayDirSize};
+                check(vx_cast_rays_host_lod(scene_, rays.data(), uint32_t(rays.size()), tMin, tMax, &p, hits.data(),
+                                            nullptr, nullptr));
+            } else {
+                check(vx_cast_rays_host(scene_, rays.data(), uint32_t(rays.size()), tMin, tMax, hits.data(),
+                                        nullptr, nullptr));
+            }
+        }
         std::vector<RayHit> out(rays.size());
         for (size_t i = 0; i < rays.size(); ++i) out[i] = toRayHit(rays[i], hits[i]);
         return out;
@@ -93,6 +149,18 @@ private:
         o.tMax = h.t + 1.0f;
         const float dd = (r.dx * r.dx + r.dy * r.dy) + r.dz * r.dz;
         const float inv = 1.0f / std::sqrt(dd);
+        if (h.brick == 0xFFFFFFFFu) {
+            // LOD hit (SVOTraversal.cpp:639-649): hitPoint = origin + dir * t,
+            // tMax = t + 2^(scale - maxLevels) * worldSize.x, normal +y.
+            const float size = std::ldexp(1.0f, int(h.scale) - cfg_.max_levels) *
+                               (cfg_.world_max[0] - cfg_.world_min[0]);
+            o.tMax = h.t + size;
+            o.hitPoint = {r.ox + (r.dx * inv) * h.t, r.oy + (r.dy * inv) * h.t, r.oz + (r.dz * inv) * h.t};
+            o.normal = {0.0f, 1.0f, 0.0f};
+            o.scale = h.scale;
+            o.node = h.node;
+            return o;
+        }
         // hitPoint in local space, then back to world (SVOBrickDDA.cpp:508, 174)
         o.hitPoint = {((r.ox + (0.0f - cfg_.world_min[0])) + (r.dx * inv) * h.t) + cfg_.world_min[0],
                       ((r.oy + (0.0f - cfg_.world_min[1])) + (r.dy * inv) * h.t) + cfg_.world_min[1],
@@ -100,7 +168,7 @@ private:
         const int axis = (h.flags & VX_HIT_AXIS_MASK) >> 1;
         const float s = (h.flags & VX_HIT_NORMAL_NEG) ? -1.0f : 1.0f;
         o.normal = {axis == 0 ? s : 0.0f, axis == 1 ? s : 0.0f, axis == 2 ? s : 0.0f};
-        o.scale = cfg_.max_levels - 1;
+        o.scale = h.scale;
         o.brick = h.brick;
         o.voxel = h.voxel;
         o.node = h.node;

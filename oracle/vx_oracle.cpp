@@ -703,9 +703,14 @@ bool handleLeafHit(const vxo_scene& s, const State& st, const Coef& c, V3 origin
     return r;
 }
 
-// LaineKarrasOctree::castRayImpl without LOD (SVOTraversal.cpp:516-691)
+// LODParameters (SVO/include/SVOLOD.h:50-177): cone diameter at the origin and
+// its growth per unit distance; LOD is on when rayDirSize > 0 (:156-158).
+struct Lod { float rayOrigSize = 0.0f, rayDirSize = 0.0f; };
+
+// LaineKarrasOctree::castRayImpl (SVOTraversal.cpp:516-691); lod == nullptr is
+// castRay, otherwise castRayWithLOD (:198-232, termination :613-651).
 Hit castRay(const vxo_scene& s, V3 origin, V3 direction, float tMin, float tMax, uint32_t& itersOut,
-            Counters& cnt) {
+            Counters& cnt, const Lod* lod = nullptr) {
     Hit miss;
     itersOut = 0;
     // validateRayInput (:238-259)
@@ -729,6 +734,7 @@ Hit castRay(const vxo_scene& s, V3 origin, V3 direction, float tMin, float tMax,
     V3 rayEntryPoint = origin + rayDir * tRayStart;
     V3 worldSize = s.worldMax - s.worldMin;
     V3 normOrigin = (rayEntryPoint - s.worldMin) / worldSize + splat(1.0f);
+    float worldRayLength = length(worldSize);  // :552
     Coef coef = computeRayCoefficients(rayDir, normOrigin);
     State st;
     if (rayStartsInside) {
@@ -796,6 +802,27 @@ Hit castRay(const vxo_scene& s, V3 origin, V3 direction, float tMin, float tMax,
         }
         bool skipToAdvance = false;
         if (shouldProcess) {
+            // Screen-space LOD termination (:613-651): world distance of the
+            // cell entry, esvoScaleToWorldSize (SVOLOD.h:189-195) and
+            // shouldTerminate (SVOLOD.h:129-146).
+            if (lod != nullptr && lod->rayDirSize > 0.0f) {
+                float worldDistance = tRayStart + st.t_min * worldRayLength;
+                float worldVoxelSize = std::ldexp(1.0f, st.scale - ESVO_MAX_SCALE - 1) * worldSize.x;
+                float projected = worldDistance * lod->rayDirSize + lod->rayOrigSize;
+                if (projected >= worldVoxelSize) {
+                    Hit h;
+                    h.hit = true;
+                    h.hitPoint = origin + rayDir * worldDistance;
+                    h.normal = V3{0.0f, 1.0f, 0.0f};
+                    h.tMin = worldDistance;
+                    h.tMax = worldDistance + worldVoxelSize;
+                    h.scale = st.scale - (ESVO_MAX_SCALE - s.maxLevels + 1);  // esvoToUserScale
+                    h.node = st.parent;  // no entity: the cut cell is child idx of this descriptor
+                    h.flags = F_HIT | (1u << 1);
+                    itersOut = uint32_t(st.iter);
+                    return h;
+                }
+            }
             if (isLeaf) {
                 Hit h;
                 if (handleLeafHit(s, st, coef, origin, tEntry, h, cnt)) {
@@ -1067,14 +1094,15 @@ void vxo_export(const vxo_scene* s, uint32_t* nodes, uint32_t* node_brick, uint3
     }
 }
 
-void vxo_cast_rays(const vxo_scene* s, const float* rays, uint64_t n, float t_min, float t_max, vxo_hit* out,
-                   int nthreads) {
+namespace {
+void cast_rays_impl(const vxo_scene* s, const float* rays, uint64_t n, float t_min, float t_max, vxo_hit* out,
+                    int nthreads, const Lod* lod) {
     auto work = [&](uint64_t b, uint64_t e) {
         for (uint64_t i = b; i < e; ++i) {
             const float* r = rays + 6 * i;
             uint32_t iters = 0;
             Counters cnt;
-            Hit h = castRay(*s, V3{r[0], r[1], r[2]}, V3{r[3], r[4], r[5]}, t_min, t_max, iters, cnt);
+            Hit h = castRay(*s, V3{r[0], r[1], r[2]}, V3{r[3], r[4], r[5]}, t_min, t_max, iters, cnt, lod);
             vxo_hit& o = out[i];
             o.t = h.hit ? h.tMin : 0.0f;
             o.t_exit = h.hit ? h.tMax : 0.0f;
@@ -1102,6 +1130,36 @@ void vxo_cast_rays(const vxo_scene* s, const float* rays, uint64_t n, float t_mi
         th.emplace_back(work, b, e);
     }
     for (auto& x : th) x.join();
+}
+}  // namespace
+
+void vxo_cast_rays(const vxo_scene* s, const float* rays, uint64_t n, float t_min, float t_max, vxo_hit* out,
+                   int nthreads) {
+    cast_rays_impl(s, rays, n, t_min, t_max, out, nthreads, nullptr);
+}
+
+void vxo_cast_rays_lod(const vxo_scene* s, const float* rays, uint64_t n, float t_min, float t_max,
+                       float ray_orig_size, float ray_dir_size, vxo_hit* out, int nthreads) {
+    Lod lod;
+    lod.rayOrigSize = ray_orig_size;
+    lod.rayDirSize = ray_dir_size;
+    cast_rays_impl(s, rays, n, t_min, t_max, out, nthreads, &lod);
+}
+
+// LODParameters::fromCameraWithNearPlane (SVOLOD.h:105-119); near_plane = 0
+// gives fromCamera (:83-92).
+void vxo_lod_from_camera(float fov_y, int32_t screen_height, float near_plane, float out[2]) {
+    float pixelAngle = fov_y / static_cast<float>(screen_height);
+    float dirSize = 2.0f * ::tanf(pixelAngle * 0.5f);
+    out[0] = near_plane * dirSize;
+    out[1] = dirSize;
+}
+
+// LODParameters::withBias (SVOLOD.h:169-176)
+void vxo_lod_with_bias(const float in[2], float bias, float out[2]) {
+    float multiplier = ::powf(2.0f, bias);
+    out[0] = in[0] * multiplier;
+    out[1] = in[1] * multiplier;
 }
 
 // DXT1ColorCompressor::decodeColorHead (DXT1Compressor.cpp:14-36)

@@ -81,6 +81,18 @@ void vxo_export(const vxo_scene* s, uint32_t* nodes, uint32_t* node_brick,
 void vxo_cast_rays(const vxo_scene* s, const float* rays, uint64_t n,
                    float t_min, float t_max, vxo_hit* out, int nthreads);
 
+/* castRayWithLOD (SVOTraversal.cpp:198-232) with LODParameters {ray_orig_size,
+ * ray_dir_size} (SVOLOD.h:50-177); ray_dir_size <= 0 is castRay.  A ray that
+ * stops at the LOD cut is a hit with brick 0xFFFFFFFF, voxel 0xFFFF, normal
+ * (0,1,0), scale = the cell's user scale and node = the parent descriptor. */
+void vxo_cast_rays_lod(const vxo_scene* s, const float* rays, uint64_t n, float t_min, float t_max,
+                       float ray_orig_size, float ray_dir_size, vxo_hit* out, int nthreads);
+
+/* LODParameters::fromCameraWithNearPlane / fromCamera (near_plane = 0) and
+ * withBias (SVOLOD.h:83-176); out = {rayOrigSize, rayDirSize}. */
+void vxo_lod_from_camera(float fov_y, int32_t screen_height, float near_plane, float out[2]);
+void vxo_lod_with_bias(const float in[2], float bias, float out[2]);
+
 /* Same as vxo_cast_rays, but replaces the octree with hand-built descriptors
  * (test_octree_queries.cpp builds such octrees with setOctree()). */
 vxo_scene* vxo_build_from_descriptors(const uint32_t* nodes, const uint32_t* node_brick,

@@ -52,6 +52,9 @@ def lib():
         L.vxo_bricks_per_axis.argtypes = [vp]
         L.vxo_export.argtypes = [vp, vp, vp, vp, vp, vp]
         L.vxo_cast_rays.argtypes = [vp, vp, u64, f32, f32, vp, C.c_int]
+        L.vxo_cast_rays_lod.argtypes = [vp, vp, u64, f32, f32, f32, f32, vp, C.c_int]
+        L.vxo_lod_from_camera.argtypes = [f32, i32, f32, vp]
+        L.vxo_lod_with_bias.argtypes = [vp, f32, vp]
         L.vxo_dxt1_decode_head.argtypes = [u32, vp]
         L.vxo_dxt1_decode_block.argtypes = [u64, vp]
         L.vxo_dxt1_encode_head.restype = u32
@@ -140,14 +143,48 @@ class OracleScene:
                             _ptr(out), int(threads))
         return out
 
+    def cast_rays_lod(self, rays: np.ndarray, lod, t_min=0.0, t_max=3.4028234663852886e38, threads=0):
+        """castRayWithLOD over many rays; lod = (rayOrigSize, rayDirSize)."""
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+        out = np.zeros(rays.shape[0], HIT_DTYPE)
+        lib().vxo_cast_rays_lod(self._h, _ptr(rays), rays.shape[0], float(t_min), float(t_max), float(lod[0]),
+                                float(lod[1]), _ptr(out), int(threads))
+        return out
+
     def castRay(self, origin, direction, tMin=0.0, tMax=3.4028234663852886e38):
         r = np.array([list(origin) + list(direction)], np.float32)
         return self.cast_rays(r, tMin, tMax, threads=1)[0]
+
+    def castRayWithLOD(self, origin, direction, lod, tMin=0.0, tMax=3.4028234663852886e38):
+        r = np.array([list(origin) + list(direction)], np.float32)
+        return self.cast_rays_lod(r, lod, tMin, tMax, threads=1)[0]
+
+    def castRayLOD(self, origin, direction, lodBias, tMin=0.0, tMax=3.4028234663852886e38):
+        """SVOTraversal.cpp:198-209: the bias is the cone spread itself."""
+        return self.castRayWithLOD(origin, direction, (0.0, lodBias), tMin, tMax)
+
+    def castRayScreenSpaceLOD(self, origin, direction, fovY, screenHeight, tMin=0.0, tMax=3.4028234663852886e38):
+        return self.castRayWithLOD(origin, direction, lod_from_camera(fovY, screenHeight), tMin, tMax)
 
     def __del__(self):
         if getattr(self, "_h", None):
             lib().vxo_free(self._h)
             self._h = None
+
+
+def lod_from_camera(fov_y: float, screen_height: int, near_plane: float = 0.0):
+    """LODParameters::fromCamera / fromCameraWithNearPlane -> (rayOrigSize, rayDirSize)."""
+    out = np.zeros(2, np.float32)
+    lib().vxo_lod_from_camera(float(fov_y), int(screen_height), float(near_plane), _ptr(out))
+    return float(out[0]), float(out[1])
+
+
+def lod_with_bias(lod, bias: float):
+    """LODParameters::withBias."""
+    a = np.array(lod, np.float32)
+    out = np.zeros(2, np.float32)
+    lib().vxo_lod_with_bias(_ptr(a), float(bias), _ptr(out))
+    return float(out[0]), float(out[1])
 
 
 def dxt1_decode_head(head: int) -> np.ndarray:

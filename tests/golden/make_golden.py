@@ -21,6 +21,7 @@ import kat_cases as K  # noqa: E402
 import vx_oracle as vo  # noqa: E402
 
 FIELDS = ["t", "brick", "node", "voxel", "flags", "iters", "grid_reads", "dda_steps", "key"]
+LOD_PARAMS = [(0.0, 0.0), (0.0, 0.02), (0.0, 0.1), (0.5, 0.05)]
 
 
 def rays_for(case_world_min, extent, n, seed):
@@ -59,6 +60,13 @@ def main():
     ex = s.export()
     for k, v in ex.items():
         out[f"dense64_{k}"] = v
+    # 3b. castRayWithLOD on the same grid and rays at four cone sizes
+    #     ({orig, dir}: off, castRayLOD-style spreads, and one with an origin size).
+    out["dense64_lod_params"] = np.array(LOD_PARAMS, np.float32)
+    for j, lod in enumerate(LOD_PARAMS):
+        h = s.cast_rays_lod(rays, lod)
+        for f in FIELDS + ["scale"]:
+            out[f"dense64_lod{j}_{f}"] = h[f]
     # 3. DXT1 decode of 256 random blocks.
     blocks = rng.integers(0, 2 ** 63, size=256, dtype=np.int64).view(np.uint64) ^ np.uint64(0x8000000000000000)
     out["dxt_blocks"] = blocks

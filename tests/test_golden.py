@@ -78,3 +78,45 @@ def test_kernel_reproduces_dense_golden(vx, golden, cuda):
     _eq(g["voxel"].astype(np.uint32), golden["dense64_voxel"], "voxel")
     _eq(c["iters"].astype(np.uint32), golden["dense64_iters"], "iters")
     _eq(c["dda_steps"].astype(np.uint32), golden["dense64_dda_steps"], "dda_steps")
+
+
+def test_oracle_reproduces_lod_golden(vo, golden):
+    s = vo.OracleScene.from_dense(golden["dense64_bits"], 64, 6)
+    for j, lod in enumerate(golden["dense64_lod_params"]):
+        h = s.cast_rays_lod(golden["dense64_rays"], tuple(float(v) for v in lod))
+        for f in FIELDS + ["scale"]:
+            _eq(h[f], golden[f"dense64_lod{j}_{f}"], f"lod{j}.{f}")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("j", range(4))
+def test_kernel_reproduces_lod_golden(vx, golden, cuda, j):
+    """castRayWithLOD on the committed device buffers: every field, including
+    the LOD hits' distance bits, cell scale and parent descriptor."""
+    import torch
+    a = vx.SceneArrays((0.0, 0.0, 0.0), (64.0, 64.0, 64.0), 6, 8, golden["dense64_nodes"],
+                       golden["dense64_node_brick"], golden["dense64_grid_lookup"], golden["dense64_brick_coord"],
+                       golden["dense64_brick_occ"])
+    s = vx.Scene(a)
+    rays = golden["dense64_rays"]
+    n = rays.shape[0]
+    r = torch.from_numpy(np.ascontiguousarray(rays)).cuda()
+    hits = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+    cnt = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+    lod = tuple(float(v) for v in golden["dense64_lod_params"][j])
+    s.cast_rays_dev(r, hits, None, cnt, lod=lod)
+    torch.cuda.synchronize()
+    g = hits.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1)
+    c = cnt.cpu().numpy().view(vx.COUNTER_DTYPE).reshape(-1)
+    p = f"dense64_lod{j}_"
+    hit = (golden[p + "flags"] & 1).astype(bool)
+    assert hit.any()
+    _eq(g["flags"].astype(np.uint32), golden[p + "flags"], "flags")
+    _eq(g["t"][hit], golden[p + "t"][hit], "t")
+    _eq(g["brick"], golden[p + "brick"], "brick")
+    _eq(g["node"], golden[p + "node"], "node")
+    _eq(g["voxel"].astype(np.uint32), golden[p + "voxel"], "voxel")
+    _eq(g["scale"].astype(np.int32), golden[p + "scale"], "scale")
+    _eq(c["iters"].astype(np.uint32), golden[p + "iters"], "iters")
+    _eq(c["grid_reads"].astype(np.uint32), golden[p + "grid_reads"], "grid_reads")
+    _eq(c["dda_steps"].astype(np.uint32), golden[p + "dda_steps"], "dda_steps")

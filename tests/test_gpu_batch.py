@@ -104,12 +104,15 @@ def test_shadow_spawn_matches_reference(vx, cuda):
     assert np.all(got[hit, 3:] == L) and np.all(got[~hit, 3:] == 0)
 
 
-def test_frame_graph_equals_eager(vx, cuda):
+@pytest.mark.parametrize("bounce_tuning", [None, (128, 64, 0, 16), (256, 256, 0, 24)])
+def test_frame_graph_equals_eager(vx, cuda, bounce_tuning):
     import torch
     from vx_b200 import workloads as W
     wls, scenes, rays, begin, allr, d_rays, d_begin = _setup(vx, W, n=8, seed=14)
     n = allr.shape[0]
     batch = vx.Batch(scenes)
+    if bounce_tuning is not None:
+        batch.set_bounce_tuning(vx.BatchTuning(*bounce_tuning))
     bb = torch.from_numpy((2 * begin).astype(np.int32)).cuda()
     ph, bh = torch.zeros((n, 4), dtype=torch.int32, device="cuda"), torch.zeros((2 * n, 4), dtype=torch.int32,
                                                                                device="cuda")
@@ -156,3 +159,6 @@ def test_batch_rejects_bad_tuning(vx, cuda):
         b.set_tuning(rays_per_task=40)
     with pytest.raises(vx.VxError):
         b.set_tuning(refill=33)
+    with pytest.raises(vx.VxError):
+        b.set_bounce_tuning(vx.BatchTuning(256, 48, 1, 0))
+    b.set_bounce_tuning(None)

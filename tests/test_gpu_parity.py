@@ -48,6 +48,7 @@ def assert_hits_equal(g, o, cnt=None, label=""):
     mism["brick"] = np.flatnonzero(g["brick"] != o["brick"])
     mism["node"] = np.flatnonzero(g["node"] != o["node"])
     mism["voxel"] = np.flatnonzero(g["voxel"].astype(np.uint32) != o["voxel"])
+    mism["scale"] = np.flatnonzero(g["scale"].astype(np.int32) != o["scale"])
     if cnt is not None:
         mism["iters"] = np.flatnonzero(cnt["iters"].astype(np.uint32) != o["iters"])
         mism["grid_reads"] = np.flatnonzero(cnt["grid_reads"].astype(np.uint32) != o["grid_reads"])

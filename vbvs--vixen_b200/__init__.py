@@ -31,7 +31,7 @@ FLT_MAX = 3.4028234663852886e38
 NONE = 0xFFFFFFFF
 
 HIT_DTYPE = np.dtype([("t", "<f4"), ("brick", "<u4"), ("node", "<u4"), ("voxel", "<u2"),
-                      ("flags", "u1"), ("reserved", "u1")])
+                      ("flags", "u1"), ("scale", "u1")])
 RAY_DTYPE = np.dtype([("o", "<f4", 3), ("d", "<f4", 3)])
 COUNTER_DTYPE = np.dtype([("iters", "<u2"), ("grid_reads", "<u2"), ("dda_steps", "<u4"), ("run_iters", "<u2"),
                           ("run_grid_reads", "<u2"), ("run_dda_steps", "<u4")])
@@ -94,6 +94,10 @@ def lib():
         "vx_scene_device_bytes": (C.c_int, [vp, vp]),
         "vx_cast_rays": (C.c_int, [vp, vp, u32, f32, f32, vp, vp, vp, vp]),
         "vx_cast_rays_host": (C.c_int, [vp, vp, u32, f32, f32, vp, vp, vp]),
+        "vx_cast_rays_lod": (C.c_int, [vp, vp, u32, f32, f32, vp, vp, vp, vp, vp]),
+        "vx_cast_rays_host_lod": (C.c_int, [vp, vp, u32, f32, f32, vp, vp, vp, vp]),
+        "vx_lod_from_camera": (C.c_int, [f32, C.c_int32, f32, vp]),
+        "vx_lod_with_bias": (C.c_int, [vp, f32, vp]),
         "vx_render": (C.c_int, [vp, vp, u32, u32, vp, vp, vp, vp]),
         "vx_camera_rays": (C.c_int, [vp, u32, u32, vp]),
         "vx_camera_rays_dev": (C.c_int, [vp, u32, u32, vp, vp]),
@@ -117,6 +121,7 @@ def lib():
         "vx_bounce_table": (C.c_int, [vp]),
         "vx_batch_capture_frame": (C.c_int, [vp, vp, vp, u32, vp, vp, vp, vp, u64, vp]),
         "vx_batch_launch_frame": (C.c_int, [vp, vp]),
+        "vx_batch_set_bounce_tuning": (C.c_int, [vp, vp]),
         "vx_cast_batch_noalloc": (C.c_int, [vp, u32, vp, vp, u32, f32, f32, vp, vp]),
         "vx_diff_forward": (C.c_int, [vp, vp, u32, u32, i32, vp, vp, vp, vp, vp]),
         "vx_diff_backward": (C.c_int, [u32, i32, vp, vp, vp, vp, vp, vp, vp]),
@@ -304,13 +309,18 @@ class Scene:
     def color_width(self) -> int:
         return {VX_COLOR_NONE: 0, VX_COLOR_RGBA8: 1, VX_COLOR_DXT1: 3}[self.color_kind]
 
-    def cast_rays_dev(self, rays, hits, color=None, counters=None, t_min=0.0, t_max=FLT_MAX, stream=None):
-        """rays: (n,6) float32 CUDA tensor; hits: (n,4) int32/uint32 CUDA tensor (16 B per ray)."""
+    def cast_rays_dev(self, rays, hits, color=None, counters=None, t_min=0.0, t_max=FLT_MAX, stream=None, lod=None):
+        """rays: (n,6) float32 CUDA tensor; hits: (n,4) int32/uint32 CUDA tensor (16 B per ray).
+        lod: LodParams for castRayWithLOD (vx_cast_rays_lod), None for castRay."""
         import torch
         n = rays.shape[0]
         s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
-        check(lib().vx_cast_rays(self._h, _p(rays), n, float(t_min), float(t_max), _p(hits), _p(color),
-                                 _p(counters), C.c_void_p(s)))
+        if lod is None:
+            check(lib().vx_cast_rays(self._h, _p(rays), n, float(t_min), float(t_max), _p(hits), _p(color),
+                                     _p(counters), C.c_void_p(s)))
+        else:
+            check(lib().vx_cast_rays_lod(self._h, _p(rays), n, float(t_min), float(t_max), C.byref(_lod(lod)),
+                                         _p(hits), _p(color), _p(counters), C.c_void_p(s)))
 
     def render_dev(self, pc: CameraPC, width: int, height: int, image=None, hits=None, color=None, stream=None):
         import torch
@@ -318,16 +328,46 @@ class Scene:
         check(lib().vx_render(self._h, C.byref(pc), width, height, _p(image), _p(hits), _p(color), C.c_void_p(s)))
 
     # -- host-buffer calls ---------------------------------------------------
-    def cast_rays_host(self, rays: np.ndarray, t_min=0.0, t_max=FLT_MAX, with_color=True):
+    def cast_rays_host(self, rays: np.ndarray, t_min=0.0, t_max=FLT_MAX, with_color=True, lod=None):
         rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
         hits = np.zeros(rays.shape[0], HIT_DTYPE)
         cw = self.color_width()
         color = None
         if with_color and cw:
             color = np.zeros((rays.shape[0], cw), np.uint32 if cw == 1 else np.float32)
-        check(lib().vx_cast_rays_host(self._h, _p(rays), rays.shape[0], float(t_min), float(t_max), _p(hits),
-                                      _p(color), None))
+        if lod is None:
+            check(lib().vx_cast_rays_host(self._h, _p(rays), rays.shape[0], float(t_min), float(t_max), _p(hits),
+                                          _p(color), None))
+        else:
+            check(lib().vx_cast_rays_host_lod(self._h, _p(rays), rays.shape[0], float(t_min), float(t_max),
+                                              C.byref(_lod(lod)), _p(hits), _p(color), None))
         return hits, color
+
+
+class LodParams(C.Structure):
+    """LODParameters (SVO/include/SVOLOD.h:50-177): vx_lod_params."""
+    _fields_ = [("ray_orig_size", C.c_float), ("ray_dir_size", C.c_float)]
+
+    def as_tuple(self):
+        return (self.ray_orig_size, self.ray_dir_size)
+
+
+def _lod(lod) -> LodParams:
+    return lod if isinstance(lod, LodParams) else LodParams(float(lod[0]), float(lod[1]))
+
+
+def lod_from_camera(fov_y: float, screen_height: int, near_plane: float = 0.0) -> LodParams:
+    """LODParameters::fromCamera (near_plane 0) / fromCameraWithNearPlane."""
+    out = LodParams()
+    check(lib().vx_lod_from_camera(float(fov_y), int(screen_height), float(near_plane), C.byref(out)))
+    return out
+
+
+def lod_with_bias(lod, bias: float) -> LodParams:
+    """LODParameters::withBias: both sizes times 2^bias."""
+    out = LodParams()
+    check(lib().vx_lod_with_bias(C.byref(_lod(lod)), float(bias), C.byref(out)))
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -358,14 +398,26 @@ class CudaOctree:
         self.world_min = np.array(a.world_min, np.float32)
         self.max_levels = a.max_levels
 
-    def castRays(self, origins, directions, tMin=0.0, tMax=FLT_MAX):
+    def castRays(self, origins, directions, tMin=0.0, tMax=FLT_MAX, lod=None):
         o = np.asarray(origins, np.float32).reshape(-1, 3)
         d = np.asarray(directions, np.float32).reshape(-1, 3)
-        hits, _ = self.scene.cast_rays_host(np.concatenate([o, d], axis=1), tMin, tMax, with_color=False)
+        hits, _ = self.scene.cast_rays_host(np.concatenate([o, d], axis=1), tMin, tMax, with_color=False, lod=lod)
         return hits
 
-    def castRay(self, origin, direction, tMin=0.0, tMax=FLT_MAX) -> RayHit:
-        h = self.castRays([origin], [direction], tMin, tMax)[0]
+    def castRayWithLOD(self, origin, direction, lod, tMin=0.0, tMax=FLT_MAX) -> RayHit:
+        """LaineKarrasOctree::castRayWithLOD (SVOTraversal.cpp:224-232)."""
+        return self.castRay(origin, direction, tMin, tMax, lod=lod)
+
+    def castRayLOD(self, origin, direction, lodBias, tMin=0.0, tMax=FLT_MAX) -> RayHit:
+        """castRayLOD (SVOTraversal.cpp:198-209): the bias is the cone spread, origin size 0."""
+        return self.castRay(origin, direction, tMin, tMax, lod=LodParams(0.0, float(lodBias)))
+
+    def castRayScreenSpaceLOD(self, origin, direction, fovY, screenHeight, tMin=0.0, tMax=FLT_MAX) -> RayHit:
+        """castRayScreenSpaceLOD (SVOTraversal.cpp:211-222)."""
+        return self.castRay(origin, direction, tMin, tMax, lod=lod_from_camera(fovY, screenHeight))
+
+    def castRay(self, origin, direction, tMin=0.0, tMax=FLT_MAX, lod=None) -> RayHit:
+        h = self.castRays([origin], [direction], tMin, tMax, lod=lod)[0]
         if not (h["flags"] & VX_HIT_HIT):
             return RayHit(False, 0.0, 0.0, (0.0, 0.0, 0.0), (0.0, 0.0, 0.0), 0, NONE, 0xFFFF, NONE, None)
         o = np.asarray(origin, np.float32)
@@ -373,6 +425,13 @@ class CudaOctree:
         dn = d * (np.float32(1.0) / np.sqrt((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]))
         t = np.float32(h["t"])
         hp = tuple(float(v) for v in (o + dn * t))
+        if h["brick"] == NONE:
+            # LOD hit (SVOTraversal.cpp:639-649): tMax = t + the cell's world size
+            # 2^(user scale - max_levels) * worldSize.x, normal +y, no entity.
+            wsx = np.float32(self.scene.arrays.world_max[0]) - np.float32(self.scene.arrays.world_min[0])
+            size = np.float32(np.ldexp(np.float32(1.0), int(h["scale"]) - self.max_levels)) * wsx
+            return RayHit(True, float(t), float(t + size), hp, (0.0, 1.0, 0.0), int(h["scale"]), NONE, 0xFFFF,
+                          int(h["node"]), None)
         axis = (int(h["flags"]) >> 1) & 3
         n = [0.0, 0.0, 0.0]
         n[axis] = -1.0 if h["flags"] & VX_HIT_NORMAL_NEG else 1.0
@@ -381,7 +440,7 @@ class CudaOctree:
         q = np.floor(self.world_min).astype(np.int64)
         ent = ((bc & 0x3FF) * 8 + (v & 7) + int(q[0]), ((bc >> 10) & 0x3FF) * 8 + ((v >> 3) & 7) + int(q[1]),
                ((bc >> 20) & 0x3FF) * 8 + (v >> 6) + int(q[2]))
-        return RayHit(True, float(t), float(t + np.float32(1.0)), hp, tuple(n), self.max_levels - 1,
+        return RayHit(True, float(t), float(t + np.float32(1.0)), hp, tuple(n), int(h["scale"]),
                       int(h["brick"]), v, int(h["node"]), ent)
 
 
@@ -432,6 +491,10 @@ class Batch:
     def set_tuning(self, block=256, rays_per_task=32, stack_in_shared=1, refill=0):
         t = BatchTuning(block, rays_per_task, stack_in_shared, refill)
         check(lib().vx_batch_set_tuning(self._h, C.byref(t)))
+
+    def set_bounce_tuning(self, tuning=None):
+        """Tuning of the bounce pass of frames captured later (None: the batch's own)."""
+        check(lib().vx_batch_set_bounce_tuning(self._h, None if tuning is None else C.byref(tuning)))
 
     def cast(self, rays, begin, hits, counters=None, t_min=0.0, t_max=FLT_MAX, stream=None):
         check(lib().vx_cast_batch(self._h, _p(rays), _p(begin), rays.shape[0], float(t_min), float(t_max), _p(hits),

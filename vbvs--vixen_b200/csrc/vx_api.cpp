@@ -25,8 +25,8 @@ int fail(int code, const std::string& msg) {
 
 const char* last_error_c_str() { return g_last_error.c_str(); }
 
-int cuda_fail(cudaError_t e, const char* what) {
-    return fail(VX_ECUDA, std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+int cuda_fail(cudaError_t e, const std::string& what) {
+    return fail(VX_ECUDA, what + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
 }
 
 CameraDev camera_from_pc(const vx_camera_pc& pc) {
@@ -166,6 +166,8 @@ int vx_scene_create(const vx_scene_desc* d, vx_scene** out) {
         ds.wsm[i] = ds.wsize[i] - 0.001f;
         ds.qwm[i] = int32_t(std::floor(c.world_min[i]));
     }
+    // glm::length: sqrt of the left-to-right dot product
+    ds.wrl = std::sqrt((ds.wsize[0] * ds.wsize[0] + ds.wsize[1] * ds.wsize[1]) + ds.wsize[2] * ds.wsize[2]);
     ds.max_levels = c.max_levels;
     ds.min_scale = 22 - c.max_levels + 1;
     ds.brick_user_scale = c.max_levels - c.brick_depth;
@@ -204,21 +206,32 @@ int vx_scene_device_bytes(const vx_scene* s, uint64_t* out) {
     return VX_OK;
 }
 
-int vx_cast_rays(const vx_scene* s, const vx_ray* rays, uint32_t n, float tmin, float tmax, vx_hit* hits,
-                 void* color, vx_ray_counters* counters, void* stream) {
-    if (!s || (n && (!rays || !hits))) return fail(VX_EINVAL, "vx_cast_rays: null argument");
-    if (std::isnan(tmin) || std::isnan(tmax)) return fail(VX_EINVAL, "vx_cast_rays: t_min / t_max is NaN");
+namespace {
+
+bool lod_ok(const vx_lod_params* lod) {
+    return !lod || (std::isfinite(lod->ray_orig_size) && std::isfinite(lod->ray_dir_size));
+}
+
+int cast_rays_dev(const char* what, const vx_scene* s, const vx_ray* rays, uint32_t n, float tmin, float tmax,
+                  const vx_lod_params* lod, vx_hit* hits, void* color, vx_ray_counters* counters, void* stream) {
+    if (!s || (n && (!rays || !hits))) return fail(VX_EINVAL, std::string(what) + ": null argument");
+    if (std::isnan(tmin) || std::isnan(tmax)) return fail(VX_EINVAL, std::string(what) + ": t_min / t_max is NaN");
+    if (!lod_ok(lod)) return fail(VX_EINVAL, std::string(what) + ": LOD sizes must be finite");
     if (reinterpret_cast<uintptr_t>(rays) % 8 || reinterpret_cast<uintptr_t>(hits) % 16 ||
         reinterpret_cast<uintptr_t>(color) % 4 || reinterpret_cast<uintptr_t>(counters) % 16)
-        return fail(VX_EINVAL, "vx_cast_rays: rays need 8-byte, hits and counters 16-byte, colour 4-byte alignment");
-    int r = vx::launch_cast(s->dev, rays, n, tmin, tmax, hits, color, counters, stream);
-    if (r != 0) return vx::cuda_fail(cudaError_t(r), "vx_cast_rays: launch");
+        return fail(VX_EINVAL,
+                    std::string(what) + ": rays need 8-byte, hits and counters 16-byte, colour 4-byte alignment");
+    int r = vx::launch_cast(s->dev, rays, n, tmin, tmax, hits, color, counters, stream, lod);
+    if (r != 0) return vx::cuda_fail(cudaError_t(r), std::string(what) + ": launch");
     return VX_OK;
 }
 
-int vx_cast_rays_host(const vx_scene* cs, const vx_ray* rays_host, uint32_t n, float tmin, float tmax,
-                      vx_hit* hits_host, void* color_host, void* stream) {
-    if (!cs || (n && (!rays_host || !hits_host))) return fail(VX_EINVAL, "vx_cast_rays_host: null argument");
+int cast_rays_host(const char* what, const vx_scene* cs, const vx_ray* rays_host, uint32_t n, float tmin,
+                   float tmax, const vx_lod_params* lod, vx_hit* hits_host, void* color_host, void* stream) {
+    const std::string w(what);
+    if (!cs || (n && (!rays_host || !hits_host))) return fail(VX_EINVAL, w + ": null argument");
+    if (std::isnan(tmin) || std::isnan(tmax)) return fail(VX_EINVAL, w + ": t_min / t_max is NaN");
+    if (!lod_ok(lod)) return fail(VX_EINVAL, w + ": LOD sizes must be finite");
     if (n == 0) return VX_OK;
     vx_scene* s = const_cast<vx_scene*>(cs);
     std::lock_guard<std::mutex> lk(s->stage_mu);
@@ -229,13 +242,13 @@ int vx_cast_rays_host(const vx_scene* cs, const vx_ray* rays_host, uint32_t n, f
     const uint64_t need = sz_r + sz_h + sz_c;
     int dev = -1;
     cudaGetDevice(&dev);
-    if (dev != s->device) return fail(VX_EINVAL, "vx_cast_rays_host: the scene belongs to another device");
+    if (dev != s->device) return fail(VX_EINVAL, w + ": the scene belongs to another device");
     if (need > s->stage_bytes) {
         if (s->stage) cudaFree(s->stage);
         s->stage = nullptr;
         s->stage_bytes = 0;
         cudaError_t e = cudaMalloc(&s->stage, need);
-        if (e != cudaSuccess) return vx::cuda_fail(e, "vx_cast_rays_host: cudaMalloc");
+        if (e != cudaSuccess) return vx::cuda_fail(e, w + ": cudaMalloc");
         s->stage_bytes = need;
     }
     char* base = static_cast<char*>(s->stage);
@@ -244,14 +257,56 @@ int vx_cast_rays_host(const vx_scene* cs, const vx_ray* rays_host, uint32_t n, f
     void* dc = sz_c ? base + sz_r + sz_h : nullptr;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaError_t e = cudaMemcpyAsync(dr, rays_host, uint64_t(n) * sizeof(vx_ray), cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) return vx::cuda_fail(e, "vx_cast_rays_host: copy in");
-    int r = vx::launch_cast(s->dev, dr, n, tmin, tmax, dh, dc, nullptr, stream);
-    if (r != 0) return vx::cuda_fail(cudaError_t(r), "vx_cast_rays_host: launch");
+    if (e != cudaSuccess) return vx::cuda_fail(e, w + ": copy in");
+    int r = vx::launch_cast(s->dev, dr, n, tmin, tmax, dh, dc, nullptr, stream, lod);
+    if (r != 0) return vx::cuda_fail(cudaError_t(r), w + ": launch");
     e = cudaMemcpyAsync(hits_host, dh, uint64_t(n) * sizeof(vx_hit), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess && dc) e = cudaMemcpyAsync(color_host, dc, uint64_t(n) * colw, cudaMemcpyDeviceToHost, st);
-    if (e != cudaSuccess) return vx::cuda_fail(e, "vx_cast_rays_host: copy out");
+    if (e != cudaSuccess) return vx::cuda_fail(e, w + ": copy out");
     e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return vx::cuda_fail(e, "vx_cast_rays_host: synchronize");
+    if (e != cudaSuccess) return vx::cuda_fail(e, w + ": synchronize");
+    return VX_OK;
+}
+
+}  // namespace
+
+int vx_cast_rays(const vx_scene* s, const vx_ray* rays, uint32_t n, float tmin, float tmax, vx_hit* hits,
+                 void* color, vx_ray_counters* counters, void* stream) {
+    return cast_rays_dev("vx_cast_rays", s, rays, n, tmin, tmax, nullptr, hits, color, counters, stream);
+}
+
+int vx_cast_rays_lod(const vx_scene* s, const vx_ray* rays, uint32_t n, float tmin, float tmax,
+                     const vx_lod_params* lod, vx_hit* hits, void* color, vx_ray_counters* counters, void* stream) {
+    if (!lod) return fail(VX_EINVAL, "vx_cast_rays_lod: null LOD parameters");
+    return cast_rays_dev("vx_cast_rays_lod", s, rays, n, tmin, tmax, lod, hits, color, counters, stream);
+}
+
+int vx_cast_rays_host(const vx_scene* s, const vx_ray* rays_host, uint32_t n, float tmin, float tmax,
+                      vx_hit* hits_host, void* color_host, void* stream) {
+    return cast_rays_host("vx_cast_rays_host", s, rays_host, n, tmin, tmax, nullptr, hits_host, color_host, stream);
+}
+
+int vx_cast_rays_host_lod(const vx_scene* s, const vx_ray* rays_host, uint32_t n, float tmin, float tmax,
+                          const vx_lod_params* lod, vx_hit* hits_host, void* color_host, void* stream) {
+    if (!lod) return fail(VX_EINVAL, "vx_cast_rays_host_lod: null LOD parameters");
+    return cast_rays_host("vx_cast_rays_host_lod", s, rays_host, n, tmin, tmax, lod, hits_host, color_host, stream);
+}
+
+int vx_lod_from_camera(float fov_y, int32_t screen_height, float near_plane, vx_lod_params* out) {
+    if (!out || screen_height <= 0) return fail(VX_EINVAL, "vx_lod_from_camera: bad argument");
+    // pixel angle = fovY / H; cone spread = 2 tan(angle / 2) (SVOLOD.h:83-119)
+    const float pixel_angle = fov_y / static_cast<float>(screen_height);
+    const float dir = 2.0f * ::tanf(pixel_angle * 0.5f);
+    out->ray_dir_size = dir;
+    out->ray_orig_size = near_plane * dir;
+    return VX_OK;
+}
+
+int vx_lod_with_bias(const vx_lod_params* in, float bias, vx_lod_params* out) {
+    if (!in || !out) return fail(VX_EINVAL, "vx_lod_with_bias: null argument");
+    const float m = ::powf(2.0f, bias);
+    const vx_lod_params r{in->ray_orig_size * m, in->ray_dir_size * m};
+    *out = r;
     return VX_OK;
 }
 

@@ -328,6 +328,7 @@ struct vx_batch {
     vx::DevScene* scenes = nullptr;  // device copy of the scene table
     uint32_t* work = nullptr;        // task counter (device scratch)
     vx_batch_tuning tuning{256, 32, 1, 0};
+    vx_batch_tuning bounce_tuning{0, 0, 0, 0};  // block 0: the bounce pass of a frame uses `tuning`
     int num_sms = 148;
     cudaGraphExec_t frame = nullptr;
     cudaGraph_t frame_graph = nullptr;
@@ -476,8 +477,10 @@ int vx_batch_get_tuning(const vx_batch* b, vx_batch_tuning* t) {
     return VX_OK;
 }
 
-int vx_cast_batch(vx_batch* b, const vx_ray* rays, const uint32_t* begin, uint32_t n, float tmin, float tmax,
-                  vx_hit* hits, vx_ray_counters* counters, void* stream) {
+namespace {
+
+int cast_batch_with(vx_batch* b, const vx_batch_tuning& t, const vx_ray* rays, const uint32_t* begin, uint32_t n,
+                    float tmin, float tmax, vx_hit* hits, vx_ray_counters* counters, void* stream) {
     if (!b || !begin || (n && (!rays || !hits))) return fail(VX_EINVAL, "vx_cast_batch: null argument");
     if (reinterpret_cast<uintptr_t>(rays) % 8 || reinterpret_cast<uintptr_t>(hits) % 16 ||
         reinterpret_cast<uintptr_t>(counters) % 16 || reinterpret_cast<uintptr_t>(begin) % 4)
@@ -487,8 +490,28 @@ int vx_cast_batch(vx_batch* b, const vx_ray* rays, const uint32_t* begin, uint32
     if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch: reset work counter");
     if (n == 0) return VX_OK;
     vx::BatchArgs a{b->scenes, b->S, begin, rays, n, tmin, tmax, hits, counters, b->work,
-                    uint32_t(b->tuning.rays_per_task), b->maxL, b->tuning.refill};
-    return launch_batch(b, b->tuning, a, st);
+                    uint32_t(t.rays_per_task), b->maxL, t.refill};
+    return launch_batch(b, t, a, st);
+}
+
+const vx_batch_tuning& bounce_tuning_of(const vx_batch* b) {
+    return b->bounce_tuning.block ? b->bounce_tuning : b->tuning;
+}
+
+}  // namespace
+
+int vx_cast_batch(vx_batch* b, const vx_ray* rays, const uint32_t* begin, uint32_t n, float tmin, float tmax,
+                  vx_hit* hits, vx_ray_counters* counters, void* stream) {
+    if (!b) return fail(VX_EINVAL, "vx_cast_batch: null argument");
+    return cast_batch_with(b, b->tuning, rays, begin, n, tmin, tmax, hits, counters, stream);
+}
+
+int vx_batch_set_bounce_tuning(vx_batch* b, const vx_batch_tuning* t) {
+    if (!b) return fail(VX_EINVAL, "vx_batch_set_bounce_tuning: null batch");
+    if (!t) { b->bounce_tuning = vx_batch_tuning{0, 0, 0, 0}; return VX_OK; }
+    if (int r = check_tuning(t)) return r;
+    b->bounce_tuning = *t;
+    return VX_OK;
 }
 
 int vx_batch_autotune(vx_batch* b, const vx_ray* rays, const uint32_t* begin, uint32_t n, vx_hit* hits, void* stream,
@@ -578,12 +601,14 @@ int vx_batch_capture_frame(vx_batch* b, const vx_ray* primary, const uint32_t* p
     if (b->frame_graph) { cudaGraphDestroy(b->frame_graph); b->frame_graph = nullptr; }
     // Resolve shared-memory attributes and occupancy outside the capture.
     if (int r = prepare_batch(b, b->tuning)) return r;
+    if (int r = prepare_batch(b, bounce_tuning_of(b))) return r;
     cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_err(e, "vx_batch_capture_frame: begin capture");
     int r = vx_cast_batch(b, primary, primary_begin, n, 0.0f, 3.402823466e+38f, primary_hits, nullptr, stream);
     if (r == VX_OK) r = vx_spawn_bounce_rays(primary, primary_hits, n, seed, bounce, stream);
     if (r == VX_OK)
-        r = vx_cast_batch(b, bounce, bounce_begin, 2 * n, 0.0f, 3.402823466e+38f, bounce_hits, nullptr, stream);
+        r = cast_batch_with(b, bounce_tuning_of(b), bounce, bounce_begin, 2 * n, 0.0f, 3.402823466e+38f, bounce_hits,
+                            nullptr, stream);
     cudaGraph_t g = nullptr;
     e = cudaStreamEndCapture(st, &g);
     if (r != VX_OK) { if (g) cudaGraphDestroy(g); return r; }

@@ -80,6 +80,7 @@ __device__ __forceinline__ uint32_t grid_lookup(const DevScene& s, int bx, int b
 struct Hit {
     float t;
     uint32_t brick, node, voxel, flags;
+    uint32_t scale;                                   // RayHit::scale (0 on a miss)
     uint32_t iters, grid_reads, dda_steps;            // the reference traversal's counts
     uint32_t run_iters, run_grid_reads, run_dda_steps;  // what this kernel executed
 };
@@ -171,6 +172,7 @@ struct CastState {
     Hit h;
     // per-ray constants
     float ox, oy, oz, dx, dy, dz, tEntry;
+    float tRayStart;       // world t where the octree walk starts (SVOTraversal.cpp:545)
     Coef c;
     float rlx, rly, rlz;   // clamped ray-entry position in [0,1] (SVOBrickDDA.cpp:107-109)
     RayB rb;
@@ -195,6 +197,12 @@ __device__ __forceinline__ void cast_finish(CastState& st) {
     if (st.iter >= MAX_ITER) st.h.flags |= F_ITER_CAP;
 }
 
+// LODParameters (SVO/include/SVOLOD.h:50-177): ray-cone diameter at the
+// origin and its growth per unit distance.
+struct LodCone {
+    float orig, dir;
+};
+
 // castRayImpl up to its loop (SVOTraversal.cpp:516-586).  Returns true when the
 // ray is already finished (invalid input or no overlap with the world box).
 __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy, float oz, float ddx, float ddy,
@@ -206,6 +214,7 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
     h.node = NONE;
     h.voxel = 0xFFFFu;
     h.flags = 0;
+    h.scale = 0;
     h.iters = 0;
     h.grid_reads = 0;
     h.dda_steps = 0;
@@ -331,6 +340,7 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
     st.ox = ox; st.oy = oy; st.oz = oz;
     st.dx = dx; st.dy = dy; st.dz = dz;
     st.tEntry = tEntry;
+    st.tRayStart = tRayStart;
     st.brick2 = 0;
     st.have_brick2 = false;
     st.scale = ESVO_MAX_SCALE;
@@ -359,9 +369,15 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
 // the 500-iteration cap: the result is the capped miss and the remaining
 // iterations' counters repeat the cycle's.  The two previous states are kept
 // in shared memory (cyc[k * stride], k < 8: one iteration back, k >= 8: two
-// back) from iteration CYCLE_START on.
+// back) from iteration CYCLE_START on.  With LOD the cut test reads only the
+// loop state and per-ray constants, so a repeating state still cannot end.
+//
+// LOD: castRayWithLOD (SVOTraversal.cpp:198-232) with LODParameters `lod`
+// (enabled, lod.dir > 0): the termination test of :613-651 runs on every
+// processed child before the leaf test.
+template <bool LOD = false>
 __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint32_t* stkN, float* stkT,
-                                          uint32_t* cyc, int stride) {
+                                          uint32_t* cyc, int stride, LodCone lod = LodCone{0.0f, 0.0f}) {
     Hit& h = st.h;
     const Coef& c = st.c;
     const int minScale = s.min_scale;
@@ -399,6 +415,23 @@ __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint
         if (st.scale - minScale == s.brick_user_scale && child_valid) isLeaf = true;
         float tv_max = 0.0f;
         if (child_valid && !(st.t_min > st.t_max) && st.t_min <= (tv_max = gmin(st.t_max, tcc))) {
+            if constexpr (LOD) {
+                // worldDistance = tRayStart + t_min * |worldSize| (:627);
+                // esvoScaleToWorldSize = 2^(scale - 23) * worldSize.x (SVOLOD.h:189-195),
+                // an exact power of two for scale in [0, 22];
+                // shouldTerminate: distance * rayDirSize + rayOrigSize >= size (SVOLOD.h:129-146).
+                const float wd = st.tRayStart + st.t_min * s.wrl;
+                const float vs = __int_as_float((st.scale - ESVO_MAX_SCALE - 1 + 127) << 23) * s.wsize[0];
+                if (wd * lod.dir + lod.orig >= vs) {
+                    // The LOD hit (:639-649): tMin = distance, normal (0,1,0), no entity.
+                    h.t = wd;
+                    h.node = st.parent;
+                    h.flags = F_HIT | (1u << 1);
+                    h.scale = uint32_t(st.scale - minScale);  // esvoToUserScale
+                    cast_finish(st);
+                    return true;
+                }
+            }
             if (isLeaf) {
                 // handleLeafHit (SVOBrickDDA.cpp:65-181)
                 float lx = st.px, ly = st.py, lz = st.pz;
@@ -466,6 +499,7 @@ __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint
                         h.brick = brick;
                         h.node = st.parent;
                         h.flags |= method << 4;
+                        h.scale = uint32_t(s.max_levels - 1);  // SVOBrickDDA.cpp:509
                         h.iters = uint32_t(st.iter);
                         h.run_iters = h.iters;
                         h.run_grid_reads = h.grid_reads;
@@ -613,13 +647,15 @@ next_iter:
     return false;
 }
 
-// castRayImpl without LOD (SVOTraversal.cpp:516-691): setup, then the loop.
+// castRayImpl (SVOTraversal.cpp:516-691): setup, then the loop.  LOD = false
+// is castRay, LOD = true castRayWithLOD with an enabled `lod`.
+template <bool LOD = false>
 __device__ __forceinline__ void cast_ray(const DevScene& s, float ox, float oy, float oz, float ddx, float ddy,
                                          float ddz, float tMinArg, float tMaxArg, uint32_t* stkN, float* stkT,
-                                         uint32_t* cyc, int stride, Hit& h) {
+                                         uint32_t* cyc, int stride, Hit& h, LodCone lod = LodCone{0.0f, 0.0f}) {
     CastState st;
     if (!cast_init(s, ox, oy, oz, ddx, ddy, ddz, tMinArg, tMaxArg, stkN, stkT, stride, st))
-        while (!cast_step(s, st, stkN, stkT, cyc, stride)) {
+        while (!cast_step<LOD>(s, st, stkN, stkT, cyc, stride, lod)) {
         }
     h = st.h;
 }
@@ -652,12 +688,13 @@ __device__ __forceinline__ void store_hit(vx_hit* hits, uint32_t i, const Hit& h
     v.x = __float_as_uint(h.t);
     v.y = h.brick;
     v.z = h.node;
-    v.w = (h.voxel & 0xFFFFu) | ((h.flags & 0xFFu) << 16);
+    v.w = (h.voxel & 0xFFFFu) | ((h.flags & 0xFFu) << 16) | (h.scale << 24);
     reinterpret_cast<uint4*>(hits)[i] = v;
 }
 
+// Colour of the hit voxel; 0 on a miss and on an LOD hit (no voxel).
 __device__ __forceinline__ void store_color(const DevScene& s, void* color, uint32_t i, const Hit& h) {
-    const bool hit = h.flags & F_HIT;
+    const bool hit = (h.flags & F_HIT) && h.brick != NONE;
     if (s.color_kind == VX_COLOR_RGBA8) {
         reinterpret_cast<uint32_t*>(color)[i] = hit ? __ldg(s.rgba + size_t(h.brick) * 512 + h.voxel) : 0u;
     } else if (s.color_kind == VX_COLOR_DXT1) {

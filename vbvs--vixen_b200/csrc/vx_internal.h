@@ -15,6 +15,7 @@ namespace vx {
 struct DevScene {
     float wmin[3], wmax[3], wsize[3];  // wsize = wmax - wmin (float subtract)
     float wsm[3];                      // wsize - 0.001 (SVOBrickDDA.cpp:128, 143)
+    float wrl;                         // length(wsize), worldRayLength (SVOTraversal.cpp:552)
     int32_t qwm[3];                    // floor(world_min), VoxelComponents.h:373-379
     int32_t max_levels;
     int32_t min_scale;                 // 22 - max_levels + 1
@@ -40,8 +41,10 @@ void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 
 // Kernel launchers (vx_kernels.cu).  Return cudaError_t as int.
+// lod: nullptr, or LODParameters {ray_orig_size, ray_dir_size} with ray_dir_size > 0.
 int launch_cast(const DevScene& s, const vx_ray* rays, uint32_t n, float tmin, float tmax,
-                vx_hit* hits, void* color, vx_ray_counters* counters, void* stream);
+                vx_hit* hits, void* color, vx_ray_counters* counters, void* stream,
+                const vx_lod_params* lod = nullptr);
 struct CameraDev {
     float pos[3], dir[3], up[3], right[3];
     float aspect, tan_half_fov;

@@ -6,10 +6,11 @@ namespace {
 
 constexpr int BLOCK = 256;
 
+template <bool LOD>
 __global__ void __launch_bounds__(BLOCK, 3) cast_kernel(DevScene s, const vx_ray* __restrict__ rays, uint32_t n,
                                                       float tmin, float tmax, vx_hit* __restrict__ hits,
                                                       void* __restrict__ color,
-                                                      vx_ray_counters* __restrict__ counters) {
+                                                      vx_ray_counters* __restrict__ counters, LodCone lod) {
     extern __shared__ uint32_t smem[];
     uint32_t* stkN = smem + threadIdx.x;
     float* stkT = reinterpret_cast<float*>(smem + s.max_levels * blockDim.x) + threadIdx.x;
@@ -19,7 +20,7 @@ __global__ void __launch_bounds__(BLOCK, 3) cast_kernel(DevScene s, const vx_ray
     const float2* r2 = reinterpret_cast<const float2*>(rays + i);
     const float2 a = __ldg(r2), b = __ldg(r2 + 1), c = __ldg(r2 + 2);
     Hit h;
-    cast_ray(s, a.x, a.y, b.x, b.y, c.x, c.y, tmin, tmax, stkN, stkT, cyc, blockDim.x, h);
+    cast_ray<LOD>(s, a.x, a.y, b.x, b.y, c.x, c.y, tmin, tmax, stkN, stkT, cyc, blockDim.x, h, lod);
     store_hit(hits, i, h);
     if (color) store_color(s, color, i, h);
     if (counters) {
@@ -95,11 +96,16 @@ size_t stack_bytes(const DevScene& s) { return (size_t(2) * size_t(s.max_levels)
 }  // namespace
 
 int launch_cast(const DevScene& s, const vx_ray* rays, uint32_t n, float tmin, float tmax, vx_hit* hits,
-                void* color, vx_ray_counters* counters, void* stream) {
+                void* color, vx_ray_counters* counters, void* stream, const vx_lod_params* lod) {
     if (n == 0) return int(cudaSuccess);
     const uint32_t grid = (n + BLOCK - 1) / BLOCK;
-    cast_kernel<<<grid, BLOCK, stack_bytes(s), static_cast<cudaStream_t>(stream)>>>(s, rays, n, tmin, tmax, hits,
-                                                                                     color, counters);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (lod && lod->ray_dir_size > 0.0f)
+        cast_kernel<true><<<grid, BLOCK, stack_bytes(s), st>>>(s, rays, n, tmin, tmax, hits, color, counters,
+                                                               LodCone{lod->ray_orig_size, lod->ray_dir_size});
+    else
+        cast_kernel<false><<<grid, BLOCK, stack_bytes(s), st>>>(s, rays, n, tmin, tmax, hits, color, counters,
+                                                                LodCone{0.0f, 0.0f});
     return int(cudaGetLastError());
 }
 
