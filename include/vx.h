@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define VX_ABI_VERSION 1
+#define VX_ABI_VERSION 2
 
 typedef enum vx_status {
     VX_OK = 0,
@@ -96,6 +96,11 @@ typedef struct vx_scene_desc {
                                       voxel i at word i>>5, bit i&31 */
     int32_t color_kind;            /* vx_color_kind */
     const void* brick_color;       /* RGBA8 or DXT1 payload, or NULL */
+    const void* brick_normal;      /* NULL, or brick_count x 32 DXT normal
+                                      blocks of 16 B {blockA, blockB}
+                                      (COMPRESSED_NORMAL_BUFFER,
+                                      SVORebuild.cpp:615-722); see
+                                      vx_build_normals */
 } vx_scene_desc;
 
 /* Ray: origin and direction (need not be normalised; the cast normalises
@@ -195,6 +200,12 @@ int vx_cast_rays(const vx_scene* scene, const vx_ray* rays_dev, uint32_t n,
 int vx_cast_rays_host(const vx_scene* scene, const vx_ray* rays_host, uint32_t n,
                       float t_min, float t_max, vx_hit* hits_host, void* color_host,
                       void* stream);
+
+/* Normalised DXT normal of each hit voxel (getCompressedVoxelNormal,
+ * VoxelRayMarch_Compressed.comp:160-165): normals_dev gets n x 3 floats,
+ * zeros for misses and LOD hits.  The scene needs a normal payload. */
+int vx_hit_normals(const vx_scene* scene, const vx_hit* hits_dev, uint32_t n, float* normals_dev,
+                   void* stream);
 
 /* ------------------------------------------------------------------------
  * Screen-space LOD cut.  Replaces LaineKarrasOctree::castRayWithLOD /
@@ -363,6 +374,19 @@ int vx_build_dense(const uint64_t* occupancy_bits, uint32_t R, int32_t max_level
  * colour fields are left empty. */
 int vx_build_desc(const vx_build* build, vx_scene_desc* desc);
 int vx_build_free(vx_build* build);
+
+/* DXT normal payload of bricks from their occupancy (16 u32 per brick, as
+ * vx_scene_desc.brick_occ): the geometric normal of every voxel
+ * (computeGeometricNormal, SVO/src/SVORebuild.cpp:145-193: central
+ * difference of the brick's occupancy, outward), empty voxels (0,1,0), each
+ * block of 16 encoded by DXTNormalCompressor::encodeBlockTyped
+ * (DXT1Compressor.cpp:242-333), empty blocks {0,0} (SVORebuild.cpp:658-722).
+ * out: brick_count x 32 x {blockA, blockB}.  The host form uses all host
+ * threads; the device form (16-byte aligned buffers) is stream-ordered.
+ * Both produce identical bits. */
+int vx_build_normals(const uint32_t* brick_occ, uint32_t brick_count, uint64_t* out);
+int vx_build_normals_dev(const uint32_t* brick_occ_dev, uint32_t brick_count, uint64_t* out_dev,
+                         void* stream);
 
 /* Converts reference-layout descriptors (64-bit ChildDescriptor,
  * SVOTypes.h:36-47: childPointer:15 far:1 valid:8 leaf:8 | brick:24 flags:8)

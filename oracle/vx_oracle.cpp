@@ -1262,3 +1262,263 @@ uint32_t vxo_shade(const float color[3], int hit, int normal_axis, int normal_ne
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// DXT normal blocks: DXTNormalCompressor (VoxelData/src/Compression/
+// DXT1Compressor.cpp:168-354), the geometric normals the rebuild encodes
+// (SVO/src/SVORebuild.cpp:145-220, 615-722) and the decode of the compressed
+// shader (shaders/Compression.glsl:115-177, VoxelRayMarch_Compressed.comp:160-165).
+// Integer <-> float conversions are C++'s (round to nearest for int -> float,
+// truncation for float -> int); int32 left shifts wrap.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr float NORMAL_COEFS[4] = {-1.0f, -1.0f / 3.0f, 1.0f / 3.0f, 1.0f};  // DXT1Compressor.h:130
+
+inline int32_t shl32(int32_t v, int s) { return static_cast<int32_t>(static_cast<uint32_t>(v) << s); }
+inline V3 neg(V3 v) { return {-v.x, -v.y, -v.z}; }
+inline int iclamp1(int v, int lo, int hi) { return v < lo ? lo : (hi < v ? hi : v); }  // std::clamp
+
+// DXTNormalCompressor::encodeRawNormal (DXT1Compressor.cpp:168-193)
+uint32_t encodeRawNormal(V3 normal) {
+    V3 a{std::abs(normal.x), std::abs(normal.y), std::abs(normal.z)};
+    float myz = (a.y < a.z) ? a.z : a.y;  // std::max(a.y, a.z)
+    int axis = (a.x >= myz) ? 0 : (a.y >= a.z) ? 1 : 2;
+    V3 tuv = axis == 0 ? normal : axis == 1 ? V3{normal.y, normal.z, normal.x} : V3{normal.z, normal.x, normal.y};
+    uint32_t result = 0;
+    if (tuv.x < 0.0f) result |= 0x80000000u;
+    result |= uint32_t(axis) << 29;
+    float absT = std::abs(tuv.x);
+    if (absT > 0.0f) {
+        int u = iclamp1(f2i((tuv.y / absT) * 16383.0f), -0x4000, 0x3FFF);
+        int v = iclamp1(f2i((tuv.z / absT) * 8191.0f), -0x2000, 0x1FFF);
+        result |= uint32_t(u & 0x7FFF) << 14;
+        result |= uint32_t(v & 0x3FFF);
+    }
+    return result;
+}
+
+// DXTNormalCompressor::decodeRawNormal (:195-207); Compression.glsl:115-138
+V3 decodeRawNormal(uint32_t value) {
+    int32_t sign = static_cast<int32_t>(value) >> 31;
+    int axis = int((value >> 29) & 3u);
+    int32_t t = sign ^ 0x7FFFFFFF;
+    int32_t u = static_cast<int32_t>(value << 3);
+    int32_t v = static_cast<int32_t>(value << 18);
+    if (axis == 0) return V3{float(t), float(u), float(v)};
+    if (axis == 1) return V3{float(v), float(t), float(u)};
+    return V3{float(u), float(v), float(t)};
+}
+
+// DXTNormalCompressor::encodeNormalAxis (:209-228).  std::exp2 of the integer
+// exponents here is an exact power of two (std::ldexp).
+uint32_t encodeNormalAxis(uint32_t headUV, V3 axis, int shift) {
+    float ax = std::abs(axis.x), ay = std::abs(axis.y), az = std::abs(axis.z);
+    float maxComp = ax;  // std::max({...}): the first largest
+    if (maxComp < ay) maxComp = ay;
+    if (maxComp < az) maxComp = az;
+    int exponent = 0;
+    if (maxComp > 0.0f) {
+        uint32_t bits;
+        std::memcpy(&bits, &maxComp, sizeof(bits));
+        exponent = iclamp1(static_cast<int>(bits >> 23) + (-127 - 31 + 1 - 3 + 13), 0, 15);
+    }
+    V3 scaled = axis * std::ldexp(1.0f, -exponent + (13 - 31));
+    headUV |= uint32_t(exponent) << shift;
+    headUV |= uint32_t(iclamp1(f2i((scaled.z + 8.5f) - float(headUV) * std::ldexp(1.0f, -4 - shift)), 0, 15) ^ 8)
+              << (4 + shift);
+    headUV |= uint32_t(iclamp1(f2i((scaled.y + 8.5f) - float(headUV) * std::ldexp(1.0f, -8 - shift)), 0, 15) ^ 8)
+              << (8 + shift);
+    headUV |= uint32_t(iclamp1(f2i((scaled.x + 8.5f) - float(headUV) * std::ldexp(1.0f, -12 - shift)), 0, 15) ^ 8)
+              << (12 + shift);
+    return headUV;
+}
+
+// DXTNormalCompressor::decodeNormalAxis (:230-240); Compression.glsl:140-156
+V3 decodeNormalAxis(uint32_t headUV, int shift) {
+    int32_t shifted = shl32(static_cast<int32_t>(headUV), 16 - shift);
+    int exponent = (shifted >> 16) & 15;
+    float scale = std::ldexp(1.0f, exponent + (3 - 13));
+    return V3{float(shifted) * scale, float(shl32(shifted, 4)) * scale, float(shl32(shifted, 8)) * scale};
+}
+
+// DXTNormalCompressor::encodeBlockTyped (:242-333) over 16 normals.
+void encodeNormalBlock(const V3* normals, size_t validCount, const int32_t* indices, uint64_t& blockA,
+                       uint64_t& blockB) {
+    blockA = blockB = 0;
+    if (validCount == 0) return;
+    V3 base = normals[0];
+    for (size_t i = 1; i < validCount; ++i) base = base + normals[i];
+    float baseLen = length(base);
+    if (baseLen < 0.1f * static_cast<float>(validCount)) {
+        int bestIdx = 0;
+        float bestDot = dot(normals[0], base);
+        for (size_t i = 1; i < validCount; ++i) {
+            float d = dot(normals[i], base);
+            if (d > bestDot) { bestIdx = int(i); bestDot = d; }
+        }
+        base = normals[bestIdx];
+    }
+    uint32_t headBase = encodeRawNormal(base);
+    base = decodeRawNormal(headBase);
+    int uIdx = 0;
+    float uDot = dot(normals[0], base);
+    for (size_t i = 1; i < validCount; ++i) {
+        float d = dot(normals[i], base);
+        if (d < uDot) { uIdx = int(i); uDot = d; }
+    }
+    uint32_t headUV = encodeNormalAxis(0, normals[uIdx] * length(base) - base, 0);
+    V3 u = decodeNormalAxis(headUV, 0);
+    V3 uRef[4];
+    for (int i = 0; i < 4; ++i) uRef[i] = normalize(base + u * NORMAL_COEFS[i]);
+    int vIdx = 0, vLerpIdx = 0;
+    float vDot = std::numeric_limits<float>::max();
+    for (size_t i = 0; i < validCount; ++i) {
+        int bestLerp = 0;
+        float bestDot = dot(normals[i], uRef[0]);
+        for (int j = 1; j < 4; ++j) {
+            float d = dot(normals[i], uRef[j]);
+            if (d > bestDot) { bestLerp = j; bestDot = d; }
+        }
+        if (bestDot < vDot) { vIdx = int(i); vLerpIdx = bestLerp; vDot = bestDot; }
+    }
+    V3 tmp = base + u * NORMAL_COEFS[vLerpIdx];
+    headUV = encodeNormalAxis(headUV, normals[vIdx] * length(tmp) - tmp, 16);
+    V3 v = decodeNormalAxis(headUV, 16);
+    V3 uvRef[16];
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) uvRef[i + j * 4] = normalize((base + u * NORMAL_COEFS[i]) + v * NORMAL_COEFS[j]);
+    uint32_t bitsU = 0, bitsV = 0;
+    for (size_t i = 0; i < validCount; ++i) {
+        int bestLerp = 0;
+        float bestDot = dot(normals[i], uvRef[0]);
+        for (int j = 1; j < 16; ++j) {
+            float d = dot(normals[i], uvRef[j]);
+            if (d > bestDot) { bestLerp = j; bestDot = d; }
+        }
+        int texelIdx = indices ? indices[i] : int(i);
+        bitsU |= uint32_t(bestLerp & 3) << (texelIdx * 2);
+        bitsV |= uint32_t(bestLerp >> 2) << (texelIdx * 2);
+    }
+    blockA = uint64_t(headBase) | (uint64_t(bitsU) << 32);
+    blockB = uint64_t(headUV) | (uint64_t(bitsV) << 32);
+}
+
+// decodeBlockTyped (:335-354) / decodeDXTNormal (Compression.glsl:158-177) of one texel.
+V3 decodeNormalTexel(uint64_t blockA, uint64_t blockB, int texel) {
+    V3 base = decodeRawNormal(uint32_t(blockA));
+    V3 u = decodeNormalAxis(uint32_t(blockB), 0);
+    V3 v = decodeNormalAxis(uint32_t(blockB), 16);
+    float cu = NORMAL_COEFS[(uint32_t(blockA >> 32) >> (texel * 2)) & 3u];
+    float cv = NORMAL_COEFS[(uint32_t(blockB >> 32) >> (texel * 2)) & 3u];
+    return (base + u * cu) + v * cv;
+}
+
+// getOccupancy / computeGeometricNormal (SVORebuild.cpp:145-193): central
+// differences of the brick's occupancy, out-of-brick neighbours empty.
+V3 geometricNormal(const uint32_t* occ, int x, int y, int z) {
+    auto o = [&](int X, int Y, int Z) -> float {
+        if (X < 0 || X >= 8 || Y < 0 || Y >= 8 || Z < 0 || Z >= 8) return 0.0f;
+        int i = Z * 64 + Y * 8 + X;
+        return ((occ[i >> 5] >> (i & 31)) & 1u) ? 1.0f : 0.0f;
+    };
+    V3 g{o(x + 1, y, z) - o(x - 1, y, z), o(x, y + 1, z) - o(x, y - 1, z), o(x, y, z + 1) - o(x, y, z - 1)};
+    float len = length(g);
+    if (len > 0.001f) return neg(normalize(g));
+    return V3{0.0f, 1.0f, 0.0f};
+}
+
+// The normal half of the rebuild's per-brick compression (SVORebuild.cpp:658-722):
+// empty texels carry (0,1,0); a block with an occupied texel is encoded over
+// all 16 texels, an empty block is {0, 0}.
+void brickNormalBlocks(const uint32_t* occ, uint64_t* out /* 64 u64 */) {
+    V3 nrm[512];
+    for (int i = 0; i < 512; ++i) nrm[i] = geometricNormal(occ, i & 7, (i >> 3) & 7, i >> 6);
+    for (int b = 0; b < 32; ++b) {
+        V3 bn[16];
+        int valid = 0;
+        for (int t = 0; t < 16; ++t) {
+            int i = b * 16 + t;
+            bool occd = (occ[i >> 5] >> (i & 31)) & 1u;
+            bn[t] = occd ? nrm[i] : V3{0.0f, 1.0f, 0.0f};
+            valid += occd;
+        }
+        if (valid) encodeNormalBlock(bn, 16, nullptr, out[2 * b], out[2 * b + 1]);
+        else out[2 * b] = out[2 * b + 1] = 0;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void vxo_dxtn_encode_block(const float* normals, uint64_t valid_count, const int32_t* indices, uint64_t out[2]) {
+    V3 n[16];
+    for (uint64_t i = 0; i < valid_count && i < 16; ++i) n[i] = V3{normals[3 * i], normals[3 * i + 1], normals[3 * i + 2]};
+    encodeNormalBlock(n, size_t(valid_count < 16 ? valid_count : 16), indices, out[0], out[1]);
+}
+
+void vxo_dxtn_decode_block(const uint64_t in[2], float out[48]) {
+    for (int t = 0; t < 16; ++t) {
+        V3 v = decodeNormalTexel(in[0], in[1], t);
+        out[3 * t] = v.x; out[3 * t + 1] = v.y; out[3 * t + 2] = v.z;
+    }
+}
+
+uint32_t vxo_encode_raw_normal(const float n[3]) { return encodeRawNormal(V3{n[0], n[1], n[2]}); }
+
+void vxo_geometric_normals(const uint32_t* occ, float out[1536]) {
+    for (int i = 0; i < 512; ++i) {
+        V3 v = geometricNormal(occ, i & 7, (i >> 3) & 7, i >> 6);
+        out[3 * i] = v.x; out[3 * i + 1] = v.y; out[3 * i + 2] = v.z;
+    }
+}
+
+void vxo_brick_normals(const uint32_t* occ, uint64_t brick_count, uint64_t* out, int nthreads) {
+    auto work = [&](uint64_t b, uint64_t e) {
+        for (uint64_t i = b; i < e; ++i) brickNormalBlocks(occ + 16 * i, out + 64 * i);
+    };
+    int T = nthreads > 0 ? nthreads : int(std::max(1u, std::thread::hardware_concurrency()));
+    if (T <= 1 || brick_count < 64) { work(0, brick_count); return; }
+    std::vector<std::thread> th;
+    uint64_t chunk = (brick_count + uint64_t(T) - 1) / uint64_t(T);
+    for (int t = 0; t < T; ++t) {
+        uint64_t b = uint64_t(t) * chunk, e = std::min(brick_count, b + chunk);
+        if (b >= e) break;
+        th.emplace_back(work, b, e);
+    }
+    for (auto& x : th) x.join();
+}
+
+// getCompressedVoxelNormal (VoxelRayMarch_Compressed.comp:160-165): the
+// normalised decode of the hit voxel's texel.
+void vxo_hit_normal_dxt(const uint64_t* brick_nrm, uint32_t brick, uint32_t voxel, float out[3]) {
+    const uint64_t* blk = brick_nrm + (uint64_t(brick) * 32 + (voxel >> 4)) * 2;
+    V3 v = normalize(decodeNormalTexel(blk[0], blk[1], int(voxel & 15)));
+    out[0] = v.x; out[1] = v.y; out[2] = v.z;
+}
+
+// Compressed shading of a hit: n = normalize(n_dxt + n_face * 0.5) (the blend of
+// VoxelRayMarch_Compressed.comp:242-256 with the hit's entry-face normal as the
+// DDA normal), then computeLighting (Lighting.glsl:19-28).  Miss: sky.
+uint32_t vxo_shade_dxt_normal(const float color[3], int hit, const float n_dxt[3], int normal_axis, int normal_neg,
+                              float uv_y) {
+    V3 c;
+    if (hit) {
+        V3 face{0, 0, 0};
+        face[normal_axis] = normal_neg ? -1.0f : 1.0f;
+        V3 n = normalize(V3{n_dxt[0], n_dxt[1], n_dxt[2]} + face * 0.5f);
+        V3 L = normalize(V3{1.0f, 1.0f, -1.0f});
+        float k = 0.3f + gmax(dot(n, L), 0.0f) * 0.7f;
+        c = V3{color[0], color[1], color[2]} * k;
+    } else {
+        c = V3{0.5f, 0.7f, 1.0f} * (1.0f - uv_y * 0.5f);
+    }
+    auto u8 = [](float v) -> uint32_t {
+        float cl = gmin(gmax(v, 0.0f), 1.0f);
+        return uint32_t(cl * 255.0f + 0.5f);
+    };
+    return u8(c.x) | (u8(c.y) << 8) | (u8(c.z) << 16) | (255u << 24);
+}
+
+}  // extern "C"

@@ -115,6 +115,30 @@ void vxo_hit_texel_dxt(const uint64_t* brick_dxt, uint32_t brick, uint32_t voxel
  * a miss (VoxelRayMarch.comp:493-499); returns RGBA8 like an UNORM imageStore. */
 uint32_t vxo_shade(const float color[3], int hit, int normal_axis, int normal_neg, float uv_y);
 
+/* DXT normal codec (DXTNormalCompressor, DXT1Compressor.cpp:168-354):
+ * encode 16 normals (valid_count <= 16, indices may be NULL) into {blockA,
+ * blockB}; decode the 16 unnormalised texels (Compression.glsl:158-177). */
+void     vxo_dxtn_encode_block(const float* normals, uint64_t valid_count, const int32_t* indices,
+                               uint64_t out[2]);
+void     vxo_dxtn_decode_block(const uint64_t in[2], float out[48]);
+uint32_t vxo_encode_raw_normal(const float n[3]);
+
+/* Geometric normals of one brick's 512 voxels from its 16-word occupancy
+ * (computeGeometricNormal, SVORebuild.cpp:145-193). */
+void vxo_geometric_normals(const uint32_t* occ, float out[1536]);
+
+/* DXT normal payload of brick_count bricks (SVORebuild.cpp:658-722):
+ * 32 blocks x {blockA, blockB} per brick. */
+void vxo_brick_normals(const uint32_t* occ, uint64_t brick_count, uint64_t* out, int nthreads);
+
+/* normalize(decodeDXTNormal) of a hit voxel (VoxelRayMarch_Compressed.comp:160-165). */
+void vxo_hit_normal_dxt(const uint64_t* brick_nrm, uint32_t brick, uint32_t voxel, float out[3]);
+
+/* Lighting with the decoded normal blended with the hit's entry-face normal:
+ * normalize(n_dxt + face * 0.5) (VoxelRayMarch_Compressed.comp:242-256). */
+uint32_t vxo_shade_dxt_normal(const float color[3], int hit, const float n_dxt[3], int normal_axis,
+                              int normal_neg, float uv_y);
+
 #ifdef __cplusplus
 }
 #endif

@@ -64,6 +64,15 @@ def lib():
         L.vxo_hit_texel_dxt.argtypes = [vp, u32, u32, vp]
         L.vxo_shade.restype = u32
         L.vxo_shade.argtypes = [vp, C.c_int, C.c_int, C.c_int, f32]
+        L.vxo_dxtn_encode_block.argtypes = [vp, u64, vp, vp]
+        L.vxo_dxtn_decode_block.argtypes = [vp, vp]
+        L.vxo_encode_raw_normal.restype = u32
+        L.vxo_encode_raw_normal.argtypes = [vp]
+        L.vxo_geometric_normals.argtypes = [vp, vp]
+        L.vxo_brick_normals.argtypes = [vp, u64, vp, C.c_int]
+        L.vxo_hit_normal_dxt.argtypes = [vp, u32, u32, vp]
+        L.vxo_shade_dxt_normal.restype = u32
+        L.vxo_shade_dxt_normal.argtypes = [vp, C.c_int, vp, C.c_int, C.c_int, f32]
         _lib = L
     return _lib
 
@@ -203,6 +212,57 @@ def dxt1_encode_block(colors, indices=None) -> int:
     c = np.ascontiguousarray(colors, dtype=np.float32).reshape(-1, 3)
     idx = None if indices is None else np.ascontiguousarray(indices, dtype=np.int32)
     return int(lib().vxo_dxt1_encode_block(_ptr(c), c.shape[0], _ptr(idx)))
+
+
+def dxtn_encode_block(normals, indices=None):
+    """DXTNormalCompressor::encodeBlockTyped -> (blockA, blockB)."""
+    n = np.ascontiguousarray(normals, dtype=np.float32).reshape(-1, 3)
+    idx = None if indices is None else np.ascontiguousarray(indices, dtype=np.int32)
+    out = np.zeros(2, np.uint64)
+    lib().vxo_dxtn_encode_block(_ptr(n), n.shape[0], _ptr(idx), _ptr(out))
+    return int(out[0]), int(out[1])
+
+
+def dxtn_decode_block(block_a: int, block_b: int) -> np.ndarray:
+    """DXTNormalCompressor::decodeBlockTyped: 16 unnormalised normals."""
+    b = np.array([block_a, block_b], np.uint64)
+    out = np.zeros(48, np.float32)
+    lib().vxo_dxtn_decode_block(_ptr(b), _ptr(out))
+    return out.reshape(16, 3)
+
+
+def encode_raw_normal(n) -> int:
+    a = np.ascontiguousarray(n, dtype=np.float32)
+    return int(lib().vxo_encode_raw_normal(_ptr(a)))
+
+
+def geometric_normals(occ16: np.ndarray) -> np.ndarray:
+    """computeGeometricNormal for the 512 voxels of one brick (16 u32 occupancy words)."""
+    occ = np.ascontiguousarray(occ16, dtype=np.uint32)
+    out = np.zeros(1536, np.float32)
+    lib().vxo_geometric_normals(_ptr(occ), _ptr(out))
+    return out.reshape(512, 3)
+
+
+def brick_normals(occ: np.ndarray, threads=0) -> np.ndarray:
+    """DXT normal payload of every brick: (bricks, 32, 2) u64 {blockA, blockB}."""
+    occ = np.ascontiguousarray(occ, dtype=np.uint32).reshape(-1, 16)
+    out = np.zeros((occ.shape[0], 32, 2), np.uint64)
+    lib().vxo_brick_normals(_ptr(occ), occ.shape[0], _ptr(out), int(threads))
+    return out
+
+
+def hit_normal_dxt(brick_nrm: np.ndarray, brick: int, voxel: int) -> np.ndarray:
+    nrm = np.ascontiguousarray(brick_nrm, dtype=np.uint64)
+    out = np.zeros(3, np.float32)
+    lib().vxo_hit_normal_dxt(_ptr(nrm), brick, voxel, _ptr(out))
+    return out
+
+
+def shade_dxt_normal(color, hit, n_dxt, axis, neg, uv_y) -> int:
+    c = np.ascontiguousarray(color, dtype=np.float32)
+    n = np.ascontiguousarray(n_dxt, dtype=np.float32)
+    return int(lib().vxo_shade_dxt_normal(_ptr(c), int(hit), _ptr(n), int(axis), int(neg), float(uv_y)))
 
 
 def hit_texel_dxt(brick_dxt: np.ndarray, brick: int, voxel: int) -> np.ndarray:

@@ -30,13 +30,13 @@ def test_library_exports_every_declared_symbol(vx):
 
 
 def test_abi_version(vx):
-    assert vx.lib().vx_abi_version() == 1
+    assert vx.lib().vx_abi_version() == 2
 
 
 def test_struct_sizes(vx):
     assert vx.HIT_DTYPE.itemsize == 16
     assert C.sizeof(vx.CameraPC) == 64
-    assert C.sizeof(vx._SceneDesc) == 104
+    assert C.sizeof(vx._SceneDesc) == 112
 
 
 def _desc(vx, **over):

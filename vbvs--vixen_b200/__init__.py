@@ -54,7 +54,7 @@ class _SceneDesc(C.Structure):
     _fields_ = [("config", _Config), ("nodes", C.c_void_p), ("node_count", C.c_uint32),
                 ("brick_count", C.c_uint32), ("node_brick", C.c_void_p), ("grid_lookup", C.c_void_p),
                 ("brick_coord", C.c_void_p), ("brick_occ", C.c_void_p), ("color_kind", C.c_int32),
-                ("brick_color", C.c_void_p)]
+                ("brick_color", C.c_void_p), ("brick_normal", C.c_void_p)]
 
 
 class CameraPC(C.Structure):
@@ -98,6 +98,9 @@ def lib():
         "vx_cast_rays_host_lod": (C.c_int, [vp, vp, u32, f32, f32, vp, vp, vp, vp]),
         "vx_lod_from_camera": (C.c_int, [f32, C.c_int32, f32, vp]),
         "vx_lod_with_bias": (C.c_int, [vp, f32, vp]),
+        "vx_build_normals": (C.c_int, [vp, u32, vp]),
+        "vx_build_normals_dev": (C.c_int, [vp, u32, vp, vp]),
+        "vx_hit_normals": (C.c_int, [vp, vp, u32, vp, vp]),
         "vx_render": (C.c_int, [vp, vp, u32, u32, vp, vp, vp, vp]),
         "vx_camera_rays": (C.c_int, [vp, u32, u32, vp]),
         "vx_camera_rays_dev": (C.c_int, [vp, u32, u32, vp, vp]),
@@ -201,6 +204,7 @@ class SceneArrays:
     brick_occ: np.ndarray    # 16 u32 per brick
     color_kind: int = VX_COLOR_NONE
     brick_color: np.ndarray | None = None
+    brick_normal: np.ndarray | None = None  # (bricks, 32, 2) u64 DXT normal blocks (build_normals)
 
     @property
     def node_count(self) -> int:
@@ -235,6 +239,19 @@ def build_dense(bits: np.ndarray, R: int, max_levels: int) -> SceneArrays:
                            take(d.brick_occ, 16 * d.brick_count, np.uint32))
     finally:
         lib().vx_build_free(h)
+
+
+def build_normals(brick_occ: np.ndarray) -> np.ndarray:
+    """DXT normal payload (bricks, 32, 2) u64 from 16-word brick occupancy (vx_build_normals, host)."""
+    occ = np.ascontiguousarray(brick_occ, np.uint32).reshape(-1, 16)
+    out = np.zeros((occ.shape[0], 32, 2), np.uint64)
+    check(lib().vx_build_normals(_p(occ), occ.shape[0], _p(out)))
+    return out
+
+
+def build_normals_dev(occ, out, stream=None):
+    """vx_build_normals_dev: occ (bricks*16) u32/int32 CUDA tensor -> out (bricks*64) 8-byte CUDA tensor."""
+    check(lib().vx_build_normals_dev(_p(occ), occ.numel() // 16, _p(out), _stream(stream)))
 
 
 def nodes_from_reference(ref_nodes: np.ndarray):
@@ -277,6 +294,10 @@ class Scene:
         if a.brick_color is not None:
             self._keep.append(np.ascontiguousarray(a.brick_color))
             d.brick_color = _p(self._keep[-1])
+        if a.brick_normal is not None:
+            assert a.brick_normal.size == a.brick_count * 64
+            self._keep.append(np.ascontiguousarray(a.brick_normal, np.uint64))
+            d.brick_normal = _p(self._keep[-1])
         self._h = C.c_void_p()
         check(lib().vx_scene_create(C.byref(d), C.byref(self._h)))
         self._keep = None  # the scene holds device copies
@@ -321,6 +342,10 @@ class Scene:
         else:
             check(lib().vx_cast_rays_lod(self._h, _p(rays), n, float(t_min), float(t_max), C.byref(_lod(lod)),
                                          _p(hits), _p(color), _p(counters), C.c_void_p(s)))
+
+    def hit_normals_dev(self, hits, out, stream=None):
+        """vx_hit_normals: hits (n,4) CUDA tensor -> out (n,3) float32 CUDA tensor."""
+        check(lib().vx_hit_normals(self._h, _p(hits), hits.shape[0], _p(out), _stream(stream)))
 
     def render_dev(self, pc: CameraPC, width: int, height: int, image=None, hits=None, color=None, stream=None):
         import torch

@@ -129,13 +129,15 @@ int vx_scene_create(const vx_scene_desc* d, vx_scene** out) {
     uint64_t sz_color = 0;
     if (d->color_kind == VX_COLOR_RGBA8) sz_color = uint64_t(d->brick_count) * 512 * 4;
     if (d->color_kind == VX_COLOR_DXT1) sz_color = uint64_t(d->brick_count) * 32 * 8;
+    const uint64_t sz_nrm = d->brick_normal ? uint64_t(d->brick_count) * 32 * 16 : 0;
     const uint64_t o_nodes = 0;
     const uint64_t o_nb = o_nodes + align256(sz_nodes);
     const uint64_t o_grid = o_nb + align256(sz_nb);
     const uint64_t o_coord = o_grid + align256(sz_grid);
     const uint64_t o_occ = o_coord + align256(sz_coord);
     const uint64_t o_color = o_occ + align256(sz_occ);
-    const uint64_t total = o_color + align256(sz_color) + 256;
+    const uint64_t o_nrm = o_color + align256(sz_color);
+    const uint64_t total = o_nrm + align256(sz_nrm) + 256;
 
     auto* s = new (std::nothrow) vx_scene();
     if (!s) return fail(VX_ENOMEM, "vx_scene_create: out of host memory");
@@ -148,7 +150,8 @@ int vx_scene_create(const vx_scene_desc* d, vx_scene** out) {
     struct Copy { uint64_t off; const void* src; uint64_t n; };
     const Copy copies[] = {{o_nodes, d->nodes, sz_nodes}, {o_nb, d->node_brick, sz_nb},
                            {o_grid, d->grid_lookup, sz_grid}, {o_coord, d->brick_coord, sz_coord},
-                           {o_occ, d->brick_occ, sz_occ}, {o_color, d->brick_color, sz_color}};
+                           {o_occ, d->brick_occ, sz_occ}, {o_color, d->brick_color, sz_color},
+                           {o_nrm, d->brick_normal, sz_nrm}};
     for (const Copy& cp : copies) {
         if (!cp.n) continue;
         e = cudaMemcpy(base + cp.off, cp.src, cp.n, cudaMemcpyHostToDevice);
@@ -182,6 +185,7 @@ int vx_scene_create(const vx_scene_desc* d, vx_scene** out) {
     ds.color_kind = d->color_kind;
     ds.rgba = d->color_kind == VX_COLOR_RGBA8 ? reinterpret_cast<const uint32_t*>(base + o_color) : nullptr;
     ds.dxt = d->color_kind == VX_COLOR_DXT1 ? reinterpret_cast<const uint2*>(base + o_color) : nullptr;
+    ds.nrm = sz_nrm ? reinterpret_cast<const uint4*>(base + o_nrm) : nullptr;
     *out = s;
     return VX_OK;
 }

@@ -29,6 +29,7 @@
 #include <climits>
 #include <cstdint>
 
+#include "vx_dxtn.h"
 #include "vx_internal.h"
 #include "vx_raygen.h"
 
@@ -681,6 +682,16 @@ __device__ __forceinline__ void dxt_texel(const uint2* dxt, uint32_t brick, uint
         g = r0y * (1.0f / 3.0f) + r1y * (2.0f / 3.0f);
         b = r0z * (1.0f / 3.0f) + r1z * (2.0f / 3.0f);
     }
+}
+
+// getCompressedVoxelNormal (VoxelRayMarch_Compressed.comp:160-165):
+// normalize(decodeDXTNormal) of the voxel's texel (Compression.glsl:158-177).
+__device__ __forceinline__ void dxt_normal(const DevScene& s, uint32_t brick, uint32_t voxel, float& x, float& y,
+                                           float& z) {
+    const uint4 q = __ldg(s.nrm + size_t(brick) * 32 + (voxel >> 4));
+    const dxtn::F3 n = dxtn::unit(dxtn::decode(uint64_t(q.x) | (uint64_t(q.y) << 32),
+                                               uint64_t(q.z) | (uint64_t(q.w) << 32), voxel & 15u));
+    x = n.x; y = n.y; z = n.z;
 }
 
 __device__ __forceinline__ void store_hit(vx_hit* hits, uint32_t i, const Hit& h) {

@@ -30,6 +30,7 @@ struct DevScene {
     int32_t color_kind;
     const uint32_t* rgba;              // 512 per brick
     const uint2* dxt;                  // 32 per brick
+    const uint4* nrm;                  // DXT normal blocks, 32 per brick, or null
 };
 
 // Accessors of an opaque vx_scene (vx_api.cpp).

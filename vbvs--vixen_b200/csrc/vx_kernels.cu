@@ -70,6 +70,15 @@ __global__ void __launch_bounds__(BLOCK, 3) render_kernel(DevScene s, CameraDev 
             float nrm[3] = {0.0f, 0.0f, 0.0f};
             const int axis = (h.flags >> 1) & 3;
             nrm[axis] = (h.flags & F_NEG) ? -1.0f : 1.0f;
+            if (s.nrm) {
+                // Compressed shading (VoxelRayMarch_Compressed.comp:242-256): the
+                // decoded normal blended with the entry-face normal,
+                // normalize(n_dxt + face * 0.5).
+                float dx, dy, dz;
+                dxt_normal(s, h.brick, h.voxel, dx, dy, dz);
+                const dxtn::F3 b = dxtn::unit(dxtn::F3{dx, dy, dz} + dxtn::F3{nrm[0], nrm[1], nrm[2]} * 0.5f);
+                nrm[0] = b.x; nrm[1] = b.y; nrm[2] = b.z;
+            }
             const float nd = (nrm[0] * L[0] + nrm[1] * L[1]) + nrm[2] * L[2];
             const float diffuse = gmax(nd, 0.0f) * 0.7f;
             const float k = 0.3f + diffuse;

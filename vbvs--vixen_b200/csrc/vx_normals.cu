@@ -1,0 +1,110 @@
+// vx_normals.cu - the DXT normal payload: built on the GPU (one thread per
+// 16-voxel block) or on the host from the same code, and the per-hit decode of
+// the compressed shader (getCompressedVoxelNormal,
+// VoxelRayMarch_Compressed.comp:160-165).
+#include <algorithm>
+#include <thread>
+#include <vector>
+
+#include "vx_cast.cuh"
+#include "vx_dxtn.h"
+
+namespace vx {
+namespace {
+
+// Thread i encodes block i & 31 of brick i >> 5.  The 32 threads of a warp
+// share one brick, so its 64 occupancy bytes are one broadcast load; each
+// thread writes its 16-byte block, a warp 512 contiguous bytes.
+__global__ void __launch_bounds__(256) build_normals_kernel(const uint4* __restrict__ occ, uint64_t blocks,
+                                                            uint4* __restrict__ out) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < blocks;
+         i += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t brick = i >> 5;
+        uint32_t w[16];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint4 q = __ldg(occ + brick * 4 + k);
+            w[4 * k] = q.x; w[4 * k + 1] = q.y; w[4 * k + 2] = q.z; w[4 * k + 3] = q.w;
+        }
+        uint64_t a, b;
+        dxtn::brick_block(w, int(i & 31), a, b);
+        out[i] = make_uint4(uint32_t(a), uint32_t(a >> 32), uint32_t(b), uint32_t(b >> 32));
+    }
+}
+
+// normalize(decode) of each hit voxel's texel; zeros on a miss or an LOD hit.
+__global__ void __launch_bounds__(256) hit_normals_kernel(DevScene s, const uint4* __restrict__ hits, uint32_t n,
+                                                          float* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint4 h = __ldg(hits + i);
+    float x = 0.0f, y = 0.0f, z = 0.0f;
+    const uint32_t flags = (h.w >> 16) & 0xFFu;
+    if ((flags & F_HIT) && h.y != NONE) dxt_normal(s, h.y, h.w & 0xFFFFu, x, y, z);
+    out[size_t(i) * 3] = x;
+    out[size_t(i) * 3 + 1] = y;
+    out[size_t(i) * 3 + 2] = z;
+}
+
+int cuda_err(cudaError_t e, const char* what) {
+    return fail(VX_ECUDA, std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+}  // namespace
+}  // namespace vx
+
+extern "C" int vx_build_normals_dev(const uint32_t* occ_dev, uint32_t brick_count, uint64_t* out_dev, void* stream) {
+    using namespace vx;
+    if (brick_count && (!occ_dev || !out_dev)) return fail(VX_EINVAL, "vx_build_normals_dev: null argument");
+    if (reinterpret_cast<uintptr_t>(occ_dev) % 16 || reinterpret_cast<uintptr_t>(out_dev) % 16)
+        return fail(VX_EINVAL, "vx_build_normals_dev: buffers need 16-byte alignment");
+    if (brick_count == 0) return VX_OK;
+    const uint64_t blocks = uint64_t(brick_count) * 32;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint64_t want = (blocks + 255) / 256;
+    const uint32_t grid = uint32_t(std::min<uint64_t>(want, uint64_t(sms) * 16));
+    build_normals_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<const uint4*>(occ_dev), blocks, reinterpret_cast<uint4*>(out_dev));
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_build_normals_dev");
+}
+
+extern "C" int vx_build_normals(const uint32_t* occ, uint32_t brick_count, uint64_t* out) {
+    using namespace vx;
+    if (brick_count && (!occ || !out)) return fail(VX_EINVAL, "vx_build_normals: null argument");
+    const unsigned T = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    auto work = [&](uint64_t b0, uint64_t b1) {
+        for (uint64_t b = b0; b < b1; ++b)
+            for (int k = 0; k < 32; ++k) dxtn::brick_block(occ + 16 * b, k, out[(b * 32 + k) * 2], out[(b * 32 + k) * 2 + 1]);
+    };
+    if (T == 1 || brick_count < 256) {
+        work(0, brick_count);
+        return VX_OK;
+    }
+    std::vector<std::thread> th;
+    const uint64_t chunk = (uint64_t(brick_count) + T - 1) / T;
+    for (unsigned t = 0; t < T; ++t) {
+        const uint64_t b0 = uint64_t(t) * chunk, b1 = std::min<uint64_t>(brick_count, b0 + chunk);
+        if (b0 >= b1) break;
+        th.emplace_back(work, b0, b1);
+    }
+    for (auto& x : th) x.join();
+    return VX_OK;
+}
+
+extern "C" int vx_hit_normals(const vx_scene* scene, const vx_hit* hits_dev, uint32_t n, float* normals_dev,
+                              void* stream) {
+    using namespace vx;
+    if (!scene || (n && (!hits_dev || !normals_dev))) return fail(VX_EINVAL, "vx_hit_normals: null argument");
+    const DevScene& s = scene_dev(scene);
+    if (!s.nrm) return fail(VX_EINVAL, "vx_hit_normals: the scene has no normal payload");
+    if (reinterpret_cast<uintptr_t>(hits_dev) % 16 || reinterpret_cast<uintptr_t>(normals_dev) % 4)
+        return fail(VX_EINVAL, "vx_hit_normals: misaligned buffer");
+    if (n == 0) return VX_OK;
+    hit_normals_kernel<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        s, reinterpret_cast<const uint4*>(hits_dev), n, normals_dev);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_hit_normals");
+}
