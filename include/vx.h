@@ -180,6 +180,33 @@ int vx_scene_destroy(vx_scene* scene);
 /* Device bytes held by the scene. */
 int vx_scene_device_bytes(const vx_scene* scene, uint64_t* out);
 
+/* What a scene holds (for vx_scene_download and cache files). */
+typedef struct vx_scene_info {
+    vx_octree_config config;
+    uint32_t node_count;
+    uint32_t brick_count;
+    int32_t color_kind;
+    int32_t has_normals;
+} vx_scene_info;
+int vx_scene_info_get(const vx_scene* scene, vx_scene_info* out);
+/* Copies the scene's device arrays into caller host buffers of the sizes
+ * vx_scene_desc gives them (nodes: node_count x 2 u32; normals: brick_count
+ * x 64 u64); any pointer may be NULL.  Synchronous. */
+int vx_scene_download(const vx_scene* scene, uint32_t* nodes, uint32_t* node_brick, uint32_t* grid_lookup,
+                      uint32_t* brick_coord, uint32_t* brick_occ, void* brick_color,
+                      uint64_t* brick_normal);
+
+/* Device scene builder: the arrays of vx_build_dense, index for index, built
+ * on the current device from R^3 occupancy bits already in device memory
+ * (bits_dev, layout of vx_build_dense, R a multiple of 64 up to 4096), written
+ * straight into a new scene.  color_kind VX_COLOR_RGBA8 / VX_COLOR_DXT1 adds
+ * the payload of vx_synth_rgba8 / vx_synth_dxt1 for color_seed; with_normals
+ * adds the DXT normal payload of vx_build_normals.  Allocates its own scratch
+ * and returns when the scene is complete. */
+int vx_scene_create_dense_dev(const uint64_t* bits_dev, uint32_t R, int32_t max_levels,
+                              int32_t color_kind, uint64_t color_seed, int32_t with_normals,
+                              vx_scene** out, void* stream);
+
 /* ------------------------------------------------------------------------
  * Ray casting.  Replaces LaineKarrasOctree::castRay
  * (SVO/src/SVOTraversal.cpp:189-196, castRayImpl :516-691, brick DDA

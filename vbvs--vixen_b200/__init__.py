@@ -101,6 +101,9 @@ def lib():
         "vx_build_normals": (C.c_int, [vp, u32, vp]),
         "vx_build_normals_dev": (C.c_int, [vp, u32, vp, vp]),
         "vx_hit_normals": (C.c_int, [vp, vp, u32, vp, vp]),
+        "vx_scene_info_get": (C.c_int, [vp, vp]),
+        "vx_scene_download": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, vp]),
+        "vx_scene_create_dense_dev": (C.c_int, [vp, u32, i32, i32, u64, i32, vp, vp]),
         "vx_render": (C.c_int, [vp, vp, u32, u32, vp, vp, vp, vp]),
         "vx_camera_rays": (C.c_int, [vp, u32, u32, vp]),
         "vx_camera_rays_dev": (C.c_int, [vp, u32, u32, vp, vp]),
@@ -254,6 +257,15 @@ def build_normals_dev(occ, out, stream=None):
     check(lib().vx_build_normals_dev(_p(occ), occ.numel() // 16, _p(out), _stream(stream)))
 
 
+def scene_from_dense_dev(bits, R: int, max_levels: int, color_kind: int = VX_COLOR_NONE, color_seed: int = 0,
+                         with_normals: bool = False, stream=None) -> "Scene":
+    """vx_scene_create_dense_dev: bits is an (R^3/64) 8-byte CUDA tensor (vx_synth_noise_dev's output)."""
+    h = C.c_void_p()
+    check(lib().vx_scene_create_dense_dev(_p(bits), R, max_levels, color_kind, color_seed, int(with_normals),
+                                          C.byref(h), _stream(stream)))
+    return Scene.from_handle(h)
+
+
 def nodes_from_reference(ref_nodes: np.ndarray):
     ref = np.ascontiguousarray(ref_nodes, np.uint64)
     nodes = np.zeros(2 * ref.size, np.uint32)
@@ -273,11 +285,53 @@ def camera_rays(pc: CameraPC, width: int, height: int) -> np.ndarray:
 # Device scene
 # ---------------------------------------------------------------------------
 
+class _SceneInfo(C.Structure):
+    _fields_ = [("config", _Config), ("node_count", C.c_uint32), ("brick_count", C.c_uint32),
+                ("color_kind", C.c_int32), ("has_normals", C.c_int32)]
+
+
 class Scene:
     """A scene resident in device memory (vx_scene)."""
 
+    @classmethod
+    def from_handle(cls, handle: C.c_void_p) -> "Scene":
+        """Wraps a vx_scene made by the library (vx_scene_create_dense_dev); the
+        host arrays are downloaded on first use of .arrays."""
+        self = cls.__new__(cls)
+        self._h = handle
+        self._arrays = None
+        return self
+
+    def info(self):
+        i = _SceneInfo()
+        check(lib().vx_scene_info_get(self._h, C.byref(i)))
+        return i
+
+    @property
+    def arrays(self) -> SceneArrays:
+        if self._arrays is None:
+            self._arrays = self.download()
+        return self._arrays
+
+    def download(self) -> SceneArrays:
+        """vx_scene_download: every device array back in host memory."""
+        i = self.info()
+        bpa, B, D = i.config.bricks_per_axis, i.brick_count, i.node_count
+        nodes, nb = np.zeros(2 * D, np.uint32), np.zeros(D, np.uint32)
+        grid, coord, occ = np.zeros(bpa ** 3, np.uint32), np.zeros(B, np.uint32), np.zeros(16 * B, np.uint32)
+        color = None
+        if i.color_kind == VX_COLOR_RGBA8:
+            color = np.zeros(512 * B, np.uint32)
+        elif i.color_kind == VX_COLOR_DXT1:
+            color = np.zeros(32 * B, np.uint64)
+        normal = np.zeros((B, 32, 2), np.uint64) if i.has_normals else None
+        check(lib().vx_scene_download(self._h, _p(nodes), _p(nb), _p(grid), _p(coord), _p(occ), _p(color),
+                                      _p(normal)))
+        return SceneArrays(tuple(i.config.world_min), tuple(i.config.world_max), i.config.max_levels, bpa, nodes,
+                           nb, grid, coord, occ, i.color_kind, color, normal)
+
     def __init__(self, arrays: SceneArrays):
-        self.arrays = arrays
+        self._arrays = arrays
         a = arrays
         d = _SceneDesc()
         d.config.world_min[:] = [float(v) for v in a.world_min]
@@ -308,7 +362,7 @@ class Scene:
 
     @property
     def color_kind(self) -> int:
-        return self.arrays.color_kind
+        return self._arrays.color_kind if self._arrays is not None else self.info().color_kind
 
     def device_bytes(self) -> int:
         v = C.c_uint64()

@@ -49,6 +49,7 @@ CameraDev camera_from_pc(const vx_camera_pc& pc) {
 
 struct vx_scene {
     int device = 0;
+    vx_octree_config cfg{};
     void* pool = nullptr;  // single device allocation, 256-byte aligned slices
     uint64_t pool_bytes = 0;
     vx::DevScene dev{};
@@ -61,6 +62,80 @@ struct vx_scene {
 namespace vx {
 const DevScene& scene_dev(const vx_scene* s) { return s->dev; }
 int scene_device(const vx_scene* s) { return s->device; }
+
+namespace {
+uint64_t align256_(uint64_t x) { return (x + 255) & ~uint64_t(255); }
+}  // namespace
+
+// One cudaMalloc with 256-byte aligned slices, like the reference's single
+// VkDeviceMemory with aligned sub-buffers (VoxelSceneCacher.cpp:736-869).
+int scene_alloc(const vx_octree_config& c, uint32_t node_count, uint32_t brick_count, int32_t color_kind,
+                bool normals, vx_scene** out, ScenePool* p) {
+    *out = nullptr;
+    const uint64_t bpa = uint64_t(c.bricks_per_axis);
+    ScenePool q{};
+    q.sz_nodes = uint64_t(node_count) * sizeof(vx_node);
+    q.sz_nb = uint64_t(node_count) * 4;
+    q.sz_grid = bpa * bpa * bpa * 4;
+    q.sz_coord = uint64_t(brick_count) * 4;
+    q.sz_occ = uint64_t(brick_count) * 64;
+    if (color_kind == VX_COLOR_RGBA8) q.sz_color = uint64_t(brick_count) * 512 * 4;
+    if (color_kind == VX_COLOR_DXT1) q.sz_color = uint64_t(brick_count) * 32 * 8;
+    q.sz_nrm = normals ? uint64_t(brick_count) * 32 * 16 : 0;
+    const uint64_t o_nodes = 0;
+    const uint64_t o_nb = o_nodes + align256_(q.sz_nodes);
+    const uint64_t o_grid = o_nb + align256_(q.sz_nb);
+    const uint64_t o_coord = o_grid + align256_(q.sz_grid);
+    const uint64_t o_occ = o_coord + align256_(q.sz_coord);
+    const uint64_t o_color = o_occ + align256_(q.sz_occ);
+    const uint64_t o_nrm = o_color + align256_(q.sz_color);
+    const uint64_t total = o_nrm + align256_(q.sz_nrm) + 256;
+    auto* s = new (std::nothrow) vx_scene();
+    if (!s) return fail(VX_ENOMEM, "scene: out of host memory");
+    cudaError_t e = cudaGetDevice(&s->device);
+    if (e != cudaSuccess) { delete s; return cuda_fail(e, "scene: cudaGetDevice"); }
+    e = cudaMalloc(&s->pool, total);
+    if (e != cudaSuccess) { delete s; return cuda_fail(e, "scene: cudaMalloc"); }
+    s->pool_bytes = total;
+    char* base = static_cast<char*>(s->pool);
+    q.nodes = base + o_nodes;
+    q.node_brick = base + o_nb;
+    q.grid = base + o_grid;
+    q.coord = base + o_coord;
+    q.occ = base + o_occ;
+    q.color = q.sz_color ? base + o_color : nullptr;
+    q.nrm = q.sz_nrm ? base + o_nrm : nullptr;
+    DevScene& ds = s->dev;
+    for (int i = 0; i < 3; ++i) {
+        ds.wmin[i] = c.world_min[i];
+        ds.wmax[i] = c.world_max[i];
+        ds.wsize[i] = c.world_max[i] - c.world_min[i];
+        ds.wsm[i] = ds.wsize[i] - 0.001f;
+        ds.qwm[i] = int32_t(std::floor(c.world_min[i]));
+    }
+    // glm::length: sqrt of the left-to-right dot product
+    ds.wrl = std::sqrt((ds.wsize[0] * ds.wsize[0] + ds.wsize[1] * ds.wsize[1]) + ds.wsize[2] * ds.wsize[2]);
+    ds.max_levels = c.max_levels;
+    ds.min_scale = 22 - c.max_levels + 1;
+    ds.brick_user_scale = c.max_levels - c.brick_depth;
+    ds.bpa = c.bricks_per_axis;
+    ds.node_count = node_count;
+    ds.brick_count = brick_count;
+    ds.nodes = reinterpret_cast<const uint2*>(q.nodes);
+    ds.node_brick = reinterpret_cast<const uint32_t*>(q.node_brick);
+    ds.grid = reinterpret_cast<const uint32_t*>(q.grid);
+    ds.coord = reinterpret_cast<const uint32_t*>(q.coord);
+    ds.occ = reinterpret_cast<const uint4*>(q.occ);
+    ds.color_kind = color_kind;
+    ds.rgba = color_kind == VX_COLOR_RGBA8 ? reinterpret_cast<const uint32_t*>(q.color) : nullptr;
+    ds.dxt = color_kind == VX_COLOR_DXT1 ? reinterpret_cast<const uint2*>(q.color) : nullptr;
+    ds.nrm = reinterpret_cast<const uint4*>(q.nrm);
+    s->cfg = c;
+    *p = q;
+    *out = s;
+    return VX_OK;
+}
+
 }  // namespace vx
 
 namespace {
@@ -119,73 +194,24 @@ int vx_scene_create(const vx_scene_desc* d, vx_scene** out) {
     if (!d || !out) return fail(VX_EINVAL, "vx_scene_create: null argument");
     *out = nullptr;
     if (int r = validate(d)) return r;
-    const vx_octree_config& c = d->config;
-    const uint64_t bpa = uint64_t(c.bricks_per_axis);
-    const uint64_t sz_nodes = uint64_t(d->node_count) * sizeof(vx_node);
-    const uint64_t sz_nb = uint64_t(d->node_count) * 4;
-    const uint64_t sz_grid = bpa * bpa * bpa * 4;
-    const uint64_t sz_coord = uint64_t(d->brick_count) * 4;
-    const uint64_t sz_occ = uint64_t(d->brick_count) * 64;
-    uint64_t sz_color = 0;
-    if (d->color_kind == VX_COLOR_RGBA8) sz_color = uint64_t(d->brick_count) * 512 * 4;
-    if (d->color_kind == VX_COLOR_DXT1) sz_color = uint64_t(d->brick_count) * 32 * 8;
-    const uint64_t sz_nrm = d->brick_normal ? uint64_t(d->brick_count) * 32 * 16 : 0;
-    const uint64_t o_nodes = 0;
-    const uint64_t o_nb = o_nodes + align256(sz_nodes);
-    const uint64_t o_grid = o_nb + align256(sz_nb);
-    const uint64_t o_coord = o_grid + align256(sz_grid);
-    const uint64_t o_occ = o_coord + align256(sz_coord);
-    const uint64_t o_color = o_occ + align256(sz_occ);
-    const uint64_t o_nrm = o_color + align256(sz_color);
-    const uint64_t total = o_nrm + align256(sz_nrm) + 256;
-
-    auto* s = new (std::nothrow) vx_scene();
-    if (!s) return fail(VX_ENOMEM, "vx_scene_create: out of host memory");
-    cudaError_t e = cudaGetDevice(&s->device);
-    if (e != cudaSuccess) { delete s; return vx::cuda_fail(e, "vx_scene_create: cudaGetDevice"); }
-    e = cudaMalloc(&s->pool, total);
-    if (e != cudaSuccess) { delete s; return vx::cuda_fail(e, "vx_scene_create: cudaMalloc"); }
-    s->pool_bytes = total;
-    char* base = static_cast<char*>(s->pool);
-    struct Copy { uint64_t off; const void* src; uint64_t n; };
-    const Copy copies[] = {{o_nodes, d->nodes, sz_nodes}, {o_nb, d->node_brick, sz_nb},
-                           {o_grid, d->grid_lookup, sz_grid}, {o_coord, d->brick_coord, sz_coord},
-                           {o_occ, d->brick_occ, sz_occ}, {o_color, d->brick_color, sz_color},
-                           {o_nrm, d->brick_normal, sz_nrm}};
+    vx::ScenePool p;
+    vx_scene* s = nullptr;
+    if (int r = vx::scene_alloc(d->config, d->node_count, d->brick_count, d->color_kind, d->brick_normal != nullptr,
+                                &s, &p))
+        return r;
+    struct Copy { void* dst; const void* src; uint64_t n; };
+    const Copy copies[] = {{p.nodes, d->nodes, p.sz_nodes}, {p.node_brick, d->node_brick, p.sz_nb},
+                           {p.grid, d->grid_lookup, p.sz_grid}, {p.coord, d->brick_coord, p.sz_coord},
+                           {p.occ, d->brick_occ, p.sz_occ}, {p.color, d->brick_color, p.sz_color},
+                           {p.nrm, d->brick_normal, p.sz_nrm}};
     for (const Copy& cp : copies) {
         if (!cp.n) continue;
-        e = cudaMemcpy(base + cp.off, cp.src, cp.n, cudaMemcpyHostToDevice);
+        cudaError_t e = cudaMemcpy(cp.dst, cp.src, cp.n, cudaMemcpyHostToDevice);
         if (e != cudaSuccess) {
-            cudaFree(s->pool);
-            delete s;
+            vx_scene_destroy(s);
             return vx::cuda_fail(e, "vx_scene_create: cudaMemcpy");
         }
     }
-    vx::DevScene& ds = s->dev;
-    for (int i = 0; i < 3; ++i) {
-        ds.wmin[i] = c.world_min[i];
-        ds.wmax[i] = c.world_max[i];
-        ds.wsize[i] = c.world_max[i] - c.world_min[i];
-        ds.wsm[i] = ds.wsize[i] - 0.001f;
-        ds.qwm[i] = int32_t(std::floor(c.world_min[i]));
-    }
-    // glm::length: sqrt of the left-to-right dot product
-    ds.wrl = std::sqrt((ds.wsize[0] * ds.wsize[0] + ds.wsize[1] * ds.wsize[1]) + ds.wsize[2] * ds.wsize[2]);
-    ds.max_levels = c.max_levels;
-    ds.min_scale = 22 - c.max_levels + 1;
-    ds.brick_user_scale = c.max_levels - c.brick_depth;
-    ds.bpa = c.bricks_per_axis;
-    ds.node_count = d->node_count;
-    ds.brick_count = d->brick_count;
-    ds.nodes = reinterpret_cast<const uint2*>(base + o_nodes);
-    ds.node_brick = reinterpret_cast<const uint32_t*>(base + o_nb);
-    ds.grid = reinterpret_cast<const uint32_t*>(base + o_grid);
-    ds.coord = reinterpret_cast<const uint32_t*>(base + o_coord);
-    ds.occ = reinterpret_cast<const uint4*>(base + o_occ);
-    ds.color_kind = d->color_kind;
-    ds.rgba = d->color_kind == VX_COLOR_RGBA8 ? reinterpret_cast<const uint32_t*>(base + o_color) : nullptr;
-    ds.dxt = d->color_kind == VX_COLOR_DXT1 ? reinterpret_cast<const uint2*>(base + o_color) : nullptr;
-    ds.nrm = sz_nrm ? reinterpret_cast<const uint4*>(base + o_nrm) : nullptr;
     *out = s;
     return VX_OK;
 }
@@ -201,6 +227,41 @@ int vx_scene_destroy(vx_scene* s) {
     delete s;
     if (e1 != cudaSuccess) return vx::cuda_fail(e1, "vx_scene_destroy: cudaFree");
     if (e2 != cudaSuccess) return vx::cuda_fail(e2, "vx_scene_destroy: cudaFree");
+    return VX_OK;
+}
+
+int vx_scene_info_get(const vx_scene* s, vx_scene_info* out) {
+    if (!s || !out) return fail(VX_EINVAL, "vx_scene_info_get: null argument");
+    vx_scene_info i{};
+    i.config = s->cfg;
+    i.node_count = s->dev.node_count;
+    i.brick_count = s->dev.brick_count;
+    i.color_kind = s->dev.color_kind;
+    i.has_normals = s->dev.nrm != nullptr;
+    *out = i;
+    return VX_OK;
+}
+
+int vx_scene_download(const vx_scene* s, uint32_t* nodes, uint32_t* node_brick, uint32_t* grid_lookup,
+                      uint32_t* brick_coord, uint32_t* brick_occ, void* brick_color, uint64_t* brick_normal) {
+    if (!s) return fail(VX_EINVAL, "vx_scene_download: null scene");
+    const vx::DevScene& d = s->dev;
+    const uint64_t bpa = uint64_t(d.bpa), B = d.brick_count;
+    const uint64_t colw = d.color_kind == VX_COLOR_RGBA8 ? 512 * 4 : d.color_kind == VX_COLOR_DXT1 ? 32 * 8 : 0;
+    const void* color_src = d.rgba ? static_cast<const void*>(d.rgba) : static_cast<const void*>(d.dxt);
+    struct Copy { void* dst; const void* src; uint64_t n; };
+    const Copy copies[] = {{nodes, d.nodes, uint64_t(d.node_count) * 8}, {node_brick, d.node_brick, uint64_t(d.node_count) * 4},
+                           {grid_lookup, d.grid, bpa * bpa * bpa * 4}, {brick_coord, d.coord, B * 4},
+                           {brick_occ, d.occ, B * 64}, {brick_color, color_src, B * colw},
+                           {brick_normal, d.nrm, d.nrm ? B * 512 : 0}};
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (dev != s->device) cudaSetDevice(s->device);
+    cudaError_t e = cudaSuccess;
+    for (const Copy& c : copies)
+        if (c.dst && c.n && e == cudaSuccess) e = cudaMemcpy(c.dst, c.src, c.n, cudaMemcpyDeviceToHost);
+    if (dev >= 0 && dev != s->device) cudaSetDevice(dev);
+    if (e != cudaSuccess) return vx::cuda_fail(e, "vx_scene_download");
     return VX_OK;
 }
 

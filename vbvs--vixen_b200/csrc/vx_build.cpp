@@ -24,24 +24,14 @@
 #include <thread>
 #include <vector>
 
+#include "vx_hash.h"
 #include "vx_internal.h"
 
 namespace {
 
 constexpr uint32_t NONE = 0xFFFFFFFFu;
 
-uint64_t expand3(uint32_t v) {  // 21-bit spread, x in bit 0 (MortonEncoding.cpp:19-27)
-    uint64_t x = v & 0x1FFFFF;
-    x = (x | x << 32) & 0x1F00000000FFFFULL;
-    x = (x | x << 16) & 0x1F0000FF0000FFULL;
-    x = (x | x << 8) & 0x100F00F00F00F00FULL;
-    x = (x | x << 4) & 0x10C30C30C30C30C3ULL;
-    x = (x | x << 2) & 0x1249249249249249ULL;
-    return x;
-}
-inline uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
-    return expand3(x) | (expand3(y) << 1) | (expand3(z) << 2);
-}
+using vx::morton3;
 
 int hw_threads() {
     unsigned t = std::thread::hardware_concurrency();
@@ -61,19 +51,7 @@ void parallel_for(int64_t n, F&& f) {
     for (auto& x : th) x.join();
 }
 
-// ---- hashing for synthetic inputs (counter based, seeded) ----
-inline uint64_t splitmix64(uint64_t z) {
-    z += 0x9E3779B97F4A7C15ULL;
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
-    return z ^ (z >> 31);
-}
-inline uint64_t hash4(uint64_t seed, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
-    uint64_t h = splitmix64(seed ^ 0x5851F42D4C957F2DULL);
-    h = splitmix64(h ^ ((uint64_t(a) << 32) | b));
-    h = splitmix64(h ^ ((uint64_t(c) << 32) | d));
-    return h;
-}
+using vx::hash4;
 
 }  // namespace
 
@@ -418,7 +396,7 @@ int vx_synth_rgba8(const uint32_t* coord, uint32_t B, uint64_t seed, uint32_t* o
     if ((!coord || !out) && B) return fail(VX_EINVAL, "vx_synth_rgba8: null argument");
     parallel_for(int64_t(B), [&](int64_t b) {
         for (uint32_t v = 0; v < 512; ++v)
-            out[size_t(b) * 512 + v] = uint32_t(hash4(seed, 0x72676261u, coord[b], v, 0)) | 0xFF000000u;
+            out[size_t(b) * 512 + v] = vx::synth_rgba8_word(seed, coord[b], v);
     });
     return VX_OK;
 }
@@ -427,7 +405,7 @@ int vx_synth_dxt1(const uint32_t* coord, uint32_t B, uint64_t seed, uint64_t* ou
     using namespace vx;
     if ((!coord || !out) && B) return fail(VX_EINVAL, "vx_synth_dxt1: null argument");
     parallel_for(int64_t(B), [&](int64_t b) {
-        for (uint32_t k = 0; k < 32; ++k) out[size_t(b) * 32 + k] = hash4(seed, 0x64787431u, coord[b], k, 0);
+        for (uint32_t k = 0; k < 32; ++k) out[size_t(b) * 32 + k] = vx::synth_dxt1_block(seed, coord[b], k);
     });
     return VX_OK;
 }

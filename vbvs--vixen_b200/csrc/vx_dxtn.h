@@ -24,11 +24,7 @@
 
 #include <cmath>
 
-#ifdef __CUDACC__
-#define VX_HD __host__ __device__ __forceinline__
-#else
-#define VX_HD inline
-#endif
+#include "vx_hd.h"
 
 namespace vx {
 namespace dxtn {

@@ -37,6 +37,17 @@ struct DevScene {
 const DevScene& scene_dev(const vx_scene* s);
 int scene_device(const vx_scene* s);
 
+// Device slices of a new scene's pool and their sizes in bytes.
+struct ScenePool {
+    void *nodes, *node_brick, *grid, *coord, *occ, *color, *nrm;
+    uint64_t sz_nodes, sz_nb, sz_grid, sz_coord, sz_occ, sz_color, sz_nrm;
+};
+// Allocates a scene on the current device for the given counts and fills its
+// device view; the caller writes the slices (vx_scene_destroy frees it).
+int scene_alloc(const vx_octree_config& c, uint32_t node_count, uint32_t brick_count, int32_t color_kind,
+                bool normals, vx_scene** out, ScenePool* p);
+int cuda_fail(cudaError_t e, const std::string& what);
+
 // Per-thread-local error string.
 void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);

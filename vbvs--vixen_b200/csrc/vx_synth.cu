@@ -8,23 +8,11 @@
 #include <cstdint>
 #include <vector>
 
+#include "vx_hash.h"
 #include "vx_internal.h"
 
 namespace vx {
 namespace {
-
-__host__ __device__ inline uint64_t splitmix64(uint64_t z) {
-    z += 0x9E3779B97F4A7C15ULL;
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
-    return z ^ (z >> 31);
-}
-__device__ inline uint64_t hash4(uint64_t seed, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
-    uint64_t h = splitmix64(seed ^ 0x5851F42D4C957F2DULL);
-    h = splitmix64(h ^ ((uint64_t(a) << 32) | b));
-    h = splitmix64(h ^ ((uint64_t(c) << 32) | d));
-    return h;
-}
 
 struct OctDev {
     uint32_t s, cells;
