@@ -36,7 +36,9 @@ typedef enum vx_status {
     VX_EOVERFLOW = -3,  /* a size is beyond a format limit */
     VX_ETIMEOUT = -4,   /* a bounded device-side wait gave up */
     VX_ENOMEM = -5,     /* host or device allocation failed */
-    VX_ENOTFOUND = -6   /* no CUDA device, or the library was built without one */
+    VX_ENOTFOUND = -6,  /* no CUDA device, or the library was built without one */
+    VX_EIO = -7,        /* a file could not be opened, read or written */
+    VX_EFORMAT = -8     /* a file is not in the expected format */
 } vx_status;
 
 /* ------------------------------------------------------------------------
@@ -195,6 +197,28 @@ int vx_scene_info_get(const vx_scene* scene, vx_scene_info* out);
 int vx_scene_download(const vx_scene* scene, uint32_t* nodes, uint32_t* node_brick, uint32_t* grid_lookup,
                       uint32_t* brick_coord, uint32_t* brick_occ, void* brick_color,
                       uint64_t* brick_normal);
+
+/* ------------------------------------------------------------------------
+ * Scene cache files.  Replaces VoxelSceneCacher::SerializeToFile /
+ * DeserializeFromFile (CashSystem/src/VoxelSceneCacher.cpp:179-364).
+ * VXSC: this library's format, every array of a scene exactly, with a
+ * checksum.  VSCA version 1: the reference's format (one entry written;
+ * reading picks entry `entry`): ESVO descriptors in ChildDescriptor layout
+ * (child pointers must fit 15 bits), brickData material words (occupied = 1),
+ * DXT1 colours, DXT normals, brickGridLookup, OctreeConfig.  A vx_cache holds
+ * the host arrays; vx_cache_desc exposes them for vx_scene_create.
+ * --------------------------------------------------------------------- */
+typedef struct vx_cache vx_cache;
+int vx_cache_write(const char* path, const vx_scene_desc* desc);
+int vx_cache_read(const char* path, vx_cache** out);
+int vx_cache_write_vsca(const char* path, const vx_scene_desc* desc, uint32_t scene_type,
+                        uint32_t resolution, float density, uint32_t seed);
+int vx_cache_read_vsca(const char* path, uint32_t entry, vx_cache** out);
+int vx_cache_desc(const vx_cache* cache, vx_scene_desc* desc);
+int vx_cache_free(vx_cache* cache);
+/* vx_scene_download + vx_cache_write, and vx_cache_read + vx_scene_create. */
+int vx_scene_save(const vx_scene* scene, const char* path);
+int vx_scene_load(const char* path, vx_scene** out);
 
 /* Device scene builder: the arrays of vx_build_dense, index for index, built
  * on the current device from R^3 occupancy bits already in device memory

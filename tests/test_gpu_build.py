@@ -101,3 +101,26 @@ def test_cfg2_scale_identical_and_casts_equal(vx, cuda):
     vx.Scene(want).cast_rays_dev(rays, h2)
     torch.cuda.synchronize()
     assert torch.equal(h1, h2)
+
+
+def test_scene_save_load_round_trip(vx, cuda, tmp_path):
+    """A device-built scene saved to a VXSC file and loaded back casts the same
+    hits and holds the same arrays."""
+    import torch
+    from vx_b200 import workloads as W
+    R = 256
+    bits = vx.synth_noise(R, 32, 4, 0.2, 6, True)
+    s = _device_scene(vx, bits, R, 8, vx.VX_COLOR_DXT1, 3, True)
+    p = str(tmp_path / "scene.vxsc")
+    s.save(p)
+    t = vx.Scene.load(p)
+    a, b = s.arrays, t.arrays
+    for k in ["nodes", "node_brick", "grid_lookup", "brick_coord", "brick_occ", "brick_color", "brick_normal"]:
+        np.testing.assert_array_equal(getattr(a, k), getattr(b, k), err_msg=k)
+    rays = torch.from_numpy(W.random_rays(50000, R, seed=8)).cuda()
+    h1 = torch.zeros((rays.shape[0], 4), dtype=torch.int32, device="cuda")
+    h2 = torch.zeros_like(h1)
+    s.cast_rays_dev(rays, h1)
+    t.cast_rays_dev(rays, h2)
+    torch.cuda.synchronize()
+    assert torch.equal(h1, h2)

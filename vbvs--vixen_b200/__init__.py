@@ -104,6 +104,14 @@ def lib():
         "vx_scene_info_get": (C.c_int, [vp, vp]),
         "vx_scene_download": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, vp]),
         "vx_scene_create_dense_dev": (C.c_int, [vp, u32, i32, i32, u64, i32, vp, vp]),
+        "vx_cache_write": (C.c_int, [C.c_char_p, vp]),
+        "vx_cache_read": (C.c_int, [C.c_char_p, vp]),
+        "vx_cache_write_vsca": (C.c_int, [C.c_char_p, vp, u32, u32, f32, u32]),
+        "vx_cache_read_vsca": (C.c_int, [C.c_char_p, u32, vp]),
+        "vx_cache_desc": (C.c_int, [vp, vp]),
+        "vx_cache_free": (C.c_int, [vp]),
+        "vx_scene_save": (C.c_int, [vp, C.c_char_p]),
+        "vx_scene_load": (C.c_int, [C.c_char_p, vp]),
         "vx_render": (C.c_int, [vp, vp, u32, u32, vp, vp, vp, vp]),
         "vx_camera_rays": (C.c_int, [vp, u32, u32, vp]),
         "vx_camera_rays_dev": (C.c_int, [vp, u32, u32, vp, vp]),
@@ -285,6 +293,85 @@ def camera_rays(pc: CameraPC, width: int, height: int) -> np.ndarray:
 # Device scene
 # ---------------------------------------------------------------------------
 
+def _desc_of(a: SceneArrays):
+    """vx_scene_desc pointing into the host arrays of `a` (kept alive by the returned list)."""
+    d = _SceneDesc()
+    d.config.world_min[:] = [float(v) for v in a.world_min]
+    d.config.world_max[:] = [float(v) for v in a.world_max]
+    d.config.max_levels = a.max_levels
+    d.config.brick_depth = 3
+    d.config.bricks_per_axis = a.bricks_per_axis
+    keep = [np.ascontiguousarray(x, np.uint32) for x in (a.nodes, a.node_brick, a.grid_lookup, a.brick_coord,
+                                                         a.brick_occ)]
+    d.nodes, d.node_brick, d.grid_lookup, d.brick_coord, d.brick_occ = [_p(x) for x in keep]
+    d.node_count = a.node_count
+    d.brick_count = a.brick_count
+    d.color_kind = a.color_kind
+    if a.brick_color is not None:
+        keep.append(np.ascontiguousarray(a.brick_color))
+        d.brick_color = _p(keep[-1])
+    if a.brick_normal is not None:
+        assert a.brick_normal.size == a.brick_count * 64
+        keep.append(np.ascontiguousarray(a.brick_normal, np.uint64))
+        d.brick_normal = _p(keep[-1])
+    return d, keep
+
+
+def _arrays_of_cache(h) -> SceneArrays:
+    d = _SceneDesc()
+    check(lib().vx_cache_desc(h, C.byref(d)))
+    bpa, B, D = d.config.bricks_per_axis, d.brick_count, d.node_count
+
+    def take(ptr, n, dt):
+        if n == 0 or not ptr:
+            return np.zeros(0, dt)
+        buf = (C.c_char * (n * np.dtype(dt).itemsize)).from_address(ptr)
+        return np.frombuffer(buf, dtype=dt, count=n).copy()
+
+    color = None
+    if d.color_kind == VX_COLOR_RGBA8:
+        color = take(d.brick_color, 512 * B, np.uint32)
+    elif d.color_kind == VX_COLOR_DXT1:
+        color = take(d.brick_color, 32 * B, np.uint64)
+    normal = take(d.brick_normal, 64 * B, np.uint64).reshape(B, 32, 2) if d.brick_normal else None
+    return SceneArrays(tuple(d.config.world_min), tuple(d.config.world_max), d.config.max_levels, bpa,
+                       take(d.nodes, 2 * D, np.uint32), take(d.node_brick, D, np.uint32),
+                       take(d.grid_lookup, bpa ** 3, np.uint32), take(d.brick_coord, B, np.uint32),
+                       take(d.brick_occ, 16 * B, np.uint32), d.color_kind if color is not None else VX_COLOR_NONE,
+                       color, normal)
+
+
+def cache_write(path: str, arrays: SceneArrays):
+    """vx_cache_write (VXSC)."""
+    d, keep = _desc_of(arrays)
+    check(lib().vx_cache_write(os.fsencode(path), C.byref(d)))
+
+
+def cache_read(path: str) -> SceneArrays:
+    """vx_cache_read (VXSC) -> host arrays."""
+    h = C.c_void_p()
+    check(lib().vx_cache_read(os.fsencode(path), C.byref(h)))
+    try:
+        return _arrays_of_cache(h)
+    finally:
+        lib().vx_cache_free(h)
+
+
+def cache_write_vsca(path: str, arrays: SceneArrays, scene_type: int, resolution: int, density: float, seed: int):
+    """vx_cache_write_vsca: the reference's VoxelSceneCacher file format."""
+    d, keep = _desc_of(arrays)
+    check(lib().vx_cache_write_vsca(os.fsencode(path), C.byref(d), scene_type, resolution, float(density), seed))
+
+
+def cache_read_vsca(path: str, entry: int = 0) -> SceneArrays:
+    h = C.c_void_p()
+    check(lib().vx_cache_read_vsca(os.fsencode(path), entry, C.byref(h)))
+    try:
+        return _arrays_of_cache(h)
+    finally:
+        lib().vx_cache_free(h)
+
+
 class _SceneInfo(C.Structure):
     _fields_ = [("config", _Config), ("node_count", C.c_uint32), ("brick_count", C.c_uint32),
                 ("color_kind", C.c_int32), ("has_normals", C.c_int32)]
@@ -332,29 +419,21 @@ class Scene:
 
     def __init__(self, arrays: SceneArrays):
         self._arrays = arrays
-        a = arrays
-        d = _SceneDesc()
-        d.config.world_min[:] = [float(v) for v in a.world_min]
-        d.config.world_max[:] = [float(v) for v in a.world_max]
-        d.config.max_levels = a.max_levels
-        d.config.brick_depth = 3
-        d.config.bricks_per_axis = a.bricks_per_axis
-        self._keep = [np.ascontiguousarray(x) for x in (a.nodes, a.node_brick, a.grid_lookup, a.brick_coord,
-                                                         a.brick_occ)]
-        d.nodes, d.node_brick, d.grid_lookup, d.brick_coord, d.brick_occ = [_p(x) for x in self._keep]
-        d.node_count = a.node_count
-        d.brick_count = a.brick_count
-        d.color_kind = a.color_kind
-        if a.brick_color is not None:
-            self._keep.append(np.ascontiguousarray(a.brick_color))
-            d.brick_color = _p(self._keep[-1])
-        if a.brick_normal is not None:
-            assert a.brick_normal.size == a.brick_count * 64
-            self._keep.append(np.ascontiguousarray(a.brick_normal, np.uint64))
-            d.brick_normal = _p(self._keep[-1])
+        d, keep = _desc_of(arrays)
         self._h = C.c_void_p()
         check(lib().vx_scene_create(C.byref(d), C.byref(self._h)))
-        self._keep = None  # the scene holds device copies
+        del keep  # the scene holds device copies
+
+    @classmethod
+    def load(cls, path: str) -> "Scene":
+        """vx_scene_load: a VXSC cache file straight into a device scene."""
+        h = C.c_void_p()
+        check(lib().vx_scene_load(os.fsencode(path), C.byref(h)))
+        return cls.from_handle(h)
+
+    def save(self, path: str):
+        """vx_scene_save: the scene's arrays into a VXSC cache file."""
+        check(lib().vx_scene_save(self._h, os.fsencode(path)))
 
     @property
     def handle(self):
