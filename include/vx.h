@@ -439,6 +439,16 @@ int vx_build_normals(const uint32_t* brick_occ, uint32_t brick_count, uint64_t* 
 int vx_build_normals_dev(const uint32_t* brick_occ_dev, uint32_t brick_count, uint64_t* out_dev,
                          void* stream);
 
+/* DXT1 colour payload of bricks from per-voxel colours (rgb: brick_count x
+ * 512 x 3 floats, voxel z*64+y*8+x) and occupancy: empty voxels (0,0,0),
+ * each block of 16 encoded by DXT1ColorCompressor::encodeBlockTyped
+ * (DXT1Compressor.cpp:57-111), empty blocks 0 (SVORebuild.cpp:658-722).
+ * out: brick_count x 32 u64, the layout of VX_COLOR_DXT1.  Host and device
+ * forms produce identical bits. */
+int vx_build_dxt1(const float* rgb, const uint32_t* brick_occ, uint32_t brick_count, uint64_t* out);
+int vx_build_dxt1_dev(const float* rgb_dev, const uint32_t* brick_occ_dev, uint32_t brick_count,
+                      uint64_t* out_dev, void* stream);
+
 /* Converts reference-layout descriptors (64-bit ChildDescriptor,
  * SVOTypes.h:36-47: childPointer:15 far:1 valid:8 leaf:8 | brick:24 flags:8)
  * into vx_node + node_brick.  Far pointers are rejected (VX_EINVAL). */

@@ -1522,3 +1522,21 @@ uint32_t vxo_shade_dxt_normal(const float color[3], int hit, const float n_dxt[3
 }
 
 }  // extern "C"
+
+// The colour half of the rebuild's per-brick compression (SVORebuild.cpp:658-722):
+// empty texels are (0,0,0); a block with an occupied texel is encoded over all
+// 16 texels (encodeBlockTyped(blockColors, 16, nullptr)), an empty block is 0.
+extern "C" void vxo_brick_dxt1(const float* rgb, const uint32_t* occ, uint64_t brick_count, uint64_t* out) {
+    for (uint64_t b = 0; b < brick_count; ++b)
+        for (int k = 0; k < 32; ++k) {
+            float cols[48];
+            bool any = false;
+            for (int t = 0; t < 16; ++t) {
+                const int i = k * 16 + t;
+                const bool o = (occ[b * 16 + (i >> 5)] >> (i & 31)) & 1u;
+                any = any || o;
+                for (int c = 0; c < 3; ++c) cols[3 * t + c] = o ? rgb[(b * 512 + i) * 3 + c] : 0.0f;
+            }
+            out[b * 32 + k] = any ? vxo_dxt1_encode_block(cols, 16, nullptr) : 0;
+        }
+}

@@ -131,6 +131,10 @@ void vxo_geometric_normals(const uint32_t* occ, float out[1536]);
  * 32 blocks x {blockA, blockB} per brick. */
 void vxo_brick_normals(const uint32_t* occ, uint64_t brick_count, uint64_t* out, int nthreads);
 
+/* DXT1 colour payload of brick_count bricks from per-voxel RGB (512 x 3
+ * floats per brick) and occupancy (SVORebuild.cpp:658-722). */
+void vxo_brick_dxt1(const float* rgb, const uint32_t* occ, uint64_t brick_count, uint64_t* out);
+
 /* normalize(decodeDXTNormal) of a hit voxel (VoxelRayMarch_Compressed.comp:160-165). */
 void vxo_hit_normal_dxt(const uint64_t* brick_nrm, uint32_t brick, uint32_t voxel, float out[3]);
 

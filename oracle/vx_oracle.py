@@ -71,6 +71,7 @@ def lib():
         L.vxo_geometric_normals.argtypes = [vp, vp]
         L.vxo_brick_normals.argtypes = [vp, u64, vp, C.c_int]
         L.vxo_hit_normal_dxt.argtypes = [vp, u32, u32, vp]
+        L.vxo_brick_dxt1.argtypes = [vp, vp, u64, vp]
         L.vxo_shade_dxt_normal.restype = u32
         L.vxo_shade_dxt_normal.argtypes = [vp, C.c_int, vp, C.c_int, C.c_int, f32]
         _lib = L
@@ -249,6 +250,15 @@ def brick_normals(occ: np.ndarray, threads=0) -> np.ndarray:
     occ = np.ascontiguousarray(occ, dtype=np.uint32).reshape(-1, 16)
     out = np.zeros((occ.shape[0], 32, 2), np.uint64)
     lib().vxo_brick_normals(_ptr(occ), occ.shape[0], _ptr(out), int(threads))
+    return out
+
+
+def brick_dxt1(rgb: np.ndarray, occ: np.ndarray) -> np.ndarray:
+    """DXT1 colour payload (bricks*32 u64) from per-voxel RGB floats and occupancy."""
+    rgb = np.ascontiguousarray(rgb, dtype=np.float32)
+    occ = np.ascontiguousarray(occ, dtype=np.uint32).reshape(-1, 16)
+    out = np.zeros(occ.shape[0] * 32, np.uint64)
+    lib().vxo_brick_dxt1(_ptr(rgb), _ptr(occ), occ.shape[0], _ptr(out))
     return out
 
 

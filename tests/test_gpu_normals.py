@@ -109,3 +109,16 @@ def test_render_with_normals_matches_oracle_shading(vx, vo, cuda, kind):
         want = vo.shade_dxt_normal(col, hit, nd, (int(oh["flags"][i]) >> 1) & 3, bool(oh["flags"][i] & 8),
                                    float(uv_y))
         assert image[i] == want, (i, hex(image[i]), hex(want))
+
+
+def test_device_dxt1_builder_equals_oracle(vx, vo, cuda):
+    import torch
+    from test_normals import _colours
+    occ = _bricks(16, 2000)
+    rgb = _colours(17, 2000)
+    o = torch.from_numpy(occ.view(np.int32).reshape(-1)).cuda()
+    c = torch.from_numpy(rgb.reshape(-1)).cuda()
+    out = torch.zeros(2000 * 32, dtype=torch.int64, device="cuda")
+    vx.build_dxt1_dev(c, o, out)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(out.cpu().numpy().view(np.uint64), vo.brick_dxt1(rgb, occ))

@@ -103,3 +103,37 @@ def test_geometric_normals_survive_compression(vo):
                 if (occ[b, i >> 5] >> (i & 31)) & 1:
                     dots.append(float(np.dot(dec[t], g[i])))
     assert np.mean(dots) > 0.8
+
+
+def _colours(seed, n):
+    rng = np.random.default_rng(seed)
+    rgb = rng.random((n, 512, 3), dtype=np.float32)
+    # smooth gradients in half the bricks, as rebuilt scene colours are
+    t = np.linspace(0, 1, 512, dtype=np.float32)[None, :, None]
+    rgb[::2] = (t * rng.random((n, 1, 3), dtype=np.float32) + (1 - t) * rng.random((n, 1, 3), dtype=np.float32))[::2]
+    return rgb
+
+
+def test_host_dxt1_builder_equals_oracle(vx, vo):
+    occ = _bricks(12, 200)
+    rgb = _colours(13, 200)
+    want = vo.brick_dxt1(rgb, occ)
+    np.testing.assert_array_equal(vx.build_dxt1(rgb, occ), want)
+    assert np.all(want[:32] == 0)  # empty brick
+
+
+def test_dxt1_payload_decodes_close(vx, vo):
+    """Decoded texels of occupied voxels stay near their colours
+    (CompressedBufferRoundTrip, test_block_compressor.cpp:205-240: 0.3)."""
+    occ = _bricks(14, 20)
+    rgb = _colours(15, 20)
+    out = vx.build_dxt1(rgb, occ)
+    errs = []
+    for b in range(2, 20, 2):
+        for k in range(32):
+            dec = vo.dxt1_decode_block(int(out[b * 32 + k]))
+            for t in range(16):
+                i = 16 * k + t
+                if (occ[b, i >> 5] >> (i & 31)) & 1:
+                    errs.append(float(np.linalg.norm(dec[t] - rgb[b, i])))
+    assert np.median(errs) < 0.3

@@ -101,6 +101,8 @@ def lib():
         "vx_build_normals": (C.c_int, [vp, u32, vp]),
         "vx_build_normals_dev": (C.c_int, [vp, u32, vp, vp]),
         "vx_hit_normals": (C.c_int, [vp, vp, u32, vp, vp]),
+        "vx_build_dxt1": (C.c_int, [vp, vp, u32, vp]),
+        "vx_build_dxt1_dev": (C.c_int, [vp, vp, u32, vp, vp]),
         "vx_scene_info_get": (C.c_int, [vp, vp]),
         "vx_scene_download": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, vp]),
         "vx_scene_create_dense_dev": (C.c_int, [vp, u32, i32, i32, u64, i32, vp, vp]),
@@ -258,6 +260,20 @@ def build_normals(brick_occ: np.ndarray) -> np.ndarray:
     out = np.zeros((occ.shape[0], 32, 2), np.uint64)
     check(lib().vx_build_normals(_p(occ), occ.shape[0], _p(out)))
     return out
+
+
+def build_dxt1(rgb: np.ndarray, brick_occ: np.ndarray) -> np.ndarray:
+    """DXT1 colour payload (bricks*32 u64) from per-voxel RGB floats (bricks, 512, 3) (vx_build_dxt1, host)."""
+    occ = np.ascontiguousarray(brick_occ, np.uint32).reshape(-1, 16)
+    c = np.ascontiguousarray(rgb, np.float32).reshape(occ.shape[0], 512, 3)
+    out = np.zeros(occ.shape[0] * 32, np.uint64)
+    check(lib().vx_build_dxt1(_p(c), _p(occ), occ.shape[0], _p(out)))
+    return out
+
+
+def build_dxt1_dev(rgb, occ, out, stream=None):
+    """vx_build_dxt1_dev: rgb (bricks*512*3) float32, occ (bricks*16) 32-bit, out (bricks*32) 8-byte CUDA tensors."""
+    check(lib().vx_build_dxt1_dev(_p(rgb), _p(occ), occ.numel() // 16, _p(out), _stream(stream)))
 
 
 def build_normals_dev(occ, out, stream=None):

@@ -1,12 +1,15 @@
-// vx_normals.cu - the DXT normal payload: built on the GPU (one thread per
-// 16-voxel block) or on the host from the same code, and the per-hit decode of
-// the compressed shader (getCompressedVoxelNormal,
+// vx_payload.cu - the compressed brick payloads the rebuild writes
+// (SVORebuild.cpp:615-722): DXT normal blocks from geometric normals and DXT1
+// colour blocks from per-voxel colours, each built on the GPU (one thread per
+// 16-voxel block) or on the host from the same code; and the per-hit normal
+// decode of the compressed shader (getCompressedVoxelNormal,
 // VoxelRayMarch_Compressed.comp:160-165).
 #include <algorithm>
 #include <thread>
 #include <vector>
 
 #include "vx_cast.cuh"
+#include "vx_dxt1.h"
 #include "vx_dxtn.h"
 
 namespace vx {
@@ -29,6 +32,23 @@ __global__ void __launch_bounds__(256) build_normals_kernel(const uint4* __restr
         uint64_t a, b;
         dxtn::brick_block(w, int(i & 31), a, b);
         out[i] = make_uint4(uint32_t(a), uint32_t(a >> 32), uint32_t(b), uint32_t(b >> 32));
+    }
+}
+
+// Thread i encodes colour block i & 31 of brick i >> 5 from the brick's 512
+// RGB texels (6 KiB per brick, read through L1 by the warp that shares it).
+__global__ void __launch_bounds__(256) build_dxt1_kernel(const float* __restrict__ rgb, const uint4* __restrict__ occ,
+                                                         uint64_t blocks, uint64_t* __restrict__ out) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < blocks;
+         i += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t brick = i >> 5;
+        uint32_t w[16];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint4 q = __ldg(occ + brick * 4 + k);
+            w[4 * k] = q.x; w[4 * k + 1] = q.y; w[4 * k + 2] = q.z; w[4 * k + 3] = q.w;
+        }
+        out[i] = dxt1::brick_block(rgb + brick * 512 * 3, w, int(i & 31));
     }
 }
 
@@ -78,6 +98,48 @@ extern "C" int vx_build_normals(const uint32_t* occ, uint32_t brick_count, uint6
     auto work = [&](uint64_t b0, uint64_t b1) {
         for (uint64_t b = b0; b < b1; ++b)
             for (int k = 0; k < 32; ++k) dxtn::brick_block(occ + 16 * b, k, out[(b * 32 + k) * 2], out[(b * 32 + k) * 2 + 1]);
+    };
+    if (T == 1 || brick_count < 256) {
+        work(0, brick_count);
+        return VX_OK;
+    }
+    std::vector<std::thread> th;
+    const uint64_t chunk = (uint64_t(brick_count) + T - 1) / T;
+    for (unsigned t = 0; t < T; ++t) {
+        const uint64_t b0 = uint64_t(t) * chunk, b1 = std::min<uint64_t>(brick_count, b0 + chunk);
+        if (b0 >= b1) break;
+        th.emplace_back(work, b0, b1);
+    }
+    for (auto& x : th) x.join();
+    return VX_OK;
+}
+
+extern "C" int vx_build_dxt1_dev(const float* rgb_dev, const uint32_t* occ_dev, uint32_t brick_count,
+                                 uint64_t* out_dev, void* stream) {
+    using namespace vx;
+    if (brick_count && (!rgb_dev || !occ_dev || !out_dev)) return fail(VX_EINVAL, "vx_build_dxt1_dev: null argument");
+    if (reinterpret_cast<uintptr_t>(occ_dev) % 16 || reinterpret_cast<uintptr_t>(out_dev) % 8 ||
+        reinterpret_cast<uintptr_t>(rgb_dev) % 4)
+        return fail(VX_EINVAL, "vx_build_dxt1_dev: misaligned buffer");
+    if (brick_count == 0) return VX_OK;
+    const uint64_t blocks = uint64_t(brick_count) * 32;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint32_t grid = uint32_t(std::min<uint64_t>((blocks + 255) / 256, uint64_t(sms) * 16));
+    build_dxt1_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        rgb_dev, reinterpret_cast<const uint4*>(occ_dev), blocks, out_dev);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_build_dxt1_dev");
+}
+
+extern "C" int vx_build_dxt1(const float* rgb, const uint32_t* occ, uint32_t brick_count, uint64_t* out) {
+    using namespace vx;
+    if (brick_count && (!rgb || !occ || !out)) return fail(VX_EINVAL, "vx_build_dxt1: null argument");
+    const unsigned T = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    auto work = [&](uint64_t b0, uint64_t b1) {
+        for (uint64_t b = b0; b < b1; ++b)
+            for (int k = 0; k < 32; ++k) out[b * 32 + k] = dxt1::brick_block(rgb + b * 512 * 3, occ + 16 * b, k);
     };
     if (T == 1 || brick_count < 256) {
         work(0, brick_count);
