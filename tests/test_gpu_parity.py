@@ -172,6 +172,21 @@ def test_host_entry_point_matches_device(vx, cuda):
     np.testing.assert_array_equal(cd.view(np.uint32), ch.view(np.uint32))
 
 
+@pytest.mark.parametrize("n", [1048575, 1048576, 2500001])
+def test_host_entry_point_pipelined_chunks(vx, cuda, n):
+    """Large host casts run as overlapped chunks; results equal the device call."""
+    import torch
+    from vx_b200 import workloads as W
+    wl = W.config2(R=128, width=8, height=8, seed=17)
+    s = vx.Scene(wl.scene)
+    rays = W.random_rays(n, 128, seed=n)
+    gd, cd, _ = gpu_cast(vx, s, rays, with_counters=False)
+    pinned = torch.from_numpy(rays).pin_memory()
+    gh, ch = s.cast_rays_host(pinned.numpy())
+    np.testing.assert_array_equal(gd.view(np.uint8), gh.view(np.uint8))
+    np.testing.assert_array_equal(cd.view(np.uint32), ch.view(np.uint32))
+
+
 def test_camera_rays_device_equal_host(vx, cuda):
     import torch
     from vx_b200 import workloads as W

@@ -1,5 +1,6 @@
 // vx_api.cpp - host side of the C ABI (include/vx.h): validation, the scene's
 // device allocation, error reporting and launches.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -47,16 +48,32 @@ CameraDev camera_from_pc(const vx_camera_pc& pc) {
 
 }  // namespace vx
 
+// Copy / cast pipeline of the host-buffer casts: smallest chunk (rays) and
+// most chunks per call.
+#ifndef VX_PIPE_MIN_CHUNK
+#define VX_PIPE_MIN_CHUNK 524288u
+#endif
+#ifndef VX_PIPE_MAX_CHUNKS
+#define VX_PIPE_MAX_CHUNKS 16u
+#endif
+#ifndef VX_PIPE_CAST_STREAMS
+#define VX_PIPE_CAST_STREAMS 4
+#endif
+
 struct vx_scene {
     int device = 0;
     vx_octree_config cfg{};
     void* pool = nullptr;  // single device allocation, 256-byte aligned slices
     uint64_t pool_bytes = 0;
     vx::DevScene dev{};
-    // staging buffer for vx_cast_rays_host, grown on demand
+    // staging buffer for vx_cast_rays_host, grown on demand, and the streams
+    // and events of its copy / cast pipeline (created on first use)
     std::mutex stage_mu;
     void* stage = nullptr;
     uint64_t stage_bytes = 0;
+    cudaStream_t pipe[2 + VX_PIPE_CAST_STREAMS] = {};  // copies in, copies out, casts
+    cudaEvent_t pipe_start = nullptr;
+    cudaEvent_t pipe_in[VX_PIPE_MAX_CHUNKS] = {}, pipe_cast[VX_PIPE_MAX_CHUNKS] = {};
 };
 
 namespace vx {
@@ -221,6 +238,13 @@ int vx_scene_destroy(vx_scene* s) {
     int dev = -1;
     cudaGetDevice(&dev);
     if (dev != s->device) cudaSetDevice(s->device);
+    for (cudaStream_t& p : s->pipe)
+        if (p) cudaStreamDestroy(p);
+    if (s->pipe_start) cudaEventDestroy(s->pipe_start);
+    for (uint32_t i = 0; i < VX_PIPE_MAX_CHUNKS; ++i) {
+        if (s->pipe_in[i]) cudaEventDestroy(s->pipe_in[i]);
+        if (s->pipe_cast[i]) cudaEventDestroy(s->pipe_cast[i]);
+    }
     cudaError_t e1 = cudaFree(s->pool);
     cudaError_t e2 = s->stage ? cudaFree(s->stage) : cudaSuccess;
     if (dev >= 0 && dev != s->device) cudaSetDevice(dev);
@@ -319,16 +343,55 @@ int cast_rays_host(const char* what, const vx_scene* cs, const vx_ray* rays_host
     char* base = static_cast<char*>(s->stage);
     vx_ray* dr = reinterpret_cast<vx_ray*>(base);
     vx_hit* dh = reinterpret_cast<vx_hit*>(base + sz_r);
-    void* dc = sz_c ? base + sz_r + sz_h : nullptr;
+    char* dc = sz_c ? base + sz_r + sz_h : nullptr;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    cudaError_t e = cudaMemcpyAsync(dr, rays_host, uint64_t(n) * sizeof(vx_ray), cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) return vx::cuda_fail(e, w + ": copy in");
-    int r = vx::launch_cast(s->dev, dr, n, tmin, tmax, dh, dc, nullptr, stream, lod);
-    if (r != 0) return vx::cuda_fail(cudaError_t(r), w + ": launch");
-    e = cudaMemcpyAsync(hits_host, dh, uint64_t(n) * sizeof(vx_hit), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess && dc) e = cudaMemcpyAsync(color_host, dc, uint64_t(n) * colw, cudaMemcpyDeviceToHost, st);
-    if (e != cudaSuccess) return vx::cuda_fail(e, w + ": copy out");
-    e = cudaStreamSynchronize(st);
+    if (!s->pipe_start) {
+        cudaError_t e = cudaEventCreateWithFlags(&s->pipe_start, cudaEventDisableTiming);
+        for (int i = 0; i < 2 + VX_PIPE_CAST_STREAMS && e == cudaSuccess; ++i)
+            e = cudaStreamCreateWithFlags(&s->pipe[i], cudaStreamNonBlocking);
+        for (uint32_t i = 0; i < VX_PIPE_MAX_CHUNKS && e == cudaSuccess; ++i) {
+            e = cudaEventCreateWithFlags(&s->pipe_in[i], cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->pipe_cast[i], cudaEventDisableTiming);
+        }
+        if (e != cudaSuccess) return vx::cuda_fail(e, w + ": pipeline streams");
+    }
+    // The rays go in, are cast and come back out in chunks: one stream streams
+    // the chunks in, each chunk is cast on one of VX_PIPE_CAST_STREAMS streams
+    // once it has arrived (so the long last rays of one chunk overlap the next
+    // chunk's cast), and one stream returns each chunk once it is cast.  The
+    // two copy directions and the casts overlap (with pinned host buffers), and
+    // no copy-in waits behind a cast.  Everything starts after the work
+    // already queued on the caller's stream.
+    const uint32_t min_chunk = VX_PIPE_MIN_CHUNK;
+    const uint32_t chunks = n >= 2 * min_chunk ? std::min<uint32_t>(VX_PIPE_MAX_CHUNKS, n / min_chunk) : 1;
+    cudaStream_t s_in = s->pipe[0], s_out = s->pipe[1];
+    cudaError_t e = cudaEventRecord(s->pipe_start, st);
+    for (int i = 0; i < 2 + VX_PIPE_CAST_STREAMS && e == cudaSuccess; ++i)
+        e = cudaStreamWaitEvent(s->pipe[i], s->pipe_start, 0);
+    if (e != cudaSuccess) return vx::cuda_fail(e, w + ": order");
+    const char* rh = reinterpret_cast<const char*>(rays_host);
+    char* hh = reinterpret_cast<char*>(hits_host);
+    char* ch = static_cast<char*>(color_host);
+    for (uint32_t c = 0; c < chunks; ++c) {
+        const uint64_t a = uint64_t(n) * c / chunks, b = uint64_t(n) * (c + 1) / chunks, m = b - a;
+        cudaStream_t s_cast = s->pipe[2 + c % VX_PIPE_CAST_STREAMS];
+        e = cudaMemcpyAsync(dr + a, rh + a * sizeof(vx_ray), m * sizeof(vx_ray), cudaMemcpyHostToDevice, s_in);
+        if (e == cudaSuccess) e = cudaEventRecord(s->pipe_in[c], s_in);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s_cast, s->pipe_in[c], 0);
+        if (e != cudaSuccess) return vx::cuda_fail(e, w + ": copy in");
+        int r = vx::launch_cast(s->dev, dr + a, uint32_t(m), tmin, tmax, dh + a, dc ? dc + a * colw : nullptr, nullptr,
+                                s_cast, lod);
+        if (r != 0) return vx::cuda_fail(cudaError_t(r), w + ": launch");
+        e = cudaEventRecord(s->pipe_cast[c], s_cast);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s_out, s->pipe_cast[c], 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(hh + a * sizeof(vx_hit), dh + a, m * sizeof(vx_hit), cudaMemcpyDeviceToHost, s_out);
+        if (e == cudaSuccess && dc)
+            e = cudaMemcpyAsync(ch + a * colw, dc + a * colw, m * colw, cudaMemcpyDeviceToHost, s_out);
+        if (e != cudaSuccess) return vx::cuda_fail(e, w + ": copy out");
+    }
+    for (int i = 1; i < 2 + VX_PIPE_CAST_STREAMS && e == cudaSuccess; ++i) e = cudaStreamSynchronize(s->pipe[i]);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s_in);
     if (e != cudaSuccess) return vx::cuda_fail(e, w + ": synchronize");
     return VX_OK;
 }
