@@ -482,6 +482,111 @@ def measure_cfg5(args, rank, world, steps, warmup):
                         "from colours + N(0, 0.05)", **out}
 
 
+def measure_next(args, steps, warmup):
+    """The rows beyond the cast (1024^3 cave, seed 2, the cfg2 scene): the device scene
+    builder against the host builder, the normal and DXT1 payload encoders, the LOD cut,
+    the compressed render and the scene cache file.  Device times are CUDA events."""
+    import math
+    import tempfile
+    import numpy as np
+    import torch
+    vx = load_pkg()
+    from vx_b200 import workloads as W
+    R, seed = args.R, args.seed
+    out = {"workload": f"cave {R}^3 (depth 10), noise spacing 64, 5 octaves, 50% fill, seed {seed}"}
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+
+    def dev_ms(fn, reps=steps):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        a, b = ev(), ev()
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    bits_t = vx.synth_noise_dev(R, 64 * R // 1024, 5 if R >= 1024 else 3, 0.5, seed, False)
+    torch.cuda.synchronize()
+    # device builder (the call returns when the scene is complete: host clock)
+    t = []
+    for k in range(3):
+        t0 = time.perf_counter()
+        sc = vx.scene_from_dense_dev(bits_t, R, 10, vx.VX_COLOR_DXT1, seed ^ 0xD7C1, k == 2)
+        t.append(time.perf_counter() - t0)
+        if k < 2:
+            sc.close()
+    bits = bits_t.cpu().numpy().view(np.uint64)
+    t0 = time.perf_counter()
+    host = vx.build_dense(bits, R, 10)
+    host_s = time.perf_counter() - t0
+    got = sc.download()
+    same = all(np.array_equal(getattr(got, k), getattr(host, k))
+               for k in ("nodes", "node_brick", "grid_lookup", "brick_coord", "brick_occ"))
+    B = host.brick_count
+    out["device_builder"] = {"bricks": B, "nodes": host.node_count, "device_s": min(t[:2]),
+                             "device_s_with_dxt1_and_normals": t[2], "host_build_dense_s": host_s,
+                             "identical_to_host_builder": bool(same)}
+    # payload encoders
+    occ_t = torch.from_numpy(host.brick_occ.view(np.int32)).cuda()
+    nrm_t = torch.zeros(B * 64, dtype=torch.int64, device="cuda")
+    ms = dev_ms(lambda: vx.build_normals_dev(occ_t, nrm_t))
+    out["normal_payload"] = {"bricks": B, "device_ms": ms, "mbricks_s": B / ms / 1e3,
+                             "equals_scene_payload": bool(np.array_equal(nrm_t.cpu().numpy().view(np.uint64),
+                                                                         got.brick_normal.reshape(-1)))}
+    nb = min(B, 262144)
+    rgba = vx.synth_rgba8(host.brick_coord[:nb], seed)
+    rgb_t = torch.from_numpy(np.stack([(rgba >> s_) & 255 for s_ in (0, 8, 16)], -1).astype(np.float32)
+                             / np.float32(255.0)).reshape(-1).cuda()
+    dxt_t = torch.zeros(nb * 32, dtype=torch.int64, device="cuda")
+    occ_sub = occ_t[:nb * 16].contiguous()
+    ms = dev_ms(lambda: vx.build_dxt1_dev(rgb_t, occ_sub, dxt_t))
+    out["dxt1_encode"] = {"bricks": nb, "colours": "RGBA8 words / 255", "device_ms": ms, "mbricks_s": nb / ms / 1e3}
+    del rgb_t, dxt_t, occ_t, nrm_t
+    # LOD cut and compressed render on the cfg2 camera
+    wl = W.config2(R=R, seed=seed, bits=bits)
+    rays = torch.from_numpy(wl.rays()).cuda()
+    n = rays.shape[0]
+    hits = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+    base = vx.lod_from_camera(math.radians(70.0), wl.height)
+    plain_ms = dev_ms(lambda: sc.cast_rays_dev(rays, hits))
+    lod_rows = []
+    for bias in (0.0, 7.0):
+        lod = vx.lod_with_bias(base, bias)
+        ms = dev_ms(lambda: sc.cast_rays_dev(rays, hits, lod=lod))
+        h = hits.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1)
+        lod_rows.append({"bias": bias, "ray_dir_size": lod.ray_dir_size, "mrays_s": n / ms / 1e3,
+                         "lod_hit_fraction": float(np.mean(((h["flags"] & 1) == 1) & (h["brick"] == 0xFFFFFFFF)))})
+    out["lod"] = {"rays": n, "castRayScreenSpaceLOD": "70 deg, 1080 rows, times 2^bias",
+                  "plain_mrays_s": n / plain_ms / 1e3, "runs": lod_rows}
+    img = torch.zeros(n, dtype=torch.int32, device="cuda")
+    ms = dev_ms(lambda: sc.render_dev(wl.camera, wl.width, wl.height, img))
+    out["compressed_render"] = {"pixels": n, "payloads": "DXT1 colour + DXT normals", "device_ms": ms,
+                                "mrays_s": n / ms / 1e3}
+    # scene cache file
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "cave.vxsc")
+        t0 = time.perf_counter()
+        sc.save(path)
+        save_s = time.perf_counter() - t0
+        size = os.path.getsize(path)
+        t0 = time.perf_counter()
+        sl = vx.Scene.load(path)
+        torch.cuda.synchronize()
+        load_s = time.perf_counter() - t0
+        h2 = torch.zeros_like(hits)
+        sl.cast_rays_dev(rays, h2)
+        sc.cast_rays_dev(rays, hits)
+        torch.cuda.synchronize()
+        out["scene_cache"] = {"format": "VXSC", "bytes": size, "save_s": save_s, "load_s": load_s,
+                              "hits_equal_after_load": bool(torch.equal(hits, h2))}
+        sl.close()
+    sc.close()
+    return out
+
+
 def config_dict(wl, world):
     return {"workload": f"{wl.name}: cave {wl.R}^3 (depth {wl.scene.max_levels}), value noise spacing "
                         f"{64 * wl.R // 1024}, 5 octaves, 50% fill, DXT1 bricks, {wl.width}x{wl.height} FP32 "
@@ -500,11 +605,12 @@ def main():
     ap.add_argument("--R", type=int, default=1024)
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg3", "cfg4", "cfg5"],
-                    help="cfg2: plain cast of the 1024^3 cave frame (with the cfg4 and cfg5 results attached "
-                         "at N=1); cfg4: 64-scene batched frame vs plain; cfg5: forward / adjoint ms per view")
+    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg3", "cfg4", "cfg5", "next"],
+                    help="cfg2: plain cast of the 1024^3 cave frame (with the cfg4, cfg5 and next-row results "
+                         "attached at N=1); cfg4: 64-scene batched frame vs plain; cfg5: forward / adjoint ms per "
+                         "view; next: device builder, payload encoders, LOD cut, compressed render, cache file")
     ap.add_argument("--no-extra", action="store_true",
-                    help="cfg2 only: skip the attached batched (cfg4) and adjoint (cfg5) measurements")
+                    help="cfg2 only: skip the attached batched (cfg4), adjoint (cfg5) and next-row measurements")
     ap.add_argument("--scenes", type=int, default=64, help="cfg4: number of scenes")
     ap.add_argument("--soak-seconds", type=float, default=1.5,
                     help="untimed launches before timing so clocks reach steady state")
@@ -527,6 +633,11 @@ def main():
                     "config": {"workload": res.pop("workload")}, "gpu_launches": args.steps * 3}
             line.update(res)
             print(json.dumps(line), flush=True)
+        return 0
+    if args.workload == "next":
+        res = measure_next(args, args.steps, args.warmup)
+        if rank == 0:
+            print(json.dumps({"workload": "next", "next_rows": res}), flush=True)
         return 0
     if args.workload == "cfg5":
         import torch
@@ -680,6 +791,8 @@ def main():
                            "steps": extra_steps}
         torch.cuda.empty_cache()
         line["adjoint"] = measure_cfg5(args, rank, world, extra_steps, extra_warmup)
+        torch.cuda.empty_cache()
+        line["next_rows"] = measure_next(args, extra_steps, extra_warmup)
     print(json.dumps(line), flush=True)
     return 0
 
