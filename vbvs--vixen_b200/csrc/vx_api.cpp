@@ -130,6 +130,11 @@ int scene_alloc(const vx_octree_config& c, uint32_t node_count, uint32_t brick_c
         ds.wsm[i] = ds.wsize[i] - 0.001f;
         ds.qwm[i] = int32_t(std::floor(c.world_min[i]));
     }
+    for (int i = 0; i < 3; ++i) {
+        int e = 0;
+        const float m = std::frexp(ds.wsize[i], &e);  // wsize = m * 2^e, m in [0.5, 1)
+        ds.wsinv[i] = (m == 0.5f && e - 1 > -126 && e - 1 < 126) ? std::ldexp(1.0f, 1 - e) : 0.0f;
+    }
     // glm::length: sqrt of the left-to-right dot product
     ds.wrl = std::sqrt((ds.wsize[0] * ds.wsize[0] + ds.wsize[1] * ds.wsize[1]) + ds.wsize[2] * ds.wsize[2]);
     ds.max_levels = c.max_levels;

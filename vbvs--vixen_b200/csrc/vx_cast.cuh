@@ -185,6 +185,8 @@ struct CastState {
     bool fetched;
     float px, py, pz, scale_exp2, t_min, t_max, hh;
     uint32_t mValid, mLeaf, pChild, pValid, pLeaf;
+    uint32_t pushed;       // stack slots written by PUSH (bit scale - minScale)
+    float t_root;          // t_max of the unwritten slots
     // cycle detection
     uint32_t d1g, d1d;
     int nrec;
@@ -229,8 +231,13 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
         const float dd = (ddx * ddx + ddy * ddy) + ddz * ddz;
         const float inv = 1.0f / sqrtf(dd);
         dx = ddx * inv; dy = ddy * inv; dz = ddz * inv;
-        const float len = sqrtf((dx * dx + dy * dy) + dz * dz);
-        if (len < 1e-6f) { h.flags = F_INVALID; return true; }
+        // length(normalize(d)) < 1e-6: for dd in [1e-30, 1e30] every component is
+        // finite and the normalised length is 1 within a few ulp, so the check
+        // can only fail outside that range.
+        if (!(dd >= 1e-30f && dd <= 1e30f)) {
+            const float len = sqrtf((dx * dx + dy * dy) + dz * dz);
+            if (len < 1e-6f) { h.flags = F_INVALID; return true; }
+        }
         if (isnan(ox) || isnan(oy) || isnan(oz) || isnan(dx) || isnan(dy) || isnan(dz) || isinf(ox) ||
             isinf(oy) || isinf(oz) || isinf(dx) || isinf(dy) || isinf(dz)) {
             h.flags = F_INVALID;
@@ -240,6 +247,11 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
     const float wminx = s.wmin[0], wminy = s.wmin[1], wminz = s.wmin[2];
     const bool inside = ox >= wminx && ox <= s.wmax[0] && oy >= wminy && oy <= s.wmax[1] && oz >= wminz &&
                         oz <= s.wmax[2];
+    // 1/d per axis, the one division every reciprocal below derives from:
+    // 1/(-|d|) = -|1/d| and 1/|d| = |1/d| exactly (IEEE division is symmetric
+    // in sign), so intersectAABB, computeRayCoefficients and the brick DDA
+    // reciprocals need no further division.
+    const float rcp[3] = {1.0f / dx, 1.0f / dy, 1.0f / dz};
     // intersectAABB (:117-149)
     float tEntry, tExit;
     {
@@ -252,7 +264,7 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
                 if (o[i] < s.wmin[i] || o[i] > s.wmax[i]) return true;
                 inv = (d[i] >= 0.0f) ? 1e20f : -1e20f;
             } else {
-                inv = 1.0f / d[i];
+                inv = rcp[i];
             }
             const float t0 = (s.wmin[i] - o[i]) * inv;
             const float t1 = (s.wmax[i] - o[i]) * inv;
@@ -268,19 +280,20 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
     if (tEntry >= tExit || tExit < 0.0f) return true;
     const float tRayStart = inside ? 0.0f : gmax(0.0f, tEntry);
     const float wsx = s.wsize[0], wsy = s.wsize[1], wsz = s.wsize[2];
-    const float nox = (ox + dx * tRayStart - wminx) / wsx + 1.0f;
-    const float noy = (oy + dy * tRayStart - wminy) / wsy + 1.0f;
-    const float noz = (oz + dz * tRayStart - wminz) / wsz + 1.0f;
+    // x / size, as a product where 1 / size is exact (a power-of-two size):
+    // both round the same real number once.
+    auto by_size = [&](float x, int i) { return s.wsinv[i] != 0.0f ? x * s.wsinv[i] : x / s.wsize[i]; };
+    const float nox = by_size(ox + dx * tRayStart - wminx, 0) + 1.0f;
+    const float noy = by_size(oy + dy * tRayStart - wminy, 1) + 1.0f;
+    const float noz = by_size(oz + dz * tRayStart - wminz, 2) + 1.0f;
     // computeRayCoefficients (:699-728)
     Coef& c = st.c;
     {
-        float sx = dx, sy = dy, sz = dz;
-        if (fabsf(sx) < 1e-5f) sx = copysignf(1e-5f, sx);
-        if (fabsf(sy) < 1e-5f) sy = copysignf(1e-5f, sy);
-        if (fabsf(sz) < 1e-5f) sz = copysignf(1e-5f, sz);
-        c.tx_coef = 1.0f / -fabsf(sx);
-        c.ty_coef = 1.0f / -fabsf(sy);
-        c.tz_coef = 1.0f / -fabsf(sz);
+        // t_coef = 1 / -|d|, with |d| raised to 1e-5 (copysign) below that
+        const float k_small = 1.0f / -1e-5f;
+        c.tx_coef = fabsf(dx) < 1e-5f ? k_small : -fabsf(rcp[0]);
+        c.ty_coef = fabsf(dy) < 1e-5f ? k_small : -fabsf(rcp[1]);
+        c.tz_coef = fabsf(dz) < 1e-5f ? k_small : -fabsf(rcp[2]);
         c.tx_bias = c.tx_coef * nox;
         c.ty_bias = c.ty_coef * noy;
         c.tz_bias = c.tz_coef * noz;
@@ -300,12 +313,11 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
         t_min = gmax(t_min, 0.0f);
         t_max = gmin(t_max, 1.0f);
     }
-    // initializeTraversalState (:261-280): stack[minScale..22] = root
-    const int minScale = s.min_scale;
-    for (int sc = minScale; sc <= ESVO_MAX_SCALE; ++sc) {
-        stkN[(sc - minScale) * stride] = 0;
-        stkT[(sc - minScale) * stride] = t_max;
-    }
+    // initializeTraversalState (:261-280): stack[minScale..22] = (root, t_max).
+    // Kept implicitly: a slot not yet pushed (bit clear in `pushed`) reads as
+    // (0, t_root), so no slot is written here.
+    st.pushed = 0u;
+    st.t_root = t_max;
     int idx = 0;
     float px = 1.0f, py = 1.0f, pz = 1.0f;
     const bool csx = fabsf(dx) >= 1e-5f, csy = fabsf(dy) >= 1e-5f, csz = fabsf(dz) >= 1e-5f;
@@ -324,9 +336,9 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
     }
     // handleLeafHit quantities that depend on the ray only (SVOBrickDDA.cpp:98-121, 140-143, 165-166)
     const float te0 = gmax(tEntry, 0.0f);
-    st.rlx = fclamp(((ox + dx * te0) - wminx) / wsx, 0.001f, 0.999f);
-    st.rly = fclamp(((oy + dy * te0) - wminy) / wsy, 0.001f, 0.999f);
-    st.rlz = fclamp(((oz + dz * te0) - wminz) / wsz, 0.001f, 0.999f);
+    st.rlx = fclamp(by_size((ox + dx * te0) - wminx, 0), 0.001f, 0.999f);
+    st.rly = fclamp(by_size((oy + dy * te0) - wminy, 1), 0.001f, 0.999f);
+    st.rlz = fclamp(by_size((oz + dz * te0) - wminz, 2), 0.001f, 0.999f);
     RayB& rb = st.rb;
     rb.lo[0] = ox + (0.0f - wminx);
     rb.lo[1] = oy + (0.0f - wminy);
@@ -334,8 +346,8 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
     rb.d[0] = dx; rb.d[1] = dy; rb.d[2] = dz;
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-        rb.inv[i] = (fabsf(rb.d[i]) < 1e-8f) ? ((rb.d[i] >= 0) ? 1e8f : -1e8f) : 1.0f / rb.d[i];
-        rb.tdel[i] = (fabsf(rb.d[i]) < 1e-8f) ? FLT_MAX_ : 1.0f / fabsf(rb.d[i]);
+        rb.inv[i] = (fabsf(rb.d[i]) < 1e-8f) ? ((rb.d[i] >= 0) ? 1e8f : -1e8f) : rcp[i];
+        rb.tdel[i] = (fabsf(rb.d[i]) < 1e-8f) ? FLT_MAX_ : fabsf(rcp[i]);
         rb.step[i] = (fabsf(rb.d[i]) < 1e-8f) ? 0 : ((rb.d[i] > 0.0f) ? 1 : -1);
     }
     st.ox = ox; st.oy = oy; st.oz = oz;
@@ -369,8 +381,8 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
 // repeats after one or two iterations the ray can neither hit nor leave before
 // the 500-iteration cap: the result is the capped miss and the remaining
 // iterations' counters repeat the cycle's.  The two previous states are kept
-// in shared memory (cyc[k * stride], k < 8: one iteration back, k >= 8: two
-// back) from iteration CYCLE_START on.  With LOD the cut test reads only the
+// in shared memory (cyc[(p * 8 + k) * stride], slot p = iteration parity)
+// from iteration CYCLE_START on.  With LOD the cut test reads only the
 // loop state and per-ray constants, so a repeating state still cannot end.
 //
 // LOD: castRayWithLOD (SVOTraversal.cpp:198-232) with LODParameters `lod`
@@ -520,6 +532,7 @@ __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint
                 if (tc_max < st.hh) {
                     stkN[(st.scale - minScale) * stride] = st.parent;
                     stkT[(st.scale - minScale) * stride] = st.t_max;
+                    st.pushed |= 1u << (st.scale - minScale);
                 }
                 st.hh = tc_max;
                 const int worldIdx = st.idx ^ (~c.octant_mask & 7);
@@ -594,13 +607,18 @@ __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint
             st.scale = 31 - __clz(diff);
             if (st.scale < minScale || st.scale > ESVO_MAX_SCALE) { cast_finish(st); return true; }
             st.scale_exp2 = __int_as_float((st.scale - ESVO_MAX_SCALE + 127) << 23);
-            st.parent = stkN[(st.scale - minScale) * stride];
-            st.t_max = stkT[(st.scale - minScale) * stride];
+            if ((st.pushed >> (st.scale - minScale)) & 1u) {
+                st.parent = stkN[(st.scale - minScale) * stride];
+                st.t_max = stkT[(st.scale - minScale) * stride];
+            } else {
+                st.parent = 0u;
+                st.t_max = st.t_root;
+            }
             const uint32_t mask = ~((1u << (ESVO_MAX_SCALE - st.scale)) - 1u);
             qx &= mask; qy &= mask; qz &= mask;
-            st.px = 1.0f + float(qx) / 4194304.0f;
-            st.py = 1.0f + float(qy) / 4194304.0f;
-            st.pz = 1.0f + float(qz) / 4194304.0f;
+            st.px = 1.0f + float(qx) * (1.0f / 4194304.0f);  // / 2^22, exact as a product
+            st.py = 1.0f + float(qy) * (1.0f / 4194304.0f);
+            st.pz = 1.0f + float(qz) * (1.0f / 4194304.0f);
             const int sh = ESVO_MAX_SCALE - st.scale - 1;
             if (sh < 0 || sh >= 32) st.idx = 0;
             else st.idx = int(((qx >> sh) & 1u) | (((qy >> sh) & 1u) << 1) | (((qz >> sh) & 1u) << 2));
@@ -617,13 +635,15 @@ next_iter:
         cur[5] = __float_as_uint(st.t_min); cur[6] = __float_as_uint(st.t_max); cur[7] = __float_as_uint(st.hh);
         const uint32_t dg = h.grid_reads - g0, ddd = h.dda_steps - dd0;
         bool eq1 = st.nrec >= 1, eq2 = st.nrec >= 2;
+        // two slots by parity: the other parity holds the state one iteration
+        // back, this parity two back; this state replaces the latter
+        uint32_t* back2 = cyc + ((st.iter & 1) * 8) * stride;
+        const uint32_t* back1 = cyc + (((st.iter & 1) ^ 1) * 8) * stride;
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            const uint32_t a = cyc[k * stride], b = cyc[(k + 8) * stride];
-            eq1 = eq1 && (cur[k] == a);
-            eq2 = eq2 && (cur[k] == b);
-            cyc[(k + 8) * stride] = a;
-            cyc[k * stride] = cur[k];
+            eq1 = eq1 && (cur[k] == back1[k * stride]);
+            eq2 = eq2 && (cur[k] == back2[k * stride]);
+            back2[k * stride] = cur[k];
         }
         if (eq1 || eq2) {
             const uint32_t rem = uint32_t(MAX_ITER - st.iter);

@@ -16,6 +16,7 @@ struct DevScene {
     float wmin[3], wmax[3], wsize[3];  // wsize = wmax - wmin (float subtract)
     float wsm[3];                      // wsize - 0.001 (SVOBrickDDA.cpp:128, 143)
     float wrl;                         // length(wsize), worldRayLength (SVOTraversal.cpp:552)
+    float wsinv[3];                    // 1 / wsize where that is exact (power-of-two size), else 0
     int32_t qwm[3];                    // floor(world_min), VoxelComponents.h:373-379
     int32_t max_levels;
     int32_t min_scale;                 // 22 - max_levels + 1
