@@ -62,13 +62,16 @@ __device__ __forceinline__ int f2i(float f) {
     return (f >= -2147483648.0f && f < 2147483648.0f) ? __float2int_rz(f) : INT_MIN;
 }
 
-// mirrorMask (SVOTypes.h:343-364): bit i moves to i ^ flip.
-__device__ __forceinline__ uint32_t mirror_mask(uint32_t m, int octant_mask) {
+// mirrorMask (SVOTypes.h:343-364): bit i moves to i ^ flip, here on the valid
+// mask (bits 0-7) and the leaf mask (bits 8-15) at once.
+__device__ __forceinline__ uint32_t mirror_masks(uint32_t m, int octant_mask) {
     const int flip = (~octant_mask) & 7;
-    if (flip & 1) m = ((m & 0x55u) << 1) | ((m & 0xAAu) >> 1);
-    if (flip & 2) m = ((m & 0x33u) << 2) | ((m & 0xCCu) >> 2);
-    if (flip & 4) m = ((m & 0x0Fu) << 4) | ((m & 0xF0u) >> 4);
-    return m;
+    const uint32_t a = ((m & 0x5555u) << 1) | ((m & 0xAAAAu) >> 1);
+    m = (flip & 1) ? a : m;
+    const uint32_t b = ((m & 0x3333u) << 2) | ((m & 0xCCCCu) >> 2);
+    m = (flip & 2) ? b : m;
+    const uint32_t c = ((m & 0x0F0Fu) << 4) | ((m & 0xF0F0u) >> 4);
+    return (flip & 4) ? c : m;
 }
 
 __device__ __forceinline__ uint32_t grid_lookup(const DevScene& s, int bx, int by, int bz) {
@@ -238,8 +241,10 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
             const float len = sqrtf((dx * dx + dy * dy) + dz * dz);
             if (len < 1e-6f) { h.flags = F_INVALID; return true; }
         }
-        if (isnan(ox) || isnan(oy) || isnan(oz) || isnan(dx) || isnan(dy) || isnan(dz) || isinf(ox) ||
-            isinf(oy) || isinf(oz) || isinf(dx) || isinf(dy) || isinf(dz)) {
+        // isnan || isinf of any component: !(|x| < inf) is both tests at once
+        const float inf = __int_as_float(0x7F800000);
+        if (!(fabsf(ox) < inf) || !(fabsf(oy) < inf) || !(fabsf(oz) < inf) || !(fabsf(dx) < inf) ||
+            !(fabsf(dy) < inf) || !(fabsf(dz) < inf)) {
             h.flags = F_INVALID;
             return true;
         }
@@ -408,8 +413,9 @@ __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint
             st.pChild = nd.x;
             st.pValid = nd.y & 0xFFu;
             st.pLeaf = (nd.y >> 8) & 0xFFu;
-            st.mValid = mirror_mask(st.pValid, c.octant_mask);
-            st.mLeaf = mirror_mask(st.pLeaf, c.octant_mask);
+            const uint32_t mm = mirror_masks(nd.y & 0xFFFFu, c.octant_mask);
+            st.mValid = mm & 0xFFu;
+            st.mLeaf = mm >> 8;
             const uint32_t nonLeaf = ~st.mLeaf & 0xFFu;
             st.fetched = (nonLeaf | (st.mValid << 8) | st.pChild) != 0u;
         }
