@@ -38,7 +38,10 @@ namespace {
 
 constexpr int ESVO_MAX_SCALE = 22;  // LaineKarrasOctree.h:337
 constexpr int MAX_ITER = 500;       // SVOTraversal.cpp:588
-constexpr int CYCLE_START = 4;      // iteration from which loop states are recorded
+#ifndef VX_CYCLE_START
+#define VX_CYCLE_START 3
+#endif
+constexpr int CYCLE_START = VX_CYCLE_START;  // iteration from which loop states are recorded
 constexpr float FLT_MAX_ = 3.402823466e+38f;
 constexpr uint32_t NONE = 0xFFFFFFFFu;
 
