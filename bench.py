@@ -390,7 +390,8 @@ def measure_cfg3(args, steps, warmup):
 def measure_cfg5(args, rank, world, steps, warmup):
     """cfg5: the 512^3 noise scene (30 % fill), 16 views of 512x512; per variant (per-voxel
     FP32 RGB, FP32 DXT1 endpoints) the forward-with-record time and the forward+adjoint time per
-    view, the FP64 CPU gradient check and central finite differences (h = 1e-3) on 1000 entries."""
+    view (the 16 views as one forward launch and one adjoint launch), the FP64 CPU gradient check
+    and central finite differences (h = 1e-3) on 1000 entries."""
     import numpy as np
     import torch
     vx = load_pkg()
@@ -406,24 +407,26 @@ def measure_cfg5(args, rank, world, steps, warmup):
         attr_d = torch.from_numpy(dw.attr).cuda()
         idx_d = None if dw.dxt_idx is None else torch.from_numpy(dw.dxt_idx.view(np.int32)).cuda()
         tgt_attr = torch.from_numpy(dw.target_attr).cuda()
-        imgs = [torch.zeros((n, 3), dtype=torch.float32, device="cuda") for _ in dw.views]
-        recs = [torch.zeros((n, 4), dtype=torch.int32, device="cuda") for _ in dw.views]
-        tgts = [torch.zeros((n, 3), dtype=torch.float32, device="cuda") for _ in dw.views]
-        for v, pc in enumerate(dw.views):
-            vx.diff_forward(scene, pc, 512, 512, kind, tgt_attr, idx_d, tgts[v], recs[v])
+        # all 16 views in one forward launch and one adjoint launch (view-major buffers)
+        V = len(dw.views)
+        img_all = torch.zeros((V * n, 3), dtype=torch.float32, device="cuda")
+        rec_all = torch.zeros((V * n, 4), dtype=torch.int32, device="cuda")
+        tgt_all = torch.zeros((V * n, 3), dtype=torch.float32, device="cuda")
+        imgs = [img_all[v * n:(v + 1) * n] for v in range(V)]
+        recs = [rec_all[v * n:(v + 1) * n] for v in range(V)]
+        tgts = [tgt_all[v * n:(v + 1) * n] for v in range(V)]
+        vx.diff_forward_views(scene, dw.views, 512, 512, kind, tgt_attr, idx_d, tgt_all, rec_all)
         grad = torch.zeros_like(attr_d)
         loss = torch.zeros(1, dtype=torch.float32, device="cuda")
 
         def fwd():
-            for v, pc in enumerate(dw.views):
-                vx.diff_forward(scene, pc, 512, 512, kind, attr_d, idx_d, imgs[v], recs[v])
+            vx.diff_forward_views(scene, dw.views, 512, 512, kind, attr_d, idx_d, img_all, rec_all)
 
         def fwdbwd():
             grad.zero_()
             loss.zero_()
-            for v, pc in enumerate(dw.views):
-                vx.diff_forward(scene, pc, 512, 512, kind, attr_d, idx_d, imgs[v], recs[v])
-                vx.diff_backward(kind, idx_d, recs[v], imgs[v], tgts[v], grad, loss)
+            vx.diff_forward_views(scene, dw.views, 512, 512, kind, attr_d, idx_d, img_all, rec_all)
+            vx.diff_backward(kind, idx_d, rec_all, img_all, tgt_all, grad, loss)
 
         def timed(fn):
             for _ in range(warmup):
@@ -650,7 +653,7 @@ def main():
                               "ms_per_step": a["fwd_bwd_ms_per_view"] * 16, "higher_is_better": False,
                               "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                               "config": {"workload": res.pop("workload")}, "adjoint": res,
-                              "gpu_launches": args.steps * 32}), flush=True)
+                              "gpu_launches": args.steps * 2}), flush=True)  # per fwd+bwd step: 1 forward, 1 adjoint
         return 0
 
     import numpy as np

@@ -405,6 +405,15 @@ int vx_batch_set_bounce_tuning(vx_batch* batch, const vx_batch_tuning* tuning);
 int vx_diff_forward(const vx_scene* scene, const vx_camera_pc* pc, uint32_t width, uint32_t height,
                     int32_t kind, const float* attr_dev, const uint32_t* dxt_idx_dev, float* image_dev,
                     vx_hit* record_dev, void* stream);
+/* The forward pass of `views` cameras in one launch (better filled than one
+ * launch per view): image_dev and record_dev are view-major (view v's pixels
+ * start at v * width * height); vx_diff_backward then takes all of them with
+ * n = views * width * height.  views <= VX_DIFF_MAX_VIEWS. */
+#define VX_DIFF_MAX_VIEWS 64
+int vx_diff_forward_views(const vx_scene* scene, const vx_camera_pc* pcs, uint32_t views,
+                          uint32_t width, uint32_t height, int32_t kind, const float* attr_dev,
+                          const uint32_t* dxt_idx_dev, float* image_dev, vx_hit* record_dev,
+                          void* stream);
 int vx_diff_backward(uint32_t n, int32_t kind, const uint32_t* dxt_idx_dev, const vx_hit* record_dev,
                      const float* image_dev, const float* target_dev, float* grad_dev, float* loss_dev,
                      void* stream);

@@ -80,3 +80,35 @@ def test_adjoint_matches_fp64_and_finite_differences(vx, vo, cuda, kind):
         fd /= 2.0 * float(h)
         err = np.abs(fd[sel] - g[sel]) / np.maximum(np.abs(g[sel]), 1e-6)
         assert np.max(err) <= 1e-2, (ch, np.max(err))
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_multi_view_forward_equals_per_view(vx, cuda, kind):
+    """One vx_diff_forward_views launch over all cameras writes, view by view,
+    exactly what one vx_diff_forward per camera writes; one backward over all
+    views gives the same gradient (up to FP32 summation order) as one per view."""
+    import torch
+    from vx_b200 import workloads as W
+    dw = W.config5(R=128, views=5, width=96, height=64, kind=kind, seed=9)
+    scene = vx.Scene(dw.wl.scene)
+    attr_d = torch.from_numpy(dw.attr).cuda()
+    idx_d = None if dw.dxt_idx is None else torch.from_numpy(dw.dxt_idx.view(np.int32)).cuda()
+    imgs, recs = _render(vx, scene, dw, attr_d, idx_d, dw.views)
+    n = dw.wl.width * dw.wl.height
+    V = len(dw.views)
+    img_all = torch.full((V * n, 3), 9.0, dtype=torch.float32, device="cuda")
+    rec_all = torch.full((V * n, 4), -1, dtype=torch.int32, device="cuda")
+    vx.diff_forward_views(scene, dw.views, dw.wl.width, dw.wl.height, kind, attr_d, idx_d, img_all, rec_all)
+    torch.cuda.synchronize()
+    for v in range(V):
+        assert torch.equal(img_all[v * n:(v + 1) * n], imgs[v])
+        assert torch.equal(rec_all[v * n:(v + 1) * n], recs[v])
+    tgt = torch.rand_like(img_all)
+    g1, g2 = torch.zeros_like(attr_d), torch.zeros_like(attr_d)
+    for v in range(V):
+        vx.diff_backward(kind, idx_d, recs[v], imgs[v], tgt[v * n:(v + 1) * n], g1)
+    vx.diff_backward(kind, idx_d, rec_all, img_all, tgt, g2)
+    torch.cuda.synchronize()
+    assert torch.allclose(g1, g2, rtol=1e-5, atol=1e-6)
+    with pytest.raises(vx.VxError):
+        vx.diff_forward_views(scene, [dw.views[0]] * 65, 8, 8, kind, attr_d, idx_d, img_all, rec_all)

@@ -101,6 +101,7 @@ def lib():
         "vx_build_normals": (C.c_int, [vp, u32, vp]),
         "vx_build_normals_dev": (C.c_int, [vp, u32, vp, vp]),
         "vx_hit_normals": (C.c_int, [vp, vp, u32, vp, vp]),
+        "vx_diff_forward_views": (C.c_int, [vp, vp, u32, u32, u32, i32, vp, vp, vp, vp, vp]),
         "vx_build_dxt1": (C.c_int, [vp, vp, u32, vp]),
         "vx_build_dxt1_dev": (C.c_int, [vp, vp, u32, vp, vp]),
         "vx_scene_info_get": (C.c_int, [vp, vp]),
@@ -729,6 +730,14 @@ def diff_forward(scene: "Scene", pc: CameraPC, width: int, height: int, kind: in
                  stream=None):
     check(lib().vx_diff_forward(scene.handle, C.byref(pc), width, height, kind, _p(attr), _p(dxt_idx), _p(image),
                                 _p(record), _stream(stream)))
+
+
+def diff_forward_views(scene: "Scene", pcs, width: int, height: int, kind: int, attr, dxt_idx, image, record,
+                       stream=None):
+    """vx_diff_forward_views: all cameras in one launch; image (views*w*h, 3), record (views*w*h, 4)."""
+    arr = (CameraPC * len(pcs))(*pcs)
+    check(lib().vx_diff_forward_views(scene.handle, arr, len(pcs), width, height, kind, _p(attr), _p(dxt_idx),
+                                      _p(image), _p(record), _stream(stream)))
 
 
 def diff_backward(kind: int, dxt_idx, record, image, target, grad, loss=None, stream=None):

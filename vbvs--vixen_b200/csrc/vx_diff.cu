@@ -43,8 +43,17 @@ __device__ __forceinline__ void dxt_weights(uint32_t sel, float& w0, float& w1) 
     w1 = (sel == 0) ? 0.0f : (sel == 1) ? 1.0f : (sel == 2) ? (1.0f / 3.0f) : (2.0f / 3.0f);
 }
 
-__global__ void __launch_bounds__(DBLOCK, 3) diff_forward_kernel(DevScene s, CameraDev cam, uint32_t w, uint32_t hgt,
-                                                                   int kind, const float* __restrict__ attr,
+// The cameras of one launch: VX_DIFF_MAX_VIEWS views at most, passed by value
+// (kernel parameter space), so a multi-view launch needs no device copy.
+struct Views {
+    CameraDev cam[VX_DIFF_MAX_VIEWS];
+};
+
+// Pixel i of the launch is pixel i % (w * hgt) of view i / (w * hgt); images
+// and records are view-major.
+__global__ void __launch_bounds__(DBLOCK, 3) diff_forward_kernel(DevScene s, Views views, uint32_t nviews, uint32_t w,
+                                                                   uint32_t hgt, int kind,
+                                                                   const float* __restrict__ attr,
                                                                    const uint32_t* __restrict__ idx,
                                                                    float* __restrict__ image,
                                                                    vx_hit* __restrict__ record) {
@@ -53,10 +62,12 @@ __global__ void __launch_bounds__(DBLOCK, 3) diff_forward_kernel(DevScene s, Cam
     float* stkT = reinterpret_cast<float*>(smem + s.max_levels * blockDim.x) + threadIdx.x;
     uint32_t* cyc = smem + 2 * s.max_levels * blockDim.x + threadIdx.x;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= w * hgt) return;
+    const uint32_t per_view = w * hgt;
+    if (i >= nviews * per_view) return;
+    const uint32_t v = i / per_view, p = i - v * per_view;
     vx_ray r;
     float uv_y;
-    camera_ray(cam, i % w, i / w, w, hgt, r, &uv_y);
+    camera_ray(views.cam[v], p % w, p / w, w, hgt, r, &uv_y);
     Hit h;
     cast_ray(s, r.ox, r.oy, r.oz, r.dx, r.dy, r.dz, 0.0f, FLT_MAX_, stkN, stkT, cyc, blockDim.x, h);
     store_hit(record, i, h);
@@ -171,22 +182,34 @@ __global__ void __launch_bounds__(DBLOCK) diff_backward_kernel(uint32_t n, int k
 }  // namespace
 }  // namespace vx
 
+extern "C" int vx_diff_forward_views(const vx_scene* scene, const vx_camera_pc* pcs, uint32_t views, uint32_t w,
+                                     uint32_t h, int32_t kind, const float* attr, const uint32_t* dxt_idx,
+                                     float* image, vx_hit* record, void* stream) {
+    using namespace vx;
+    if (!scene || !pcs || !attr || !image || !record || (kind == 1 && !dxt_idx) || (kind != 0 && kind != 1))
+        return fail(VX_EINVAL, "vx_diff_forward: bad argument");
+    if (views > VX_DIFF_MAX_VIEWS)
+        return fail(VX_EOVERFLOW, "vx_diff_forward_views: more than VX_DIFF_MAX_VIEWS views in one call");
+    const uint64_t n = uint64_t(w) * h * views;
+    if (n > 0xFFFFFFFFull) return fail(VX_EOVERFLOW, "vx_diff_forward: views * width * height exceeds 2^32");
+    if (reinterpret_cast<uintptr_t>(record) % 16 || reinterpret_cast<uintptr_t>(image) % 4)
+        return fail(VX_EINVAL, "vx_diff_forward: misaligned output");
+    if (n == 0) return VX_OK;
+    const DevScene& s = scene_dev(scene);
+    Views v{};
+    for (uint32_t k = 0; k < views; ++k) v.cam[k] = camera_from_pc(pcs[k]);
+    const size_t smem = (size_t(2) * size_t(s.max_levels) + 16) * DBLOCK * sizeof(uint32_t);
+    diff_forward_kernel<<<uint32_t((n + DBLOCK - 1) / DBLOCK), DBLOCK, smem, static_cast<cudaStream_t>(stream)>>>(
+        s, v, views, w, h, kind, attr, dxt_idx, image, record);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? VX_OK : fail(VX_ECUDA, std::string("vx_diff_forward: ") + cudaGetErrorString(e));
+}
+
 extern "C" int vx_diff_forward(const vx_scene* scene, const vx_camera_pc* pc, uint32_t w, uint32_t h, int32_t kind,
                                const float* attr, const uint32_t* dxt_idx, float* image, vx_hit* record,
                                void* stream) {
-    using namespace vx;
-    if (!scene || !pc || !attr || !image || !record || (kind == 1 && !dxt_idx) || (kind != 0 && kind != 1))
-        return fail(VX_EINVAL, "vx_diff_forward: bad argument");
-    if (uint64_t(w) * h > 0xFFFFFFFFull) return fail(VX_EOVERFLOW, "vx_diff_forward: width * height exceeds 2^32");
-    const uint64_t n = uint64_t(w) * h;
-    if (n == 0) return VX_OK;
-    const DevScene& s = scene_dev(scene);
-    const CameraDev cam = camera_from_pc(*pc);
-    const size_t smem = (size_t(2) * size_t(s.max_levels) + 16) * DBLOCK * sizeof(uint32_t);
-    diff_forward_kernel<<<uint32_t((n + DBLOCK - 1) / DBLOCK), DBLOCK, smem, static_cast<cudaStream_t>(stream)>>>(
-        s, cam, w, h, kind, attr, dxt_idx, image, record);
-    cudaError_t e = cudaGetLastError();
-    return e == cudaSuccess ? VX_OK : fail(VX_ECUDA, std::string("vx_diff_forward: ") + cudaGetErrorString(e));
+    if (!pc) return vx::fail(VX_EINVAL, "vx_diff_forward: bad argument");
+    return vx_diff_forward_views(scene, pc, 1, w, h, kind, attr, dxt_idx, image, record, stream);
 }
 
 extern "C" int vx_diff_backward(uint32_t n, int32_t kind, const uint32_t* dxt_idx, const vx_hit* record,
