@@ -170,7 +170,7 @@ def run_reference(args, rank, world):
     except Exception:
         pass
     wl = make_workload(vx, args.R, args.seed, 0, use_gpu)
-    rays = wl.rays()
+    rays = wl.rays(order="tiled")
     threads = os.cpu_count() or 1
     o = vo.OracleScene.from_dense(wl.bits, wl.R, wl.scene.max_levels)
     n = min(rays.shape[0], 1 << 15)
@@ -247,7 +247,7 @@ def measure_cfg4(args, rank, world, steps, warmup):
                                       False).cpu().numpy().view(np.uint64)
         wl = W.build_spec(sp, bits)
         scenes.append(vx.Scene(wl.scene))
-        rays.append(wl.rays())
+        rays.append(wl.rays(order="tiled"))
         wl.scene.brick_color = None  # host copies are no longer needed
         wls.append(wl)
     setup_s = time.perf_counter() - t_setup
@@ -323,6 +323,7 @@ def measure_cfg4(args, rank, world, steps, warmup):
                                    f"one camera each 256x256..1920x1080, 2 bounce rays per hit; batched "
                                    f"persistent kernel in a CUDA graph vs {2 * len(specs)} plain launches",
                        "primary_rays": n, "rays_per_frame": rays_per_frame, "hits": nhit,
+                       "ray_order": "primary rays in 8x4-pixel warp tiles (workloads.tile_order)",
                        "scene_R": [sp.R for sp in specs], "setup_s": setup_s,
                        "l2": "flushed before every timed frame (256 MiB write)"},
             "batched": {"value": value, "unit": "Mrays/s", "ms_per_frame": batched_total / steps,
@@ -348,7 +349,7 @@ def measure_cfg3(args, steps, warmup):
     setup_s = time.perf_counter() - t0
     bricks, nodes, dev_bytes = wl.scene.brick_count, wl.scene.node_count, scene.device_bytes()
     wl.scene.brick_color = None
-    rays_np = wl.rays()
+    rays_np = wl.rays(order="tiled")
     n = rays_np.shape[0]
     rays = torch.from_numpy(rays_np).cuda()
     hits = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
@@ -382,6 +383,7 @@ def measure_cfg3(args, steps, warmup):
     rays_per_frame = n + nhit
     return {"workload": f"{wl.name}: urban {wl.R}^3 (depth {wl.scene.max_levels}), 32x32 blocks, heights "
                         f"U[64,1800], DXT1; {wl.width}x{wl.height} primary + 1 shadow ray per hit",
+            "ray_order": "primary rays in 8x4-pixel warp tiles (workloads.tile_order)",
             "mrays_s": rays_per_frame / (ms / 1e3) / 1e6, "ms_per_frame": ms, "primary_rays": n,
             "shadow_rays": nhit, "primary_hit_rate": nhit / n, "shadowed_fraction": shit / max(nhit, 1),
             "bricks": bricks, "nodes": nodes, "scene_device_bytes": dev_bytes, "setup_s": setup_s}
@@ -550,7 +552,7 @@ def measure_next(args, steps, warmup):
     del rgb_t, dxt_t, occ_t, nrm_t
     # LOD cut and compressed render on the cfg2 camera
     wl = W.config2(R=R, seed=seed, bits=bits)
-    rays = torch.from_numpy(wl.rays()).cuda()
+    rays = torch.from_numpy(wl.rays(order="tiled")).cuda()
     n = rays.shape[0]
     hits = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
     base = vx.lod_from_camera(math.radians(70.0), wl.height)
@@ -594,6 +596,7 @@ def config_dict(wl, world):
     return {"workload": f"{wl.name}: cave {wl.R}^3 (depth {wl.scene.max_levels}), value noise spacing "
                         f"{64 * wl.R // 1024}, 5 octaves, 50% fill, DXT1 bricks, {wl.width}x{wl.height} FP32 "
                         f"primary rays per rank, plain cast kernel",
+            "ray_order": "8x4-pixel warp tiles in 32x8 blocks (vx_render's order; workloads.tile_order)",
             "rays_per_step_per_gpu": wl.width * wl.height, "bricks": int(wl.scene.brick_count),
             "nodes": int(wl.scene.node_count), "parallelism": f"replicated scene, {world} camera(s)",
             "l2": "flushed between timed steps (256 MiB write)"}
@@ -666,7 +669,7 @@ def main():
     vx = load_pkg()
     wl = make_workload(vx, args.R, args.seed, rank, True)
     scene = vx.Scene(wl.scene)
-    rays_np = wl.rays()
+    rays_np = wl.rays(order="tiled")
     n = rays_np.shape[0]
     rays = torch.from_numpy(rays_np).cuda()
     hits = torch.zeros((n, 4), dtype=torch.int32, device="cuda")

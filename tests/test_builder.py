@@ -112,3 +112,16 @@ def test_synth_urban_shape(vx):
     assert not dense[pitch - street:pitch, :, :].any()          # street in z
     col = dense[:pitch - street, :, :pitch - street]
     assert col.any()
+
+
+def test_tile_order_is_vx_render_lane_order(vx):
+    """workloads.tile_order: a permutation of the pixels; 32 x 8 tiles, warps of 8 x 4."""
+    from vx_b200 import workloads as W
+    for w, h in ((1920, 1080), (100, 37), (33, 9), (8, 4)):
+        o = W.tile_order(w, h)
+        assert np.array_equal(np.sort(o), np.arange(w * h))
+    o = W.tile_order(64, 8)
+    first_warp = [y * 64 + x for y in range(4) for x in range(8)]
+    assert list(o[:32]) == first_warp
+    assert list(o[32:40]) == list(range(8, 16))   # the next warp starts 8 pixels to the right
+    assert o[4 * 32] == 4 * 64                    # warp 4 starts 4 rows down

@@ -26,6 +26,9 @@ namespace vx {
 namespace {
 
 constexpr int DBLOCK = 256;
+#ifndef VX_DIFF_TILED
+#define VX_DIFF_TILED 1
+#endif
 
 __device__ __forceinline__ float lambert_k(uint32_t flags) {
     const float Ld = (1.0f * 1.0f + 1.0f * 1.0f) + (-1.0f) * (-1.0f);
@@ -49,8 +52,10 @@ struct Views {
     CameraDev cam[VX_DIFF_MAX_VIEWS];
 };
 
-// Pixel i of the launch is pixel i % (w * hgt) of view i / (w * hgt); images
-// and records are view-major.
+// Images and records are view-major: pixel p of view v is entry v * w * hgt + p.
+// With VX_DIFF_TILED each block covers a 32 x 8 pixel tile of one view and each
+// warp an 8 x 4 piece of it, so a warp's rays are neighbours in both image
+// directions and their traversals stay closer together than along a row.
 __global__ void __launch_bounds__(DBLOCK, 3) diff_forward_kernel(DevScene s, Views views, uint32_t nviews, uint32_t w,
                                                                    uint32_t hgt, int kind,
                                                                    const float* __restrict__ attr,
@@ -61,13 +66,24 @@ __global__ void __launch_bounds__(DBLOCK, 3) diff_forward_kernel(DevScene s, Vie
     uint32_t* stkN = smem + threadIdx.x;
     float* stkT = reinterpret_cast<float*>(smem + s.max_levels * blockDim.x) + threadIdx.x;
     uint32_t* cyc = smem + 2 * s.max_levels * blockDim.x + threadIdx.x;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t per_view = w * hgt;
+#if VX_DIFF_TILED
+    const uint32_t tw = (w + 31) / 32, tiles = tw * ((hgt + 7) / 8);
+    const uint32_t v = blockIdx.x / tiles, tl = blockIdx.x - v * tiles;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t px = (tl % tw) * 32 + (warp & 3u) * 8 + (lane & 7u);
+    const uint32_t py = (tl / tw) * 8 + (warp >> 2) * 4 + (lane >> 3);
+    if (v >= nviews || px >= w || py >= hgt) return;
+    const uint32_t i = v * per_view + py * w + px;
+#else
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nviews * per_view) return;
     const uint32_t v = i / per_view, p = i - v * per_view;
+    const uint32_t px = p % w, py = p / w;
+#endif
     vx_ray r;
     float uv_y;
-    camera_ray(views.cam[v], p % w, p / w, w, hgt, r, &uv_y);
+    camera_ray(views.cam[v], px, py, w, hgt, r, &uv_y);
     Hit h;
     cast_ray(s, r.ox, r.oy, r.oz, r.dx, r.dy, r.dz, 0.0f, FLT_MAX_, stkN, stkT, cyc, blockDim.x, h);
     store_hit(record, i, h);
@@ -199,7 +215,14 @@ extern "C" int vx_diff_forward_views(const vx_scene* scene, const vx_camera_pc* 
     Views v{};
     for (uint32_t k = 0; k < views; ++k) v.cam[k] = camera_from_pc(pcs[k]);
     const size_t smem = (size_t(2) * size_t(s.max_levels) + 16) * DBLOCK * sizeof(uint32_t);
-    diff_forward_kernel<<<uint32_t((n + DBLOCK - 1) / DBLOCK), DBLOCK, smem, static_cast<cudaStream_t>(stream)>>>(
+#if VX_DIFF_TILED
+    static_assert(DBLOCK == 256, "a block covers one 32 x 8 tile");
+    const uint64_t blocks = uint64_t(views) * ((w + 31) / 32) * ((h + 7) / 8);
+#else
+    const uint64_t blocks = (n + DBLOCK - 1) / DBLOCK;
+#endif
+    if (blocks > 0x7FFFFFFFull) return fail(VX_EOVERFLOW, "vx_diff_forward: too many pixels for one launch");
+    diff_forward_kernel<<<uint32_t(blocks), DBLOCK, smem, static_cast<cudaStream_t>(stream)>>>(
         s, v, views, w, h, kind, attr, dxt_idx, image, record);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? VX_OK : fail(VX_ECUDA, std::string("vx_diff_forward: ") + cudaGetErrorString(e));

@@ -33,6 +33,10 @@ __global__ void __launch_bounds__(BLOCK, 3) cast_kernel(DevScene s, const vx_ray
     }
 }
 
+// One block per 32 x 8 pixel tile, one warp per 8 x 4 piece of it (the
+// reference dispatches 8 x 8 workgroups, ComputeDispatchNode.cpp:272-301): a
+// warp's rays are neighbours in both image directions, so their traversals
+// diverge less than along a row.  Outputs are indexed by pixel (y * w + x).
 __global__ void __launch_bounds__(BLOCK, 3) render_kernel(DevScene s, CameraDev cam, uint32_t w, uint32_t hgt,
                                                         uint32_t* __restrict__ image, vx_hit* __restrict__ hits,
                                                         void* __restrict__ color) {
@@ -40,9 +44,12 @@ __global__ void __launch_bounds__(BLOCK, 3) render_kernel(DevScene s, CameraDev 
     uint32_t* stkN = smem + threadIdx.x;
     float* stkT = reinterpret_cast<float*>(smem + s.max_levels * blockDim.x) + threadIdx.x;
     uint32_t* cyc = smem + 2 * s.max_levels * blockDim.x + threadIdx.x;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= w * hgt) return;
-    const uint32_t px = i % w, py = i / w;
+    const uint32_t tw = (w + 31) / 32;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t px = (blockIdx.x % tw) * 32 + (warp & 3u) * 8 + (lane & 7u);
+    const uint32_t py = (blockIdx.x / tw) * 8 + (warp >> 2) * 4 + (lane >> 3);
+    if (px >= w || py >= hgt) return;
+    const uint32_t i = py * w + px;
     vx_ray r;
     float uv_y;
     camera_ray(cam, px, py, w, hgt, r, &uv_y);
@@ -122,9 +129,11 @@ int launch_render(const DevScene& s, const CameraDev& cam, uint32_t w, uint32_t 
                   void* color, void* stream) {
     const uint64_t n = uint64_t(w) * h;
     if (n == 0) return int(cudaSuccess);
-    const uint32_t grid = uint32_t((n + BLOCK - 1) / BLOCK);
-    render_kernel<<<grid, BLOCK, stack_bytes(s), static_cast<cudaStream_t>(stream)>>>(s, cam, w, h, image, hits,
-                                                                                       color);
+    static_assert(BLOCK == 256, "a block covers one 32 x 8 tile");
+    const uint64_t grid = uint64_t((w + 31) / 32) * ((h + 7) / 8);
+    if (grid > 0x7FFFFFFFull) return int(cudaErrorInvalidValue);
+    render_kernel<<<uint32_t(grid), BLOCK, stack_bytes(s), static_cast<cudaStream_t>(stream)>>>(s, cam, w, h, image,
+                                                                                                 hits, color);
     return int(cudaGetLastError());
 }
 

@@ -78,8 +78,25 @@ class Workload:
     width: int
     height: int
 
-    def rays(self) -> np.ndarray:
-        return camera_rays(self.camera, self.width, self.height)
+    def rays(self, order: str = "rows") -> np.ndarray:
+        """The camera's primary rays (vx_camera_rays).  order="rows": pixel y * width + x;
+        order="tiled": the order vx_render gives them to warps (tile_order)."""
+        r = camera_rays(self.camera, self.width, self.height)
+        return r if order == "rows" else r[tile_order(self.width, self.height)]
+
+
+def tile_order(width: int, height: int) -> np.ndarray:
+    """Pixel indices in the order vx_render assigns them to threads: 32 x 8 tiles row by row,
+    inside a tile eight 8 x 4 warp pieces (4 across, 2 down), inside a piece row-major;
+    pixels outside the image are skipped."""
+    tw, th = -(-width // 32), -(-height // 8)
+    t = np.arange(tw * th * 256, dtype=np.int64)
+    tile, thr = t // 256, t % 256
+    warp, lane = thr // 32, thr % 32
+    x = (tile % tw) * 32 + (warp % 4) * 8 + lane % 8
+    y = (tile // tw) * 8 + (warp // 4) * 4 + lane // 8
+    keep = (x < width) & (y < height)
+    return (y * width + x)[keep].astype(np.int64)
 
 
 def noise_scene(R, spacing, octaves, fill, seed, shell, color, max_levels=None):
