@@ -182,6 +182,16 @@ int vx_scene_destroy(vx_scene* scene);
 /* Device bytes held by the scene. */
 int vx_scene_device_bytes(const vx_scene* scene, uint64_t* out);
 
+/* Bounds checks.  libvx_checked.so (make checked) is this library with every
+ * device index into the scene arrays, the traversal stack and the batch's
+ * scene table tested before its load; a failing test sets a bit (1 node, 2
+ * brick grid, 4 brick, 8 voxel, 16 stack slot, 32 scene table) and the load
+ * reads element 0 instead.  This call reports whether the loaded library is
+ * that build and returns the bits set since the last call (clearing them)
+ * after synchronising the device; the default build reports 0 / 0.  It stands
+ * in for a memory checker where none can run. */
+int vx_bounds_checks(int32_t* enabled, uint32_t* violations);
+
 /* What a scene holds (for vx_scene_download and cache files). */
 typedef struct vx_scene_info {
     vx_octree_config config;

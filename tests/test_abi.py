@@ -98,3 +98,9 @@ def test_camera_rays_host(vx):
     n = np.linalg.norm(r[:, 3:].astype(np.float64), axis=1)
     assert np.all(np.abs(n - 1) < 1e-6)
     assert r[0, 4] > 0 and r[-1, 4] < 0  # row 0 is the top of the image
+
+
+def test_default_build_compiles_no_bounds_checks(vx):
+    en = C.c_int32(-1)
+    assert vx.lib().vx_bounds_checks(C.byref(en), None) == 0
+    assert en.value == 0

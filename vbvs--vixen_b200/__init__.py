@@ -19,7 +19,8 @@ from dataclasses import dataclass
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libvx.so")
+# VX_LIBRARY=checked loads the bounds-checked build (vx_bounds_checks).
+LIB_PATH = os.path.join(_HERE, "libvx_checked.so" if os.environ.get("VX_LIBRARY") == "checked" else "libvx.so")
 
 VX_OK = 0
 VX_HIT_HIT = 0x01
@@ -101,6 +102,7 @@ def lib():
         "vx_build_normals": (C.c_int, [vp, u32, vp]),
         "vx_build_normals_dev": (C.c_int, [vp, u32, vp, vp]),
         "vx_hit_normals": (C.c_int, [vp, vp, u32, vp, vp]),
+        "vx_bounds_checks": (C.c_int, [vp, vp]),
         "vx_diff_forward_views": (C.c_int, [vp, vp, u32, u32, u32, i32, vp, vp, vp, vp, vp]),
         "vx_build_dxt1": (C.c_int, [vp, vp, u32, vp]),
         "vx_build_dxt1_dev": (C.c_int, [vp, vp, u32, vp, vp]),
@@ -253,6 +255,13 @@ def build_dense(bits: np.ndarray, R: int, max_levels: int) -> SceneArrays:
                            take(d.brick_occ, 16 * d.brick_count, np.uint32))
     finally:
         lib().vx_build_free(h)
+
+
+def bounds_checks():
+    """vx_bounds_checks: (checked build loaded, violation bits since the last call)."""
+    en, v = C.c_int32(), C.c_uint32()
+    check(lib().vx_bounds_checks(C.byref(en), C.byref(v)))
+    return bool(en.value), v.value
 
 
 def build_normals(brick_occ: np.ndarray) -> np.ndarray:

@@ -259,6 +259,20 @@ int vx_scene_destroy(vx_scene* s) {
     return VX_OK;
 }
 
+int vx_bounds_checks(int32_t* enabled, uint32_t* violations) {
+#ifndef VX_CHECKED
+#define VX_CHECKED 0
+#endif
+    if (enabled) *enabled = VX_CHECKED;
+    if (violations) {
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) return vx::cuda_fail(e, "vx_bounds_checks: synchronize");
+        *violations = vx::violations_kernels() | vx::violations_batch() | vx::violations_diff() |
+                      vx::violations_payload();
+    }
+    return VX_OK;
+}
+
 int vx_scene_info_get(const vx_scene* s, vx_scene_info* out) {
     if (!s || !out) return fail(VX_EINVAL, "vx_scene_info_get: null argument");
     vx_scene_info i{};

@@ -50,7 +50,7 @@ __device__ __forceinline__ int scene_of(const uint32_t* beg, uint32_t S, uint32_
         if (beg[mid] <= r) lo = mid;
         else hi = mid;
     }
-    return lo;
+    return int(bounded(uint32_t(lo), S, V_SCENE));
 }
 
 __device__ __forceinline__ void store_counters(vx_ray_counters* counters, uint32_t r, const Hit& h) {
@@ -726,3 +726,7 @@ extern "C" int vx_cast_batch_noalloc(const vx_scene* const* scenes, uint32_t cou
     if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch_noalloc: launch");
     return VX_OK;
 }
+
+namespace vx {
+VX_VIOLATION_READER(violations_batch)
+}  // namespace vx

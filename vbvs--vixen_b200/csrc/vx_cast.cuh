@@ -45,6 +45,31 @@ constexpr int CYCLE_START = VX_CYCLE_START;  // iteration from which loop states
 constexpr float FLT_MAX_ = 3.402823466e+38f;
 constexpr uint32_t NONE = 0xFFFFFFFFu;
 
+// Bounds-checked build (make checked -> libvx_checked.so, -DVX_CHECKED=1): every
+// index into a scene array, the traversal stack and the batch's scene table is
+// tested before its load; a failed test sets its bit in this translation
+// unit's violation word (vx_bounds_checks reads and clears them) and the load
+// uses index 0 instead.  The default build compiles no test.
+#ifndef VX_CHECKED
+#define VX_CHECKED 0
+#endif
+constexpr uint32_t V_NODE = 1u, V_GRID = 2u, V_BRICK = 4u, V_VOXEL = 8u, V_STACK = 16u, V_SCENE = 32u;
+#if VX_CHECKED
+static __device__ unsigned int vx_violation = 0u;
+#endif
+__device__ __forceinline__ uint32_t bounded(uint32_t i, uint32_t n, uint32_t code) {
+#if VX_CHECKED
+    if (i >= n) {
+        atomicOr(&vx_violation, code);
+        return 0u;
+    }
+#else
+    (void)n;
+    (void)code;
+#endif
+    return i;
+}
+
 constexpr uint32_t F_HIT = 1u;
 constexpr uint32_t F_NEG = 1u << 3;
 constexpr uint32_t F_ITER_CAP = 1u << 6;
@@ -80,7 +105,11 @@ __device__ __forceinline__ uint32_t mirror_masks(uint32_t m, int octant_mask) {
 __device__ __forceinline__ uint32_t grid_lookup(const DevScene& s, int bx, int by, int bz) {
     // getBrickViewByGrid (SVOBuilder.h:107-116) over the dense table
     // (VoxelSceneCacher.cpp:670-713).
-    const size_t li = size_t(bx) + size_t(by) * size_t(s.bpa) + size_t(bz) * size_t(s.bpa) * size_t(s.bpa);
+    size_t li = size_t(bx) + size_t(by) * size_t(s.bpa) + size_t(bz) * size_t(s.bpa) * size_t(s.bpa);
+#if VX_CHECKED
+    const size_t slots = size_t(s.bpa) * size_t(s.bpa) * size_t(s.bpa);
+    if (li >= slots || bx < 0 || by < 0 || bz < 0) { atomicOr(&vx_violation, V_GRID); li = 0; }
+#endif
     return __ldg(s.grid + li);
 }
 
@@ -119,7 +148,7 @@ __device__ __forceinline__ bool brick_dda(const DevScene& s, uint32_t brick, con
             tNext[a] = tMin + (ep - (bmn[a] + float(cur[a]))) / fabsf(rb.d[a]);
         }
     }
-    const uint32_t* occ = reinterpret_cast<const uint32_t*>(s.occ) + size_t(brick) * 16;
+    const uint32_t* occ = reinterpret_cast<const uint32_t*>(s.occ) + size_t(bounded(brick, s.brick_count, V_BRICK)) * 16;
     for (int stepCount = 0; stepCount < 24; ++stepCount) {
         if (uint32_t(cur[0]) >= 8u || uint32_t(cur[1]) >= 8u || uint32_t(cur[2]) >= 8u) return false;
         ++h.dda_steps;
@@ -287,7 +316,6 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
     tExit = gmin(tExit, tMaxArg);
     if (tEntry >= tExit || tExit < 0.0f) return true;
     const float tRayStart = inside ? 0.0f : gmax(0.0f, tEntry);
-    const float wsx = s.wsize[0], wsy = s.wsize[1], wsz = s.wsize[2];
     // x / size, as a product where 1 / size is exact (a power-of-two size):
     // both round the same real number once.
     auto by_size = [&](float x, int i) { return s.wsinv[i] != 0.0f ? x * s.wsinv[i] : x / s.wsize[i]; };
@@ -412,7 +440,7 @@ __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint
     {  // one iteration; `goto next_iter` is the reference's `continue`
         // fetchChildDescriptor (:282-293)
         if (!st.fetched) {
-            const uint2 nd = __ldg(s.nodes + st.parent);
+            const uint2 nd = __ldg(s.nodes + bounded(st.parent, s.node_count, V_NODE));
             st.pChild = nd.x;
             st.pValid = nd.y & 0xFFu;
             st.pLeaf = (nd.y >> 8) & 0xFFu;
@@ -504,7 +532,7 @@ __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint
                 }
                 if (brick != NONE) {
                     // traverseBrickAndReturnHit (SVOBrickDDA.cpp:187-225)
-                    const uint32_t bc = __ldg(s.coord + brick);
+                    const uint32_t bc = __ldg(s.coord + bounded(brick, s.brick_count, V_BRICK));
                     const float bmn[3] = {float(int(bc & 0x3FFu) * 8), float(int((bc >> 10) & 0x3FFu) * 8),
                                           float(int((bc >> 20) & 0x3FFu) * 8)};
                     float tn[3], tf[3];
@@ -539,8 +567,9 @@ __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint
                 const float tz_center = half * c.tz_coef + tz;
                 const float tc_max = min3(tx, ty, tz);
                 if (tc_max < st.hh) {
-                    stkN[(st.scale - minScale) * stride] = st.parent;
-                    stkT[(st.scale - minScale) * stride] = st.t_max;
+                    const uint32_t k = bounded(uint32_t(st.scale - minScale), uint32_t(s.max_levels), V_STACK);
+                    stkN[k * stride] = st.parent;
+                    stkT[k * stride] = st.t_max;
                     st.pushed |= 1u << (st.scale - minScale);
                 }
                 st.hh = tc_max;
@@ -617,8 +646,9 @@ __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint
             if (st.scale < minScale || st.scale > ESVO_MAX_SCALE) { cast_finish(st); return true; }
             st.scale_exp2 = __int_as_float((st.scale - ESVO_MAX_SCALE + 127) << 23);
             if ((st.pushed >> (st.scale - minScale)) & 1u) {
-                st.parent = stkN[(st.scale - minScale) * stride];
-                st.t_max = stkT[(st.scale - minScale) * stride];
+                const uint32_t k = bounded(uint32_t(st.scale - minScale), uint32_t(s.max_levels), V_STACK);
+                st.parent = stkN[k * stride];
+                st.t_max = stkT[k * stride];
             } else {
                 st.parent = 0u;
                 st.t_max = st.t_root;
@@ -717,7 +747,8 @@ __device__ __forceinline__ void dxt_texel(const uint2* dxt, uint32_t brick, uint
 // normalize(decodeDXTNormal) of the voxel's texel (Compression.glsl:158-177).
 __device__ __forceinline__ void dxt_normal(const DevScene& s, uint32_t brick, uint32_t voxel, float& x, float& y,
                                            float& z) {
-    const uint4 q = __ldg(s.nrm + size_t(brick) * 32 + (voxel >> 4));
+    const uint4 q = __ldg(s.nrm + size_t(bounded(brick, s.brick_count, V_BRICK)) * 32 +
+                          (bounded(voxel, 512u, V_VOXEL) >> 4));
     const dxtn::F3 n = dxtn::unit(dxtn::decode(uint64_t(q.x) | (uint64_t(q.y) << 32),
                                                uint64_t(q.z) | (uint64_t(q.w) << 32), voxel & 15u));
     x = n.x; y = n.y; z = n.z;
@@ -736,14 +767,32 @@ __device__ __forceinline__ void store_hit(vx_hit* hits, uint32_t i, const Hit& h
 __device__ __forceinline__ void store_color(const DevScene& s, void* color, uint32_t i, const Hit& h) {
     const bool hit = (h.flags & F_HIT) && h.brick != NONE;
     if (s.color_kind == VX_COLOR_RGBA8) {
-        reinterpret_cast<uint32_t*>(color)[i] = hit ? __ldg(s.rgba + size_t(h.brick) * 512 + h.voxel) : 0u;
+        reinterpret_cast<uint32_t*>(color)[i] =
+            hit ? __ldg(s.rgba + size_t(bounded(h.brick, s.brick_count, V_BRICK)) * 512 +
+                        bounded(h.voxel, 512u, V_VOXEL))
+                : 0u;
     } else if (s.color_kind == VX_COLOR_DXT1) {
         float r = 0.0f, g = 0.0f, b = 0.0f;
-        if (hit) dxt_texel(s.dxt, h.brick, h.voxel, r, g, b);
+        if (hit) dxt_texel(s.dxt, bounded(h.brick, s.brick_count, V_BRICK), bounded(h.voxel, 512u, V_VOXEL), r, g, b);
         float* c = reinterpret_cast<float*>(color) + size_t(i) * 3;
         c[0] = r; c[1] = g; c[2] = b;
     }
 }
 
 }  // namespace
+// Host reader of this translation unit's violation word (read and clear).
+#if VX_CHECKED
+#define VX_VIOLATION_READER(fn)                                              \
+    uint32_t fn() {                                                          \
+        unsigned int v = 0u, z = 0u;                                         \
+        if (cudaMemcpyFromSymbol(&v, vx_violation, sizeof(v)) != cudaSuccess) \
+            return 0x80000000u;                                              \
+        cudaMemcpyToSymbol(vx_violation, &z, sizeof(z));                     \
+        return v;                                                            \
+    }
+#else
+#define VX_VIOLATION_READER(fn) \
+    uint32_t fn() { return 0u; }
+#endif
+
 }  // namespace vx

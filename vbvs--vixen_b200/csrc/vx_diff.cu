@@ -246,3 +246,7 @@ extern "C" int vx_diff_backward(uint32_t n, int32_t kind, const uint32_t* dxt_id
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? VX_OK : fail(VX_ECUDA, std::string("vx_diff_backward: ") + cudaGetErrorString(e));
 }
+
+namespace vx {
+VX_VIOLATION_READER(violations_diff)
+}  // namespace vx

@@ -49,6 +49,13 @@ int scene_alloc(const vx_octree_config& c, uint32_t node_count, uint32_t brick_c
                 bool normals, vx_scene** out, ScenePool* p);
 int cuda_fail(cudaError_t e, const std::string& what);
 
+// Violation words of the bounds-checked build, one per translation unit with
+// device code (read and cleared; 0 in the default build).
+uint32_t violations_kernels();
+uint32_t violations_batch();
+uint32_t violations_diff();
+uint32_t violations_payload();
+
 // Per-thread-local error string.
 void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);

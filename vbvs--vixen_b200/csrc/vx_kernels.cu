@@ -145,3 +145,7 @@ int launch_camera_rays(const CameraDev& cam, uint32_t w, uint32_t h, vx_ray* ray
 }
 
 }  // namespace vx
+
+namespace vx {
+VX_VIOLATION_READER(violations_kernels)
+}  // namespace vx

@@ -170,3 +170,7 @@ extern "C" int vx_hit_normals(const vx_scene* scene, const vx_hit* hits_dev, uin
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_hit_normals");
 }
+
+namespace vx {
+VX_VIOLATION_READER(violations_payload)
+}  // namespace vx
