@@ -172,3 +172,65 @@ CASES += [
         ((3, 3, 0), (0, 0, 1), lambda h: hit(h) and abs(h["hit_point"][0] - 3) <= 1 and abs(h["hit_point"][1] - 3) <= 1),
     ])
 ]
+
+
+def cornell_box_voxels():
+    """CornellBoxTest::buildCornellBox (test_cornell_box.cpp:66-136): float positions with
+    step 0.5 and wall thickness 0.2 in a 10^3 box (the loops' float32 accumulation is exact), in
+    creation order, each with its wall colour."""
+    f = np.float32
+    size, thick, step = f(10.0), f(0.2), f(0.5)
+    grey, red, green, white = (0.8, 0.8, 0.8), (0.8, 0.1, 0.1), (0.1, 0.8, 0.1), (1.0, 1.0, 1.0)
+
+    def rng(lo, hi):
+        out, v = [], f(lo)
+        while v < hi:
+            out.append(float(v))
+            v = f(v + step)
+        return out
+    vox = []
+    for x in rng(0, size):
+        for z in rng(0, size):
+            for y in rng(0, thick):
+                vox.append(((x, y, z), grey))
+    for x in rng(0, size):
+        for z in rng(0, size):
+            for y in rng(size - thick, size):
+                d = np.hypot(f(x) - f(5.0), f(z) - f(5.0))
+                vox.append(((x, y, z), white if d < 2.0 else grey))
+    for y in rng(0, size):
+        for z in rng(0, size):
+            for x in rng(0, thick):
+                vox.append(((x, y, z), red))
+    for y in rng(0, size):
+        for z in rng(0, size):
+            for x in rng(size - thick, size):
+                vox.append(((x, y, z), green))
+    for x in rng(0, size):
+        for y in rng(0, size):
+            for z in rng(size - thick, size):
+                vox.append(((x, y, z), grey))
+    return vox
+
+
+_CB = [p for p, _ in cornell_box_voxels()]
+FACE_DIVERGES = ("positions quantise to integer keys (floor(p + 1e-5), MortonCode64::fromWorldPos), so the floor and "
+                 "left-wall voxels span [0, 1) and the traversal reports the entry face at exactly 1.0; the test's "
+                 "strict < 1.0 fails on the restated code (traverseBrickView, SVOBrickDDA.cpp:492-507)")
+CB_BOUNDS = ((0.0, 0.0, 0.0), (10.0, 10.0, 10.0))  # rebuild(world, vec3(0), vec3(boxSize)) (:52)
+
+# --- test_cornell_box.cpp (depth 8): every assertion there is conditional on a hit
+CASES += [
+    Case("cbox_floor", _CB, 8, (5, 5, 5), (0, -1, 0), lambda h: (not hit(h)) or h["hit_point"][1] < 1.0,
+         bounds=CB_BOUNDS, diverges=FACE_DIVERGES),                                                                # :152-164, :290-322
+    Case("cbox_ceiling", _CB, 8, (5, 5, 5), (0, 1, 0), lambda h: (not hit(h)) or h["hit_point"][1] > 9.0,
+         bounds=CB_BOUNDS),                                                                # :169-181
+    Case("cbox_left", _CB, 8, (5, 5, 5), (-1, 0, 0), lambda h: (not hit(h)) or h["hit_point"][0] < 1.0,
+         bounds=CB_BOUNDS, diverges=FACE_DIVERGES),                                                                # :186-207
+    Case("cbox_right", _CB, 8, (5, 5, 5), (1, 0, 0), lambda h: (not hit(h)) or h["hit_point"][0] > 9.0,
+         bounds=CB_BOUNDS),                                                                # :212-233
+    Case("cbox_back", _CB, 8, (5, 5, 5), (0, 0, 1), lambda h: (not hit(h)) or h["hit_point"][2] > 9.0,
+         bounds=CB_BOUNDS),                                                                # :238-250
+    Case("cbox_diagonal", _CB, 8, (1, 1, 1), _norm((1, 1, 1)), lambda h: True, bounds=CB_BOUNDS),  # :255-267
+    Case("cbox_outside", _CB, 8, (-5, 5, 5), (-1, 0, 0), lambda h: True, bounds=CB_BOUNDS),       # :272-285
+]

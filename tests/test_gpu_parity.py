@@ -225,3 +225,35 @@ def test_render_matches_oracle_shading(vx, vo, cuda):
         uv_y = (np.float32(i // wl.width) + np.float32(0.5)) / np.float32(wl.height)
         want = vo.shade(col, hit, (int(oh["flags"][i]) >> 1) & 3, bool(oh["flags"][i] & 8), float(uv_y))
         assert image[i] == want, (i, hex(image[i]), hex(want))
+
+
+def test_cornell_box_wall_colours(vx, vo, cuda):
+    """CornellBoxTest (test_cornell_box.cpp:186-233, 290-322): the hit voxel's colour is its
+    wall's (red left, grey floor), read through the RGBA8 colour output of the cast."""
+    import math
+    import torch
+    cb = K.cornell_box_voxels()
+    keys = {}
+    for p, col in cb:  # later voxels at the same integer key replace earlier ones
+        k = tuple(int(math.floor(np.float32(c) + np.float32(1e-5))) for c in p)
+        keys[k] = col
+    o = vo.OracleScene.from_positions([p for p, _ in cb], *K.CB_BOUNDS, 8)
+    a = scene_from_oracle(vx, o, K.CB_BOUNDS, 8)
+    B = a.brick_count
+    rgba = np.zeros(B * 512, np.uint32)
+    for b in range(B):
+        c = int(a.brick_coord[b])
+        bx, by, bz = (c & 0x3FF) * 8, ((c >> 10) & 0x3FF) * 8, ((c >> 20) & 0x3FF) * 8
+        for v in range(512):
+            col = keys.get((bx + (v & 7), by + ((v >> 3) & 7), bz + (v >> 6)))
+            if col is not None:
+                r, g, bl = (int(np.float32(x) * 255 + 0.5) for x in col)
+                rgba[b * 512 + v] = r | (g << 8) | (bl << 16) | (255 << 24)
+    a.color_kind, a.brick_color = vx.VX_COLOR_RGBA8, rgba
+    rays = np.array([[5, 5, 5, 0, -1, 0], [5, 5, 5, -1, 0, 0]], np.float32)
+    g, col, _ = gpu_cast(vx, a, rays, 0.0, 100.0)
+    assert_hits_equal(g, o.cast_rays(rays, 0.0, 100.0), None, "cornell")
+    assert g["flags"][0] & 1 and g["flags"][1] & 1
+    c0, c1 = int(col[0, 0]) & 0xFFFFFFFF, int(col[1, 0]) & 0xFFFFFFFF
+    assert (c0 & 255) == (c0 >> 8) & 255 == 204          # floor: grey 0.8
+    assert (c1 & 255) > 127 and ((c1 >> 8) & 255) < 77   # left wall: red
