@@ -154,3 +154,32 @@ def test_vsca_write_rejects_wide_child_pointers(vx, tmp_path):
         vx.cache_write_vsca(str(tmp_path / "big.vsca"), a, 0, R, 1.0, 0)
     vx.cache_write(str(tmp_path / "big.vxsc"), a)
     _same(a, vx.cache_read(str(tmp_path / "big.vxsc")), False, False)
+
+
+def test_vxsc_header_sizes_checked_before_allocating(vx, tmp_path):
+    """A header that promises 2^32 descriptors in a small file is rejected as a format error
+    (no allocation of the promised size)."""
+    import struct as st
+    a, _ = _scene(vx)
+    p = tmp_path / "s.vxsc"
+    vx.cache_write(str(p), a)
+    raw = bytearray(p.read_bytes())
+    off = 8 + 40  # magic, version, vx_octree_config
+    raw[off:off + 4] = st.pack("<I", 0xFFFFFFFF)
+    q = tmp_path / "huge.vxsc"
+    q.write_bytes(bytes(raw))
+    with pytest.raises(vx.VxError):
+        vx.cache_read(str(q))
+
+
+def test_vsca_vector_sizes_checked(vx, tmp_path):
+    a, _ = _scene(vx, "dxt1", R=64, seed=5)
+    p = tmp_path / "w.vsca"
+    vx.cache_write_vsca(str(p), a, 2, 64, 0.5, 7)
+    raw = bytearray(p.read_bytes())
+    import struct as st
+    raw[12 + 8 + 16:12 + 8 + 16 + 8] = st.pack("<Q", 1 << 39)  # esvoNodes length
+    q = tmp_path / "huge.vsca"
+    q.write_bytes(bytes(raw))
+    with pytest.raises(vx.VxError):
+        vx.cache_read_vsca(str(q), 0)

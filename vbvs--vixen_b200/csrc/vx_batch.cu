@@ -422,7 +422,7 @@ int check_tuning(const vx_batch_tuning* t) {
 
 extern "C" {
 
-int vx_batch_create(const vx_scene* const* scenes, uint32_t count, vx_batch** out) {
+static int vx_batch_create_body(const vx_scene* const* scenes, uint32_t count, vx_batch** out) {
     if (!out || (!scenes && count) || count == 0 || count > 256)
         return fail(VX_EINVAL, "vx_batch_create: need 1..256 scenes");
     *out = nullptr;
@@ -452,6 +452,10 @@ int vx_batch_create(const vx_scene* const* scenes, uint32_t count, vx_batch** ou
     }
     *out = b;
     return VX_OK;
+}
+
+int vx_batch_create(const vx_scene* const* scenes, uint32_t count, vx_batch** out) {
+    return vx::guarded("vx_batch_create", [&] { return vx_batch_create_body(scenes, count, out); });
 }
 
 int vx_batch_destroy(vx_batch* b) {
@@ -514,7 +518,7 @@ int vx_batch_set_bounce_tuning(vx_batch* b, const vx_batch_tuning* t) {
     return VX_OK;
 }
 
-int vx_batch_autotune(vx_batch* b, const vx_ray* rays, const uint32_t* begin, uint32_t n, vx_hit* hits, void* stream,
+static int vx_batch_autotune_body(vx_batch* b, const vx_ray* rays, const uint32_t* begin, uint32_t n, vx_hit* hits, void* stream,
                       vx_batch_tuning* best_out, float* best_ms_out) {
     if (!b || !begin || !rays || !hits || n == 0) return fail(VX_EINVAL, "vx_batch_autotune: bad argument");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -559,6 +563,11 @@ int vx_batch_autotune(vx_batch* b, const vx_ray* rays, const uint32_t* begin, ui
     if (best_out) *best_out = bt;
     if (best_ms_out) *best_ms_out = best;
     return VX_OK;
+}
+
+int vx_batch_autotune(vx_batch* b, const vx_ray* rays, const uint32_t* begin, uint32_t n, vx_hit* hits, void* stream,
+                      vx_batch_tuning* best_out, float* best_ms_out) {
+    return vx::guarded("vx_batch_autotune", [&] { return vx_batch_autotune_body(b, rays, begin, n, hits, stream, best_out, best_ms_out); });
 }
 
 int vx_bounce_table(float* out) {
@@ -682,7 +691,7 @@ int noalloc_setup(int dev, NoallocDevice*& out) {
 }  // namespace
 }  // namespace vx
 
-extern "C" int vx_cast_batch_noalloc(const vx_scene* const* scenes, uint32_t count, const vx_ray* rays,
+static int vx_cast_batch_noalloc_body(const vx_scene* const* scenes, uint32_t count, const vx_ray* rays,
                                      const uint32_t* begin, uint32_t n, float tmin, float tmax, vx_hit* hits,
                                      void* stream) {
     using namespace vx;
@@ -725,6 +734,12 @@ extern "C" int vx_cast_batch_noalloc(const vx_scene* const* scenes, uint32_t cou
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch_noalloc: launch");
     return VX_OK;
+}
+
+extern "C" int vx_cast_batch_noalloc(const vx_scene* const* scenes, uint32_t count, const vx_ray* rays,
+                                     const uint32_t* begin, uint32_t n, float tmin, float tmax, vx_hit* hits,
+                                     void* stream) {
+    return vx::guarded("vx_cast_batch_noalloc", [&] { return vx_cast_batch_noalloc_body(scenes, count, rays, begin, n, tmin, tmax, hits, stream); });
 }
 
 namespace vx {

@@ -64,7 +64,7 @@ struct vx_build {
 
 extern "C" {
 
-int vx_build_dense(const uint64_t* bits, uint32_t R, int32_t max_levels, vx_build** out) {
+static int vx_build_dense_body(const uint64_t* bits, uint32_t R, int32_t max_levels, vx_build** out) {
     using namespace vx;
     if (!bits || !out) return fail(VX_EINVAL, "vx_build_dense: null argument");
     *out = nullptr;
@@ -181,6 +181,10 @@ int vx_build_dense(const uint64_t* bits, uint32_t R, int32_t max_levels, vx_buil
     return VX_OK;
 }
 
+int vx_build_dense(const uint64_t* bits, uint32_t R, int32_t max_levels, vx_build** out) {
+    return vx::guarded("vx_build_dense", [&] { return vx_build_dense_body(bits, R, max_levels, out); });
+}
+
 int vx_build_desc(const vx_build* b, vx_scene_desc* d) {
     using namespace vx;
     if (!b || !d) return fail(VX_EINVAL, "vx_build_desc: null argument");
@@ -228,7 +232,7 @@ int vx_nodes_from_reference(const uint64_t* ref, uint32_t n, vx_node* nodes, uin
 // (hash >> 40) * 2^-24.  Voxel (x,y,z) samples p = (x + 0.5) / s_o with
 // s_o = spacing >> o, f = p - floor(p), w = f*f*(3 - 2f); the cell is blended
 // along y, then z, then x; octaves are summed with weight 0.5^o in order.
-int vx_synth_noise(uint32_t R, uint32_t spacing, uint32_t octaves, float fill, uint64_t seed, int32_t shell,
+static int vx_synth_noise_body(uint32_t R, uint32_t spacing, uint32_t octaves, float fill, uint64_t seed, int32_t shell,
                    uint64_t* out_bits) {
     using namespace vx;
     if (!out_bits || R < 64 || R % 64 != 0 || R > 4096 || octaves < 1 || octaves > 16 || spacing < 1 ||
@@ -361,7 +365,12 @@ int vx_synth_noise(uint32_t R, uint32_t spacing, uint32_t octaves, float fill, u
     return VX_OK;
 }
 
-int vx_synth_urban(uint32_t R, uint32_t hmin, uint32_t hmax, uint64_t seed, uint64_t* out_bits) {
+int vx_synth_noise(uint32_t R, uint32_t spacing, uint32_t octaves, float fill, uint64_t seed, int32_t shell,
+                   uint64_t* out_bits) {
+    return vx::guarded("vx_synth_noise", [&] { return vx_synth_noise_body(R, spacing, octaves, fill, seed, shell, out_bits); });
+}
+
+static int vx_synth_urban_body(uint32_t R, uint32_t hmin, uint32_t hmax, uint64_t seed, uint64_t* out_bits) {
     using namespace vx;
     if (!out_bits || R < 64 || R % 64 != 0 || R > 8192 || hmin > hmax)
         return fail(VX_EINVAL, "vx_synth_urban: bad arguments");
@@ -391,7 +400,11 @@ int vx_synth_urban(uint32_t R, uint32_t hmin, uint32_t hmax, uint64_t seed, uint
     return VX_OK;
 }
 
-int vx_synth_rgba8(const uint32_t* coord, uint32_t B, uint64_t seed, uint32_t* out) {
+int vx_synth_urban(uint32_t R, uint32_t hmin, uint32_t hmax, uint64_t seed, uint64_t* out_bits) {
+    return vx::guarded("vx_synth_urban", [&] { return vx_synth_urban_body(R, hmin, hmax, seed, out_bits); });
+}
+
+static int vx_synth_rgba8_body(const uint32_t* coord, uint32_t B, uint64_t seed, uint32_t* out) {
     using namespace vx;
     if ((!coord || !out) && B) return fail(VX_EINVAL, "vx_synth_rgba8: null argument");
     parallel_for(int64_t(B), [&](int64_t b) {
@@ -401,13 +414,21 @@ int vx_synth_rgba8(const uint32_t* coord, uint32_t B, uint64_t seed, uint32_t* o
     return VX_OK;
 }
 
-int vx_synth_dxt1(const uint32_t* coord, uint32_t B, uint64_t seed, uint64_t* out) {
+int vx_synth_rgba8(const uint32_t* coord, uint32_t B, uint64_t seed, uint32_t* out) {
+    return vx::guarded("vx_synth_rgba8", [&] { return vx_synth_rgba8_body(coord, B, seed, out); });
+}
+
+static int vx_synth_dxt1_body(const uint32_t* coord, uint32_t B, uint64_t seed, uint64_t* out) {
     using namespace vx;
     if ((!coord || !out) && B) return fail(VX_EINVAL, "vx_synth_dxt1: null argument");
     parallel_for(int64_t(B), [&](int64_t b) {
         for (uint32_t k = 0; k < 32; ++k) out[size_t(b) * 32 + k] = vx::synth_dxt1_block(seed, coord[b], k);
     });
     return VX_OK;
+}
+
+int vx_synth_dxt1(const uint32_t* coord, uint32_t B, uint64_t seed, uint64_t* out) {
+    return vx::guarded("vx_synth_dxt1", [&] { return vx_synth_dxt1_body(coord, B, seed, out); });
 }
 
 }  // extern "C"

@@ -48,6 +48,16 @@ struct File {
     }
 };
 
+// Bytes left to read in f (sizes in a file are checked against this before
+// anything is allocated for them).
+uint64_t remaining(FILE* f) {
+    const long here = std::ftell(f);
+    if (here < 0 || std::fseek(f, 0, SEEK_END) != 0) return 0;
+    const long end = std::ftell(f);
+    std::fseek(f, here, SEEK_SET);
+    return end > here ? uint64_t(end - here) : 0;
+}
+
 bool put(FILE* f, const void* p, size_t n) { return n == 0 || std::fwrite(p, 1, n, f) == n; }
 bool get(FILE* f, void* p, size_t n) { return n == 0 || std::fread(p, 1, n, f) == n; }
 template <class T>
@@ -115,7 +125,7 @@ static_assert(sizeof(RefOctreeConfig) == 260, "OctreeConfig is 260 bytes");
 
 extern "C" {
 
-int vx_cache_write(const char* path, const vx_scene_desc* d) {
+static int vx_cache_write_body(const char* path, const vx_scene_desc* d) {
     if (!path) return fail(VX_EINVAL, "vx_cache_write: null path");
     vx_cache c;
     if (int r = cache_from_desc(d, c, "vx_cache_write")) return r;
@@ -141,7 +151,11 @@ int vx_cache_write(const char* path, const vx_scene_desc* d) {
     return VX_OK;
 }
 
-int vx_cache_read(const char* path, vx_cache** out) {
+int vx_cache_write(const char* path, const vx_scene_desc* d) {
+    return vx::guarded("vx_cache_write", [&] { return vx_cache_write_body(path, d); });
+}
+
+static int vx_cache_read_body(const char* path, vx_cache** out) {
     if (!path || !out) return fail(VX_EINVAL, "vx_cache_read: null argument");
     *out = nullptr;
     File f;
@@ -159,6 +173,9 @@ int vx_cache_read(const char* path, vx_cache** out) {
         return fail(VX_EFORMAT, "vx_cache_read: bad header");
     const uint64_t want[7] = {uint64_t(D) * 8, uint64_t(D) * 4, uint64_t(bpa * bpa * bpa) * 4, uint64_t(B) * 4,
                               uint64_t(B) * 64, color_bytes_per_brick(c->color_kind) * B, has_n ? uint64_t(B) * 512 : 0};
+    uint64_t total = 0;
+    for (uint64_t w : want) total += w + 8;
+    if (total + 8 > remaining(f.f)) return fail(VX_EFORMAT, "vx_cache_read: the file is shorter than its header says");
     c->nodes.resize(2 * uint64_t(D));
     c->node_brick.resize(D);
     c->grid.resize(uint64_t(bpa * bpa * bpa));
@@ -181,12 +198,16 @@ int vx_cache_read(const char* path, vx_cache** out) {
     return VX_OK;
 }
 
+int vx_cache_read(const char* path, vx_cache** out) {
+    return vx::guarded("vx_cache_read", [&] { return vx_cache_read_body(path, out); });
+}
+
 // VoxelSceneCacher::SerializeToFile (VoxelSceneCacher.cpp:209-265) for one
 // entry.  The reference's ChildDescriptor holds a 15-bit child pointer and no
 // far pointers, so scenes whose child pointers reach 2^15 cannot be written
 // (VX_EOVERFLOW) rather than truncated.  brickData holds material 1 for every
 // occupied voxel; the material table is written empty.
-int vx_cache_write_vsca(const char* path, const vx_scene_desc* d, uint32_t scene_type, uint32_t resolution,
+static int vx_cache_write_vsca_body(const char* path, const vx_scene_desc* d, uint32_t scene_type, uint32_t resolution,
                         float density, uint32_t seed) {
     if (!path) return fail(VX_EINVAL, "vx_cache_write_vsca: null path");
     vx_cache c;
@@ -252,11 +273,16 @@ int vx_cache_write_vsca(const char* path, const vx_scene_desc* d, uint32_t scene
     return VX_OK;
 }
 
+int vx_cache_write_vsca(const char* path, const vx_scene_desc* d, uint32_t scene_type, uint32_t resolution,
+                        float density, uint32_t seed) {
+    return vx::guarded("vx_cache_write_vsca", [&] { return vx_cache_write_vsca_body(path, d, scene_type, resolution, density, seed); });
+}
+
 // VoxelSceneCacher::DeserializeFromFile (:267-364), entry `entry` of the
 // file, into this library's arrays: descriptors as vx_nodes_from_reference
 // converts them, occupancy = brickData word != 0 (the compressed shader's test,
 // VoxelRayMarch_Compressed.comp), brick coordinates from brickGridLookup.
-int vx_cache_read_vsca(const char* path, uint32_t entry, vx_cache** out) {
+static int vx_cache_read_vsca_body(const char* path, uint32_t entry, vx_cache** out) {
     if (!path || !out) return fail(VX_EINVAL, "vx_cache_read_vsca: null argument");
     *out = nullptr;
     File f;
@@ -268,7 +294,7 @@ int vx_cache_read_vsca(const char* path, uint32_t entry, vx_cache** out) {
     if (!get_v(f.f, entries) || entry >= entries) return fail(VX_EINVAL, "vx_cache_read_vsca: no such entry");
     auto rvec = [&](std::vector<uint8_t>& v, uint64_t elem) {
         uint64_t n = 0;
-        if (!get_v(f.f, n) || n > (uint64_t(1) << 40) / elem) return false;
+        if (!get_v(f.f, n) || n > (uint64_t(1) << 40) / elem || n * elem > remaining(f.f)) return false;
         v.resize(n * elem);
         return get(f.f, v.data(), v.size());
     };
@@ -333,6 +359,10 @@ int vx_cache_read_vsca(const char* path, uint32_t entry, vx_cache** out) {
     return fail(VX_EINVAL, "vx_cache_read_vsca: no such entry");
 }
 
+int vx_cache_read_vsca(const char* path, uint32_t entry, vx_cache** out) {
+    return vx::guarded("vx_cache_read_vsca", [&] { return vx_cache_read_vsca_body(path, entry, out); });
+}
+
 int vx_cache_desc(const vx_cache* c, vx_scene_desc* d) {
     if (!c || !d) return fail(VX_EINVAL, "vx_cache_desc: null argument");
     std::memset(d, 0, sizeof(*d));
@@ -355,7 +385,7 @@ int vx_cache_free(vx_cache* c) {
     return VX_OK;
 }
 
-int vx_scene_save(const vx_scene* s, const char* path) {
+static int vx_scene_save_body(const vx_scene* s, const char* path) {
     vx_scene_info i{};
     if (int r = vx_scene_info_get(s, &i)) return r;
     vx_cache c;
@@ -378,7 +408,11 @@ int vx_scene_save(const vx_scene* s, const char* path) {
     return vx_cache_write(path, &d);
 }
 
-int vx_scene_load(const char* path, vx_scene** out) {
+int vx_scene_save(const vx_scene* s, const char* path) {
+    return vx::guarded("vx_scene_save", [&] { return vx_scene_save_body(s, path); });
+}
+
+static int vx_scene_load_body(const char* path, vx_scene** out) {
     if (!out) return fail(VX_EINVAL, "vx_scene_load: null argument");
     vx_cache* c = nullptr;
     if (int r = vx_cache_read(path, &c)) return r;
@@ -387,6 +421,10 @@ int vx_scene_load(const char* path, vx_scene** out) {
     const int r = vx_scene_create(&d, out);
     vx_cache_free(c);
     return r;
+}
+
+int vx_scene_load(const char* path, vx_scene** out) {
+    return vx::guarded("vx_scene_load", [&] { return vx_scene_load_body(path, out); });
 }
 
 }  // extern "C"

@@ -238,7 +238,7 @@ int cerr(cudaError_t e, const char* what) {
 }  // namespace
 }  // namespace vx
 
-extern "C" int vx_scene_create_dense_dev(const uint64_t* bits_dev, uint32_t R, int32_t max_levels, int32_t color_kind,
+static int vx_scene_create_dense_dev_body(const uint64_t* bits_dev, uint32_t R, int32_t max_levels, int32_t color_kind,
                                          uint64_t color_seed, int32_t with_normals, vx_scene** out, void* stream) {
     using namespace vx;
     if (!bits_dev || !out) return fail(VX_EINVAL, "vx_scene_create_dense_dev: null argument");
@@ -357,4 +357,9 @@ extern "C" int vx_scene_create_dense_dev(const uint64_t* bits_dev, uint32_t R, i
     if (e != cudaSuccess) { vx_scene_destroy(scene); return done(cerr(e, "synchronize")); }
     *out = scene;
     return done(VX_OK);
+}
+
+extern "C" int vx_scene_create_dense_dev(const uint64_t* bits_dev, uint32_t R, int32_t max_levels, int32_t color_kind,
+                                         uint64_t color_seed, int32_t with_normals, vx_scene** out, void* stream) {
+    return vx::guarded("vx_scene_create_dense_dev", [&] { return vx_scene_create_dense_dev_body(bits_dev, R, max_levels, color_kind, color_seed, with_normals, out, stream); });
 }

@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <exception>
+#include <new>
 #include <string>
 
 #include "../../include/vx.h"
@@ -59,6 +61,21 @@ uint32_t violations_payload();
 // Per-thread-local error string.
 void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
+
+// Runs an entry point's body and turns a C++ exception (an allocation or a
+// thread that could not be made) into a status: no exception crosses the ABI.
+template <class F>
+int guarded(const char* what, F&& body) noexcept {
+    try {
+        return body();
+    } catch (const std::bad_alloc&) {
+        return fail(VX_ENOMEM, std::string(what) + ": out of host memory");
+    } catch (const std::exception& e) {
+        return fail(VX_EINVAL, std::string(what) + ": " + e.what());
+    } catch (...) {
+        return fail(VX_EINVAL, std::string(what) + ": unexpected exception");
+    }
+}
 
 // Kernel launchers (vx_kernels.cu).  Return cudaError_t as int.
 // lod: nullptr, or LODParameters {ray_orig_size, ray_dir_size} with ray_dir_size > 0.

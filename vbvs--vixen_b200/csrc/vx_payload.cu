@@ -91,7 +91,7 @@ extern "C" int vx_build_normals_dev(const uint32_t* occ_dev, uint32_t brick_coun
     return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_build_normals_dev");
 }
 
-extern "C" int vx_build_normals(const uint32_t* occ, uint32_t brick_count, uint64_t* out) {
+static int vx_build_normals_body(const uint32_t* occ, uint32_t brick_count, uint64_t* out) {
     using namespace vx;
     if (brick_count && (!occ || !out)) return fail(VX_EINVAL, "vx_build_normals: null argument");
     const unsigned T = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
@@ -114,6 +114,10 @@ extern "C" int vx_build_normals(const uint32_t* occ, uint32_t brick_count, uint6
     return VX_OK;
 }
 
+extern "C" int vx_build_normals(const uint32_t* occ, uint32_t brick_count, uint64_t* out) {
+    return vx::guarded("vx_build_normals", [&] { return vx_build_normals_body(occ, brick_count, out); });
+}
+
 extern "C" int vx_build_dxt1_dev(const float* rgb_dev, const uint32_t* occ_dev, uint32_t brick_count,
                                  uint64_t* out_dev, void* stream) {
     using namespace vx;
@@ -133,7 +137,7 @@ extern "C" int vx_build_dxt1_dev(const float* rgb_dev, const uint32_t* occ_dev, 
     return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_build_dxt1_dev");
 }
 
-extern "C" int vx_build_dxt1(const float* rgb, const uint32_t* occ, uint32_t brick_count, uint64_t* out) {
+static int vx_build_dxt1_body(const float* rgb, const uint32_t* occ, uint32_t brick_count, uint64_t* out) {
     using namespace vx;
     if (brick_count && (!rgb || !occ || !out)) return fail(VX_EINVAL, "vx_build_dxt1: null argument");
     const unsigned T = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
@@ -154,6 +158,10 @@ extern "C" int vx_build_dxt1(const float* rgb, const uint32_t* occ, uint32_t bri
     }
     for (auto& x : th) x.join();
     return VX_OK;
+}
+
+extern "C" int vx_build_dxt1(const float* rgb, const uint32_t* occ, uint32_t brick_count, uint64_t* out) {
+    return vx::guarded("vx_build_dxt1", [&] { return vx_build_dxt1_body(rgb, occ, brick_count, out); });
 }
 
 extern "C" int vx_hit_normals(const vx_scene* scene, const vx_hit* hits_dev, uint32_t n, float* normals_dev,

@@ -114,7 +114,7 @@ struct DevBuf {
 }  // namespace
 }  // namespace vx
 
-extern "C" int vx_synth_noise_dev(uint32_t R, uint32_t spacing, uint32_t octaves, float fill, uint64_t seed,
+static int vx_synth_noise_dev_body(uint32_t R, uint32_t spacing, uint32_t octaves, float fill, uint64_t seed,
                                   int32_t shell, uint64_t* out_bits_dev, void* stream) {
     using namespace vx;
     if (!out_bits_dev || R < 64 || R % 64 != 0 || R > 2048 || octaves < 1 || octaves > 16 || spacing < 1 ||
@@ -184,4 +184,9 @@ extern "C" int vx_synth_noise_dev(uint32_t R, uint32_t spacing, uint32_t octaves
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cerr(e, "pack_kernel");
     return VX_OK;
+}
+
+extern "C" int vx_synth_noise_dev(uint32_t R, uint32_t spacing, uint32_t octaves, float fill, uint64_t seed,
+                                  int32_t shell, uint64_t* out_bits_dev, void* stream) {
+    return vx::guarded("vx_synth_noise_dev", [&] { return vx_synth_noise_dev_body(R, spacing, octaves, fill, seed, shell, out_bits_dev, stream); });
 }
