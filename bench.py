@@ -487,6 +487,61 @@ def measure_cfg5(args, rank, world, steps, warmup):
                         "from colours + N(0, 0.05)", **out}
 
 
+def measure_cfg5_multi(args, rank, world, steps, warmup):
+    """cfg5 on N GPUs (strong scaling): the 16 views of a step split over the ranks
+    (multigpu.view_range), each rank's forward + adjoint into its own gradient pool, one NCCL sum
+    all-reduce of the pool (the adjoint's one exchange); ms per view = max over ranks / 16."""
+    import numpy as np
+    import torch
+    vx = load_pkg()
+    from vx_b200 import workloads as W
+    from vx_b200 import multigpu as M
+    R = 512
+    bits = vx.synth_noise_dev(R, 32, 4, 0.30, 5, False).cpu().numpy().view(np.uint64)
+    out = {}
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for kind, name in ((0, "voxel_rgb"), (1, "dxt1_endpoints")):
+        dw = W.config5(R=R, views=16, width=512, height=512, kind=kind, seed=5, bits=bits)
+        scene = vx.Scene(dw.wl.scene)
+        b, e = M.view_range(len(dw.views), rank, world)
+        mine = dw.views[b:e]
+        n = 512 * 512 * max(1, len(mine))
+        attr_d = torch.from_numpy(dw.attr).cuda()
+        idx_d = None if dw.dxt_idx is None else torch.from_numpy(dw.dxt_idx.view(np.int32)).cuda()
+        img = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+        rec = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+        tgt = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+        if mine:
+            vx.diff_forward_views(scene, mine, 512, 512, kind, torch.from_numpy(dw.target_attr).cuda(), idx_d, tgt,
+                                  rec)
+        grad = torch.zeros_like(attr_d)
+
+        def step():
+            grad.zero_()
+            if mine:
+                vx.diff_forward_views(scene, mine, 512, 512, kind, attr_d, idx_d, img, rec)
+                vx.diff_backward(kind, idx_d, rec, img, tgt, grad)
+            M.allreduce_sum_(grad)
+
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        torch.distributed.barrier()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for a, bb in ev:
+            flush.zero_()
+            a.record()
+            step()
+            bb.record()
+        torch.cuda.synchronize()
+        ms = M.max_over_ranks([sum(a.elapsed_time(bb) for a, bb in ev) / steps])[0]
+        out[name] = {"fwd_bwd_allreduce_ms_per_view": ms / 16, "views_per_rank": len(mine),
+                     "gradient_pool_bytes": int(attr_d.numel() * 4)}
+        del scene
+    return {"workload": "cfg5: 512^3 noise 30% fill, 16 views 512x512 on an orbit split over ranks, gradient "
+                        "pool summed by one NCCL all-reduce per step", **out}
+
+
 def measure_next(args, steps, warmup):
     """The rows beyond the cast (1024^3 cave, seed 2, the cfg2 scene): the device scene
     builder against the host builder, the normal and DXT1 payload encoders, the LOD cut,
@@ -618,6 +673,9 @@ def main():
     ap.add_argument("--no-extra", action="store_true",
                     help="cfg2 only: skip the attached batched (cfg4), adjoint (cfg5) and next-row measurements")
     ap.add_argument("--scenes", type=int, default=64, help="cfg4: number of scenes")
+    ap.add_argument("--split-views", action="store_true",
+                    help="cfg5: split the views over the ranks and all-reduce the gradient (default when N > 1; "
+                         "needs a process group, i.e. torchrun, also for N = 1)")
     ap.add_argument("--soak-seconds", type=float, default=1.5,
                     help="untimed launches before timing so clocks reach steady state")
     args = ap.parse_args()
@@ -644,6 +702,23 @@ def main():
         res = measure_next(args, args.steps, args.warmup)
         if rank == 0:
             print(json.dumps({"workload": "next", "next_rows": res}), flush=True)
+        return 0
+    if args.workload == "cfg5" and (world > 1 or args.split_views):
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+        res = measure_cfg5_multi(args, rank, world, args.steps, args.warmup)
+        dist.destroy_process_group()
+        if rank == 0:
+            a = res["voxel_rgb"]
+            print(json.dumps({"metric": METRIC, "value": a["fwd_bwd_allreduce_ms_per_view"], "unit": "ms/view",
+                              "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                              "ms_per_step": a["fwd_bwd_allreduce_ms_per_view"] * 16, "higher_is_better": False,
+                              "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                              "config": {"workload": res.pop("workload")}, "adjoint": res,
+                              "gpu_launches": args.steps * 2}), flush=True)
         return 0
     if args.workload == "cfg5":
         import torch

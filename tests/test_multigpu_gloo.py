@@ -80,3 +80,54 @@ def test_two_rank_gloo_split_matches_single_process(vo, tmp_path):
     whole = vo.OracleScene.from_dense(wl.bits, 64, wl.scene.max_levels).cast_rays(wl.rays(), threads=1)
     assert np.array_equal(gathered.view(np.uint8), whole.view(np.uint8))
     assert list(np.load(tmp_path / "tmax.npy")) == [2.0, 5.0]
+
+
+def _adjoint_worker(rank, world, port, out_dir):
+    import sys
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import torch
+    import torch.distributed as dist
+    from conftest import load_vx
+    import vx_oracle as vo
+    load_vx()
+    from vx_b200 import multigpu as M
+    from vx_b200 import workloads as W
+    from datetime import timedelta
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    dw = W.config5(R=64, views=5, width=32, height=24, kind=1, seed=8)
+    o = vo.OracleScene.from_dense(dw.wl.bits, 64, dw.wl.scene.max_levels)
+    b, e = M.view_range(len(dw.views), rank, world)
+    rng = np.random.default_rng(100)
+    targets = [rng.random((32 * 24, 3)).astype(np.float32) for _ in dw.views]
+    recs = [o.cast_rays(W.camera_rays(pc, 32, 24), threads=1) for pc in dw.views[b:e]]
+    g = torch.from_numpy(W.adjoint_reference64(dw, recs, targets[b:e]))
+    M.allreduce_sum_(g)
+    np.save(os.path.join(out_dir, f"grad{rank}.npy"), g.numpy())
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_adjoint_split_views_allreduce(vo, tmp_path):
+    """Views split over two gloo ranks, per-rank gradients summed by all-reduce: every rank
+    holds the single-process gradient of all views."""
+    import multiprocessing as mp
+    from vx_b200 import workloads as W
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_adjoint_worker, args=(r, 2, port, str(tmp_path))) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=180)
+        assert p.exitcode == 0
+    dw = W.config5(R=64, views=5, width=32, height=24, kind=1, seed=8)
+    o = vo.OracleScene.from_dense(dw.wl.bits, 64, dw.wl.scene.max_levels)
+    rng = np.random.default_rng(100)
+    targets = [rng.random((32 * 24, 3)).astype(np.float32) for _ in dw.views]
+    recs = [o.cast_rays(W.camera_rays(pc, 32, 24), threads=1) for pc in dw.views]
+    whole = W.adjoint_reference64(dw, recs, targets)
+    assert np.count_nonzero(whole) > 0
+    for r in range(2):
+        np.testing.assert_allclose(np.load(tmp_path / f"grad{r}.npy"), whole, rtol=1e-12, atol=1e-12)

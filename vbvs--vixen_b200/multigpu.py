@@ -8,8 +8,12 @@ between GPUs in the data path.  Two ways to give ranks their rays:
   - strong scaling: the rays of one frame are split into contiguous,
     near-equal ranges (`ray_range`), and the hit records concatenate back in
     rank order.
-The only collective is the timing reduction: the max over ranks of each
-rank's device-measured time (`max_over_ranks`).
+The only collective of the casts is the timing reduction: the max over ranks
+of each rank's device-measured time (`max_over_ranks`).  The adjoint has one
+real exchange when a step's views are split across ranks (`view_range`): each
+rank accumulates the gradient of its views into its own copy of the attribute
+gradient pool, and one sum all-reduce (`allreduce_sum_`, NCCL over NVLink on
+GPUs) leaves the gradient of all views on every rank.
 """
 from __future__ import annotations
 
@@ -43,3 +47,16 @@ def max_over_ranks(values, group=None):
 def aggregate_throughput(units_per_rank: int, world: int, max_time_s: float) -> float:
     """Whole-job throughput: the units all ranks processed over the slowest rank's time."""
     return units_per_rank * world / max_time_s
+
+
+def view_range(views: int, rank: int, world: int) -> tuple[int, int]:
+    """Contiguous [begin, end) share of a step's views for `rank` of `world`."""
+    return ray_range(views, rank, world)
+
+
+def allreduce_sum_(tensor, group=None):
+    """Sum `tensor` over ranks in place (identity without a process group); returns it."""
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized():
+        dist.all_reduce(tensor, op=dist.ReduceOp.SUM, group=group)
+    return tensor
