@@ -625,6 +625,20 @@ def measure_next(args, steps, warmup):
     ms = dev_ms(lambda: sc.render_dev(wl.camera, wl.width, wl.height, img))
     out["compressed_render"] = {"pixels": n, "payloads": "DXT1 colour + DXT normals", "device_ms": ms,
                                 "mrays_s": n / ms / 1e3}
+    # the reference's published benchmark shape: noise 256^3, 1920x1080 primary rays (context only:
+    # the reference's numbers are Vulkan runs on other GPUs, with its own scene instance and camera)
+    wl256 = W.config2(R=256, seed=seed)
+    s256 = vx.Scene(wl256.scene)
+    r256 = torch.from_numpy(wl256.rays(order="tiled")).cuda()
+    h256 = torch.zeros((r256.shape[0], 4), dtype=torch.int32, device="cuda")
+    c256 = torch.zeros((r256.shape[0], 3), dtype=torch.float32, device="cuda")
+    ms = dev_ms(lambda: s256.cast_rays_dev(r256, h256, c256))
+    out["noise256_1080p"] = {"workload": "noise 256^3 (50% fill, DXT1), 1920x1080 primary rays, plain cast",
+                             "mrays_s": r256.shape[0] / ms / 1e3, "ms_per_frame": ms,
+                             "published_context": "4,573 / 4,688 Mrays/s uncompressed / DXT, RTX 4080 Laptop, Vulkan "
+                                                  "(BASELINE.md section 1; not comparable hardware or scene instance)"}
+    s256.close()
+    del r256, h256, c256
     # scene cache file
     with tempfile.TemporaryDirectory() as d:
         path = os.path.join(d, "cave.vxsc")
