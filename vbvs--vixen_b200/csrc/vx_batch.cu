@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_refill_kernel(BatchArgs a) 
     uint32_t* stk_base = beg + ((a.S + 1 + 3) & ~3u);
     uint32_t lnode[SMEM_STACK ? 1 : MAX_LEVELS_ALL];
     float ltmax[SMEM_STACK ? 1 : MAX_LEVELS_ALL];
-    uint32_t lcyc[SMEM_STACK ? 1 : 16];
+    uint32_t lcyc[SMEM_STACK ? 1 : CYC_WORDS];
     uint32_t* stkN;
     float* stkT;
     uint32_t* cyc;
@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
     uint32_t* stk_base = beg + ((a.S + 1 + 3) & ~3u);
     uint32_t lnode[SMEM_STACK ? 1 : MAX_LEVELS_ALL];
     float ltmax[SMEM_STACK ? 1 : MAX_LEVELS_ALL];
-    uint32_t lcyc[SMEM_STACK ? 1 : 16];
+    uint32_t lcyc[SMEM_STACK ? 1 : CYC_WORDS];
     uint32_t* stkN;
     float* stkT;
     uint32_t* cyc;
@@ -344,7 +344,7 @@ int cuda_err(cudaError_t e, const char* what) {
 
 size_t batch_smem(const vx_batch* b, bool smem_stack, int block) {
     size_t bytes = size_t(b->S) * sizeof(vx::DevScene) + ((size_t(b->S) + 1 + 3) & ~size_t(3)) * 4;
-    if (smem_stack) bytes += (size_t(2) * size_t(b->maxL) + 16) * size_t(block) * 4;
+    if (smem_stack) bytes += (size_t(2) * size_t(b->maxL) + vx::CYC_WORDS) * size_t(block) * 4;
     return bytes;
 }
 
@@ -672,7 +672,7 @@ int noalloc_setup(int dev, NoallocDevice*& out) {
         auto kern = batch_kernel<256, 3, true>;
         const size_t smem_max = size_t(VX_NOALLOC_MAX_SCENES) * sizeof(DevScene) +
                                 ((size_t(VX_NOALLOC_MAX_SCENES) + 1 + 3) & ~size_t(3)) * 4 +
-                                (size_t(2) * MAX_LEVELS_ALL + 16) * 256 * 4;
+                                (size_t(2) * MAX_LEVELS_ALL + CYC_WORDS) * 256 * 4;
         e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_max));
         if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch_noalloc: shared memory attribute");
         int per_sm = 0, sms = 0;
@@ -729,7 +729,7 @@ static int vx_cast_batch_noalloc_body(const vx_scene* const* scenes, uint32_t co
     BatchArgs a{reinterpret_cast<const DevScene*>(d->scratch + NOALLOC_TABLE_OFFSET), count, begin, rays, n, tmin,
                 tmax, hits, nullptr, reinterpret_cast<uint32_t*>(d->scratch), 32u, maxL};
     const size_t smem = size_t(count) * sizeof(DevScene) + ((size_t(count) + 1 + 3) & ~size_t(3)) * 4 +
-                        (size_t(2) * size_t(maxL) + 16) * 256 * 4;
+                        (size_t(2) * size_t(maxL) + CYC_WORDS) * 256 * 4;
     batch_kernel<256, 3, true><<<d->blocks, 256, smem, st>>>(a);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch_noalloc: launch");

@@ -42,6 +42,8 @@ constexpr int MAX_ITER = 500;       // SVOTraversal.cpp:588
 #define VX_CYCLE_START 3
 #endif
 constexpr int CYCLE_START = VX_CYCLE_START;  // iteration from which loop states are recorded
+constexpr int CYC_SLOT = 9;                   // words of one recorded state: 8 + their sum
+constexpr int CYC_WORDS = 2 * CYC_SLOT;       // cycle-detection words per ray
 constexpr float FLT_MAX_ = 3.402823466e+38f;
 constexpr uint32_t NONE = 0xFFFFFFFFu;
 
@@ -417,8 +419,8 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
 // repeats after one or two iterations the ray can neither hit nor leave before
 // the 500-iteration cap: the result is the capped miss and the remaining
 // iterations' counters repeat the cycle's.  The two previous states are kept
-// in shared memory (cyc[(p * 8 + k) * stride], slot p = iteration parity)
-// from iteration CYCLE_START on.  With LOD the cut test reads only the
+// in shared memory (cyc[(p * CYC_SLOT + k) * stride], slot p = iteration
+// parity) from iteration CYCLE_START on.  With LOD the cut test reads only the
 // loop state and per-ray constants, so a repeating state still cannot end.
 //
 // LOD: castRayWithLOD (SVOTraversal.cpp:198-232) with LODParameters `lod`
@@ -673,17 +675,25 @@ next_iter:
         cur[2] = __float_as_uint(st.px); cur[3] = __float_as_uint(st.py); cur[4] = __float_as_uint(st.pz);
         cur[5] = __float_as_uint(st.t_min); cur[6] = __float_as_uint(st.t_max); cur[7] = __float_as_uint(st.hh);
         const uint32_t dg = h.grid_reads - g0, ddd = h.dda_steps - dd0;
-        bool eq1 = st.nrec >= 1, eq2 = st.nrec >= 2;
         // two slots by parity: the other parity holds the state one iteration
-        // back, this parity two back; this state replaces the latter
-        uint32_t* back2 = cyc + ((st.iter & 1) * 8) * stride;
-        const uint32_t* back1 = cyc + (((st.iter & 1) ^ 1) * 8) * stride;
+        // back, this parity two back; this state replaces the latter.  Each
+        // slot also keeps a sum of its words: states are compared word by
+        // word only when the sums agree (a repeat always has equal sums).
+        uint32_t* back2 = cyc + ((st.iter & 1) * CYC_SLOT) * stride;
+        const uint32_t* back1 = cyc + (((st.iter & 1) ^ 1) * CYC_SLOT) * stride;
+        const uint32_t sum = ((cur[0] + cur[1] + cur[2]) + (cur[3] + cur[4] + cur[5])) + (cur[6] + cur[7]);
+        bool eq1 = st.nrec >= 1 && back1[8 * stride] == sum;
+        bool eq2 = st.nrec >= 2 && back2[8 * stride] == sum;
+        if (eq1 || eq2) {
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            eq1 = eq1 && (cur[k] == back1[k * stride]);
-            eq2 = eq2 && (cur[k] == back2[k * stride]);
-            back2[k * stride] = cur[k];
+            for (int k = 0; k < 8; ++k) {
+                eq1 = eq1 && (cur[k] == back1[k * stride]);
+                eq2 = eq2 && (cur[k] == back2[k * stride]);
+            }
         }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) back2[k * stride] = cur[k];
+        back2[8 * stride] = sum;
         if (eq1 || eq2) {
             const uint32_t rem = uint32_t(MAX_ITER - st.iter);
             h.run_iters = uint32_t(st.iter);

@@ -214,7 +214,7 @@ extern "C" int vx_diff_forward_views(const vx_scene* scene, const vx_camera_pc* 
     const DevScene& s = scene_dev(scene);
     Views v{};
     for (uint32_t k = 0; k < views; ++k) v.cam[k] = camera_from_pc(pcs[k]);
-    const size_t smem = (size_t(2) * size_t(s.max_levels) + 16) * DBLOCK * sizeof(uint32_t);
+    const size_t smem = (size_t(2) * size_t(s.max_levels) + CYC_WORDS) * DBLOCK * sizeof(uint32_t);
 #if VX_DIFF_TILED
     static_assert(DBLOCK == 256, "a block covers one 32 x 8 tile");
     const uint64_t blocks = uint64_t(views) * ((w + 31) / 32) * ((h + 7) / 8);

@@ -107,7 +107,9 @@ __global__ void camera_rays_kernel(CameraDev cam, uint32_t w, uint32_t hgt, vx_r
     rays[i] = r;
 }
 
-size_t stack_bytes(const DevScene& s) { return (size_t(2) * size_t(s.max_levels) + 16) * BLOCK * sizeof(uint32_t); }
+size_t stack_bytes(const DevScene& s) {
+    return (size_t(2) * size_t(s.max_levels) + CYC_WORDS) * BLOCK * sizeof(uint32_t);
+}
 
 }  // namespace
 
