@@ -128,78 +128,11 @@ VX_HD F3 decode(uint64_t a, uint64_t b, uint32_t t) {
     return (base + u * wu) + v * wv;
 }
 
-// encodeBlockTyped over all 16 texels (the rebuild passes validCount = 16).
-VX_HD void encode(const F3* n, uint64_t& out_a, uint64_t& out_b) {
-    F3 base = n[0];
-    for (int i = 1; i < 16; ++i) base = base + n[i];
-    if (len(base) < 0.1f * 16.0f) {
-        // nearly cancelling normals: the input closest to the sum
-        int bi = 0;
-        float bd = dot(n[0], base);
-        for (int i = 1; i < 16; ++i) {
-            const float d = dot(n[i], base);
-            if (d > bd) { bi = i; bd = d; }
-        }
-        base = n[bi];
-    }
-    const uint32_t head_base = pack_base(base);
-    base = unpack_base(head_base);
-    // U: toward the input furthest from the base
-    int ui = 0;
-    float ud = dot(n[0], base);
-    for (int i = 1; i < 16; ++i) {
-        const float d = dot(n[i], base);
-        if (d < ud) { ui = i; ud = d; }
-    }
-    uint32_t head_uv = pack_axis(0u, n[ui] * len(base) - base, 0);
-    const F3 u = unpack_axis(head_uv, 0);
-    // V: toward the input the U line fits worst
-    F3 uref[4];
-    for (int j = 0; j < 4; ++j) uref[j] = unit(base + u * weight(uint32_t(j)));
-    int vi = 0, vj = 0;
-    float vd = 3.402823466e+38f;
-    for (int i = 0; i < 16; ++i) {
-        int bj = 0;
-        float bd = dot(n[i], uref[0]);
-        for (int j = 1; j < 4; ++j) {
-            const float d = dot(n[i], uref[j]);
-            if (d > bd) { bj = j; bd = d; }
-        }
-        if (bd < vd) { vi = i; vj = bj; vd = bd; }
-    }
-    const F3 tmp = base + u * weight(uint32_t(vj));
-    head_uv = pack_axis(head_uv, n[vi] * len(tmp) - tmp, 16);
-    const F3 v = unpack_axis(head_uv, 16);
-    // weights: the best of the 4 x 4 grid per texel
-    F3 grid[16];
-    for (int i = 0; i < 4; ++i)
-        for (int j = 0; j < 4; ++j) grid[i + 4 * j] = unit((base + u * weight(uint32_t(i))) + v * weight(uint32_t(j)));
-    uint32_t bu = 0, bv = 0;
-    for (int t = 0; t < 16; ++t) {
-        int bk = 0;
-        float bd = dot(n[t], grid[0]);
-        for (int k = 1; k < 16; ++k) {
-            const float d = dot(n[t], grid[k]);
-            if (d > bd) { bk = k; bd = d; }
-        }
-        bu |= uint32_t(bk & 3) << (2 * t);
-        bv |= uint32_t(bk >> 2) << (2 * t);
-    }
-    out_a = uint64_t(head_base) | (uint64_t(bu) << 32);
-    out_b = uint64_t(head_uv) | (uint64_t(bv) << 32);
-}
-
-VX_HD bool occupied(const uint32_t* occ, int x, int y, int z) {
-    if (unsigned(x) > 7u || unsigned(y) > 7u || unsigned(z) > 7u) return false;
-    const int i = z * 64 + y * 8 + x;
-    return (occ[i >> 5] >> (i & 31)) & 1u;
-}
-
-// computeGeometricNormal: outward central difference of the brick's
-// occupancy (neighbours outside the brick count as empty); (0,1,0) when flat.
-VX_HD F3 geometric(const uint32_t* occ, int x, int y, int z) {
-    auto o = [&](int X, int Y, int Z) { return occupied(occ, X, Y, Z) ? 1.0f : 0.0f; };
-    const F3 g{o(x + 1, y, z) - o(x - 1, y, z), o(x, y + 1, z) - o(x, y - 1, z), o(x, y, z + 1) - o(x, y, z - 1)};
+// computeGeometricNormal (SVO/src/SVORebuild.cpp:145-193) takes the central
+// difference g of the brick's occupancy (neighbours outside the brick count as
+// empty) and returns the outward unit normal -normalize(g), or (0,1,0) when g
+// is (near) zero.
+VX_HD F3 normal_of_gradient(F3 g) {
     if (len(g) > 0.001f) {
         const F3 u = unit(g);
         return F3{-u.x, -u.y, -u.z};
@@ -207,19 +140,176 @@ VX_HD F3 geometric(const uint32_t* occ, int x, int y, int z) {
     return F3{0.0f, 1.0f, 0.0f};
 }
 
+// The encoder's input normal of a texel is a function of its neighbour code
+// c = (gx + 1) + 3 (gy + 1) + 9 (gz + 1) alone, g in {-1, 0, 1}^3 the central
+// difference: the reference forms each component of g as a difference of
+// occupancy floats, 1 - 0, 0 - 1, 0 - 0 or 1 - 1, i.e. exactly float(gx) etc.
+// (+0 for the zero cases), so code_normal(c) returns the bits of that texel's
+// normal.  Empty texels take FLAT_CODE: g = 0 gives (0,1,0), the empty texel's
+// normal, bit for bit.
+constexpr int NUM_CODES = 27;
+constexpr int FLAT_CODE = 13;
+
+VX_HD F3 code_normal(int c) {
+    return normal_of_gradient(F3{float(c % 3 - 1), float(c / 3 % 3 - 1), float(c / 9 - 1)});
+}
+
+// code_normal of every code, as 16-byte entries {x, y, z, 0} (shared memory on
+// the device: one 128-bit load per lookup).
+struct CodeTable {
+    const float4* e;
+    VX_HD F3 operator()(int c) const {
+        const float4 q = e[c];
+        return F3{q.x, q.y, q.z};
+    }
+};
+
+VX_HD float4 code_entry(int c) {
+    const F3 n = code_normal(c);
+    return float4{n.x, n.y, n.z, 0.0f};
+}
+
+// Occupancy row (8 bits, x = bit) of row y of slice z; 0 outside the brick.
+VX_HD uint32_t row8(const uint32_t* occ, int y, int z) {
+    if (unsigned(y) > 7u || unsigned(z) > 7u) return 0u;
+    return (occ[2 * z + (y >> 2)] >> ((y & 3) * 8)) & 0xFFu;
+}
+
+// Neighbour codes of the 16 texels of block `block` (voxels block*16 ..
+// block*16 + 15: rows y = 2p and 2p + 1 of slice z, p = block & 3,
+// z = block >> 2).  Returns whether any texel is occupied.
+VX_HD bool block_codes(const uint32_t* occ, int block, uint8_t* code) {
+    const int z = block >> 2, y0 = (block & 3) * 2;
+    bool any = false;
+    VX_UNROLL
+    for (int r = 0; r < 2; ++r) {
+        const int y = y0 + r;
+        const uint32_t row = row8(occ, y, z);
+        any = any || row != 0u;
+        const uint32_t xp = row >> 1, xm = (row << 1) & 0xFFu;
+        const uint32_t yp = row8(occ, y + 1, z), ym = row8(occ, y - 1, z);
+        const uint32_t zp = row8(occ, y, z + 1), zm = row8(occ, y, z - 1);
+        VX_UNROLL
+        for (int x = 0; x < 8; ++x) {
+            const int c = FLAT_CODE + (int((xp >> x) & 1u) - int((xm >> x) & 1u)) +
+                          3 * (int((yp >> x) & 1u) - int((ym >> x) & 1u)) +
+                          9 * (int((zp >> x) & 1u) - int((zm >> x) & 1u));
+            code[r * 8 + x] = uint8_t(((row >> x) & 1u) ? c : FLAT_CODE);
+        }
+    }
+    return any;
+}
+
+// encodeBlockTyped (DXT1Compressor.cpp:242-333) over all 16 texels (the rebuild
+// passes validCount = 16), for texels given as neighbour codes.  Every step is
+// the reference's over the 16 texel normals in order, except that the searches
+// visit each distinct normal once, in the order of first occurrence.  That is
+// exact: a later texel with the same normal yields the same value, and a value
+// equal to one already seen never passes a strict comparison whose running best
+// is at least as good (or NaN, which blocks all), so the reference's pick is
+// always a first occurrence.  The distinct codes sit in a byte list (two
+// 64-bit words), so the searches run `m` iterations, m the number of distinct
+// normals of the block, instead of 16.
+VX_HD void encode_coded(const uint8_t* code, CodeTable tab, uint64_t& out_a, uint64_t& out_b) {
+    uint64_t list0 = 0, list1 = 0;  // distinct codes, first occurrences in texel order
+    uint32_t seen = 0;
+    int m = 0;
+    VX_UNROLL
+    for (int t = 0; t < 16; ++t) {
+        const uint32_t bit = 1u << code[t];
+        if (!(seen & bit)) {
+            const uint64_t e = uint64_t(code[t]) << (8 * (m & 7));
+            if (m < 8) list0 |= e;
+            else list1 |= e;
+            ++m;
+        }
+        seen |= bit;
+    }
+    const auto listed = [&](int j) { return int(((j < 8 ? list0 : list1) >> (8 * (j & 7))) & 0xFFu); };
+    F3 base = tab(code[0]);
+    VX_UNROLL
+    for (int t = 1; t < 16; ++t) base = base + tab(code[t]);
+    if (len(base) < 0.1f * 16.0f) {
+        // nearly cancelling normals: the input closest to the sum
+        int bc = code[0];
+        float bd = dot(tab(code[0]), base);
+        for (int j = 1; j < m; ++j) {
+            const int c = listed(j);
+            const float d = dot(tab(c), base);
+            if (d > bd) { bc = c; bd = d; }
+        }
+        base = tab(bc);
+    }
+    const uint32_t head_base = pack_base(base);
+    base = unpack_base(head_base);
+    // U: toward the input furthest from the base
+    int uc = code[0];
+    float ud = dot(tab(code[0]), base);
+    for (int j = 1; j < m; ++j) {
+        const int c = listed(j);
+        const float d = dot(tab(c), base);
+        if (d < ud) { uc = c; ud = d; }
+    }
+    uint32_t head_uv = pack_axis(0u, tab(uc) * len(base) - base, 0);
+    const F3 u = unpack_axis(head_uv, 0);
+    // V: toward the input the U line fits worst
+    F3 uref[4];
+    VX_UNROLL
+    for (int j = 0; j < 4; ++j) uref[j] = unit(base + u * weight(uint32_t(j)));
+    int vc = code[0], vj = 0;
+    float vd = 3.402823466e+38f;
+    for (int j = 0; j < m; ++j) {
+        const int c = listed(j);
+        const F3 n = tab(c);
+        int bj = 0;
+        float bd = dot(n, uref[0]);
+        VX_UNROLL
+        for (int i = 1; i < 4; ++i) {
+            const float d = dot(n, uref[i]);
+            if (d > bd) { bj = i; bd = d; }
+        }
+        if (bd < vd) { vc = c; vj = bj; vd = bd; }
+    }
+    const F3 tmp = base + u * weight(uint32_t(vj));
+    head_uv = pack_axis(head_uv, tab(vc) * len(tmp) - tmp, 16);
+    const F3 v = unpack_axis(head_uv, 16);
+    // weights: the best of the 4 x 4 grid, once per distinct normal, kept per code
+    F3 grid[16];
+    VX_UNROLL
+    for (int i = 0; i < 4; ++i)
+        VX_UNROLL
+        for (int j = 0; j < 4; ++j) grid[i + 4 * j] = unit((base + u * weight(uint32_t(i))) + v * weight(uint32_t(j)));
+    uint64_t best_lo = 0, best_hi = 0;  // 4 bits per code: codes 0-15, 16-26
+    for (int j = 0; j < m; ++j) {
+        const int c = listed(j);
+        const F3 n = tab(c);
+        int bk = 0;
+        float bd = dot(n, grid[0]);
+        VX_UNROLL
+        for (int k = 1; k < 16; ++k) {
+            const float d = dot(n, grid[k]);
+            if (d > bd) { bk = k; bd = d; }
+        }
+        if (c < 16) best_lo |= uint64_t(bk) << (4 * c);
+        else best_hi |= uint64_t(bk) << (4 * (c - 16));
+    }
+    uint32_t bu = 0, bv = 0;
+    VX_UNROLL
+    for (int t = 0; t < 16; ++t) {
+        const int c = code[t];
+        const uint32_t bk = uint32_t(c < 16 ? best_lo >> (4 * c) : best_hi >> (4 * (c - 16))) & 15u;
+        bu |= (bk & 3u) << (2 * t);
+        bv |= (bk >> 2) << (2 * t);
+    }
+    out_a = uint64_t(head_base) | (uint64_t(bu) << 32);
+    out_b = uint64_t(head_uv) | (uint64_t(bv) << 32);
+}
+
 // One block of a brick's normal payload (SVORebuild.cpp:658-722): empty texels
 // are (0,1,0); a block without occupied texels is {0, 0}.
-VX_HD void brick_block(const uint32_t* occ, int block, uint64_t& a, uint64_t& b) {
-    F3 n[16];
-    bool any = false;
-    for (int t = 0; t < 16; ++t) {
-        const int i = block * 16 + t;
-        const int x = i & 7, y = (i >> 3) & 7, z = i >> 6;
-        const bool occd = occupied(occ, x, y, z);
-        any = any || occd;
-        n[t] = occd ? geometric(occ, x, y, z) : F3{0.0f, 1.0f, 0.0f};
-    }
-    if (any) encode(n, a, b);
+VX_HD void brick_block(const uint32_t* occ, int block, CodeTable tab, uint64_t& a, uint64_t& b) {
+    uint8_t code[16];
+    if (block_codes(occ, block, code)) encode_coded(code, tab, a, b);
     else a = b = 0;
 }
 

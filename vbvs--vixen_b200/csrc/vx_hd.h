@@ -7,3 +7,11 @@
 #else
 #define VX_HD inline
 #endif
+
+// Full unrolling of a fixed-trip loop in device code (keeps small per-thread
+// arrays in registers); no effect on the host.
+#ifdef __CUDA_ARCH__
+#define VX_UNROLL _Pragma("unroll")
+#else
+#define VX_UNROLL
+#endif

@@ -16,21 +16,20 @@ namespace vx {
 namespace {
 
 // Thread i encodes block i & 31 of brick i >> 5.  The 32 threads of a warp
-// share one brick, so its 64 occupancy bytes are one broadcast load; each
-// thread writes its 16-byte block, a warp 512 contiguous bytes.
-__global__ void __launch_bounds__(256) build_normals_kernel(const uint4* __restrict__ occ, uint64_t blocks,
+// share one brick, so the occupancy words a thread reads (at most 6 of the
+// brick's 16) come from the same 64 bytes in L1; each thread writes its
+// 16-byte block, a warp 512 contiguous bytes.  The 27 neighbour-code normals
+// sit in shared memory, one 16-byte entry each.
+__global__ void __launch_bounds__(128) build_normals_kernel(const uint32_t* __restrict__ occ, uint64_t blocks,
                                                             uint4* __restrict__ out) {
+    __shared__ float4 tab[dxtn::NUM_CODES];
+    if (threadIdx.x < dxtn::NUM_CODES) tab[threadIdx.x] = dxtn::code_entry(int(threadIdx.x));
+    __syncthreads();
+    const dxtn::CodeTable lookup{tab};
     for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < blocks;
          i += uint64_t(gridDim.x) * blockDim.x) {
-        const uint64_t brick = i >> 5;
-        uint32_t w[16];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const uint4 q = __ldg(occ + brick * 4 + k);
-            w[4 * k] = q.x; w[4 * k + 1] = q.y; w[4 * k + 2] = q.z; w[4 * k + 3] = q.w;
-        }
         uint64_t a, b;
-        dxtn::brick_block(w, int(i & 31), a, b);
+        dxtn::brick_block(occ + (i >> 5) * 16, int(i & 31), lookup, a, b);
         out[i] = make_uint4(uint32_t(a), uint32_t(a >> 32), uint32_t(b), uint32_t(b >> 32));
     }
 }
@@ -83,10 +82,10 @@ extern "C" int vx_build_normals_dev(const uint32_t* occ_dev, uint32_t brick_coun
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const uint64_t want = (blocks + 255) / 256;
-    const uint32_t grid = uint32_t(std::min<uint64_t>(want, uint64_t(sms) * 16));
-    build_normals_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        reinterpret_cast<const uint4*>(occ_dev), blocks, reinterpret_cast<uint4*>(out_dev));
+    const uint64_t want = (blocks + 127) / 128;
+    const uint32_t grid = uint32_t(std::min<uint64_t>(want, uint64_t(sms) * 64));
+    build_normals_kernel<<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(occ_dev, blocks,
+                                                                             reinterpret_cast<uint4*>(out_dev));
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_build_normals_dev");
 }
@@ -95,9 +94,13 @@ static int vx_build_normals_body(const uint32_t* occ, uint32_t brick_count, uint
     using namespace vx;
     if (brick_count && (!occ || !out)) return fail(VX_EINVAL, "vx_build_normals: null argument");
     const unsigned T = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    float4 tab[dxtn::NUM_CODES];
+    for (int c = 0; c < dxtn::NUM_CODES; ++c) tab[c] = dxtn::code_entry(c);
+    const dxtn::CodeTable lookup{tab};
     auto work = [&](uint64_t b0, uint64_t b1) {
         for (uint64_t b = b0; b < b1; ++b)
-            for (int k = 0; k < 32; ++k) dxtn::brick_block(occ + 16 * b, k, out[(b * 32 + k) * 2], out[(b * 32 + k) * 2 + 1]);
+            for (int k = 0; k < 32; ++k)
+                dxtn::brick_block(occ + 16 * b, k, lookup, out[(b * 32 + k) * 2], out[(b * 32 + k) * 2 + 1]);
     };
     if (T == 1 || brick_count < 256) {
         work(0, brick_count);
