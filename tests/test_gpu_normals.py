@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from test_gpu_parity import assert_hits_equal
-from test_normals import _bricks
+from test_normals import _bricks, _shaped_bricks
 
 pytestmark = pytest.mark.gpu
 
@@ -23,6 +23,11 @@ def _dev_normals(vx, occ):
 
 def test_device_builder_equals_oracle_random_bricks(vx, vo, cuda):
     occ = _bricks(7, 3000)
+    np.testing.assert_array_equal(_dev_normals(vx, occ), vo.brick_normals(occ))
+
+
+def test_device_builder_equals_oracle_shaped_bricks(vx, vo, cuda):
+    occ = _shaped_bricks(8, 1500)
     np.testing.assert_array_equal(_dev_normals(vx, occ), vo.brick_normals(occ))
 
 

@@ -137,3 +137,30 @@ def test_dxt1_payload_decodes_close(vx, vo):
                 if (occ[b, i >> 5] >> (i & 31)) & 1:
                     errs.append(float(np.linalg.norm(dec[t] - rgb[b, i])))
     assert np.median(errs) < 0.3
+
+
+def _shaped_bricks(seed, n):
+    """Bricks cut by planes, spheres and thin slabs, plus checkerboards and single
+    voxels: many distinct neighbour codes per block and cancelling normals."""
+    rng = np.random.default_rng(seed)
+    z, y, x = np.meshgrid(np.arange(8), np.arange(8), np.arange(8), indexing="ij")
+    p = np.stack([x.ravel(), y.ravel(), z.ravel()], 1).astype(np.float64)
+    nrm = rng.normal(size=(n, 3))
+    side = p @ nrm.T - rng.uniform(-6, 6, size=n) * np.linalg.norm(nrm, axis=1)
+    c = rng.uniform(-2, 10, size=(n, 3))
+    sphere = np.linalg.norm(p[:, None] - c[None], axis=2) < rng.uniform(0.5, 8, size=n)
+    slab = np.abs(side) < rng.uniform(0.3, 2, size=n)
+    cb = ((x + y + z) % 2 == 0).ravel()
+    bits = np.concatenate([(side > 0).T, sphere.T, slab.T, np.stack([cb, ~cb, np.eye(512, dtype=bool)[5],
+                                                                     np.eye(512, dtype=bool)[511]])])
+    occ = np.zeros((bits.shape[0], 16), np.uint32)
+    for w in range(16):
+        occ[:, w] = np.sum(bits[:, 32 * w:32 * w + 32].astype(np.uint64) << np.arange(32, dtype=np.uint64), axis=1)
+    return occ
+
+
+def test_host_builder_shaped_bricks_equal_oracle(vx, vo):
+    """The host builder looks normals up by neighbour code and searches distinct
+    codes only; the oracle evaluates every texel."""
+    occ = _shaped_bricks(5, 1500)
+    np.testing.assert_array_equal(vx.build_normals(occ), vo.brick_normals(occ))
