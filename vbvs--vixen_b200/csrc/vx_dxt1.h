@@ -51,24 +51,31 @@ VX_HD void decode_head(uint32_t head, C3 ref[4]) {
                 ref[0].b * (1.0f / 3.0f) + ref[1].b * (2.0f / 3.0f)};
 }
 
-// encodeBlockTyped (:57-111) over 16 texels.
-VX_HD uint64_t encode16(const C3* c) {
+VX_HD C3 texel(const float* p, int t) { return C3{p[3 * t], p[3 * t + 1], p[3 * t + 2]}; }
+
+// encodeBlockTyped (:57-111) over 16 texels, texel t at p[3t .. 3t + 2].
+VX_HD uint64_t encode16(const float* p) {
     int i0 = 0, i1 = 0;
     float best = -3.402823466e+38f;
+    VX_UNROLL
     for (int i = 0; i < 16; ++i)
+        VX_UNROLL
         for (int j = i + 1; j < 16; ++j) {
-            const float d = dist2(c[i], c[j]);
+            const float d = dist2(texel(p, i), texel(p, j));
             if (d > best) { i0 = i; i1 = j; best = d; }
         }
-    const uint32_t head = encode_head(c[i0], c[i1]);
+    const uint32_t head = encode_head(texel(p, i0), texel(p, i1));
     C3 ref[4];
     decode_head(head, ref);
     uint32_t bits = 0;
+    VX_UNROLL
     for (int t = 0; t < 16; ++t) {
+        const C3 c = texel(p, t);
         int bi = 0;
         float bd = 3.402823466e+38f;
+        VX_UNROLL
         for (int j = 0; j < 4; ++j) {
-            const float d = dist2(c[t], ref[j]);
+            const float d = dist2(c, ref[j]);
             if (d < bd) { bi = j; bd = d; }
         }
         bits |= uint32_t(bi) << (2 * t);
@@ -76,18 +83,24 @@ VX_HD uint64_t encode16(const C3* c) {
     return uint64_t(head) | (uint64_t(bits) << 32);
 }
 
-// Block k of a brick's colour payload (SVORebuild.cpp:658-722): empty texels
-// (0,0,0), a block without occupied texels 0.  rgb: 512 x 3 floats.
+// Zero the empty texels of a 16-texel block in place (the rebuild's input for
+// them is (0,0,0)).
+VX_HD void mask_empty(float* p, uint32_t occ16) {
+    VX_UNROLL
+    for (int t = 0; t < 16; ++t)
+        if (!((occ16 >> t) & 1u)) p[3 * t] = p[3 * t + 1] = p[3 * t + 2] = 0.0f;
+}
+
+// Block k of a brick's colour payload (SVORebuild.cpp:658-722); rgb: the
+// brick's 512 x 3 floats, occ its 16 occupancy words.  A block without
+// occupied texels is 0.
 VX_HD uint64_t brick_block(const float* rgb, const uint32_t* occ, int k) {
-    C3 c[16];
-    bool any = false;
-    for (int t = 0; t < 16; ++t) {
-        const int i = k * 16 + t;
-        const bool o = (occ[i >> 5] >> (i & 31)) & 1u;
-        any = any || o;
-        c[t] = o ? C3{rgb[3 * i], rgb[3 * i + 1], rgb[3 * i + 2]} : C3{0.0f, 0.0f, 0.0f};
-    }
-    return any ? encode16(c) : 0;
+    const uint32_t occ16 = (occ[k >> 1] >> ((k & 1) * 16)) & 0xFFFFu;
+    if (!occ16) return 0;
+    float c[48];
+    for (int f = 0; f < 48; ++f) c[f] = rgb[48 * k + f];
+    mask_empty(c, occ16);
+    return encode16(c);
 }
 
 }  // namespace dxt1

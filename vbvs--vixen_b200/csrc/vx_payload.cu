@@ -34,20 +34,46 @@ __global__ void __launch_bounds__(128) build_normals_kernel(const uint32_t* __re
     }
 }
 
-// Thread i encodes colour block i & 31 of brick i >> 5 from the brick's 512
-// RGB texels (6 KiB per brick, read through L1 by the warp that shares it).
-__global__ void __launch_bounds__(256) build_dxt1_kernel(const float* __restrict__ rgb, const uint4* __restrict__ occ,
-                                                         uint64_t blocks, uint64_t* __restrict__ out) {
-    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < blocks;
-         i += uint64_t(gridDim.x) * blockDim.x) {
-        const uint64_t brick = i >> 5;
-        uint32_t w[16];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const uint4 q = __ldg(occ + brick * 4 + k);
-            w[4 * k] = q.x; w[4 * k + 1] = q.y; w[4 * k + 2] = q.z; w[4 * k + 3] = q.w;
+// One warp per brick: the brick's 512 RGB texels (6 KiB) come in with
+// coalesced loads (16-byte loads when the colours are 16-byte aligned) and are
+// staged in shared memory with a 49-word stride per 16-texel block, so that the
+// lanes' texel reads (lane k = block k) fall in 32 different banks; lane k then
+// encodes block k and the warp writes its 256 output bytes contiguously.
+constexpr int DXT1_WARPS = 4;
+constexpr int DXT1_STRIDE = 49;
+
+template <bool VEC>
+__global__ void __launch_bounds__(DXT1_WARPS * 32) build_dxt1_kernel(const float* __restrict__ rgb,
+                                                                     const uint32_t* __restrict__ occ,
+                                                                     uint64_t bricks, uint64_t* __restrict__ out) {
+    __shared__ float stage[DXT1_WARPS][32 * DXT1_STRIDE];
+    const int lane = threadIdx.x & 31;
+    float* s = stage[threadIdx.x >> 5];
+    for (uint64_t brick = uint64_t(blockIdx.x) * DXT1_WARPS + (threadIdx.x >> 5); brick < bricks;
+         brick += uint64_t(gridDim.x) * DXT1_WARPS) {
+        const float* src = rgb + brick * 1536;
+        if (VEC) {
+            for (int q = lane; q < 384; q += 32) {  // 12 float4 per block
+                const float4 v = __ldg(reinterpret_cast<const float4*>(src) + q);
+                float* d = s + (q / 12) * DXT1_STRIDE + (q % 12) * 4;
+                d[0] = v.x;
+                d[1] = v.y;
+                d[2] = v.z;
+                d[3] = v.w;
+            }
+        } else {
+            for (int f = lane; f < 1536; f += 32) s[(f / 48) * DXT1_STRIDE + f % 48] = __ldg(src + f);
         }
-        out[i] = dxt1::brick_block(rgb + brick * 512 * 3, w, int(i & 31));
+        __syncwarp();
+        const uint32_t o = (__ldg(occ + brick * 16 + (lane >> 1)) >> ((lane & 1) * 16)) & 0xFFFFu;
+        float* mine = s + lane * DXT1_STRIDE;
+        uint64_t block = 0;
+        if (o) {
+            dxt1::mask_empty(mine, o);
+            block = dxt1::encode16(mine);
+        }
+        out[brick * 32 + lane] = block;
+        __syncwarp();
     }
 }
 
@@ -129,13 +155,16 @@ extern "C" int vx_build_dxt1_dev(const float* rgb_dev, const uint32_t* occ_dev, 
         reinterpret_cast<uintptr_t>(rgb_dev) % 4)
         return fail(VX_EINVAL, "vx_build_dxt1_dev: misaligned buffer");
     if (brick_count == 0) return VX_OK;
-    const uint64_t blocks = uint64_t(brick_count) * 32;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const uint32_t grid = uint32_t(std::min<uint64_t>((blocks + 255) / 256, uint64_t(sms) * 16));
-    build_dxt1_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        rgb_dev, reinterpret_cast<const uint4*>(occ_dev), blocks, out_dev);
+    const uint32_t grid =
+        uint32_t(std::min<uint64_t>((uint64_t(brick_count) + DXT1_WARPS - 1) / DXT1_WARPS, uint64_t(sms) * 32));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (reinterpret_cast<uintptr_t>(rgb_dev) % 16 == 0)
+        build_dxt1_kernel<true><<<grid, DXT1_WARPS * 32, 0, st>>>(rgb_dev, occ_dev, brick_count, out_dev);
+    else
+        build_dxt1_kernel<false><<<grid, DXT1_WARPS * 32, 0, st>>>(rgb_dev, occ_dev, brick_count, out_dev);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_build_dxt1_dev");
 }
