@@ -661,6 +661,118 @@ def measure_next(args, steps, warmup):
     return out
 
 
+def measure_tour(args):
+    """One pass over every kernel of the library on the cfg2 scene (1024^3 cave) and small
+    companions, each step timed with CUDA events (mean of 3 after 1 warm-up): noise synthesis,
+    device builder with both payloads, the RGBA8 builder, plain / counting / LOD casts, the
+    compressed render, per-hit normal decode, the payload encoders, the batched kernels (static
+    and refilling lanes, bounce and shadow spawn, the no-allocation entry point) and the
+    adjoint pair.  Meant as the command an ncu launch list or a per-kernel capture runs."""
+    import math
+    import numpy as np
+    import torch
+    vx = load_pkg()
+    from vx_b200 import workloads as W
+    out = {}
+
+    def ev_ms(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    R, seed = 1024, 2
+    holder = {}
+    out["synth_noise_1024"] = ev_ms(lambda: holder.__setitem__("bits", vx.synth_noise_dev(R, 64, 5, 0.5, seed, False)))
+    bits = holder["bits"]
+    t0 = time.perf_counter()
+    sc = vx.scene_from_dense_dev(bits, R, 10, vx.VX_COLOR_DXT1, seed ^ 0xD7C1, True)
+    torch.cuda.synchronize()
+    out["device_build_1024_dxt1_normals_host_clock"] = (time.perf_counter() - t0) * 1e3
+    bits256 = vx.synth_noise_dev(256, 16, 3, 0.5, 3, False)
+    sc_rgba = vx.scene_from_dense_dev(bits256, 256, 8, vx.VX_COLOR_RGBA8, 3, False)
+    bits_np = bits.cpu().numpy().view(np.uint64)
+    cam = W.empty_voxel_camera(bits_np, R, seed, 70.0, 1920, 1080)
+    rays = torch.from_numpy(vx.camera_rays(cam, 1920, 1080)[W.tile_order(1920, 1080)]).cuda()
+    n = rays.shape[0]
+    hits = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+    color = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+    counters = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+    out["cast_1080p"] = ev_ms(lambda: sc.cast_rays_dev(rays, hits, color))
+    out["cast_1080p_counters"] = ev_ms(lambda: sc.cast_rays_dev(rays, hits, color, counters))
+    lod = vx.lod_with_bias(vx.lod_from_camera(math.radians(70.0), 1080), 7.0)
+    out["cast_1080p_lod_bias7"] = ev_ms(lambda: sc.cast_rays_dev(rays, hits, lod=lod))
+    img = torch.zeros(n, dtype=torch.int32, device="cuda")
+    out["render_1080p_dxt1_normals"] = ev_ms(lambda: sc.render_dev(cam, 1920, 1080, img, hits))
+    nrm = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+    out["hit_normals_1080p"] = ev_ms(lambda: sc.hit_normals_dev(hits, nrm))
+    a = sc.download()
+    B = a.brick_count
+    occ = torch.from_numpy(a.brick_occ.view(np.int32).reshape(-1)).cuda()
+    nout = torch.zeros(B * 64, dtype=torch.int64, device="cuda")
+    out["normal_payload_1024"] = ev_ms(lambda: vx.build_normals_dev(occ, nout))
+    nb = min(B, 262144)
+    rgba = vx.synth_rgba8(a.brick_coord[:nb], seed)
+    rgb = torch.from_numpy(np.stack([(rgba >> s_) & 255 for s_ in (0, 8, 16)], -1).astype(np.float32)
+                           / np.float32(255.0)).reshape(-1).cuda()
+    dout = torch.zeros(nb * 32, dtype=torch.int64, device="cuda")
+    occ_sub = occ[:nb * 16].contiguous()
+    out["dxt1_payload_262k"] = ev_ms(lambda: vx.build_dxt1_dev(rgb, occ_sub, dout))
+    del a, occ, nout, rgb, dout, occ_sub
+    # batched: the cave frame and 2^18 random rays through the 256^3 RGBA8 scene
+    r2 = torch.from_numpy(W.random_rays(262144, 256, seed=9)).cuda()
+    brays = torch.cat([rays, r2])
+    begin = torch.tensor([0, n, n + r2.shape[0]], dtype=torch.int32, device="cuda")
+    bh = torch.zeros((brays.shape[0], 4), dtype=torch.int32, device="cuda")
+    batch = vx.Batch([sc, sc_rgba])
+    batch.set_tuning(256, 32, 1, 0)
+    out["batch_static"] = ev_ms(lambda: batch.cast(brays, begin, bh))
+    bounce = torch.zeros((2 * brays.shape[0], 6), dtype=torch.float32, device="cuda")
+    out["spawn_bounce"] = ev_ms(lambda: vx.spawn_bounce_rays(brays, bh, 77, bounce))
+    bbegin = begin * 2
+    bbh = torch.zeros((bounce.shape[0], 4), dtype=torch.int32, device="cuda")
+    batch.set_tuning(128, 256, 0, 24)
+    out["batch_refill_bounce"] = ev_ms(lambda: batch.cast(bounce, bbegin, bbh))
+    shadow = torch.zeros_like(brays)
+    out["spawn_shadow"] = ev_ms(lambda: vx.spawn_shadow_rays(brays, bh, [0.3, 0.8, 0.5], shadow))
+    out["batch_noalloc"] = ev_ms(lambda: vx.cast_batch_noalloc([sc, sc_rgba], brays, begin, bh))
+    batch.close()
+    del bounce, bbh, shadow, brays, bh
+    # adjoint pair on a 256^3 scene, 4 views of 512x512, per-voxel RGB and DXT1 endpoints
+    bits_d = vx.synth_noise_dev(256, 16, 3, 0.30, 5, False)
+    sd = vx.scene_from_dense_dev(bits_d, 256, 8, vx.VX_COLOR_NONE, 0, False)
+    Bd = int(sd.info().brick_count)
+    c = 128.0
+    views = [W.look_camera([c + 243 * math.cos(t), c + 20.0, c + 243 * math.sin(t)],
+                           [-243 * math.cos(t), -20.0, -243 * math.sin(t)], 60.0, 512, 512)
+             for t in (0.3, 1.9, 3.5, 5.1)]
+    V, npx = len(views), 512 * 512
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    for kind, name, per in ((0, "rgb", Bd * 512 * 3), (1, "dxt1_endpoints", Bd * 32 * 6)):
+        attr = torch.rand(per, device="cuda", generator=gen)
+        idx = None if kind == 0 else torch.randint(-2 ** 31, 2 ** 31 - 1, (Bd * 32,), device="cuda",
+                                                   dtype=torch.int32, generator=gen)
+        imgs = torch.zeros((V * npx, 3), dtype=torch.float32, device="cuda")
+        rec = torch.zeros((V * npx, 4), dtype=torch.int32, device="cuda")
+        tgt = torch.rand((V * npx, 3), device="cuda", generator=gen)
+        grad = torch.zeros_like(attr)
+        loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+        out[f"diff_forward_4x512_{name}"] = ev_ms(
+            lambda: vx.diff_forward_views(sd, views, 512, 512, kind, attr, idx, imgs, rec))
+        out[f"diff_backward_4x512_{name}"] = ev_ms(lambda: vx.diff_backward(kind, idx, rec, imgs, tgt, grad, loss))
+    sd.close()
+    sc_rgba.close()
+    sc.close()
+    return {"workload": "kernel tour: cave 1024^3 (cfg2 scene, DXT1 + normals), 1920x1080 tiled rays, "
+                        "256^3 RGBA8 companion with 2^18 random rays, 256^3 adjoint scene with 4 views of 512x512",
+            "ms": out}
+
+
 def config_dict(wl, world):
     return {"workload": f"{wl.name}: cave {wl.R}^3 (depth {wl.scene.max_levels}), value noise spacing "
                         f"{64 * wl.R // 1024}, 5 octaves, 50% fill, DXT1 bricks, {wl.width}x{wl.height} FP32 "
@@ -680,10 +792,11 @@ def main():
     ap.add_argument("--R", type=int, default=1024)
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg3", "cfg4", "cfg5", "next"],
+    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg3", "cfg4", "cfg5", "next", "tour"],
                     help="cfg2: plain cast of the 1024^3 cave frame (with the cfg4, cfg5 and next-row results "
                          "attached at N=1); cfg4: 64-scene batched frame vs plain; cfg5: forward / adjoint ms per "
-                         "view; next: device builder, payload encoders, LOD cut, compressed render, cache file")
+                         "view; next: device builder, payload encoders, LOD cut, compressed render, cache file; "
+                         "tour: every kernel once, CUDA-event times per step (the command for ncu captures)")
     ap.add_argument("--no-extra", action="store_true",
                     help="cfg2 only: skip the attached batched (cfg4), adjoint (cfg5) and next-row measurements")
     ap.add_argument("--scenes", type=int, default=64, help="cfg4: number of scenes")
@@ -711,6 +824,13 @@ def main():
                     "config": {"workload": res.pop("workload")}, "gpu_launches": args.steps * 3}
             line.update(res)
             print(json.dumps(line), flush=True)
+        return 0
+    if args.workload == "tour":
+        import torch
+        torch.cuda.set_device(local)
+        res = measure_tour(args)
+        if rank == 0:
+            print(json.dumps({"workload": "tour", "tour": res}), flush=True)
         return 0
     if args.workload == "next":
         res = measure_next(args, args.steps, args.warmup)
