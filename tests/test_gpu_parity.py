@@ -100,6 +100,48 @@ def test_noise_scene_rgba8_bit_exact(vx, vo, cuda, R):
     np.testing.assert_array_equal(col[:, 0].view(np.uint32), want)
 
 
+@pytest.mark.parametrize("L", [16, 20, 23])
+def test_deep_scene_bit_exact(vx, vo, cuda, L):
+    """max_levels 16-23 over a 64^3 grid: the per-thread stacks grow to two words per level
+    plus the cycle-detection slots, 51-64 KiB of shared memory for the batched kernel's
+    256-thread blocks (above the 48 KiB a launch gets without opting in).  Plain cast,
+    render, batched cast and the adjoint forward run and stay bit-exact."""
+    import torch
+    from vx_b200 import workloads as W
+    bits = vx.synth_noise(64, 8, 3, 0.5, 41, False)
+    a = W.scene_from_bits(bits, 64, "rgba8", 41, max_levels=L)
+    o = vo.OracleScene.from_dense(bits, 64, L)
+    cam = W.empty_voxel_camera(bits, 64, 41, 70.0, 64, 48)
+    cam_rays = vx.camera_rays(cam, 64, 48)
+    rays = np.concatenate([cam_rays, W.random_rays(8000, 64, seed=43)])
+    s = vx.Scene(a)
+    g, col, cnt = gpu_cast(vx, s, rays)
+    oh = o.cast_rays(rays)
+    assert_hits_equal(g, oh, cnt, f"deep L={L}")
+    assert (oh["flags"] & 1).mean() > 0.1
+    n = 64 * 48
+    want = o.cast_rays(cam_rays)
+    img = torch.zeros(n, dtype=torch.int32, device="cuda")
+    hits = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+    s.render_dev(cam, 64, 48, img, hits)
+    torch.cuda.synchronize()
+    assert_hits_equal(hits.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1), want, None, "render")
+    r = torch.from_numpy(rays).cuda()
+    bh = torch.zeros((rays.shape[0], 4), dtype=torch.int32, device="cuda")
+    batch = vx.Batch([s])
+    batch.set_tuning(256, 32, 1, 0)
+    batch.cast(r, torch.tensor([0, rays.shape[0]], dtype=torch.int32, device="cuda"), bh)
+    torch.cuda.synchronize()
+    assert_hits_equal(bh.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1), oh, None, "batched")
+    batch.close()
+    attr = torch.rand(a.brick_count * 512 * 3, device="cuda")
+    image = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+    rec = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+    vx.diff_forward(s, cam, 64, 48, 0, attr, None, image, rec)
+    torch.cuda.synchronize()
+    assert_hits_equal(rec.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1), want, None, "adjoint forward")
+
+
 def test_dxt_scene_texels_bit_exact(vx, vo, cuda):
     from vx_b200 import workloads as W
     wl = W.config2(R=128, width=160, height=90, seed=5)

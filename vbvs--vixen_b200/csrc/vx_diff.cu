@@ -20,6 +20,7 @@
 // w1 g to dL/de0, dL/de1 (kind 1).  Lanes of a warp that hit the same voxel /
 // block are combined first (__match_any_sync + shuffles) so each distinct
 // target costs one atomicAdd per channel per warp.
+
 #include "vx_cast.cuh"
 
 namespace vx {
@@ -52,38 +53,15 @@ struct Views {
     CameraDev cam[VX_DIFF_MAX_VIEWS];
 };
 
-// Images and records are view-major: pixel p of view v is entry v * w * hgt + p.
-// With VX_DIFF_TILED each block covers a 32 x 8 pixel tile of one view and each
-// warp an 8 x 4 piece of it, so a warp's rays are neighbours in both image
-// directions and their traversals stay closer together than along a row.
-__global__ void __launch_bounds__(DBLOCK, 3) diff_forward_kernel(DevScene s, Views views, uint32_t nviews, uint32_t w,
-                                                                   uint32_t hgt, int kind,
-                                                                   const float* __restrict__ attr,
-                                                                   const uint32_t* __restrict__ idx,
-                                                                   float* __restrict__ image,
-                                                                   vx_hit* __restrict__ record) {
-    extern __shared__ uint32_t smem[];
-    uint32_t* stkN = smem + threadIdx.x;
-    float* stkT = reinterpret_cast<float*>(smem + s.max_levels * blockDim.x) + threadIdx.x;
-    uint32_t* cyc = smem + 2 * s.max_levels * blockDim.x + threadIdx.x;
-    const uint32_t per_view = w * hgt;
-#if VX_DIFF_TILED
-    const uint32_t tw = (w + 31) / 32, tiles = tw * ((hgt + 7) / 8);
-    const uint32_t v = blockIdx.x / tiles, tl = blockIdx.x - v * tiles;
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-    const uint32_t px = (tl % tw) * 32 + (warp & 3u) * 8 + (lane & 7u);
-    const uint32_t py = (tl / tw) * 8 + (warp >> 2) * 4 + (lane >> 3);
-    if (v >= nviews || px >= w || py >= hgt) return;
-    const uint32_t i = v * per_view + py * w + px;
-#else
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nviews * per_view) return;
-    const uint32_t v = i / per_view, p = i - v * per_view;
-    const uint32_t px = p % w, py = p / w;
-#endif
+// One pixel of the forward pass: cast, record, shade.
+__device__ __forceinline__ void forward_pixel(const DevScene& s, const CameraDev& cam, uint32_t px, uint32_t py,
+                                              uint32_t w, uint32_t hgt, uint32_t i, int kind,
+                                              const float* __restrict__ attr, const uint32_t* __restrict__ idx,
+                                              float* __restrict__ image, vx_hit* __restrict__ record,
+                                              uint32_t* stkN, float* stkT, uint32_t* cyc) {
     vx_ray r;
     float uv_y;
-    camera_ray(views.cam[v], px, py, w, hgt, r, &uv_y);
+    camera_ray(cam, px, py, w, hgt, r, &uv_y);
     Hit h;
     cast_ray(s, r.ox, r.oy, r.oz, r.dx, r.dy, r.dz, 0.0f, FLT_MAX_, stkN, stkT, cyc, blockDim.x, h);
     store_hit(record, i, h);
@@ -108,6 +86,47 @@ __global__ void __launch_bounds__(DBLOCK, 3) diff_forward_kernel(DevScene s, Vie
     }
     float* o = image + size_t(i) * 3;
     o[0] = c[0]; o[1] = c[1]; o[2] = c[2];
+}
+
+// Images and records are view-major: pixel p of view v is entry v * w * hgt + p.
+// With VX_DIFF_TILED the work is split into warp tasks of 8 x 4 pixels (the
+// eight pieces of a 32 x 8 tile are consecutive tasks), so a warp's rays are
+// neighbours in both image directions.  A block holds FWD_WARPS warps, one task
+// each: small blocks free their slot as soon as their warps finish, where one
+// block per 32 x 8 tile would hold its slot until the slowest of its eight
+// warps finished (the orbit views mix rays that hit near with rays that miss far).
+#ifndef VX_DIFF_FWD_WARPS
+#define VX_DIFF_FWD_WARPS 2
+#endif
+constexpr int FWD_WARPS = VX_DIFF_FWD_WARPS;
+constexpr int FWD_THREADS = VX_DIFF_TILED ? FWD_WARPS * 32 : DBLOCK;
+
+__global__ void __launch_bounds__(FWD_THREADS, 768 / FWD_THREADS) diff_forward_kernel(
+    DevScene s, Views views, uint32_t nviews, uint32_t w, uint32_t hgt, int kind, const float* __restrict__ attr,
+    const uint32_t* __restrict__ idx, float* __restrict__ image, vx_hit* __restrict__ record) {
+    extern __shared__ uint32_t smem[];
+    uint32_t* stkN = smem + threadIdx.x;
+    float* stkT = reinterpret_cast<float*>(smem + s.max_levels * blockDim.x) + threadIdx.x;
+    uint32_t* cyc = smem + 2 * s.max_levels * blockDim.x + threadIdx.x;
+    const uint32_t per_view = w * hgt;
+#if VX_DIFF_TILED
+    const uint32_t tw = (w + 31) / 32, tiles = tw * ((hgt + 7) / 8);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t t = uint64_t(blockIdx.x) * FWD_WARPS + (threadIdx.x >> 5);
+    if (t >= uint64_t(nviews) * tiles * 8) return;
+    const uint32_t piece = uint32_t(t & 7u), tt = uint32_t(t >> 3);
+    const uint32_t v = tt / tiles, tl = tt - v * tiles;
+    const uint32_t px = (tl % tw) * 32 + (piece & 3u) * 8 + (lane & 7u);
+    const uint32_t py = (tl / tw) * 8 + (piece >> 2) * 4 + (lane >> 3);
+    if (px >= w || py >= hgt) return;
+    forward_pixel(s, views.cam[v], px, py, w, hgt, v * per_view + py * w + px, kind, attr, idx, image, record, stkN,
+                  stkT, cyc);
+#else
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nviews * per_view) return;
+    const uint32_t v = i / per_view, p = i - v * per_view;
+    forward_pixel(s, views.cam[v], p % w, p / w, w, hgt, i, kind, attr, idx, image, record, stkN, stkT, cyc);
+#endif
 }
 
 // Sum v over the lanes of `group` (lanes sharing one key); every lane of the
@@ -214,15 +233,21 @@ extern "C" int vx_diff_forward_views(const vx_scene* scene, const vx_camera_pc* 
     const DevScene& s = scene_dev(scene);
     Views v{};
     for (uint32_t k = 0; k < views; ++k) v.cam[k] = camera_from_pc(pcs[k]);
-    const size_t smem = (size_t(2) * size_t(s.max_levels) + CYC_WORDS) * DBLOCK * sizeof(uint32_t);
+    const size_t smem = (size_t(2) * size_t(s.max_levels) + CYC_WORDS) * FWD_THREADS * sizeof(uint32_t);
+    // stacks of scenes deeper than 15 levels need more than 48 KiB per 256 threads
+    if (smem > 48 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(diff_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   int(smem));
+        if (e != cudaSuccess) return fail(VX_ECUDA, std::string("vx_diff_forward: ") + cudaGetErrorString(e));
+    }
 #if VX_DIFF_TILED
-    static_assert(DBLOCK == 256, "a block covers one 32 x 8 tile");
-    const uint64_t blocks = uint64_t(views) * ((w + 31) / 32) * ((h + 7) / 8);
+    const uint64_t tasks = uint64_t(views) * ((w + 31) / 32) * ((h + 7) / 8) * 8;
+    const uint64_t blocks = (tasks + FWD_WARPS - 1) / FWD_WARPS;
 #else
     const uint64_t blocks = (n + DBLOCK - 1) / DBLOCK;
 #endif
     if (blocks > 0x7FFFFFFFull) return fail(VX_EOVERFLOW, "vx_diff_forward: too many pixels for one launch");
-    diff_forward_kernel<<<uint32_t(blocks), DBLOCK, smem, static_cast<cudaStream_t>(stream)>>>(
+    diff_forward_kernel<<<uint32_t(blocks), FWD_THREADS, smem, static_cast<cudaStream_t>(stream)>>>(
         s, v, views, w, h, kind, attr, dxt_idx, image, record);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? VX_OK : fail(VX_ECUDA, std::string("vx_diff_forward: ") + cudaGetErrorString(e));

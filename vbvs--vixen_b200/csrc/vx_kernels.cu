@@ -4,10 +4,20 @@
 namespace vx {
 namespace {
 
-constexpr int BLOCK = 256;
+// Threads per block of the cast kernel, and warps per block of the render
+// kernel (each warp one 8 x 4 piece of a 32 x 8 tile).
+#ifndef VX_CAST_BLOCK
+#define VX_CAST_BLOCK 64
+#endif
+#ifndef VX_RENDER_WARPS
+#define VX_RENDER_WARPS 2
+#endif
+constexpr int BLOCK = VX_CAST_BLOCK;
+constexpr int RENDER_WARPS = VX_RENDER_WARPS;
+constexpr int RENDER_THREADS = RENDER_WARPS * 32;
 
 template <bool LOD>
-__global__ void __launch_bounds__(BLOCK, 3) cast_kernel(DevScene s, const vx_ray* __restrict__ rays, uint32_t n,
+__global__ void __launch_bounds__(BLOCK, 768 / BLOCK) cast_kernel(DevScene s, const vx_ray* __restrict__ rays, uint32_t n,
                                                       float tmin, float tmax, vx_hit* __restrict__ hits,
                                                       void* __restrict__ color,
                                                       vx_ray_counters* __restrict__ counters, LodCone lod) {
@@ -33,21 +43,24 @@ __global__ void __launch_bounds__(BLOCK, 3) cast_kernel(DevScene s, const vx_ray
     }
 }
 
-// One block per 32 x 8 pixel tile, one warp per 8 x 4 piece of it (the
-// reference dispatches 8 x 8 workgroups, ComputeDispatchNode.cpp:272-301): a
-// warp's rays are neighbours in both image directions, so their traversals
-// diverge less than along a row.  Outputs are indexed by pixel (y * w + x).
-__global__ void __launch_bounds__(BLOCK, 3) render_kernel(DevScene s, CameraDev cam, uint32_t w, uint32_t hgt,
-                                                        uint32_t* __restrict__ image, vx_hit* __restrict__ hits,
-                                                        void* __restrict__ color) {
+// Pixels go to warps in 8 x 4 pieces of 32 x 8 tiles (the reference dispatches
+// 8 x 8 workgroups, ComputeDispatchNode.cpp:272-301): a warp's rays are
+// neighbours in both image directions, so their traversals diverge less than
+// along a row.  Warp task t is piece t & 7 of tile t >> 3; a block holds
+// RENDER_WARPS consecutive tasks.  Outputs are indexed by pixel (y * w + x).
+__global__ void __launch_bounds__(RENDER_THREADS, 768 / RENDER_THREADS) render_kernel(
+    DevScene s, CameraDev cam, uint32_t w, uint32_t hgt, uint32_t* __restrict__ image, vx_hit* __restrict__ hits,
+    void* __restrict__ color) {
     extern __shared__ uint32_t smem[];
     uint32_t* stkN = smem + threadIdx.x;
     float* stkT = reinterpret_cast<float*>(smem + s.max_levels * blockDim.x) + threadIdx.x;
     uint32_t* cyc = smem + 2 * s.max_levels * blockDim.x + threadIdx.x;
     const uint32_t tw = (w + 31) / 32;
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-    const uint32_t px = (blockIdx.x % tw) * 32 + (warp & 3u) * 8 + (lane & 7u);
-    const uint32_t py = (blockIdx.x / tw) * 8 + (warp >> 2) * 4 + (lane >> 3);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t t = uint64_t(blockIdx.x) * RENDER_WARPS + (threadIdx.x >> 5);
+    const uint32_t piece = uint32_t(t & 7u), tile = uint32_t(t >> 3);
+    const uint32_t px = (tile % tw) * 32 + (piece & 3u) * 8 + (lane & 7u);
+    const uint32_t py = (tile / tw) * 8 + (piece >> 2) * 4 + (lane >> 3);
     if (px >= w || py >= hgt) return;
     const uint32_t i = py * w + px;
     vx_ray r;
@@ -107,8 +120,16 @@ __global__ void camera_rays_kernel(CameraDev cam, uint32_t w, uint32_t hgt, vx_r
     rays[i] = r;
 }
 
-size_t stack_bytes(const DevScene& s) {
-    return (size_t(2) * size_t(s.max_levels) + CYC_WORDS) * BLOCK * sizeof(uint32_t);
+size_t stack_bytes(const DevScene& s, int threads) {
+    return (size_t(2) * size_t(s.max_levels) + CYC_WORDS) * size_t(threads) * sizeof(uint32_t);
+}
+
+// Stacks of scenes deeper than 15 levels take more than the 48 KiB of dynamic
+// shared memory a launch gets without opting in (64 KiB at 23 levels).
+template <class K>
+cudaError_t allow_smem(K kernel, size_t bytes) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
 }
 
 }  // namespace
@@ -118,12 +139,16 @@ int launch_cast(const DevScene& s, const vx_ray* rays, uint32_t n, float tmin, f
     if (n == 0) return int(cudaSuccess);
     const uint32_t grid = (n + BLOCK - 1) / BLOCK;
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (lod && lod->ray_dir_size > 0.0f)
-        cast_kernel<true><<<grid, BLOCK, stack_bytes(s), st>>>(s, rays, n, tmin, tmax, hits, color, counters,
-                                                               LodCone{lod->ray_orig_size, lod->ray_dir_size});
-    else
-        cast_kernel<false><<<grid, BLOCK, stack_bytes(s), st>>>(s, rays, n, tmin, tmax, hits, color, counters,
-                                                                LodCone{0.0f, 0.0f});
+    const size_t smem = stack_bytes(s, BLOCK);
+    if (lod && lod->ray_dir_size > 0.0f) {
+        if (cudaError_t e = allow_smem(cast_kernel<true>, smem)) return int(e);
+        cast_kernel<true><<<grid, BLOCK, smem, st>>>(s, rays, n, tmin, tmax, hits, color, counters,
+                                                     LodCone{lod->ray_orig_size, lod->ray_dir_size});
+    } else {
+        if (cudaError_t e = allow_smem(cast_kernel<false>, smem)) return int(e);
+        cast_kernel<false><<<grid, BLOCK, smem, st>>>(s, rays, n, tmin, tmax, hits, color, counters,
+                                                      LodCone{0.0f, 0.0f});
+    }
     return int(cudaGetLastError());
 }
 
@@ -131,11 +156,13 @@ int launch_render(const DevScene& s, const CameraDev& cam, uint32_t w, uint32_t 
                   void* color, void* stream) {
     const uint64_t n = uint64_t(w) * h;
     if (n == 0) return int(cudaSuccess);
-    static_assert(BLOCK == 256, "a block covers one 32 x 8 tile");
-    const uint64_t grid = uint64_t((w + 31) / 32) * ((h + 7) / 8);
+    static_assert(8 % RENDER_WARPS == 0, "a block covers whole 8 x 4 pieces of one 32 x 8 tile");
+    const uint64_t grid = uint64_t((w + 31) / 32) * ((h + 7) / 8) * (8 / RENDER_WARPS);
     if (grid > 0x7FFFFFFFull) return int(cudaErrorInvalidValue);
-    render_kernel<<<uint32_t(grid), BLOCK, stack_bytes(s), static_cast<cudaStream_t>(stream)>>>(s, cam, w, h, image,
-                                                                                                 hits, color);
+    const size_t smem = stack_bytes(s, RENDER_THREADS);
+    if (cudaError_t e = allow_smem(render_kernel, smem)) return int(e);
+    render_kernel<<<uint32_t(grid), RENDER_THREADS, smem, static_cast<cudaStream_t>(stream)>>>(s, cam, w, h, image, hits,
+                                                                                        color);
     return int(cudaGetLastError());
 }
 
