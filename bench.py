@@ -218,7 +218,9 @@ def run_cfg4(args, rank, world):
         line = {"metric": METRIC, "value": res["batched"]["value"], "unit": "Mrays/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["batched"]["ms_per_frame"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic", "config": res.pop("config"), "gpu_launches": args.steps * 3}
+                "data": "synthetic", "config": res.pop("config"),
+                # per frame: primary cast, hit count, chunk scan, bounce spawn, scene offsets, bounce cast
+                "gpu_launches": args.steps * 6}
         line.update(res)
         print(json.dumps(line), flush=True)
     return 0
@@ -281,13 +283,21 @@ def measure_cfg4(args, rank, world, steps, warmup):
     torch.cuda.synchronize()
     ref_p, ref_b = ph.cpu().numpy().copy(), bh.cpu().numpy().copy()
     stream = torch.cuda.Stream()
-    with torch.cuda.stream(stream):
-        batch.capture_frame(d_rays, d_begin, ph, bounce, d_bbegin, bh, seed, stream.cuda_stream)
-        ph.zero_()
-        bh.zero_()
-        batch.launch_frame(stream.cuda_stream)
-    torch.cuda.synchronize()
-    identical = bool(np.array_equal(ph.cpu().numpy(), ref_p) and np.array_equal(bh.cpu().numpy(), ref_b))
+
+    def capture(compact):
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            if compact:  # the bounce pass casts only the bounce rays of primary hits
+                batch.capture_frame_compact(d_rays, d_begin, ph, bounce, bh, seed, stream.cuda_stream)
+            else:
+                batch.capture_frame(d_rays, d_begin, ph, bounce, d_bbegin, bh, seed, stream.cuda_stream)
+            ph.zero_()
+            bh.zero_()
+            batch.launch_frame(stream.cuda_stream)
+        torch.cuda.synchronize()
+        return bool(np.array_equal(ph.cpu().numpy(), ref_p) and np.array_equal(bh.cpu().numpy(), ref_b))
+
+    identical_full = capture(False)
     nhit = int(np.count_nonzero(ref_p.view(vx.HIT_DTYPE).reshape(-1)["flags"] & 1))
     rays_per_frame = n + 2 * nhit  # primary + bounce rays of hits (miss slots carry a zero direction)
 
@@ -313,10 +323,12 @@ def measure_cfg4(args, rank, world, steps, warmup):
         return [a.elapsed_time(b) for a, b in ev]
 
     plain_ms = timed(plain_frame, stream)
+    full_ms = timed(lambda: batch.launch_frame(stream.cuda_stream), stream)
+    identical = capture(True) and identical_full
     batched_ms = timed(lambda: batch.launch_frame(stream.cuda_stream), stream)
     clocks = sampler.stop()
     from vx_b200 import multigpu as M
-    plain_total, batched_total = M.max_over_ranks([sum(plain_ms), sum(batched_ms)])
+    plain_total, batched_total, full_total = M.max_over_ranks([sum(plain_ms), sum(batched_ms), sum(full_ms)])
     value = world * rays_per_frame * steps / (batched_total / 1e3) / 1e6
     plain_value = world * rays_per_frame * steps / (plain_total / 1e3) / 1e6
     return {"config": {"workload": f"cfg4: {len(specs)} scenes 64^3..1024^3 (noise 10/50%, urban 90%, half DXT1), "
@@ -327,6 +339,9 @@ def measure_cfg4(args, rank, world, steps, warmup):
                        "scene_R": [sp.R for sp in specs], "setup_s": setup_s,
                        "l2": "flushed before every timed frame (256 MiB write)"},
             "batched": {"value": value, "unit": "Mrays/s", "ms_per_frame": batched_total / steps,
+                        "frame": "vx_batch_capture_frame_compact: the bounce pass casts the 2 bounce rays of "
+                                 "each primary hit only",
+                        "ms_per_frame_uncompacted": full_total / steps,
                         "tuning": tuning.as_dict(), "autotune_best_ms_primary": tune_ms,
                         "bounce_tuning": btuning.as_dict(), "autotune_best_ms_bounce": btune_ms},
             "plain": {"value": plain_value, "unit": "Mrays/s", "ms_per_frame": plain_total / steps,

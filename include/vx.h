@@ -389,6 +389,17 @@ int vx_batch_capture_frame(vx_batch* batch, const vx_ray* primary_dev, const uin
                            uint32_t n, vx_hit* primary_hits_dev, vx_ray* bounce_dev,
                            const uint32_t* bounce_begin_dev, vx_hit* bounce_hits_dev, uint64_t seed,
                            void* stream);
+/* The same frame with the bounce rays compacted: the bounce pass casts only
+ * the 2 rays of every primary hit.  bounce_dev (2n rays of scratch) receives
+ * them in primary order, 2h of them for h primary hits; the frame computes the
+ * per-scene offsets itself.  bounce_hits_dev (2n records) ends up exactly as
+ * with vx_batch_capture_frame: slot 2i + k holds bounce k of primary ray i,
+ * and the slots of primary misses hold the invalid-ray record a cast writes
+ * for their zero-direction rays.  Scratch of about 8n bytes is allocated at
+ * capture time (the first capture, or a larger n). */
+int vx_batch_capture_frame_compact(vx_batch* batch, const vx_ray* primary_dev, const uint32_t* primary_begin_dev,
+                                   uint32_t n, vx_hit* primary_hits_dev, vx_ray* bounce_dev,
+                                   vx_hit* bounce_hits_dev, uint64_t seed, void* stream);
 int vx_batch_launch_frame(vx_batch* batch, void* stream);
 /* Tuning of the bounce pass of a captured frame (default, or after a null
  * tuning: the batch's own).  Incoherent bounce rays favour other shapes than

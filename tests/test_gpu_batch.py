@@ -134,6 +134,59 @@ def test_frame_graph_equals_eager(vx, cuda, bounce_tuning):
     np.testing.assert_array_equal(bh.cpu().numpy(), eager[1])
 
 
+@pytest.mark.parametrize("big,bounce_tuning", [(False, None), (False, (256, 256, 0, 24)), (True, (128, 64, 0, 16))])
+def test_compacted_frame_equals_eager(vx, cuda, big, bounce_tuning):
+    """vx_batch_capture_frame_compact: primary and bounce hit records equal the eager frame's
+    (whose bounce pass casts all 2n slots, zero-direction rays included), and the compacted
+    bounce rays are the eager bounce rays of the primary hits in primary order.  `big`
+    (more than 2^20 primary rays) runs the chunk-count scan over several rounds and puts
+    scene boundaries inside chunks."""
+    import torch
+    from vx_b200 import workloads as W
+    if big:
+        specs = W.config4_specs(4, seed=21, r_range=(6, 7.4), res_lo=(640, 480), res_hi=(1280, 720))
+        wls = [W.build_spec(sp) for sp in specs]
+        scenes = [vx.Scene(w.scene) for w in wls]
+        rays = [w.rays(order="tiled") for w in wls]
+        begin = np.concatenate([[0], np.cumsum([r.shape[0] for r in rays])]).astype(np.uint32)
+        d_rays = torch.from_numpy(np.concatenate(rays).astype(np.float32)).cuda()
+        d_begin = torch.from_numpy(begin.astype(np.int32)).cuda()
+        assert d_rays.shape[0] > 1 << 20
+    else:
+        wls, scenes, rays, begin, allr, d_rays, d_begin = _setup(vx, W, n=8, seed=14)
+    n = d_rays.shape[0]
+    batch = vx.Batch(scenes)
+    if bounce_tuning is not None:
+        batch.set_bounce_tuning(vx.BatchTuning(*bounce_tuning))
+    bb = torch.from_numpy((2 * begin.astype(np.int64)).astype(np.int32)).cuda()
+    ph = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+    bh = torch.zeros((2 * n, 4), dtype=torch.int32, device="cuda")
+    bounce = torch.zeros((2 * n, 6), dtype=torch.float32, device="cuda")
+    batch.cast(d_rays, d_begin, ph)
+    vx.spawn_bounce_rays(d_rays, ph, 7, bounce)
+    batch.set_tuning(*(bounce_tuning or (256, 32, 1, 0)))
+    batch.cast(bounce, bb, bh)
+    batch.set_tuning(256, 32, 1, 0)
+    torch.cuda.synchronize()
+    eager_ph, eager_bh, eager_bounce = ph.cpu().numpy().copy(), bh.cpu().numpy().copy(), bounce.cpu().numpy().copy()
+    ph.fill_(-1), bh.fill_(-1), bounce.zero_()
+    torch.cuda.synchronize()
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        batch.capture_frame_compact(d_rays, d_begin, ph, bounce, bh, 7, s.cuda_stream)
+        batch.launch_frame(s.cuda_stream)
+        bh.fill_(-1)
+        batch.launch_frame(s.cuda_stream)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(ph.cpu().numpy(), eager_ph)
+    np.testing.assert_array_equal(bh.cpu().numpy(), eager_bh)
+    hit = (eager_ph.view(vx.HIT_DTYPE).reshape(-1)["flags"] & 1).astype(bool)
+    h = int(hit.sum())
+    assert 0 < h < n
+    want = eager_bounce.reshape(n, 2, 6)[hit].reshape(-1, 6)
+    np.testing.assert_array_equal(bounce.cpu().numpy()[:2 * h].view(np.uint32), want.view(np.uint32))
+
+
 def test_autotune_keeps_results(vx, cuda):
     import torch
     from vx_b200 import workloads as W

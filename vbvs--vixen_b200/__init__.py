@@ -139,6 +139,7 @@ def lib():
         "vx_spawn_shadow_rays": (C.c_int, [vp, vp, u32, vp, vp, vp]),
         "vx_bounce_table": (C.c_int, [vp]),
         "vx_batch_capture_frame": (C.c_int, [vp, vp, vp, u32, vp, vp, vp, vp, u64, vp]),
+        "vx_batch_capture_frame_compact": (C.c_int, [vp, vp, vp, u32, vp, vp, vp, u64, vp]),
         "vx_batch_launch_frame": (C.c_int, [vp, vp]),
         "vx_batch_set_bounce_tuning": (C.c_int, [vp, vp]),
         "vx_cast_batch_noalloc": (C.c_int, [vp, u32, vp, vp, u32, f32, f32, vp, vp]),
@@ -695,6 +696,13 @@ class Batch:
         check(lib().vx_batch_capture_frame(self._h, _p(primary), _p(primary_begin), primary.shape[0],
                                            _p(primary_hits), _p(bounce), _p(bounce_begin), _p(bounce_hits), seed,
                                            C.c_void_p(stream)))
+
+    def capture_frame_compact(self, primary, primary_begin, primary_hits, bounce, bounce_hits, seed, stream):
+        """vx_batch_capture_frame_compact: the bounce pass casts only the bounce rays of primary hits
+        (compacted into `bounce`, 2 * hits of its 2n rows); `bounce_hits` ends up as with capture_frame."""
+        check(lib().vx_batch_capture_frame_compact(self._h, _p(primary), _p(primary_begin), primary.shape[0],
+                                                   _p(primary_hits), _p(bounce), _p(bounce_hits), seed,
+                                                   C.c_void_p(stream)))
 
     def launch_frame(self, stream=None):
         check(lib().vx_batch_launch_frame(self._h, _stream(stream)))

@@ -41,7 +41,19 @@ struct BatchArgs {
     uint32_t K;      // rays per warp task
     int maxL;        // largest max_levels in the batch
     int refill;      // refill idle lanes once this many are idle (refilling kernels)
+    const uint32_t* map = nullptr;    // hit / counter slot of ray r (null: slot r)
+    const uint32_t* n_dev = nullptr;  // ray count known on the device only (null: n)
 };
+
+// Rays of the launch: n, or the device-side count when the rays were
+// compacted on the device (at most n).
+__device__ __forceinline__ uint32_t ray_count(const BatchArgs& a) {
+    return a.n_dev ? min(a.n, __ldg(a.n_dev)) : a.n;
+}
+
+__device__ __forceinline__ uint32_t out_slot(const BatchArgs& a, uint32_t r) {
+    return a.map ? __ldg(a.map + r) : r;
+}
 
 __device__ __forceinline__ int scene_of(const uint32_t* beg, uint32_t S, uint32_t r) {
     int lo = 0, hi = int(S);
@@ -105,6 +117,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_refill_kernel(BatchArgs a) 
     const uint32_t FULL = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t below = (1u << lane) - 1u;
+    const uint32_t n = ray_count(a);
     uint64_t next = 0, end = 0;  // warp-uniform cursor into the current task
     bool tasks_left = true;
     bool active = false;
@@ -121,8 +134,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_refill_kernel(BatchArgs a) 
                     if (lane == 0) t = atomicAdd(a.work, 1u);
                     t = __shfl_sync(FULL, t, 0);
                     next = uint64_t(t) * a.K;
-                    if (next >= a.n) { tasks_left = false; next = end = 0; break; }
-                    end = min(next + a.K, uint64_t(a.n));
+                    if (next >= n) { tasks_left = false; next = end = 0; break; }
+                    end = min(next + a.K, uint64_t(n));
                 }
                 const uint32_t avail = uint32_t(end - next);
                 const uint32_t rank = __popc(idle & below);
@@ -134,8 +147,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_refill_kernel(BatchArgs a) 
                     const float2* r2 = reinterpret_cast<const float2*>(a.rays + ray);
                     const float2 p = __ldg(r2), q = __ldg(r2 + 1), w = __ldg(r2 + 2);
                     if (cast_init(sc[sid], p.x, p.y, q.x, q.y, w.x, w.y, a.tmin, a.tmax, stkN, stkT, stride, st)) {
-                        store_hit(a.hits, ray, st.h);
-                        store_counters(a.counters, ray, st.h);
+                        store_hit(a.hits, out_slot(a, ray), st.h);
+                        store_counters(a.counters, out_slot(a, ray), st.h);
                     } else {
                         active = true;
                     }
@@ -149,8 +162,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_refill_kernel(BatchArgs a) 
             continue;
         }
         if (active && cast_step(sc[sid], st, stkN, stkT, cyc, stride)) {
-            store_hit(a.hits, ray, st.h);
-            store_counters(a.counters, ray, st.h);
+            store_hit(a.hits, out_slot(a, ray), st.h);
+            store_counters(a.counters, out_slot(a, ray), st.h);
             active = false;
         }
     }
@@ -189,21 +202,22 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
         stride = 1;
     }
     const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t n = ray_count(a);
     for (;;) {
         uint32_t t = 0;
         if (lane == 0) t = atomicAdd(a.work, 1u);
         t = __shfl_sync(0xFFFFFFFFu, t, 0);
         const uint64_t r0 = uint64_t(t) * a.K;
-        if (r0 >= a.n) break;
-        const uint32_t r1 = uint32_t(min(r0 + a.K, uint64_t(a.n)));
+        if (r0 >= n) break;
+        const uint32_t r1 = uint32_t(min(r0 + a.K, uint64_t(n)));
         for (uint32_t r = uint32_t(r0) + lane; r < r1; r += 32) {
             const int lo = scene_of(beg, a.S, r);
             const float2* r2 = reinterpret_cast<const float2*>(a.rays + r);
             const float2 p = __ldg(r2), q = __ldg(r2 + 1), w = __ldg(r2 + 2);
             Hit h;
             cast_ray(sc[lo], p.x, p.y, q.x, q.y, w.x, w.y, a.tmin, a.tmax, stkN, stkT, cyc, stride, h);
-            store_hit(a.hits, r, h);
-            store_counters(a.counters, r, h);
+            store_hit(a.hits, out_slot(a, r), h);
+            store_counters(a.counters, out_slot(a, r), h);
         }
     }
 }
@@ -231,6 +245,23 @@ __device__ __forceinline__ bool secondary_origin(const vx_ray& r, const vx_hit& 
     return true;
 }
 
+// Bounce ray k (0 or 1) of primary ray i from its secondary origin: table
+// direction j = mix64(seed ^ mix64(2i + k)) mod 4096, its z axis turned onto
+// the hit normal.
+__device__ __forceinline__ vx_ray bounce_ray(const float org[3], int axis, float sgn, uint64_t i, uint32_t k,
+                                             uint64_t seed) {
+    const uint32_t j = uint32_t(mix64(seed ^ mix64((i << 1) | k)) & (NUM_BOUNCE_DIRS - 1));
+    const float u = g_bounce_dirs[3 * j], v = g_bounce_dirs[3 * j + 1], w = g_bounce_dirs[3 * j + 2] * sgn;
+    vx_ray b;
+    b.ox = org[0];
+    b.oy = org[1];
+    b.oz = org[2];
+    if (axis == 0) { b.dx = w; b.dy = u; b.dz = v; }
+    else if (axis == 1) { b.dx = v; b.dy = w; b.dz = u; }
+    else { b.dx = u; b.dy = v; b.dz = w; }
+    return b;
+}
+
 __global__ void spawn_bounce_kernel(const vx_ray* __restrict__ rays, const vx_hit* __restrict__ hits, uint32_t n,
                                     uint64_t seed, vx_ray* __restrict__ out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -246,18 +277,7 @@ __global__ void spawn_bounce_kernel(const vx_ray* __restrict__ rays, const vx_hi
         out[2 * size_t(i) + 1] = z;
         return;
     }
-    for (uint32_t k = 0; k < 2; ++k) {
-        const uint32_t j = uint32_t(mix64(seed ^ mix64((uint64_t(i) << 1) | k)) & (NUM_BOUNCE_DIRS - 1));
-        const float u = g_bounce_dirs[3 * j], v = g_bounce_dirs[3 * j + 1], w = g_bounce_dirs[3 * j + 2] * sgn;
-        vx_ray b;
-        b.ox = org[0];
-        b.oy = org[1];
-        b.oz = org[2];
-        if (axis == 0) { b.dx = w; b.dy = u; b.dz = v; }
-        else if (axis == 1) { b.dx = v; b.dy = w; b.dz = u; }
-        else { b.dx = u; b.dy = v; b.dz = w; }
-        out[2 * size_t(i) + k] = b;
-    }
+    for (uint32_t k = 0; k < 2; ++k) out[2 * size_t(i) + k] = bounce_ray(org, axis, sgn, i, k, seed);
 }
 
 __global__ void spawn_shadow_kernel(const vx_ray* __restrict__ rays, const vx_hit* __restrict__ hits, uint32_t n,
@@ -274,6 +294,139 @@ __global__ void spawn_shadow_kernel(const vx_ray* __restrict__ rays, const vx_hi
         return;
     }
     out[i] = vx_ray{org[0], org[1], org[2], lx, ly, lz};
+}
+
+// Bounce-ray compaction of a frame: the bounce pass casts only the 2 rays of
+// every primary hit.  Primary rays go in chunks of COMPACT_CHUNK (256 threads
+// x 4 rounds); a chunk's hits are counted, the counts scanned, and each chunk
+// writes the bounce rays of its hits at 2 x (hits before them), in primary
+// order, with the hit slot (2i + k) of each in `map`.
+constexpr uint32_t COMPACT_CHUNK = 1024;
+
+__device__ __forceinline__ bool hit_flag(const vx_hit* hits, uint64_t i) {
+    return (reinterpret_cast<const uint4*>(hits)[i].w >> 16) & VX_HIT_HIT;
+}
+
+__global__ void __launch_bounds__(256) hit_count_kernel(const vx_hit* __restrict__ hits, uint32_t n,
+                                                        uint32_t* __restrict__ counts) {
+    __shared__ uint32_t part[8];
+    uint32_t c = 0;
+    for (uint32_t k = 0; k < 4; ++k) {
+        const uint64_t i = uint64_t(blockIdx.x) * COMPACT_CHUNK + k * 256 + threadIdx.x;
+        c += (i < n && hit_flag(hits, i)) ? 1u : 0u;
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xFFFFFFFFu, c, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < 8; ++w) t += part[w];
+        counts[blockIdx.x] = t;
+    }
+}
+
+// Exclusive scan of the chunk counts (one block, 1,024 chunks per round).
+__global__ void __launch_bounds__(1024) chunk_scan_kernel(const uint32_t* __restrict__ counts, uint32_t nb,
+                                                          uint32_t* __restrict__ offs) {
+    __shared__ uint32_t wsum[32];
+    __shared__ uint32_t carry;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < nb; base += 1024) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = i < nb ? counts[i] : 0u;
+        uint32_t x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if (lane >= uint32_t(o)) x += y;
+        }
+        if (lane == 31) wsum[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t w = wsum[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+                if (lane >= uint32_t(o)) w += y;
+            }
+            wsum[lane] = w;
+        }
+        __syncthreads();
+        const uint32_t excl = carry + (warp ? wsum[warp - 1] : 0u) + (x - v);
+        if (i < nb) offs[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = excl + v;
+        __syncthreads();
+    }
+}
+
+// The record a cast writes for a zero-direction ray (cast_init: the ray fails
+// validation before any scene data is read).
+__device__ __forceinline__ void store_invalid(vx_hit* hits, uint64_t slot) {
+    reinterpret_cast<uint4*>(hits)[slot] = make_uint4(0u, NONE, NONE, 0xFFFFu | (uint32_t(F_INVALID) << 16));
+}
+
+__global__ void __launch_bounds__(256) spawn_compact_kernel(const vx_ray* __restrict__ rays,
+                                                            const vx_hit* __restrict__ hits, uint32_t n,
+                                                            uint64_t seed, const uint32_t* __restrict__ offs,
+                                                            vx_ray* __restrict__ out, uint32_t* __restrict__ map,
+                                                            vx_hit* __restrict__ bounce_hits) {
+    __shared__ uint32_t wcount[8];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t run = offs[blockIdx.x];
+    for (uint32_t k = 0; k < 4; ++k) {
+        const uint64_t i = uint64_t(blockIdx.x) * COMPACT_CHUNK + k * 256 + threadIdx.x;
+        vx_ray r{};
+        vx_hit h{};
+        float org[3];
+        int axis = 0;
+        float sgn = 1.0f;
+        bool hit = false;
+        if (i < n) {
+            r = rays[i];
+            h = hits[i];
+            hit = secondary_origin(r, h, org, axis, sgn);
+        }
+        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, hit);
+        if (lane == 0) wcount[warp] = __popc(bal);
+        __syncthreads();
+        uint32_t before = 0, round = 0;
+        for (uint32_t w = 0; w < 8; ++w) {
+            before += w < warp ? wcount[w] : 0u;
+            round += wcount[w];
+        }
+        if (hit) {
+            const uint64_t pos = 2 * uint64_t(run + before + __popc(bal & ((1u << lane) - 1u)));
+            for (uint32_t b = 0; b < 2; ++b) {
+                out[pos + b] = bounce_ray(org, axis, sgn, i, b, seed);
+                map[pos + b] = uint32_t(2 * i + b);
+            }
+        } else if (i < n) {
+            store_invalid(bounce_hits, 2 * i);
+            store_invalid(bounce_hits, 2 * i + 1);
+        }
+        run += round;
+        __syncthreads();
+    }
+}
+
+// Per-scene offsets into the compacted bounce rays: 2 x (hits among the
+// primary rays before the scene's first ray); cbegin[S] is the bounce count.
+__global__ void compact_offsets_kernel(const vx_hit* __restrict__ hits, uint32_t n, const uint32_t* __restrict__ begin,
+                                       uint32_t S, const uint32_t* __restrict__ offs, const uint32_t* __restrict__ counts,
+                                       uint32_t nb, uint32_t* __restrict__ cbegin) {
+    for (uint32_t j = threadIdx.x; j <= S; j += blockDim.x) {
+        const uint32_t p = min(begin[j], n);
+        const uint32_t c = p / COMPACT_CHUNK;
+        uint32_t before;
+        if (c < nb) {
+            before = offs[c];
+            for (uint64_t i = uint64_t(c) * COMPACT_CHUNK; i < p; ++i) before += hit_flag(hits, i) ? 1u : 0u;
+        } else {
+            before = nb ? offs[nb - 1] + counts[nb - 1] : 0u;
+        }
+        cbegin[j] = 2 * before;
+    }
 }
 
 // The direction table (host), generated once: stratum-free cosine-weighted
@@ -332,6 +485,8 @@ struct vx_batch {
     int num_sms = 148;
     cudaGraphExec_t frame = nullptr;
     cudaGraph_t frame_graph = nullptr;
+    void* fscratch = nullptr;  // compacted frame: chunk counts and offsets, scene offsets, hit slots
+    uint64_t fscratch_bytes = 0;
 };
 
 namespace {
@@ -464,6 +619,7 @@ int vx_batch_destroy(vx_batch* b) {
     if (b->frame_graph) cudaGraphDestroy(b->frame_graph);
     cudaFree(b->scenes);
     cudaFree(b->work);
+    cudaFree(b->fscratch);
     delete b;
     return VX_OK;
 }
@@ -484,7 +640,8 @@ int vx_batch_get_tuning(const vx_batch* b, vx_batch_tuning* t) {
 namespace {
 
 int cast_batch_with(vx_batch* b, const vx_batch_tuning& t, const vx_ray* rays, const uint32_t* begin, uint32_t n,
-                    float tmin, float tmax, vx_hit* hits, vx_ray_counters* counters, void* stream) {
+                    float tmin, float tmax, vx_hit* hits, vx_ray_counters* counters, void* stream,
+                    const uint32_t* map = nullptr, const uint32_t* n_dev = nullptr) {
     if (!b || !begin || (n && (!rays || !hits))) return fail(VX_EINVAL, "vx_cast_batch: null argument");
     if (reinterpret_cast<uintptr_t>(rays) % 8 || reinterpret_cast<uintptr_t>(hits) % 16 ||
         reinterpret_cast<uintptr_t>(counters) % 16 || reinterpret_cast<uintptr_t>(begin) % 4)
@@ -494,7 +651,7 @@ int cast_batch_with(vx_batch* b, const vx_batch_tuning& t, const vx_ray* rays, c
     if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch: reset work counter");
     if (n == 0) return VX_OK;
     vx::BatchArgs a{b->scenes, b->S, begin, rays, n, tmin, tmax, hits, counters, b->work,
-                    uint32_t(t.rays_per_task), b->maxL, t.refill};
+                    uint32_t(t.rays_per_task), b->maxL, t.refill, map, n_dev};
     return launch_batch(b, t, a, st);
 }
 
@@ -626,6 +783,73 @@ int vx_batch_capture_frame(vx_batch* b, const vx_ray* primary, const uint32_t* p
     if (e != cudaSuccess) { cudaGraphDestroy(g); return cuda_err(e, "vx_batch_capture_frame: instantiate"); }
     b->frame_graph = g;
     return VX_OK;
+}
+
+static int vx_batch_capture_frame_compact_body(vx_batch* b, const vx_ray* primary, const uint32_t* primary_begin,
+                                               uint32_t n, vx_hit* primary_hits, vx_ray* bounce, vx_hit* bounce_hits,
+                                               uint64_t seed, void* stream) {
+    if (!b || !primary || !primary_begin || !primary_hits || !bounce || !bounce_hits || n == 0 || n > 0x7FFFFFFFu)
+        return fail(VX_EINVAL, "vx_batch_capture_frame_compact: bad argument");
+    if (reinterpret_cast<uintptr_t>(bounce) % 8 || reinterpret_cast<uintptr_t>(bounce_hits) % 16 ||
+        reinterpret_cast<uintptr_t>(primary_hits) % 16)
+        return fail(VX_EINVAL, "vx_batch_capture_frame_compact: misaligned buffer");
+    if (int r = vx::ensure_bounce_table()) return r;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (!st) return fail(VX_EINVAL, "vx_batch_capture_frame_compact: capture needs a non-default stream");
+    if (b->frame) { cudaGraphExecDestroy(b->frame); b->frame = nullptr; }
+    if (b->frame_graph) { cudaGraphDestroy(b->frame_graph); b->frame_graph = nullptr; }
+    if (int r = prepare_batch(b, b->tuning)) return r;
+    if (int r = prepare_batch(b, bounce_tuning_of(b))) return r;
+    // Scratch (allocated outside the capture): chunk counts, chunk offsets,
+    // the S + 1 scene offsets of the compacted rays and their 2n hit slots.
+    const uint32_t nb = (n + vx::COMPACT_CHUNK - 1) / vx::COMPACT_CHUNK;
+    auto a256 = [](uint64_t x) { return (x + 255) & ~uint64_t(255); };
+    const uint64_t o_offs = a256(uint64_t(nb) * 4), o_cbeg = o_offs + a256(uint64_t(nb) * 4);
+    const uint64_t o_map = o_cbeg + a256((uint64_t(b->S) + 1) * 4), need = o_map + a256(uint64_t(n) * 8);
+    if (need > b->fscratch_bytes) {
+        cudaFree(b->fscratch);
+        b->fscratch = nullptr;
+        b->fscratch_bytes = 0;
+        cudaError_t e = cudaMalloc(&b->fscratch, need);
+        if (e != cudaSuccess) return cuda_err(e, "vx_batch_capture_frame_compact: scratch");
+        b->fscratch_bytes = need;
+    }
+    char* base = static_cast<char*>(b->fscratch);
+    uint32_t* counts = reinterpret_cast<uint32_t*>(base);
+    uint32_t* offs = reinterpret_cast<uint32_t*>(base + o_offs);
+    uint32_t* cbegin = reinterpret_cast<uint32_t*>(base + o_cbeg);
+    uint32_t* map = reinterpret_cast<uint32_t*>(base + o_map);
+    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_err(e, "vx_batch_capture_frame_compact: begin capture");
+    int r = vx_cast_batch(b, primary, primary_begin, n, 0.0f, 3.402823466e+38f, primary_hits, nullptr, stream);
+    if (r == VX_OK) {
+        vx::hit_count_kernel<<<nb, 256, 0, st>>>(primary_hits, n, counts);
+        vx::chunk_scan_kernel<<<1, 1024, 0, st>>>(counts, nb, offs);
+        vx::spawn_compact_kernel<<<nb, 256, 0, st>>>(primary, primary_hits, n, seed, offs, bounce, map, bounce_hits);
+        vx::compact_offsets_kernel<<<1, 256, 0, st>>>(primary_hits, n, primary_begin, b->S, offs, counts, nb, cbegin);
+        const cudaError_t le = cudaGetLastError();
+        if (le != cudaSuccess) r = cuda_err(le, "vx_batch_capture_frame_compact: compaction launch");
+    }
+    if (r == VX_OK)
+        r = cast_batch_with(b, bounce_tuning_of(b), bounce, cbegin, 2 * n, 0.0f, 3.402823466e+38f, bounce_hits,
+                            nullptr, stream, map, cbegin + b->S);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(st, &g);
+    if (r != VX_OK) { if (g) cudaGraphDestroy(g); return r; }
+    if (e != cudaSuccess) return cuda_err(e, "vx_batch_capture_frame_compact: end capture");
+    e = cudaGraphInstantiate(&b->frame, g, 0);
+    if (e != cudaSuccess) { cudaGraphDestroy(g); return cuda_err(e, "vx_batch_capture_frame_compact: instantiate"); }
+    b->frame_graph = g;
+    return VX_OK;
+}
+
+int vx_batch_capture_frame_compact(vx_batch* b, const vx_ray* primary, const uint32_t* primary_begin, uint32_t n,
+                                   vx_hit* primary_hits, vx_ray* bounce, vx_hit* bounce_hits, uint64_t seed,
+                                   void* stream) {
+    return vx::guarded("vx_batch_capture_frame_compact", [&] {
+        return vx_batch_capture_frame_compact_body(b, primary, primary_begin, n, primary_hits, bounce, bounce_hits,
+                                                   seed, stream);
+    });
 }
 
 int vx_batch_launch_frame(vx_batch* b, void* stream) {
