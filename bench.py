@@ -681,8 +681,8 @@ def measure_tour(args):
     companions, each step timed with CUDA events (mean of 3 after 1 warm-up): noise synthesis,
     device builder with both payloads, the RGBA8 builder, plain / counting / LOD casts, the
     compressed render, per-hit normal decode, the payload encoders, the batched kernels (static
-    and refilling lanes, bounce and shadow spawn, the no-allocation entry point) and the
-    adjoint pair.  Meant as the command an ncu launch list or a per-kernel capture runs."""
+    and refilling lanes, bounce and shadow spawn, the no-allocation entry point, a frame with
+    bounce compaction) and the adjoint pair.  Meant as the command an ncu launch list or a per-kernel capture runs."""
     import math
     import numpy as np
     import torch
@@ -756,6 +756,14 @@ def measure_tour(args):
     shadow = torch.zeros_like(brays)
     out["spawn_shadow"] = ev_ms(lambda: vx.spawn_shadow_rays(brays, bh, [0.3, 0.8, 0.5], shadow))
     out["batch_noalloc"] = ev_ms(lambda: vx.cast_batch_noalloc([sc, sc_rgba], brays, begin, bh))
+    # a frame with bounce compaction (hit count, chunk scan, compacted spawn, scene offsets)
+    batch.set_tuning(256, 32, 1, 0)
+    batch.set_bounce_tuning(vx.BatchTuning(128, 256, 0, 24))
+    fs = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(fs):
+        batch.capture_frame_compact(brays, begin, bh, bounce, bbh, 77, fs.cuda_stream)
+        out["frame_compact"] = ev_ms(lambda: batch.launch_frame(fs.cuda_stream))
     batch.close()
     del bounce, bbh, shadow, brays, bh
     # adjoint pair on a 256^3 scene, 4 views of 512x512, per-voxel RGB and DXT1 endpoints
