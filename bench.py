@@ -1025,6 +1025,8 @@ def main():
         line["batched"] = {"workload": b["config"]["workload"], "rays_per_frame": b["config"]["rays_per_frame"],
                            "batched_mrays_s": b["batched"]["value"], "plain_mrays_s": b["plain"]["value"],
                            "speedup_batched_vs_plain": b["speedup_batched_vs_plain"],
+                           "batched_ms_per_frame": b["batched"]["ms_per_frame"],
+                           "batched_ms_per_frame_uncompacted": b["batched"]["ms_per_frame_uncompacted"],
                            "hits_identical": b["hits_identical_batched_vs_plain"], "tuning": b["batched"]["tuning"],
                            "steps": extra_steps}
         torch.cuda.empty_cache()
