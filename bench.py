@@ -650,8 +650,9 @@ def measure_next(args, steps, warmup):
     ms = dev_ms(lambda: s256.cast_rays_dev(r256, h256, c256))
     out["noise256_1080p"] = {"workload": "noise 256^3 (50% fill, DXT1), 1920x1080 primary rays, plain cast",
                              "mrays_s": r256.shape[0] / ms / 1e3, "ms_per_frame": ms,
-                             "published_context": "4,573 / 4,688 Mrays/s uncompressed / DXT, RTX 4080 Laptop, Vulkan "
-                                                  "(BASELINE.md section 1; not comparable hardware or scene instance)"}
+                             "published_context": "the reference's published runs of this shape: 4,573 / 4,688 "
+                                                  "Mrays/s uncompressed / DXT, RTX 4080 Laptop, Vulkan (not "
+                                                  "comparable hardware or scene instance)"}
     s256.close()
     del r256, h256, c256
     # scene cache file
