@@ -75,6 +75,10 @@ def test_null_arguments(vx):
     assert L.vx_cast_rays(None, None, 1, 0.0, 1.0, None, None, None, None) == -1
     assert L.vx_render(None, None, 1, 1, None, None, None, None) == -1
     assert L.vx_build_dense(None, 64, 6, None) == -1
+    assert L.vx_batch_capture_frame(None, None, None, 1, None, None, None, None, 0, None) == -1
+    assert L.vx_batch_capture_frame_compact(None, None, None, 1, None, None, None, 0, None) == -1
+    assert b"capture_frame_compact" in L.vx_last_error_string()
+    assert L.vx_batch_launch_frame(None, None) == -1
     assert L.vx_scene_destroy(None) == 0
 
 
