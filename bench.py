@@ -340,7 +340,7 @@ def measure_cfg4(args, rank, world, steps, warmup):
                        "l2": "flushed before every timed frame (256 MiB write)"},
             "batched": {"value": value, "unit": "Mrays/s", "ms_per_frame": batched_total / steps,
                         "frame": "vx_batch_capture_frame_compact: the bounce pass casts the 2 bounce rays of "
-                                 "each primary hit only",
+                                 "each primary hit only, per scene grouped by direction octant",
                         "ms_per_frame_uncompacted": full_total / steps,
                         "tuning": tuning.as_dict(), "autotune_best_ms_primary": tune_ms,
                         "bounce_tuning": btuning.as_dict(), "autotune_best_ms_bounce": btune_ms},

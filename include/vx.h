@@ -391,8 +391,10 @@ int vx_batch_capture_frame(vx_batch* batch, const vx_ray* primary_dev, const uin
                            void* stream);
 /* The same frame with the bounce rays compacted: the bounce pass casts only
  * the 2 rays of every primary hit.  bounce_dev (2n rays of scratch) receives
- * them in primary order, 2h of them for h primary hits; the frame computes the
- * per-scene offsets itself.  bounce_hits_dev (2n records) ends up exactly as
+ * them, 2h of them for h primary hits, per scene grouped by direction octant
+ * (primary order inside a group, the same order on every launch); the frame
+ * computes the per-scene offsets itself.  primary_begin_dev is read once, at
+ * capture (it must run from 0 to n and not decrease).  bounce_hits_dev (2n records) ends up exactly as
  * with vx_batch_capture_frame: slot 2i + k holds bounce k of primary ray i,
  * and the slots of primary misses hold the invalid-ray record a cast writes
  * for their zero-direction rays.  Scratch of about 8n bytes is allocated at

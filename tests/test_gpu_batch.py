@@ -137,10 +137,10 @@ def test_frame_graph_equals_eager(vx, cuda, bounce_tuning):
 @pytest.mark.parametrize("big,bounce_tuning", [(False, None), (False, (256, 256, 0, 24)), (True, (128, 64, 0, 16))])
 def test_compacted_frame_equals_eager(vx, cuda, big, bounce_tuning):
     """vx_batch_capture_frame_compact: primary and bounce hit records equal the eager frame's
-    (whose bounce pass casts all 2n slots, zero-direction rays included), and the compacted
-    bounce rays are the eager bounce rays of the primary hits in primary order.  `big`
-    (more than 2^20 primary rays) runs the chunk-count scan over several rounds and puts
-    scene boundaries inside chunks."""
+    (whose bounce pass casts all 2n slots, zero-direction rays included); the compacted bounce
+    rays are the eager bounce rays of the primary hits, per scene grouped by direction octant
+    in primary order, the same on every launch.  `big` (more than 2^20 primary rays) gives
+    scenes of many chunks with a partial last chunk."""
     import torch
     from vx_b200 import workloads as W
     if big:
@@ -175,16 +175,30 @@ def test_compacted_frame_equals_eager(vx, cuda, big, bounce_tuning):
     with torch.cuda.stream(s):
         batch.capture_frame_compact(d_rays, d_begin, ph, bounce, bh, 7, s.cuda_stream)
         batch.launch_frame(s.cuda_stream)
+    torch.cuda.synchronize()
+    first = bounce.cpu().numpy().copy()
+    with torch.cuda.stream(s):
         bh.fill_(-1)
+        bounce.zero_()
         batch.launch_frame(s.cuda_stream)
     torch.cuda.synchronize()
     np.testing.assert_array_equal(ph.cpu().numpy(), eager_ph)
     np.testing.assert_array_equal(bh.cpu().numpy(), eager_bh)
+    got = bounce.cpu().numpy()
+    np.testing.assert_array_equal(got.view(np.uint32), first.view(np.uint32))
     hit = (eager_ph.view(vx.HIT_DTYPE).reshape(-1)["flags"] & 1).astype(bool)
     h = int(hit.sum())
     assert 0 < h < n
-    want = eager_bounce.reshape(n, 2, 6)[hit].reshape(-1, 6)
-    np.testing.assert_array_equal(bounce.cpu().numpy()[:2 * h].view(np.uint32), want.view(np.uint32))
+    # expected order: scene, then octant of the direction, then (primary ray, k)
+    pair = eager_bounce.reshape(n, 2, 6)
+    scene = np.repeat(np.arange(len(begin) - 1), np.diff(begin.astype(np.int64)))
+    idx = np.flatnonzero(hit)
+    rows = pair[idx].reshape(-1, 6)
+    sc = np.repeat(scene[idx], 2)
+    octant = (rows[:, 3] > 0).astype(np.int64) | ((rows[:, 4] > 0).astype(np.int64) << 1) | \
+        ((rows[:, 5] > 0).astype(np.int64) << 2)
+    want = rows[np.lexsort((np.arange(rows.shape[0]), octant, sc))]
+    np.testing.assert_array_equal(got[:2 * h].view(np.uint32), want.view(np.uint32))
 
 
 def test_autotune_keeps_results(vx, cuda):

@@ -297,67 +297,92 @@ __global__ void spawn_shadow_kernel(const vx_ray* __restrict__ rays, const vx_hi
 }
 
 // Bounce-ray compaction of a frame: the bounce pass casts only the 2 rays of
-// every primary hit.  Primary rays go in chunks of COMPACT_CHUNK (256 threads
-// x 4 rounds); a chunk's hits are counted, the counts scanned, and each chunk
-// writes the bounce rays of its hits at 2 x (hits before them), in primary
-// order, with the hit slot (2i + k) of each in `map`.
+// every primary hit, grouped per scene by direction octant (rays that head the
+// same way through the same scene take similar paths through the octree), in
+// primary order inside a group.  The primary rays are split into chunks of at
+// most COMPACT_CHUNK rays that never straddle a scene (chunk c: rays
+// [start, end) of scene `scene`).  Per chunk and octant the bounce rays are
+// counted, the counts turned into offsets per scene and octant, and each chunk
+// writes its bounce rays at their place with the hit slot (2i + k) of each in
+// `map`.  Every position follows from the counts alone, so the order is the
+// same on every run.
 constexpr uint32_t COMPACT_CHUNK = 1024;
 
-__device__ __forceinline__ bool hit_flag(const vx_hit* hits, uint64_t i) {
-    return (reinterpret_cast<const uint4*>(hits)[i].w >> 16) & VX_HIT_HIT;
+struct CompactChunk {
+    uint32_t start, end, scene, pad;
+};
+
+__device__ __forceinline__ uint32_t octant_of(const vx_ray& r) {
+    return uint32_t(r.dx > 0.0f) | (uint32_t(r.dy > 0.0f) << 1) | (uint32_t(r.dz > 0.0f) << 2);
 }
 
-__global__ void __launch_bounds__(256) hit_count_kernel(const vx_hit* __restrict__ hits, uint32_t n,
-                                                        uint32_t* __restrict__ counts) {
-    __shared__ uint32_t part[8];
-    uint32_t c = 0;
-    for (uint32_t k = 0; k < 4; ++k) {
-        const uint64_t i = uint64_t(blockIdx.x) * COMPACT_CHUNK + k * 256 + threadIdx.x;
-        c += (i < n && hit_flag(hits, i)) ? 1u : 0u;
+// The 2 bounce rays of primary ray i, or false on a miss.
+__device__ __forceinline__ bool bounce_pair(const vx_ray* __restrict__ rays, const vx_hit* __restrict__ hits,
+                                            uint64_t i, uint64_t seed, vx_ray out[2]) {
+    const vx_ray r = rays[i];
+    const vx_hit h = hits[i];
+    float org[3];
+    int axis;
+    float sgn;
+    if (!secondary_origin(r, h, org, axis, sgn)) return false;
+    out[0] = bounce_ray(org, axis, sgn, i, 0, seed);
+    out[1] = bounce_ray(org, axis, sgn, i, 1, seed);
+    return true;
+}
+
+// counts[c * 8 + o]: bounce rays of chunk c heading into octant o.
+__global__ void __launch_bounds__(256) compact_count_kernel(const CompactChunk* __restrict__ chunks,
+                                                            const vx_ray* __restrict__ rays,
+                                                            const vx_hit* __restrict__ hits, uint64_t seed,
+                                                            uint32_t* __restrict__ counts) {
+    __shared__ uint32_t hist[8];
+    if (threadIdx.x < 8) hist[threadIdx.x] = 0;
+    __syncthreads();
+    const CompactChunk ch = chunks[blockIdx.x];
+    for (uint32_t i = ch.start + threadIdx.x; i < ch.end; i += blockDim.x) {
+        vx_ray b[2];
+        if (bounce_pair(rays, hits, i, seed, b)) {
+            atomicAdd(&hist[octant_of(b[0])], 1u);
+            atomicAdd(&hist[octant_of(b[1])], 1u);
+        }
     }
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xFFFFFFFFu, c, o);
-    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x < 8) counts[blockIdx.x * 8 + threadIdx.x] = hist[threadIdx.x];
+}
+
+// One block: offs[c * 8 + o] = bounce rays of scene s = chunk c's scene that
+// come before chunk c's octant-o rays in the compacted order, i.e. the rays of
+// the scenes before s, of s's octants below o, and of s's earlier chunks in
+// octant o.  cbegin[s] is scene s's first compacted ray, cbegin[S] the count.
+// tot (S * 8 words of scratch) holds the per-scene, per-octant totals.
+__global__ void __launch_bounds__(1024) compact_offsets_kernel(const uint32_t* __restrict__ counts,
+                                                               const uint32_t* __restrict__ first_chunk, uint32_t S,
+                                                               uint32_t* __restrict__ offs, uint32_t* __restrict__ tot,
+                                                               uint32_t* __restrict__ cbegin) {
+    for (uint32_t t = threadIdx.x; t < S * 8; t += blockDim.x) {
+        const uint32_t sc = t >> 3, o = t & 7u;
+        uint32_t run = 0;
+        for (uint32_t c = first_chunk[sc]; c < first_chunk[sc + 1]; ++c) {
+            offs[c * 8 + o] = run;
+            run += counts[c * 8 + o];
+        }
+        tot[t] = run;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
-        uint32_t t = 0;
-        for (int w = 0; w < 8; ++w) t += part[w];
-        counts[blockIdx.x] = t;
+        uint32_t run = 0;
+        for (uint32_t t = 0; t < S * 8; ++t) {
+            if ((t & 7u) == 0) cbegin[t >> 3] = run;
+            const uint32_t v = tot[t];
+            tot[t] = run;  // now the base of (scene, octant)
+            run += v;
+        }
+        cbegin[S] = run;
     }
-}
-
-// Exclusive scan of the chunk counts (one block, 1,024 chunks per round).
-__global__ void __launch_bounds__(1024) chunk_scan_kernel(const uint32_t* __restrict__ counts, uint32_t nb,
-                                                          uint32_t* __restrict__ offs) {
-    __shared__ uint32_t wsum[32];
-    __shared__ uint32_t carry;
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    for (uint32_t base = 0; base < nb; base += 1024) {
-        const uint32_t i = base + threadIdx.x;
-        const uint32_t v = i < nb ? counts[i] : 0u;
-        uint32_t x = v;
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
-            if (lane >= uint32_t(o)) x += y;
-        }
-        if (lane == 31) wsum[warp] = x;
-        __syncthreads();
-        if (warp == 0) {
-            uint32_t w = wsum[lane];
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
-                if (lane >= uint32_t(o)) w += y;
-            }
-            wsum[lane] = w;
-        }
-        __syncthreads();
-        const uint32_t excl = carry + (warp ? wsum[warp - 1] : 0u) + (x - v);
-        if (i < nb) offs[i] = excl;
-        __syncthreads();
-        if (threadIdx.x == 1023) carry = excl + v;
-        __syncthreads();
-    }
+    for (uint32_t sc = 0; sc < S; ++sc)
+        for (uint32_t c = first_chunk[sc] + threadIdx.x / 8; c < first_chunk[sc + 1]; c += blockDim.x / 8)
+            offs[c * 8 + (threadIdx.x & 7u)] += tot[sc * 8 + (threadIdx.x & 7u)];
 }
 
 // The record a cast writes for a zero-direction ray (cast_init: the ray fails
@@ -366,66 +391,59 @@ __device__ __forceinline__ void store_invalid(vx_hit* hits, uint64_t slot) {
     reinterpret_cast<uint4*>(hits)[slot] = make_uint4(0u, NONE, NONE, 0xFFFFu | (uint32_t(F_INVALID) << 16));
 }
 
-__global__ void __launch_bounds__(256) spawn_compact_kernel(const vx_ray* __restrict__ rays,
-                                                            const vx_hit* __restrict__ hits, uint32_t n,
-                                                            uint64_t seed, const uint32_t* __restrict__ offs,
-                                                            vx_ray* __restrict__ out, uint32_t* __restrict__ map,
-                                                            vx_hit* __restrict__ bounce_hits) {
-    __shared__ uint32_t wcount[8];
+// Writes chunk c's bounce rays at offs[c * 8 + o] + their rank among the
+// chunk's octant-o rays in (i, k) order; the slots of misses get the invalid
+// record.  256 primary rays per round: lane ranks by ballot per octant, warp
+// totals through shared memory, a running count per octant across rounds.
+__global__ void __launch_bounds__(256) compact_scatter_kernel(const CompactChunk* __restrict__ chunks,
+                                                              const vx_ray* __restrict__ rays,
+                                                              const vx_hit* __restrict__ hits, uint64_t seed,
+                                                              const uint32_t* __restrict__ offs,
+                                                              vx_ray* __restrict__ out, uint32_t* __restrict__ map,
+                                                              vx_hit* __restrict__ bounce_hits) {
+    __shared__ uint32_t wcnt[8][8];  // [warp][octant]
+    __shared__ uint32_t run[8];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    uint32_t run = offs[blockIdx.x];
-    for (uint32_t k = 0; k < 4; ++k) {
-        const uint64_t i = uint64_t(blockIdx.x) * COMPACT_CHUNK + k * 256 + threadIdx.x;
-        vx_ray r{};
-        vx_hit h{};
-        float org[3];
-        int axis = 0;
-        float sgn = 1.0f;
-        bool hit = false;
-        if (i < n) {
-            r = rays[i];
-            h = hits[i];
-            hit = secondary_origin(r, h, org, axis, sgn);
+    const uint32_t below = (1u << lane) - 1u;
+    const CompactChunk ch = chunks[blockIdx.x];
+    if (threadIdx.x < 8) run[threadIdx.x] = offs[blockIdx.x * 8 + threadIdx.x];
+    __syncthreads();
+    for (uint32_t base = ch.start; base < ch.end; base += 256) {
+        const uint32_t i = base + threadIdx.x;
+        vx_ray b[2];
+        const bool hit = i < ch.end && bounce_pair(rays, hits, i, seed, b);
+        const uint32_t o0 = hit ? octant_of(b[0]) : 8u, o1 = hit ? octant_of(b[1]) : 8u;
+        uint32_t r0 = 0, r1 = 0;
+#pragma unroll
+        for (uint32_t o = 0; o < 8; ++o) {
+            const uint32_t m0 = __ballot_sync(0xFFFFFFFFu, o0 == o), m1 = __ballot_sync(0xFFFFFFFFu, o1 == o);
+            const uint32_t before = __popc(m0 & below) + __popc(m1 & below);
+            if (o0 == o) r0 = before;
+            if (o1 == o) r1 = before + (o0 == o ? 1u : 0u);
+            if (lane == 0) wcnt[warp][o] = __popc(m0) + __popc(m1);
         }
-        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, hit);
-        if (lane == 0) wcount[warp] = __popc(bal);
         __syncthreads();
-        uint32_t before = 0, round = 0;
-        for (uint32_t w = 0; w < 8; ++w) {
-            before += w < warp ? wcount[w] : 0u;
-            round += wcount[w];
-        }
         if (hit) {
-            const uint64_t pos = 2 * uint64_t(run + before + __popc(bal & ((1u << lane) - 1u)));
-            for (uint32_t b = 0; b < 2; ++b) {
-                out[pos + b] = bounce_ray(org, axis, sgn, i, b, seed);
-                map[pos + b] = uint32_t(2 * i + b);
+            uint32_t p0 = run[o0] + r0, p1 = run[o1] + r1;
+            for (uint32_t w = 0; w < warp; ++w) {
+                p0 += wcnt[w][o0];
+                p1 += wcnt[w][o1];
             }
-        } else if (i < n) {
-            store_invalid(bounce_hits, 2 * i);
-            store_invalid(bounce_hits, 2 * i + 1);
+            out[p0] = b[0];
+            map[p0] = 2 * i;
+            out[p1] = b[1];
+            map[p1] = 2 * i + 1;
+        } else if (i < ch.end) {
+            store_invalid(bounce_hits, 2 * uint64_t(i));
+            store_invalid(bounce_hits, 2 * uint64_t(i) + 1);
         }
-        run += round;
         __syncthreads();
-    }
-}
-
-// Per-scene offsets into the compacted bounce rays: 2 x (hits among the
-// primary rays before the scene's first ray); cbegin[S] is the bounce count.
-__global__ void compact_offsets_kernel(const vx_hit* __restrict__ hits, uint32_t n, const uint32_t* __restrict__ begin,
-                                       uint32_t S, const uint32_t* __restrict__ offs, const uint32_t* __restrict__ counts,
-                                       uint32_t nb, uint32_t* __restrict__ cbegin) {
-    for (uint32_t j = threadIdx.x; j <= S; j += blockDim.x) {
-        const uint32_t p = min(begin[j], n);
-        const uint32_t c = p / COMPACT_CHUNK;
-        uint32_t before;
-        if (c < nb) {
-            before = offs[c];
-            for (uint64_t i = uint64_t(c) * COMPACT_CHUNK; i < p; ++i) before += hit_flag(hits, i) ? 1u : 0u;
-        } else {
-            before = nb ? offs[nb - 1] + counts[nb - 1] : 0u;
+        if (threadIdx.x < 8) {
+            uint32_t add = 0;
+            for (uint32_t w = 0; w < 8; ++w) add += wcnt[w][threadIdx.x];
+            run[threadIdx.x] += add;
         }
-        cbegin[j] = 2 * before;
+        __syncthreads();
     }
 }
 
@@ -800,33 +818,61 @@ static int vx_batch_capture_frame_compact_body(vx_batch* b, const vx_ray* primar
     if (b->frame_graph) { cudaGraphDestroy(b->frame_graph); b->frame_graph = nullptr; }
     if (int r = prepare_batch(b, b->tuning)) return r;
     if (int r = prepare_batch(b, bounce_tuning_of(b))) return r;
-    // Scratch (allocated outside the capture): chunk counts, chunk offsets,
+    // The chunk table follows the scene offsets, read once here: primary rays
+    // of scene s are [begin[s], begin[s + 1]), split into chunks of at most
+    // COMPACT_CHUNK rays.
+    std::vector<uint32_t> hb(size_t(b->S) + 1);
+    cudaError_t e = cudaMemcpyAsync(hb.data(), primary_begin, hb.size() * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_err(e, "vx_batch_capture_frame_compact: read scene offsets");
+    if (hb[0] != 0 || hb[b->S] != n)
+        return fail(VX_EINVAL, "vx_batch_capture_frame_compact: primary_begin must run from 0 to n");
+    std::vector<vx::CompactChunk> chunks;
+    std::vector<uint32_t> first(size_t(b->S) + 1, 0);
+    for (uint32_t sc = 0; sc < b->S; ++sc) {
+        if (hb[sc + 1] < hb[sc]) return fail(VX_EINVAL, "vx_batch_capture_frame_compact: primary_begin decreases");
+        first[sc] = uint32_t(chunks.size());
+        for (uint32_t a = hb[sc]; a < hb[sc + 1]; a += std::min(vx::COMPACT_CHUNK, hb[sc + 1] - a))
+            chunks.push_back(vx::CompactChunk{a, a + std::min(vx::COMPACT_CHUNK, hb[sc + 1] - a), sc, 0u});
+    }
+    first[b->S] = uint32_t(chunks.size());
+    const uint32_t nc = uint32_t(chunks.size());
+    // Scratch (allocated outside the capture): chunk table, per-chunk octant
+    // counts and offsets, first chunk of each scene, per-scene octant bases,
     // the S + 1 scene offsets of the compacted rays and their 2n hit slots.
-    const uint32_t nb = (n + vx::COMPACT_CHUNK - 1) / vx::COMPACT_CHUNK;
     auto a256 = [](uint64_t x) { return (x + 255) & ~uint64_t(255); };
-    const uint64_t o_offs = a256(uint64_t(nb) * 4), o_cbeg = o_offs + a256(uint64_t(nb) * 4);
+    const uint64_t o_cnt = a256(uint64_t(nc) * sizeof(vx::CompactChunk));
+    const uint64_t o_offs = o_cnt + a256(uint64_t(nc) * 32), o_first = o_offs + a256(uint64_t(nc) * 32);
+    const uint64_t o_tot = o_first + a256((uint64_t(b->S) + 1) * 4), o_cbeg = o_tot + a256(uint64_t(b->S) * 32);
     const uint64_t o_map = o_cbeg + a256((uint64_t(b->S) + 1) * 4), need = o_map + a256(uint64_t(n) * 8);
     if (need > b->fscratch_bytes) {
         cudaFree(b->fscratch);
         b->fscratch = nullptr;
         b->fscratch_bytes = 0;
-        cudaError_t e = cudaMalloc(&b->fscratch, need);
+        e = cudaMalloc(&b->fscratch, need);
         if (e != cudaSuccess) return cuda_err(e, "vx_batch_capture_frame_compact: scratch");
         b->fscratch_bytes = need;
     }
     char* base = static_cast<char*>(b->fscratch);
-    uint32_t* counts = reinterpret_cast<uint32_t*>(base);
+    auto* chunk_dev = reinterpret_cast<vx::CompactChunk*>(base);
+    uint32_t* counts = reinterpret_cast<uint32_t*>(base + o_cnt);
     uint32_t* offs = reinterpret_cast<uint32_t*>(base + o_offs);
+    uint32_t* first_dev = reinterpret_cast<uint32_t*>(base + o_first);
+    uint32_t* tot = reinterpret_cast<uint32_t*>(base + o_tot);
     uint32_t* cbegin = reinterpret_cast<uint32_t*>(base + o_cbeg);
     uint32_t* map = reinterpret_cast<uint32_t*>(base + o_map);
-    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    e = cudaMemcpyAsync(chunk_dev, chunks.data(), chunks.size() * sizeof(vx::CompactChunk), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(first_dev, first.data(), first.size() * 4, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_err(e, "vx_batch_capture_frame_compact: chunk table");
+    e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_err(e, "vx_batch_capture_frame_compact: begin capture");
     int r = vx_cast_batch(b, primary, primary_begin, n, 0.0f, 3.402823466e+38f, primary_hits, nullptr, stream);
     if (r == VX_OK) {
-        vx::hit_count_kernel<<<nb, 256, 0, st>>>(primary_hits, n, counts);
-        vx::chunk_scan_kernel<<<1, 1024, 0, st>>>(counts, nb, offs);
-        vx::spawn_compact_kernel<<<nb, 256, 0, st>>>(primary, primary_hits, n, seed, offs, bounce, map, bounce_hits);
-        vx::compact_offsets_kernel<<<1, 256, 0, st>>>(primary_hits, n, primary_begin, b->S, offs, counts, nb, cbegin);
+        vx::compact_count_kernel<<<nc, 256, 0, st>>>(chunk_dev, primary, primary_hits, seed, counts);
+        vx::compact_offsets_kernel<<<1, 1024, 0, st>>>(counts, first_dev, b->S, offs, tot, cbegin);
+        vx::compact_scatter_kernel<<<nc, 256, 0, st>>>(chunk_dev, primary, primary_hits, seed, offs, bounce, map,
+                                                       bounce_hits);
         const cudaError_t le = cudaGetLastError();
         if (le != cudaSuccess) r = cuda_err(le, "vx_batch_capture_frame_compact: compaction launch");
     }
