@@ -359,14 +359,23 @@ __global__ void __launch_bounds__(1024) compact_offsets_kernel(const uint32_t* _
                                                                const uint32_t* __restrict__ first_chunk, uint32_t S,
                                                                uint32_t* __restrict__ offs, uint32_t* __restrict__ tot,
                                                                uint32_t* __restrict__ cbegin) {
-    for (uint32_t t = threadIdx.x; t < S * 8; t += blockDim.x) {
-        const uint32_t sc = t >> 3, o = t & 7u;
+    // one warp per (scene, octant): exclusive scan over the scene's chunks, 32 at a time
+    const uint32_t lane = threadIdx.x & 31u, nwarps = blockDim.x >> 5;
+    for (uint32_t t = threadIdx.x >> 5; t < S * 8; t += nwarps) {
+        const uint32_t sc = t >> 3, o = t & 7u, end = first_chunk[sc + 1];
         uint32_t run = 0;
-        for (uint32_t c = first_chunk[sc]; c < first_chunk[sc + 1]; ++c) {
-            offs[c * 8 + o] = run;
-            run += counts[c * 8 + o];
+        for (uint32_t c0 = first_chunk[sc]; c0 < end; c0 += 32) {
+            const uint32_t c = c0 + lane;
+            const uint32_t v = c < end ? counts[c * 8 + o] : 0u;
+            uint32_t x = v;
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+                if (lane >= uint32_t(d)) x += y;
+            }
+            if (c < end) offs[c * 8 + o] = run + (x - v);
+            run += __shfl_sync(0xFFFFFFFFu, x, 31);
         }
-        tot[t] = run;
+        if (lane == 0) tot[t] = run;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
