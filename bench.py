@@ -219,8 +219,8 @@ def run_cfg4(args, rank, world):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["batched"]["ms_per_frame"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic", "config": res.pop("config"),
-                # per frame: primary cast, hit count, chunk scan, bounce spawn, scene offsets, bounce cast
-                "gpu_launches": args.steps * 6}
+                # per frame: primary cast, octant counts, offsets, compacted bounce spawn, bounce cast
+                "gpu_launches": args.steps * 5}
         line.update(res)
         print(json.dumps(line), flush=True)
     return 0
