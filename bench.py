@@ -373,33 +373,49 @@ def measure_cfg3(args, steps, warmup):
     sh = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
     L = W.light_dir(3)
 
-    def frame():
+    def frame_all_slots():  # shadow rays of all n slots, misses included (zero-direction rays)
         scene.cast_rays_dev(rays, hits, col)
         vx.spawn_shadow_rays(rays, hits, L, shadow)
         scene.cast_rays_dev(shadow, sh)
 
-    frame()
+    def frame():  # the shadow rays of the hits only, compacted on the device
+        scene.cast_rays_dev(rays, hits, col)
+        scene.cast_shadow_rays_dev(rays, hits, L, sh)
+
+    frame_all_slots()
     torch.cuda.synchronize()
     g = hits.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1)
     nhit = int(np.count_nonzero(g["flags"] & 1))
-    shit = int(np.count_nonzero(sh.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1)["flags"] & 1))
+    ref_sh = sh.cpu().numpy().copy()
+    shit = int(np.count_nonzero(ref_sh.view(vx.HIT_DTYPE).reshape(-1)["flags"] & 1))
+    sh.fill_(-1)
+    frame()
+    torch.cuda.synchronize()
+    same = bool(np.array_equal(sh.cpu().numpy(), ref_sh))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    for _ in range(warmup):
-        frame()
-    torch.cuda.synchronize()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
-    for a, b in ev:
-        flush.zero_()
-        a.record()
-        frame()
-        b.record()
-    torch.cuda.synchronize()
-    ms = sum(a.elapsed_time(b) for a, b in ev) / steps
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for a, b in ev:
+            flush.zero_()
+            a.record()
+            fn()
+            b.record()
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in ev) / steps
+
+    ms_all = timed(frame_all_slots)
+    ms = timed(frame)
     rays_per_frame = n + nhit
     return {"workload": f"{wl.name}: urban {wl.R}^3 (depth {wl.scene.max_levels}), 32x32 blocks, heights "
                         f"U[64,1800], DXT1; {wl.width}x{wl.height} primary + 1 shadow ray per hit",
             "ray_order": "primary rays in 8x4-pixel warp tiles (workloads.tile_order)",
-            "mrays_s": rays_per_frame / (ms / 1e3) / 1e6, "ms_per_frame": ms, "primary_rays": n,
+            "mrays_s": rays_per_frame / (ms / 1e3) / 1e6, "ms_per_frame": ms,
+            "frame": "primary cast, then vx_cast_shadow_rays (the shadow rays of hits, compacted)",
+            "ms_per_frame_all_slots": ms_all, "shadow_hits_equal_all_slots": same, "primary_rays": n,
             "shadow_rays": nhit, "primary_hit_rate": nhit / n, "shadowed_fraction": shit / max(nhit, 1),
             "bricks": bricks, "nodes": nodes, "scene_device_bytes": dev_bytes, "setup_s": setup_s}
 
@@ -845,7 +861,8 @@ def main():
             line = {"metric": METRIC, "value": res["mrays_s"], "unit": "Mrays/s", "n_gpus": 1, "steps": args.steps,
                     "warmup": args.warmup, "ms_per_step": res["ms_per_frame"], "higher_is_better": True,
                     "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                    "config": {"workload": res.pop("workload")}, "gpu_launches": args.steps * 3}
+                    # per frame: primary cast, shadow hit count, scan, compacted spawn, shadow cast
+                    "config": {"workload": res.pop("workload")}, "gpu_launches": args.steps * 5}
             line.update(res)
             print(json.dumps(line), flush=True)
         return 0

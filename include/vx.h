@@ -382,6 +382,20 @@ int vx_spawn_shadow_rays(const vx_ray* rays_dev, const vx_hit* hits_dev, uint32_
                          const float light_dir[3], vx_ray* out_dev, void* stream);
 int vx_bounce_table(float* out /* 4096 x 3 */);
 
+/* The shadow pass of a frame in one call: for every primary ray i with a hit,
+ * the shadow ray toward light_dir (vx_spawn_shadow_rays' ray), cast in
+ * [t_min, t_max]; shadow_hits_dev[i] receives exactly what
+ * vx_spawn_shadow_rays followed by vx_cast_rays over all n slots writes (the
+ * invalid-ray record for primary misses, whose shadow rays have no
+ * direction).  Only the rays of hits are cast: they are compacted on the
+ * device first.  No reference counterpart (the reference's shaders trace no
+ * secondary rays).  Uses scratch held by the scene (about 28 bytes per
+ * primary ray, allocated on the first call and when n grows); calls on the
+ * same scene that overlap on the GPU race on it. */
+int vx_cast_shadow_rays(const vx_scene* scene, const vx_ray* rays_dev, const vx_hit* hits_dev, uint32_t n,
+                        const float light_dir[3], float t_min, float t_max, vx_hit* shadow_hits_dev,
+                        void* stream);
+
 /* One frame as a CUDA graph: batched primary cast, bounce spawn, batched
  * bounce cast (bounce_begin = 2 x primary begin).  Capture needs a
  * non-default stream; launch replays it on any stream. */

@@ -140,6 +140,7 @@ def lib():
         "vx_bounce_table": (C.c_int, [vp]),
         "vx_batch_capture_frame": (C.c_int, [vp, vp, vp, u32, vp, vp, vp, vp, u64, vp]),
         "vx_batch_capture_frame_compact": (C.c_int, [vp, vp, vp, u32, vp, vp, vp, u64, vp]),
+        "vx_cast_shadow_rays": (C.c_int, [vp, vp, vp, u32, vp, C.c_float, C.c_float, vp, vp]),
         "vx_batch_launch_frame": (C.c_int, [vp, vp]),
         "vx_batch_set_bounce_tuning": (C.c_int, [vp, vp]),
         "vx_cast_batch_noalloc": (C.c_int, [vp, u32, vp, vp, u32, f32, f32, vp, vp]),
@@ -502,6 +503,13 @@ class Scene:
         else:
             check(lib().vx_cast_rays_lod(self._h, _p(rays), n, float(t_min), float(t_max), C.byref(_lod(lod)),
                                          _p(hits), _p(color), _p(counters), C.c_void_p(s)))
+
+    def cast_shadow_rays_dev(self, rays, hits, light_dir, shadow_hits, t_min=0.0, t_max=FLT_MAX, stream=None):
+        """vx_cast_shadow_rays: the shadow ray of every primary hit, compacted and cast; shadow_hits
+        (n,4) gets what spawn_shadow_rays + cast_rays_dev over all n slots would write."""
+        ld = (C.c_float * 3)(*[float(v) for v in light_dir])
+        check(lib().vx_cast_shadow_rays(self._h, _p(rays), _p(hits), rays.shape[0], ld, float(t_min), float(t_max),
+                                        _p(shadow_hits), _stream(stream)))
 
     def hit_normals_dev(self, hits, out, stream=None):
         """vx_hit_normals: hits (n,4) CUDA tensor -> out (n,3) float32 CUDA tensor."""

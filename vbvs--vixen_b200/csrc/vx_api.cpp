@@ -74,6 +74,9 @@ struct vx_scene {
     cudaStream_t pipe[2 + VX_PIPE_CAST_STREAMS] = {};  // copies in, copies out, casts
     cudaEvent_t pipe_start = nullptr;
     cudaEvent_t pipe_in[VX_PIPE_MAX_CHUNKS] = {}, pipe_cast[VX_PIPE_MAX_CHUNKS] = {};
+    // scratch of vx_cast_shadow_rays (compacted shadow rays and their slots), grown on demand
+    void* shadow = nullptr;
+    uint64_t shadow_bytes = 0;
 };
 
 namespace vx {
@@ -252,6 +255,7 @@ int vx_scene_destroy(vx_scene* s) {
     }
     cudaError_t e1 = cudaFree(s->pool);
     cudaError_t e2 = s->stage ? cudaFree(s->stage) : cudaSuccess;
+    if (s->shadow && e2 == cudaSuccess) e2 = cudaFree(s->shadow);
     if (dev >= 0 && dev != s->device) cudaSetDevice(dev);
     delete s;
     if (e1 != cudaSuccess) return vx::cuda_fail(e1, "vx_scene_destroy: cudaFree");
@@ -420,6 +424,41 @@ int cast_rays_host(const char* what, const vx_scene* cs, const vx_ray* rays_host
 int vx_cast_rays(const vx_scene* s, const vx_ray* rays, uint32_t n, float tmin, float tmax, vx_hit* hits,
                  void* color, vx_ray_counters* counters, void* stream) {
     return cast_rays_dev("vx_cast_rays", s, rays, n, tmin, tmax, nullptr, hits, color, counters, stream);
+}
+
+int vx_cast_shadow_rays(const vx_scene* cs, const vx_ray* rays, const vx_hit* hits, uint32_t n,
+                        const float light_dir[3], float tmin, float tmax, vx_hit* shadow_hits, void* stream) {
+    return vx::guarded("vx_cast_shadow_rays", [&]() -> int {
+        if (!cs || !light_dir || (n && (!rays || !hits || !shadow_hits)))
+            return fail(VX_EINVAL, "vx_cast_shadow_rays: null argument");
+        if (reinterpret_cast<uintptr_t>(rays) % 8 || reinterpret_cast<uintptr_t>(hits) % 16 ||
+            reinterpret_cast<uintptr_t>(shadow_hits) % 16)
+            return fail(VX_EINVAL, "vx_cast_shadow_rays: misaligned buffer");
+        if (std::isnan(tmin) || std::isnan(tmax)) return fail(VX_EINVAL, "vx_cast_shadow_rays: t_min / t_max is NaN");
+        if (n == 0) return VX_OK;
+        vx_scene* s = const_cast<vx_scene*>(cs);
+        int dev = -1;
+        cudaGetDevice(&dev);
+        if (dev != s->device) return fail(VX_EINVAL, "vx_cast_shadow_rays: the scene belongs to another device");
+        std::lock_guard<std::mutex> lk(s->stage_mu);
+        const uint64_t need = vx::shadow_scratch_bytes(n);
+        if (need > s->shadow_bytes) {
+            if (s->shadow) cudaFree(s->shadow);
+            s->shadow = nullptr;
+            s->shadow_bytes = 0;
+            const cudaError_t e = cudaMalloc(&s->shadow, need);
+            if (e != cudaSuccess) return vx::cuda_fail(e, "vx_cast_shadow_rays: cudaMalloc");
+            s->shadow_bytes = need;
+        }
+        vx_ray* crays = nullptr;
+        uint32_t* map = nullptr;
+        uint32_t* count = nullptr;
+        int r = vx::launch_shadow_compact(rays, hits, n, light_dir, s->shadow, &crays, &map, &count, shadow_hits, stream);
+        if (r != 0) return vx::cuda_fail(cudaError_t(r), "vx_cast_shadow_rays: compaction launch");
+        r = vx::launch_cast_mapped(s->dev, crays, n, count, map, tmin, tmax, shadow_hits, stream);
+        if (r != 0) return vx::cuda_fail(cudaError_t(r), "vx_cast_shadow_rays: launch");
+        return VX_OK;
+    });
 }
 
 int vx_cast_rays_lod(const vx_scene* s, const vx_ray* rays, uint32_t n, float tmin, float tmax,

@@ -456,6 +456,112 @@ __global__ void __launch_bounds__(256) compact_scatter_kernel(const CompactChunk
     }
 }
 
+// Shadow-ray compaction (vx_cast_shadow_rays): one shadow ray per primary
+// hit, in primary order.  Chunks of SHADOW_CHUNK primary rays: hits counted
+// per chunk, counts scanned (the total is the device-side ray count of the
+// cast), then each chunk writes its shadow rays at their offset with the
+// primary index of each in `map`, and the invalid record into the slots of
+// misses (what a cast writes for their zero-direction rays).
+constexpr uint32_t SHADOW_CHUNK = 1024;
+
+__device__ __forceinline__ bool hit_of(const vx_hit* hits, uint64_t i) {
+    return (reinterpret_cast<const uint4*>(hits)[i].w >> 16) & VX_HIT_HIT;
+}
+
+__global__ void __launch_bounds__(256) shadow_count_kernel(const vx_hit* __restrict__ hits, uint32_t n,
+                                                           uint32_t* __restrict__ counts) {
+    __shared__ uint32_t part[8];
+    uint32_t c = 0;
+    for (uint32_t k = 0; k < 4; ++k) {
+        const uint64_t i = uint64_t(blockIdx.x) * SHADOW_CHUNK + k * 256 + threadIdx.x;
+        c += (i < n && hit_of(hits, i)) ? 1u : 0u;
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xFFFFFFFFu, c, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < 8; ++w) t += part[w];
+        counts[blockIdx.x] = t;
+    }
+}
+
+// One block: exclusive scan of the nb chunk counts, 1,024 per round; *total
+// receives the sum.
+__global__ void __launch_bounds__(1024) shadow_scan_kernel(const uint32_t* __restrict__ counts, uint32_t nb,
+                                                           uint32_t* __restrict__ offs, uint32_t* __restrict__ total) {
+    __shared__ uint32_t wsum[32];
+    __shared__ uint32_t carry;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < nb; base += 1024) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = i < nb ? counts[i] : 0u;
+        uint32_t x = v;
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+            if (lane >= uint32_t(d)) x += y;
+        }
+        if (lane == 31) wsum[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t w = wsum[lane];
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, d);
+                if (lane >= uint32_t(d)) w += y;
+            }
+            wsum[lane] = w;
+        }
+        __syncthreads();
+        const uint32_t excl = carry + (warp ? wsum[warp - 1] : 0u) + (x - v);
+        if (i < nb) offs[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = excl + v;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void __launch_bounds__(256) shadow_scatter_kernel(const vx_ray* __restrict__ rays,
+                                                             const vx_hit* __restrict__ hits, uint32_t n, float lx,
+                                                             float ly, float lz, const uint32_t* __restrict__ offs,
+                                                             vx_ray* __restrict__ out, uint32_t* __restrict__ map,
+                                                             vx_hit* __restrict__ shadow_hits) {
+    __shared__ uint32_t wcount[8];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t run = offs[blockIdx.x];
+    for (uint32_t k = 0; k < 4; ++k) {
+        const uint64_t i = uint64_t(blockIdx.x) * SHADOW_CHUNK + k * 256 + threadIdx.x;
+        float org[3];
+        int axis = 0;
+        float sgn = 1.0f;
+        bool hit = false;
+        if (i < n) {
+            const vx_ray r = rays[i];
+            const vx_hit h = hits[i];
+            hit = secondary_origin(r, h, org, axis, sgn);
+        }
+        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, hit);
+        if (lane == 0) wcount[warp] = __popc(bal);
+        __syncthreads();
+        uint32_t before = 0, round = 0;
+        for (uint32_t w = 0; w < 8; ++w) {
+            before += w < warp ? wcount[w] : 0u;
+            round += wcount[w];
+        }
+        if (hit) {
+            const uint32_t pos = run + before + __popc(bal & ((1u << lane) - 1u));
+            out[pos] = vx_ray{org[0], org[1], org[2], lx, ly, lz};
+            map[pos] = uint32_t(i);
+        } else if (i < n) {
+            store_invalid(shadow_hits, i);
+        }
+        run += round;
+        __syncthreads();
+    }
+}
+
 // The direction table (host), generated once: stratum-free cosine-weighted
 // samples from a counter hash, evaluated in double and rounded to binary32.
 const std::vector<float>& bounce_table() {
@@ -780,6 +886,38 @@ int vx_spawn_shadow_rays(const vx_ray* rays, const vx_hit* hits, uint32_t n, con
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_spawn_shadow_rays");
 }
+
+}  // extern "C"
+
+namespace vx {
+
+uint64_t shadow_scratch_bytes(uint32_t n) {
+    const uint64_t nb = (uint64_t(n) + SHADOW_CHUNK - 1) / SHADOW_CHUNK;
+    auto a256 = [](uint64_t x) { return (x + 255) & ~uint64_t(255); };
+    return a256(nb * 4) * 2 + 256 + a256(uint64_t(n) * 4) + a256(uint64_t(n) * sizeof(vx_ray));
+}
+
+int launch_shadow_compact(const vx_ray* rays, const vx_hit* hits, uint32_t n, const float light_dir[3], void* scratch,
+                          vx_ray** out_rays, uint32_t** map, uint32_t** count, vx_hit* shadow_hits, void* stream) {
+    const uint32_t nb = (n + SHADOW_CHUNK - 1) / SHADOW_CHUNK;
+    auto a256 = [](uint64_t x) { return (x + 255) & ~uint64_t(255); };
+    char* base = static_cast<char*>(scratch);
+    uint32_t* counts = reinterpret_cast<uint32_t*>(base);
+    uint32_t* offs = reinterpret_cast<uint32_t*>(base + a256(uint64_t(nb) * 4));
+    *count = reinterpret_cast<uint32_t*>(base + 2 * a256(uint64_t(nb) * 4));
+    *map = reinterpret_cast<uint32_t*>(base + 2 * a256(uint64_t(nb) * 4) + 256);
+    *out_rays = reinterpret_cast<vx_ray*>(base + 2 * a256(uint64_t(nb) * 4) + 256 + a256(uint64_t(n) * 4));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    shadow_count_kernel<<<nb, 256, 0, st>>>(hits, n, counts);
+    shadow_scan_kernel<<<1, 1024, 0, st>>>(counts, nb, offs, *count);
+    shadow_scatter_kernel<<<nb, 256, 0, st>>>(rays, hits, n, light_dir[0], light_dir[1], light_dir[2], offs, *out_rays,
+                                              *map, shadow_hits);
+    return int(cudaGetLastError());
+}
+
+}  // namespace vx
+
+extern "C" {
 
 int vx_batch_capture_frame(vx_batch* b, const vx_ray* primary, const uint32_t* primary_begin, uint32_t n,
                            vx_hit* primary_hits, vx_ray* bounce, const uint32_t* bounce_begin, vx_hit* bounce_hits,

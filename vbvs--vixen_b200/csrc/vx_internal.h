@@ -89,6 +89,16 @@ struct CameraDev {
 int launch_render(const DevScene& s, const CameraDev& cam, uint32_t w, uint32_t h, uint32_t* image,
                   vx_hit* hits, void* color, void* stream);
 int launch_camera_rays(const CameraDev& cam, uint32_t w, uint32_t h, vx_ray* rays, void* stream);
+// cast of device-compacted rays: min(n_max, *count) rays, ray i's record to slot map[i]
+int launch_cast_mapped(const DevScene& s, const vx_ray* rays, uint32_t n_max, const uint32_t* count,
+                       const uint32_t* map, float tmin, float tmax, vx_hit* hits, void* stream);
+
+// Shadow-ray compaction (vx_batch.cu): scratch bytes for n primary rays, and
+// the launches that fill it (compacted rays, their slots, the device-side
+// count) and write the invalid record into the slots of primary misses.
+uint64_t shadow_scratch_bytes(uint32_t n);
+int launch_shadow_compact(const vx_ray* rays, const vx_hit* hits, uint32_t n, const float light_dir[3], void* scratch,
+                          vx_ray** out_rays, uint32_t** map, uint32_t** count, vx_hit* shadow_hits, void* stream);
 
 // Host camera setup shared by vx_render and vx_camera_rays: tan(radians(fov/2))
 // is evaluated once on the host (RayGeneration.glsl:62).

@@ -43,6 +43,26 @@ __global__ void __launch_bounds__(BLOCK, 768 / BLOCK) cast_kernel(DevScene s, co
     }
 }
 
+// The cast of rays compacted on the device: `count` (device) rays of at most
+// n_max, the hit record of ray i going to slot map[i].  The per-ray work is
+// cast_kernel's (castRay, no colour or counters).
+__global__ void __launch_bounds__(BLOCK, 768 / BLOCK) cast_mapped_kernel(DevScene s, const vx_ray* __restrict__ rays,
+                                                                        uint32_t n_max, const uint32_t* __restrict__ count,
+                                                                        const uint32_t* __restrict__ map, float tmin,
+                                                                        float tmax, vx_hit* __restrict__ hits) {
+    extern __shared__ uint32_t smem[];
+    uint32_t* stkN = smem + threadIdx.x;
+    float* stkT = reinterpret_cast<float*>(smem + s.max_levels * blockDim.x) + threadIdx.x;
+    uint32_t* cyc = smem + 2 * s.max_levels * blockDim.x + threadIdx.x;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= min(n_max, __ldg(count))) return;
+    const float2* r2 = reinterpret_cast<const float2*>(rays + i);
+    const float2 a = __ldg(r2), b = __ldg(r2 + 1), c = __ldg(r2 + 2);
+    Hit h;
+    cast_ray(s, a.x, a.y, b.x, b.y, c.x, c.y, tmin, tmax, stkN, stkT, cyc, blockDim.x, h);
+    store_hit(hits, __ldg(map + i), h);
+}
+
 // Pixels go to warps in 8 x 4 pieces of 32 x 8 tiles (the reference dispatches
 // 8 x 8 workgroups, ComputeDispatchNode.cpp:272-301): a warp's rays are
 // neighbours in both image directions, so their traversals diverge less than
@@ -149,6 +169,16 @@ int launch_cast(const DevScene& s, const vx_ray* rays, uint32_t n, float tmin, f
         cast_kernel<false><<<grid, BLOCK, smem, st>>>(s, rays, n, tmin, tmax, hits, color, counters,
                                                       LodCone{0.0f, 0.0f});
     }
+    return int(cudaGetLastError());
+}
+
+int launch_cast_mapped(const DevScene& s, const vx_ray* rays, uint32_t n_max, const uint32_t* count,
+                       const uint32_t* map, float tmin, float tmax, vx_hit* hits, void* stream) {
+    if (n_max == 0) return int(cudaSuccess);
+    const size_t smem = stack_bytes(s, BLOCK);
+    if (cudaError_t e = allow_smem(cast_mapped_kernel, smem)) return int(e);
+    cast_mapped_kernel<<<(n_max + BLOCK - 1) / BLOCK, BLOCK, smem, static_cast<cudaStream_t>(stream)>>>(
+        s, rays, n_max, count, map, tmin, tmax, hits);
     return int(cudaGetLastError());
 }
 
