@@ -67,6 +67,23 @@ def main(out_path):
     bbh = torch.zeros((bounce.shape[0], 4), dtype=torch.int32, device="cuda")
     batch.cast(bounce, torch.from_numpy(2 * begin).cuda(), bbh)
     out["bounce_hits"] = bbh.cpu().numpy()
+    # the frame with bounce compaction, and the compacted shadow pass
+    fh = torch.zeros_like(bh)
+    fbh = torch.zeros_like(bbh)
+    fs = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(fs):
+        batch.capture_frame_compact(br, bb, fh, bounce, fbh, 5, fs.cuda_stream)
+        batch.launch_frame(fs.cuda_stream)
+    torch.cuda.synchronize()
+    out.update(frame_hits=fh.cpu().numpy(), frame_bounce_hits=fbh.cpu().numpy())
+    sh = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+    s.cast_shadow_rays_dev(r, h, [0.3, 0.8, 0.5], sh)
+    srays = torch.zeros((n, 6), dtype=torch.float32, device="cuda")
+    vx.spawn_shadow_rays(r, h, [0.3, 0.8, 0.5], srays)
+    sh_all = torch.zeros_like(sh)
+    s.cast_rays_dev(srays, sh_all)
+    out.update(shadow_hits=sh.cpu().numpy(), shadow_hits_all_slots=sh_all.cpu().numpy())
     # adjoint
     dw = W.config5(R=128, views=3, width=64, height=48, kind=1, seed=45)
     s5 = vx.Scene(dw.wl.scene)

@@ -1,6 +1,7 @@
 """The bounds-checked build (libvx_checked.so, every device index tested before
 its load) on one of every device path (needs a B200): no index goes out of
-bounds, and every output equals the default build's bit for bit."""
+bounds, and every output equals the default build's bit for bit.  The compacted
+batched frame and the compacted shadow pass also equal their all-slots forms."""
 import os
 import subprocess
 import sys
@@ -35,3 +36,7 @@ def test_checked_build_has_no_violations_and_same_results(tmp_path):
             continue
         np.testing.assert_array_equal(checked[k].view(np.uint8), default[k].view(np.uint8), err_msg=k)
     assert int(default["diff_grad_nonzero"][0]) > 0
+    # the compacted frame reproduces the eager batched casts
+    np.testing.assert_array_equal(default["frame_hits"], default["batch_16"])
+    np.testing.assert_array_equal(default["frame_bounce_hits"], default["bounce_hits"])
+    np.testing.assert_array_equal(default["shadow_hits"], default["shadow_hits_all_slots"])
