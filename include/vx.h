@@ -12,8 +12,10 @@
  *    last error on the calling thread is in vx_last_error_string().  No C++
  *    exception crosses this boundary (the reference nodes throw
  *    std::runtime_error, ComputeDispatchNode.cpp:67,78,100,227).
- *  - A vx_scene is immutable after creation and may be used from any host
- *    thread; device work is ordered on the stream given to each call.
+ *  - A vx_scene's arrays are immutable after creation and it may be used
+ *    from any host thread; device work is ordered on the stream given to
+ *    each call.  Exception: vx_cast_shadow_rays keeps scratch in the scene,
+ *    so its calls on one scene must not overlap on the GPU.
  *  - "_dev" pointers are device pointers (cudaMalloc / torch tensors) on the
  *    scene's device; "_host" pointers are host memory (pinned for best speed).
  */
@@ -360,9 +362,11 @@ int vx_batch_autotune(vx_batch* batch, const vx_ray* rays_dev, const uint32_t* b
  * VX_NOALLOC_MAX_SCENES is rejected (VX_EOVERFLOW).  The first call on a
  * device resolves the array's address and the launch shape; make that first
  * call before any stream capture.  Every call shares the one array: the call
- * rewrites the table and clears the counter on its stream, and calls that
- * overlap on the GPU race.  Uses block 256, 32 rays per task, stack in shared
- * memory; hits are identical to vx_cast_batch. */
+ * rewrites the table and clears the counter on its stream (the table goes to
+ * a one-block staging kernel as a launch parameter, so the call copies nothing
+ * from host memory and does not wait on the stream), and calls that overlap on
+ * the GPU race.  Uses block 256, 32 rays per task, stack in shared memory;
+ * hits are identical to vx_cast_batch. */
 #define VX_NOALLOC_MAX_SCENES 64
 #define VX_NOALLOC_SCRATCH_BYTES 16384
 int vx_cast_batch_noalloc(const vx_scene* const* scenes, uint32_t count, const vx_ray* rays_dev,

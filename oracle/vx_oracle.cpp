@@ -193,6 +193,13 @@ struct vxo_scene {
 
 namespace {
 
+// splitmix64 finaliser: a well-spread 64-bit hash of a packed key.
+inline uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
 void setErr(char* err, int errlen, const std::string& m) {
     if (err && errlen > 0) {
         std::strncpy(err, m.c_str(), size_t(errlen) - 1);
@@ -234,10 +241,15 @@ bool rebuildHierarchy(vxo_scene& s, const std::vector<I3>& populated, std::strin
             return depth == o.depth && coord.x == o.coord.x && coord.y == o.coord.y && coord.z == o.coord.z;
         }
     };
+    // The maps below only change the order in which nodes enter
+    // tempDescriptors, which the BFS re-ordering removes; a mixing hash
+    // replaces the reference's xor of shifted coordinates (which puts most
+    // keys of a large scene into a few thousand buckets) without changing
+    // any output.
     struct NodeKeyHash {
         size_t operator()(const NodeKey& k) const {
-            return std::hash<int>{}(k.depth) ^ (std::hash<int>{}(k.coord.x) << 1) ^
-                   (std::hash<int>{}(k.coord.y) << 2) ^ (std::hash<int>{}(k.coord.z) << 3);
+            return size_t(mix64(uint64_t(uint32_t(k.depth)) << 60 ^ uint64_t(uint32_t(k.coord.x)) ^
+                                uint64_t(uint32_t(k.coord.y)) << 20 ^ uint64_t(uint32_t(k.coord.z)) << 40));
         }
     };
     std::unordered_map<NodeKey, uint32_t, NodeKeyHash> nodeToDescriptorIndex;
@@ -266,7 +278,8 @@ bool rebuildHierarchy(vxo_scene& s, const std::vector<I3>& populated, std::strin
     for (int currentDepth = brickDepth + 1; currentDepth <= s.maxLevels; ++currentDepth) {
         struct IH {
             size_t operator()(const I3& v) const {
-                return std::hash<int>{}(v.x) ^ (std::hash<int>{}(v.y) << 1) ^ (std::hash<int>{}(v.z) << 2);
+                return size_t(mix64(uint64_t(uint32_t(v.x)) ^ uint64_t(uint32_t(v.y)) << 21 ^
+                                    uint64_t(uint32_t(v.z)) << 42));
             }
         };
         struct IE {
@@ -1146,6 +1159,35 @@ void vxo_cast_rays_lod(const vxo_scene* s, const float* rays, uint64_t n, float 
     cast_rays_impl(s, rays, n, t_min, t_max, out, nthreads, &lod);
 }
 
+// Primary rays of the compute shader: the pixel uv of VoxelRayMarch.comp:453-455,
+// uv = (vec2(pixel) + 0.5) / vec2(imageSize), and getRayDir
+// (shaders/RayGeneration.glsl:61-71) with the push constants of
+// VoxelRayMarch.comp:85-94 (pc: 16 words, fov in degrees).  Expressions are
+// evaluated left to right as GLSL writes them; normalize is glm's
+// v * (1 / sqrt(dot(v, v))) (the CPU column), radians(x) = x * (pi / 180).
+// out: w * h rays {origin, direction}, row-major from the top row; uv_y
+// (optional): each pixel's uv.y, which the miss colour reads.
+void vxo_camera_rays(const float pc[16], uint32_t w, uint32_t h, float* out, float* uv_y) {
+    const V3 camPos{pc[0], pc[1], pc[2]}, camDir{pc[4], pc[5], pc[6]};
+    const V3 camUp{pc[8], pc[9], pc[10]}, camRight{pc[12], pc[13], pc[14]};
+    const float fov = pc[7], aspect = pc[11];
+    const float tanHalfFov = std::tan((fov * 0.5f) * 0.0174532925199432957692f);
+    for (uint32_t py = 0; py < h; ++py)
+        for (uint32_t px = 0; px < w; ++px) {
+            const float uvx = (float(px) + 0.5f) / float(w);
+            const float uvy = (float(py) + 0.5f) / float(h);
+            const float ndcx = uvx * 2.0f - 1.0f;
+            const float ndcy = -(uvy * 2.0f - 1.0f);
+            const V3 rayDir = (camDir + ((camRight * ndcx) * tanHalfFov) * aspect) + (camUp * ndcy) * tanHalfFov;
+            const float inv = 1.0f / std::sqrt(dot(rayDir, rayDir));
+            const V3 d = rayDir * inv;
+            float* r = out + (uint64_t(py) * w + px) * 6;
+            r[0] = camPos.x; r[1] = camPos.y; r[2] = camPos.z;
+            r[3] = d.x; r[4] = d.y; r[5] = d.z;
+            if (uv_y) uv_y[uint64_t(py) * w + px] = uvy;
+        }
+}
+
 // LODParameters::fromCameraWithNearPlane (SVOLOD.h:105-119); near_plane = 0
 // gives fromCamera (:83-92).
 void vxo_lod_from_camera(float fov_y, int32_t screen_height, float near_plane, float out[2]) {
@@ -1239,6 +1281,18 @@ void vxo_hit_texel_dxt(const uint64_t* brick_dxt, uint32_t brick, uint32_t voxel
     vxo_dxt1_decode_head(uint32_t(block), ref);
     uint32_t sel = (uint32_t(block >> 32) >> ((voxel & 15) * 2)) & 3;
     out[0] = ref[3 * sel]; out[1] = ref[3 * sel + 1]; out[2] = ref[3 * sel + 2];
+}
+
+// vxo_hit_texel_dxt over n hit records; misses (brick 0xFFFFFFFF) give zeros.
+void vxo_hit_texels_dxt(const uint64_t* brick_dxt, uint64_t n, const uint32_t* brick, const uint32_t* voxel,
+                        float* out) {
+    for (uint64_t i = 0; i < n; ++i) {
+        if (brick[i] == 0xFFFFFFFFu) {
+            out[3 * i] = out[3 * i + 1] = out[3 * i + 2] = 0.0f;
+        } else {
+            vxo_hit_texel_dxt(brick_dxt, brick[i], voxel[i], out + 3 * i);
+        }
+    }
 }
 
 // computeLighting (shaders/Lighting.glsl:19-28); sky colour (VoxelRayMarch.comp:493-499).

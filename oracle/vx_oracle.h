@@ -109,7 +109,13 @@ uint64_t vxo_dxt1_encode_block(const float* colors, uint64_t valid_count,
 
 /* Colour fetch of a hit, restating the compressed shader's addressing
  * (VoxelRayMarch_Compressed.comp:142-158): block = voxel >> 4, texel = voxel & 15. */
+/* Primary rays of a camera (VoxelRayMarch.comp:453-455, RayGeneration.glsl:61-71):
+ * pc = the 64-byte push constants as 16 words; out: w*h x 6 floats, row-major
+ * from the top row; uv_y (may be NULL): each pixel's uv.y. */
+void vxo_camera_rays(const float pc[16], uint32_t w, uint32_t h, float* out, float* uv_y);
 void vxo_hit_texel_dxt(const uint64_t* brick_dxt, uint32_t brick, uint32_t voxel, float out[3]);
+void vxo_hit_texels_dxt(const uint64_t* brick_dxt, uint64_t n, const uint32_t* brick, const uint32_t* voxel,
+                        float* out);
 
 /* Lambert shading of a hit colour (Lighting.glsl:19-28) and the sky colour on
  * a miss (VoxelRayMarch.comp:493-499); returns RGBA8 like an UNORM imageStore. */

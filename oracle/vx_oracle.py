@@ -62,6 +62,8 @@ def lib():
         L.vxo_dxt1_encode_block.restype = u64
         L.vxo_dxt1_encode_block.argtypes = [vp, u64, vp]
         L.vxo_hit_texel_dxt.argtypes = [vp, u32, u32, vp]
+        L.vxo_camera_rays.argtypes = [vp, u32, u32, vp, vp]
+        L.vxo_hit_texels_dxt.argtypes = [vp, u64, vp, vp, vp]
         L.vxo_shade.restype = u32
         L.vxo_shade.argtypes = [vp, C.c_int, C.c_int, C.c_int, f32]
         L.vxo_dxtn_encode_block.argtypes = [vp, u64, vp, vp]
@@ -279,6 +281,32 @@ def hit_texel_dxt(brick_dxt: np.ndarray, brick: int, voxel: int) -> np.ndarray:
     out = np.zeros(3, np.float32)
     d = np.ascontiguousarray(brick_dxt, dtype=np.uint64)
     lib().vxo_hit_texel_dxt(_ptr(d), brick, voxel, _ptr(out))
+    return out
+
+
+def camera_rays(pc, width: int, height: int, with_uv_y: bool = False):
+    """Primary rays of the shader's camera (getRayDir, RayGeneration.glsl:61-71; uv,
+    VoxelRayMarch.comp:453-455).  pc: the 64-byte push-constant block (any object exposing
+    the buffer protocol, e.g. a ctypes structure) or 16 floats.  Returns (width*height, 6)
+    float32 rows {origin, direction}, row-major from the top row (and uv.y per pixel)."""
+    if isinstance(pc, np.ndarray):
+        words = np.ascontiguousarray(pc, dtype=np.float32)
+    else:
+        words = np.frombuffer(bytes(memoryview(pc)), dtype=np.float32).copy()
+    assert words.size == 16
+    out = np.zeros((width * height, 6), np.float32)
+    uv = np.zeros(width * height, np.float32) if with_uv_y else None
+    lib().vxo_camera_rays(_ptr(words), width, height, _ptr(out), _ptr(uv))
+    return (out, uv) if with_uv_y else out
+
+
+def hit_texels_dxt(brick_dxt: np.ndarray, hits: np.ndarray) -> np.ndarray:
+    """DXT1 texel (n x 3 float) of every oracle hit record; zeros where brick is 0xFFFFFFFF."""
+    d = np.ascontiguousarray(brick_dxt, dtype=np.uint64)
+    b = np.ascontiguousarray(hits["brick"], dtype=np.uint32)
+    v = np.ascontiguousarray(hits["voxel"], dtype=np.uint32)
+    out = np.zeros((b.size, 3), np.float32)
+    lib().vxo_hit_texels_dxt(_ptr(d), b.size, _ptr(b), _ptr(v), _ptr(out))
     return out
 
 

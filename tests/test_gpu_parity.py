@@ -229,16 +229,22 @@ def test_host_entry_point_pipelined_chunks(vx, cuda, n):
     np.testing.assert_array_equal(cd.view(np.uint32), ch.view(np.uint32))
 
 
-def test_camera_rays_device_equal_host(vx, cuda):
+def test_camera_rays_device_equal_oracle(vx, vo, cuda):
+    """vx_camera_rays_dev equals the oracle's restatement of getRayDir (RayGeneration.glsl:61-71)
+    and the shader's pixel uv (VoxelRayMarch.comp:453-455) bit for bit, as does the host form."""
+    import ctypes as C
     import torch
     from vx_b200 import workloads as W
-    pc = W.look_camera([10.5, 20.25, -3.0], [0.3, -0.2, 1.0], 70.0, 333, 177)
-    host = vx.camera_rays(pc, 333, 177)
-    dev = torch.zeros((333 * 177, 6), dtype=torch.float32, device="cuda")
-    import ctypes as C
-    vx.check(vx.lib().vx_camera_rays_dev(C.byref(pc), 333, 177, C.c_void_p(dev.data_ptr()), None))
-    torch.cuda.synchronize()
-    np.testing.assert_array_equal(dev.cpu().numpy().view(np.uint32), host.view(np.uint32))
+    for pos, d, fov, w, h in [([10.5, 20.25, -3.0], [0.3, -0.2, 1.0], 70.0, 333, 177),
+                              ([512.5, 100.0, 3.0], [-0.7, 0.1, 0.2], 60.0, 1920, 1080),
+                              ([1.0, 2.0, 3.0], [0.0, -1.0, 0.0], 90.0, 64, 64)]:
+        pc = W.look_camera(pos, d, fov, w, h)
+        want = vo.camera_rays(pc, w, h)
+        dev = torch.zeros((w * h, 6), dtype=torch.float32, device="cuda")
+        vx.check(vx.lib().vx_camera_rays_dev(C.byref(pc), w, h, C.c_void_p(dev.data_ptr()), None))
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(dev.cpu().numpy().view(np.uint32), want.view(np.uint32))
+        np.testing.assert_array_equal(vx.camera_rays(pc, w, h).view(np.uint32), want.view(np.uint32))
 
 
 def test_render_matches_oracle_shading(vx, vo, cuda):
@@ -254,7 +260,9 @@ def test_render_matches_oracle_shading(vx, vo, cuda):
     g = hits.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1)
     image = img.cpu().numpy().view(np.uint32)
     o = vo.OracleScene.from_dense(wl.bits, 128, wl.scene.max_levels)
-    rays = wl.rays()
+    # the render kernel's in-kernel rays are checked through its hits: the oracle casts the rays of
+    # its own restatement of the shader's ray generation
+    rays, uv_y = vo.camera_rays(wl.camera, wl.width, wl.height, with_uv_y=True)
     oh = o.cast_rays(rays)
     assert_hits_equal(g, oh, None, "render hits")
     for i in range(n):
@@ -264,8 +272,7 @@ def test_render_matches_oracle_shading(vx, vo, cuda):
             col = np.array([c & 255, (c >> 8) & 255, (c >> 16) & 255], np.float32) / np.float32(255.0)
         else:
             col = np.zeros(3, np.float32)
-        uv_y = (np.float32(i // wl.width) + np.float32(0.5)) / np.float32(wl.height)
-        want = vo.shade(col, hit, (int(oh["flags"][i]) >> 1) & 3, bool(oh["flags"][i] & 8), float(uv_y))
+        want = vo.shade(col, hit, (int(oh["flags"][i]) >> 1) & 3, bool(oh["flags"][i] & 8), float(uv_y[i]))
         assert image[i] == want, (i, hex(image[i]), hex(want))
 
 

@@ -253,13 +253,14 @@ int vx_scene_destroy(vx_scene* s) {
         if (s->pipe_in[i]) cudaEventDestroy(s->pipe_in[i]);
         if (s->pipe_cast[i]) cudaEventDestroy(s->pipe_cast[i]);
     }
-    cudaError_t e1 = cudaFree(s->pool);
-    cudaError_t e2 = s->stage ? cudaFree(s->stage) : cudaSuccess;
-    if (s->shadow && e2 == cudaSuccess) e2 = cudaFree(s->shadow);
+    // Every buffer is freed whatever the others' outcome; the first error is reported.
+    const cudaError_t e1 = cudaFree(s->pool);
+    const cudaError_t e2 = s->stage ? cudaFree(s->stage) : cudaSuccess;
+    const cudaError_t e3 = s->shadow ? cudaFree(s->shadow) : cudaSuccess;
     if (dev >= 0 && dev != s->device) cudaSetDevice(dev);
     delete s;
-    if (e1 != cudaSuccess) return vx::cuda_fail(e1, "vx_scene_destroy: cudaFree");
-    if (e2 != cudaSuccess) return vx::cuda_fail(e2, "vx_scene_destroy: cudaFree");
+    for (cudaError_t e : {e1, e2, e3})
+        if (e != cudaSuccess) return vx::cuda_fail(e, "vx_scene_destroy: cudaFree");
     return VX_OK;
 }
 

@@ -1069,6 +1069,28 @@ static_assert(NOALLOC_TABLE_OFFSET + VX_NOALLOC_MAX_SCENES * sizeof(DevScene) <=
               "no-alloc scratch too small for its scene table");
 static __device__ __align__(256) unsigned char g_noalloc_scratch[VX_NOALLOC_SCRATCH_BYTES];
 
+// The call's scene table travels as a kernel parameter (64 x 176 B, inside the
+// 32 KB parameter limit of CUDA 12.1+), so staging it into the scratch is a
+// stream-ordered kernel: no host-to-device copy from pageable memory, which
+// would wait on the caller's stream.
+struct NoallocTable {
+    DevScene scene[VX_NOALLOC_MAX_SCENES];
+    uint32_t count;
+};
+static_assert(sizeof(NoallocTable) <= 32000, "no-alloc scene table exceeds the kernel parameter space");
+
+// One block: writes the first `count` table entries behind the counter and
+// clears the counter (the previous call left its final value there).
+__global__ void __launch_bounds__(256) noalloc_stage_kernel(const __grid_constant__ NoallocTable t,
+                                                            unsigned char* scratch) {
+    constexpr uint32_t WORDS = sizeof(DevScene) / 4;
+    static_assert(sizeof(DevScene) % 4 == 0, "DevScene is copied word by word");
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(t.scene);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(scratch + NOALLOC_TABLE_OFFSET);
+    for (uint32_t i = threadIdx.x; i < t.count * WORDS; i += blockDim.x) dst[i] = src[i];
+    if (threadIdx.x == 0) *reinterpret_cast<uint32_t*>(scratch) = 0u;
+}
+
 struct NoallocDevice {
     bool ready = false;
     unsigned char* scratch = nullptr;  // device address of g_noalloc_scratch on this device
@@ -1124,24 +1146,24 @@ static int vx_cast_batch_noalloc_body(const vx_scene* const* scenes, uint32_t co
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch_noalloc: cudaGetDevice");
     if (dev < 0 || dev >= 64) return fail(VX_EINVAL, "vx_cast_batch_noalloc: device ordinal out of range");
-    DevScene table[VX_NOALLOC_MAX_SCENES];
+    NoallocTable table{};
+    table.count = count;
     int maxL = 1;
     for (uint32_t i = 0; i < count; ++i) {
         if (!scenes[i]) return fail(VX_EINVAL, "vx_cast_batch_noalloc: null scene");
         if (scene_device(scenes[i]) != dev)
             return fail(VX_EINVAL, "vx_cast_batch_noalloc: every scene must live on the current device");
-        table[i] = scene_dev(scenes[i]);
-        maxL = std::max(maxL, table[i].max_levels);
+        table.scene[i] = scene_dev(scenes[i]);
+        maxL = std::max(maxL, table.scene[i].max_levels);
     }
     NoallocDevice* d = nullptr;
     if (int r = noalloc_setup(dev, d)) return r;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     // The scratch keeps the previous call's contents: rewrite the scene table
     // and clear the task counter on this call's stream.
-    e = cudaMemcpyAsync(d->scratch + NOALLOC_TABLE_OFFSET, table, count * sizeof(DevScene), cudaMemcpyHostToDevice,
-                        st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(d->scratch, 0, 4, st);
-    if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch_noalloc: scratch upload");
+    noalloc_stage_kernel<<<1, 256, 0, st>>>(table, d->scratch);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch_noalloc: scratch staging");
     if (n == 0) return VX_OK;
     BatchArgs a{reinterpret_cast<const DevScene*>(d->scratch + NOALLOC_TABLE_OFFSET), count, begin, rays, n, tmin,
                 tmax, hits, nullptr, reinterpret_cast<uint32_t*>(d->scratch), 32u, maxL};
