@@ -109,6 +109,19 @@ uint64_t vxo_dxt1_encode_block(const float* colors, uint64_t valid_count,
 
 /* Colour fetch of a hit, restating the compressed shader's addressing
  * (VoxelRayMarch_Compressed.comp:142-158): block = voxel >> 4, texel = voxel & 15. */
+/* Seeded synthetic inputs of the benchmark frames (vx_oracle_synth.cpp): the
+ * same bits as the product's vx_synth_noise / vx_synth_urban /
+ * vx_bounce_table / vx_spawn_*_rays, computed without the product library.
+ * threads = 0: all cores.  Return 0, or -1 on bad arguments. */
+int vxo_synth_noise(uint32_t R, uint32_t spacing, uint32_t octaves, float fill, uint64_t seed, int32_t shell,
+                    uint64_t* out, int threads);
+int vxo_synth_urban(uint32_t R, uint32_t hmin, uint32_t hmax, uint64_t seed, uint64_t* out);
+void vxo_bounce_table(float* out /* 4096 x 3 */);
+/* kind 0: 2 bounce rays per ray (out 2n x 6); kind 1: a shadow ray toward
+ * light (out n x 6).  index: each ray's position in its frame (NULL: i). */
+void vxo_spawn_rays(const float* rays, const vxo_hit* hits, const uint64_t* index, uint64_t n, int kind,
+                    uint64_t seed, const float light[3], float* out);
+
 /* Primary rays of a camera (VoxelRayMarch.comp:453-455, RayGeneration.glsl:61-71):
  * pc = the 64-byte push constants as 16 words; out: w*h x 6 floats, row-major
  * from the top row; uv_y (may be NULL): each pixel's uv.y. */

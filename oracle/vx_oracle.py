@@ -63,6 +63,12 @@ def lib():
         L.vxo_dxt1_encode_block.argtypes = [vp, u64, vp]
         L.vxo_hit_texel_dxt.argtypes = [vp, u32, u32, vp]
         L.vxo_camera_rays.argtypes = [vp, u32, u32, vp, vp]
+        L.vxo_synth_noise.restype = C.c_int
+        L.vxo_synth_noise.argtypes = [u32, u32, u32, f32, u64, i32, vp, C.c_int]
+        L.vxo_synth_urban.restype = C.c_int
+        L.vxo_synth_urban.argtypes = [u32, u32, u32, u64, vp]
+        L.vxo_bounce_table.argtypes = [vp]
+        L.vxo_spawn_rays.argtypes = [vp, vp, vp, u64, C.c_int, u64, vp, vp]
         L.vxo_hit_texels_dxt.argtypes = [vp, u64, vp, vp, vp]
         L.vxo_shade.restype = u32
         L.vxo_shade.argtypes = [vp, C.c_int, C.c_int, C.c_int, f32]
