@@ -1,17 +1,26 @@
 #!/usr/bin/env python
 """Benchmark of the ESVO ray-casting path on B200.
 
-Workload (one step = one frame): the 1024^3 cave scene (value noise, spacing
-64, 5 octaves, 50 % fill, depth 10, DXT1 bricks) and 1920x1080 FP32 primary
-rays from a seeded empty voxel in a seeded direction; each rank renders its
-own camera (weak scaling, no data-path collective).  `value` is Mrays/s of the
-device-resident cast kernel (rays and hits in HBM, L2 flushed between steps);
-`e2e` is the same metric through vx_cast_rays_host with pinned host buffers,
-copies included.  `--impl reference` times the CPU restatement of the
-reference castRay on this host's cores instead.
+Headline (default, one step = one frame): the batched frame of 64 scenes
+(64^3..1024^3; noise at 10/50 % fill, urban lattices at 90 %; half of them
+with DXT1 bricks), one camera each (256x256..1920x1080) and two
+cosine-weighted bounce rays per primary hit.  The frame runs as one CUDA
+graph: the persistent batched cast of every primary ray, the compaction of
+the bounce rays of hits, the batched bounce cast.  `value` is Mrays/s of that
+frame (primary rays + bounce rays of hits) with every input resident in HBM;
+the plain arm casts the same rays with one launch per scene and pass; `e2e`
+is the same frame through vx_batch_launch_frame_host with pinned host
+buffers.  The line also carries the 1024^3 cave frame (cfg2), the 2048^3
+urban frame with shadow rays (cfg3), the adjoint (cfg5) and the rows beyond
+the cast.  `--impl reference` times the CPU restatement of the reference
+castRay (the oracle) on this host's cores over a sample of the same frame,
+its inputs built on the oracle side without the product library.
 """
 import argparse
+import concurrent.futures as cf
 import ctypes as C
+import glob
+import hashlib
 import importlib.util
 import json
 import os
@@ -21,9 +30,12 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG_DIR = os.path.join(ROOT, "vbvs--vixen_b200")
 METRIC = "Mrays/s on 1 B200, batched vs plain at bit-exact hits; fwd+bwd ms/view"
+CFG4_SEED = 77  # bounce-ray seed of the batched frame
 
 
 def load_pkg():
@@ -38,9 +50,17 @@ def load_pkg():
 
 
 def load_oracle():
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    d = os.path.join(ROOT, "oracle")
+    if d not in sys.path:
+        sys.path.insert(0, d)
     import vx_oracle
     return vx_oracle
+
+
+def load_oracle_workloads():
+    load_oracle()
+    import workloads_ref
+    return workloads_ref
 
 
 def measured_peaks():
@@ -50,6 +70,30 @@ def measured_peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def source_hash():
+    """sha256 over the library's CUDA / C++ sources: identifies the build a profile was taken of."""
+    h = hashlib.sha256()
+    for p in sorted(glob.glob(os.path.join(PKG_DIR, "csrc", "*"))):
+        with open(p, "rb") as f:
+            h.update(os.path.basename(p).encode() + b"\0" + f.read())
+    return h.hexdigest()[:16]
+
+
+def profiled_traffic(kernel, workload):
+    """DRAM bytes per launch of `kernel` on `workload` from profiles/dram_traffic.json, only when
+    the entry was captured from the current sources (else None)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "dram_traffic.json")) as f:
+            entries = json.load(f)
+    except Exception:
+        return None
+    want = source_hash()
+    for e in entries:
+        if e.get("kernel") == kernel and e.get("workload") == workload and e.get("source_sha256") == want:
+            return e.get("dram_bytes_per_launch")
+    return None
 
 
 class ClockSampler:
@@ -73,6 +117,7 @@ class ClockSampler:
             self.t.start()
         except Exception:
             self.proc = None
+        return self
 
     def _read(self):
         for line in self.proc.stdout:
@@ -106,21 +151,6 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def make_workload(vx, R, seed, rank, use_gpu_gen):
-    from vx_b200 import workloads as W
-    import numpy as np
-    spacing, octaves = 64 * R // 1024, 5 if R >= 1024 else 3
-    if use_gpu_gen:
-        bits = vx.synth_noise_dev(R, spacing, octaves, 0.5, seed, False).cpu().numpy().view(np.uint64)
-    else:
-        bits = vx.synth_noise(R, spacing, octaves, 0.5, seed, False)
-    from vx_b200 import multigpu as M
-    wl = W.config2(R=R, seed=seed, bits=bits)
-    if rank:
-        wl.camera = W.empty_voxel_camera(bits, R, M.rank_seed(seed, rank), 70.0, wl.width, wl.height)
-    return wl
-
-
 def bytes_per_launch(n, iters, grid_reads, dda_steps, hits, color_kind):
     """Algorithmic bytes of one cast launch (per-ray terms counted by the traversal):
     24 ray in + 16 hit record out + colour out (12 B DXT1 texel / 4 B RGBA8) per ray,
@@ -130,117 +160,126 @@ def bytes_per_launch(n, iters, grid_reads, dda_steps, hits, color_kind):
     return n * (24 + 16 + cout) + 8 * iters + 4 * grid_reads + 4 * dda_steps + cin * hits
 
 
-def cpu_baseline(vo, wl, rays, g_hits, budget_s=12.0):
-    """Times the oracle (CPU restatement of castRay) on a bounded prefix of the
-    frame with every host thread, and checks those rays against the GPU."""
-    import numpy as np
-    threads = os.cpu_count() or 1
+def counter_totals(vx, counters):
+    cnt = counters.cpu().numpy().view(vx.COUNTER_DTYPE).reshape(-1)
+    return {k: int(cnt[k].astype(np.int64).sum()) for k in cnt.dtype.names}
+
+
+def events_ms(fn, steps, warmup, flush, stream=None):
+    """Per-step CUDA-event times of fn on `stream` (the current stream by default), L2 flushed
+    before every step."""
+    import torch
+    s = stream or torch.cuda.current_stream()
+    with torch.cuda.stream(s):
+        for _ in range(warmup):
+            fn()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    with torch.cuda.stream(s):
+        for a, b in ev:
+            flush.zero_()
+            a.record(s)
+            fn()
+            b.record(s)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ev]
+
+
+def mismatches(g, o, g_col=None, o_col=None, cnt=None):
+    """Per-field mismatch counts of product hit records g against oracle records o (t compared as
+    bits on hits; texels as bits; counters when given)."""
+    hit = (o["flags"] & 1).astype(bool)
+    m = {"flags": int(np.count_nonzero(g["flags"].astype(np.uint32) != o["flags"])),
+         "brick": int(np.count_nonzero(g["brick"] != o["brick"])),
+         "node": int(np.count_nonzero(g["node"] != o["node"])),
+         "voxel": int(np.count_nonzero(g["voxel"].astype(np.uint32) != o["voxel"])),
+         "scale": int(np.count_nonzero(g["scale"].astype(np.int32) != o["scale"])),
+         "t": int(np.count_nonzero(hit & (g["t"].view(np.uint32) != o["t"].view(np.uint32))))}
+    if g_col is not None:
+        m["texel"] = int(np.count_nonzero(np.any(g_col.view(np.uint32) != o_col.view(np.uint32), axis=1)))
+    if cnt is not None:
+        m["iters"] = int(np.count_nonzero(cnt["iters"].astype(np.uint32) != o["iters"]))
+        m["dda_steps"] = int(np.count_nonzero(cnt["dda_steps"].astype(np.uint32) != o["dda_steps"]))
+    return m
+
+
+def oracle_scenes(vo, frames, threads=None):
+    """Oracle octrees of (bits, R, max_levels) triples, built concurrently (each build is one
+    C++ call that releases the interpreter lock)."""
+    with cf.ThreadPoolExecutor(max_workers=threads or min(16, os.cpu_count() or 1)) as ex:
+        return list(ex.map(lambda f: vo.OracleScene.from_dense(f[0], f[1], f[2]), frames))
+
+
+# ---------------------------------------------------------------------------
+# cfg4: the batched frame (headline)
+# ---------------------------------------------------------------------------
+
+def cfg4_config(specs):
+    n = sum(s.width * s.height for s in specs)
+    return {"workload": f"cfg4: {len(specs)} scenes 64^3..1024^3 (noise 10/50%, urban 90%, half DXT1), one camera "
+                        f"each 256x256..1920x1080, 2 cosine-weighted bounce rays per primary hit; one frame = batched "
+                        f"primary cast + bounce compaction + batched bounce cast in one CUDA graph",
+            "primary_rays": n, "scenes": len(specs), "scene_R": [s.R for s in specs],
+            "ray_order": "primary rays in 8x4-pixel warp tiles of 32x8 blocks (vx_render's order)",
+            "rays_counted": "primary rays + the 2 bounce rays of every primary hit",
+            "l2": "flushed before every timed frame (256 MiB write)", "parallelism": "replicated scenes, weak scaling"}
+
+
+def cfg4_sample(begin, target):
+    """Global primary indices of a stride sample of about `target` rays over every scene."""
+    n = int(begin[-1])
+    stride = max(1, n // max(1, target))
+    return np.arange(0, n, stride, dtype=np.int64)
+
+
+def oracle_cfg4_pass(vo, wr, oscenes, rays_all, begin, idx, threads, pool=None):
+    """The oracle's frame over sampled primary rays idx (global indices): primary casts per scene,
+    the bounce rays of the hits, their casts.  The casts run as chunks of at most 2048 rays of one
+    scene on `threads` host threads (one oracle thread per chunk).  Returns (primary records, bounce
+    records (2 per sampled ray), bounce rays, seconds)."""
     t0 = time.perf_counter()
-    o = vo.OracleScene.from_dense(wl.bits, wl.R, wl.scene.max_levels)
-    build_s = time.perf_counter() - t0
-    n = min(rays.shape[0], 1 << 16)
-    while True:
-        t0 = time.perf_counter()
-        oh = o.cast_rays(rays[:n], threads=threads)
-        dt = time.perf_counter() - t0
-        if dt >= budget_s / 4 or n >= rays.shape[0]:
-            break
-        n = min(rays.shape[0], n * 4)
-    g = g_hits[:n]
-    hit = (oh["flags"] & 1).astype(bool)
-    mism = int(np.count_nonzero((g["flags"].astype(np.uint32) != oh["flags"]) | (g["brick"] != oh["brick"]) |
-                                (g["node"] != oh["node"]) | (g["voxel"].astype(np.uint32) != oh["voxel"]) |
-                                (hit & (g["t"].view(np.uint32) != oh["t"].view(np.uint32)))))
-    return {"value": n / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
-            "sample": f"first {n} rays of the frame ({n / rays.shape[0]:.1%}), {threads} threads, "
-                      f"{dt:.2f} s; oracle build {build_s:.1f} s"}, {"checked": n, "mismatches": mism}
+    own = pool is None
+    pool = pool or cf.ThreadPoolExecutor(max_workers=threads)
+
+    def cast_all(rays, scene_of, out, sel_mask=None):
+        jobs = []
+        for s in np.unique(scene_of if sel_mask is None else scene_of[sel_mask]):
+            sel = np.flatnonzero((scene_of == s) if sel_mask is None else ((scene_of == s) & sel_mask))
+            for c in range(0, sel.size, 2048):
+                part = sel[c:c + 2048]
+                jobs.append((part, pool.submit(oscenes[s].cast_rays, rays[part], 0.0, 3.4028234663852886e38, 1)))
+        for part, fut in jobs:
+            out[part] = fut.result()
+
+    sc = np.searchsorted(begin, idx, side="right") - 1
+    prim_rays = rays_all[idx]
+    prim = np.zeros(idx.size, vo.HIT_DTYPE)
+    cast_all(prim_rays, sc, prim)
+    bounce = wr.spawn_bounce(prim_rays, prim, CFG4_SEED, idx.astype(np.uint64))
+    bsc = np.repeat(sc, 2)
+    brec = np.zeros(bounce.shape[0], vo.HIT_DTYPE)
+    live = np.repeat((prim["flags"] & 1).astype(bool), 2)
+    cast_all(bounce, bsc, brec, live)
+    dead = np.flatnonzero(~live)
+    if dead.size:  # zero-direction rays: the invalid record, as the cast writes it
+        brec[dead] = oscenes[0].cast_rays(bounce[dead], threads=1)
+    if own:
+        pool.shutdown()
+    return prim, brec, bounce, time.perf_counter() - t0
 
 
-def run_reference(args, rank, world):
-    """CPU restatement of the reference castRay on all host cores."""
-    if rank != 0:
-        return 0
-    import numpy as np
-    vx = load_pkg()
-    vo = load_oracle()
-    use_gpu = False
-    try:
-        import torch
-        use_gpu = torch.cuda.is_available()
-    except Exception:
-        pass
-    wl = make_workload(vx, args.R, args.seed, 0, use_gpu)
-    rays = wl.rays(order="tiled")
-    threads = os.cpu_count() or 1
-    o = vo.OracleScene.from_dense(wl.bits, wl.R, wl.scene.max_levels)
-    n = min(rays.shape[0], 1 << 15)
-    while True:  # size one step at about 3 s
-        t0 = time.perf_counter()
-        o.cast_rays(rays[:n], threads=threads)
-        dt = time.perf_counter() - t0
-        if dt >= 0.75 or n >= rays.shape[0]:
-            break
-        n = min(rays.shape[0], n * 4)
-    n = min(rays.shape[0], max(1024, int(n * 3.0 / max(dt, 1e-3))))
-    for _ in range(args.warmup):
-        o.cast_rays(rays[:n], threads=threads)
-    times = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        o.cast_rays(rays[:n], threads=threads)
-        times.append(time.perf_counter() - t0)
-    total = sum(times)
-    v = n * args.steps / total / 1e6
-    line = {"metric": METRIC, "value": v, "unit": "Mrays/s", "impl": "reference", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": config_dict(wl, world),
-            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": threads, "kind": "port",
-                             "sample": f"first {n} of {rays.shape[0]} rays per step, {threads} threads"},
-            "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
-    return 0
-
-
-def run_cfg4(args, rank, world):
-    """Prints the cfg4 line (see measure_cfg4)."""
+def measure_cfg4(args, rank, world, steps, warmup, with_cpu):
+    """The batched frame against the plain launches, the per-pass roofline, e2e through host
+    buffers, and (with_cpu) the oracle on a sample of the frame's rays."""
     import torch
     import torch.distributed as dist
-    from datetime import timedelta
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
-    res = measure_cfg4(args, rank, world, args.steps, args.warmup)
-    if world > 1:
-        dist.destroy_process_group()
-    if rank == 0:
-        line = {"metric": METRIC, "value": res["batched"]["value"], "unit": "Mrays/s", "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["batched"]["ms_per_frame"],
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic", "config": res.pop("config"),
-                # per frame: primary cast, octant counts, offsets, compacted bounce spawn, bounce cast
-                "gpu_launches": args.steps * 5}
-        line.update(res)
-        print(json.dumps(line), flush=True)
-    return 0
-
-
-def measure_cfg4(args, rank, world, steps, warmup):
-    """cfg4: 64 scenes (64^3..1024^3; noise 10/50 %, urban 90 %; half DXT1) with one camera
-    each (256x256..1920x1080) and 2 cosine-weighted bounce rays per hit.  One frame = primary
-    pass, bounce spawn, bounce pass.  Batched: the persistent kernel (autotuned) in a CUDA
-    graph; plain: one cast launch per scene and pass.  Both produce identical hits."""
-    import numpy as np
-    import torch
-    import torch.distributed as dist
-    local = int(os.environ.get("LOCAL_RANK", "0"))
     vx = load_pkg()
     from vx_b200 import workloads as W
-    t_setup = time.perf_counter()
     from vx_b200 import multigpu as M
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    t_setup = time.perf_counter()
     specs = W.config4_specs(args.scenes, seed=M.rank_seed(4, rank))
-    wls, scenes, rays = [], [], []
+    scenes, rays, frames = [], [], []
     for sp in specs:
         bits = None
         if sp.kind == "noise" and sp.R >= 256:
@@ -250,174 +289,493 @@ def measure_cfg4(args, rank, world, steps, warmup):
         wl = W.build_spec(sp, bits)
         scenes.append(vx.Scene(wl.scene))
         rays.append(wl.rays(order="tiled"))
-        wl.scene.brick_color = None  # host copies are no longer needed
-        wls.append(wl)
+        frames.append((wl.bits, wl.R, wl.scene.max_levels))
+        wl.scene.brick_color = None
     setup_s = time.perf_counter() - t_setup
     begin = np.concatenate([[0], np.cumsum([r.shape[0] for r in rays])]).astype(np.int64)
     n = int(begin[-1])
-    d_rays = torch.from_numpy(np.concatenate(rays)).cuda()
+    rays_all = np.concatenate(rays)
+    del rays
+    d_rays = torch.from_numpy(rays_all).cuda()
     d_begin = torch.from_numpy(begin.astype(np.int32)).cuda()
     d_bbegin = torch.from_numpy((2 * begin).astype(np.int32)).cuda()
     ph = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
     bh = torch.zeros((2 * n, 4), dtype=torch.int32, device="cuda")
     bounce = torch.zeros((2 * n, 6), dtype=torch.float32, device="cuda")
     batch = vx.Batch(scenes)
-    seed = 77
-    # Tune each pass on its own rays: the bounce pass is tuned on the bounce rays of this frame.
+    # each pass tuned on its own rays (the bounce pass on this frame's bounce rays)
     tuning, tune_ms = batch.autotune(d_rays, d_begin, ph)
-    vx.spawn_bounce_rays(d_rays, ph, seed, bounce)
+    vx.spawn_bounce_rays(d_rays, ph, CFG4_SEED, bounce)
     btuning, btune_ms = batch.autotune(bounce, d_bbegin, bh)
     batch.set_tuning(tuning.block, tuning.rays_per_task, tuning.stack_in_shared, tuning.refill)
     batch.set_bounce_tuning(btuning)
-
-    def plain_frame():
-        for i, sc in enumerate(scenes):
-            a, b = int(begin[i]), int(begin[i + 1])
-            sc.cast_rays_dev(d_rays[a:b], ph[a:b])
-        vx.spawn_bounce_rays(d_rays, ph, seed, bounce)
-        for i, sc in enumerate(scenes):
-            a, b = 2 * int(begin[i]), 2 * int(begin[i + 1])
-            sc.cast_rays_dev(bounce[a:b], bh[a:b])
-
-    plain_frame()
-    torch.cuda.synchronize()
-    ref_p, ref_b = ph.cpu().numpy().copy(), bh.cpu().numpy().copy()
     stream = torch.cuda.Stream()
 
     def capture(compact):
         torch.cuda.synchronize()
         with torch.cuda.stream(stream):
-            if compact:  # the bounce pass casts only the bounce rays of primary hits
-                batch.capture_frame_compact(d_rays, d_begin, ph, bounce, bh, seed, stream.cuda_stream)
+            if compact:
+                batch.capture_frame_compact(d_rays, d_begin, ph, bounce, bh, CFG4_SEED, stream.cuda_stream)
             else:
-                batch.capture_frame(d_rays, d_begin, ph, bounce, d_bbegin, bh, seed, stream.cuda_stream)
+                batch.capture_frame(d_rays, d_begin, ph, bounce, d_bbegin, bh, CFG4_SEED, stream.cuda_stream)
             ph.zero_()
             bh.zero_()
             batch.launch_frame(stream.cuda_stream)
         torch.cuda.synchronize()
-        return bool(np.array_equal(ph.cpu().numpy(), ref_p) and np.array_equal(bh.cpu().numpy(), ref_b))
-
-    identical_full = capture(False)
-    nhit = int(np.count_nonzero(ref_p.view(vx.HIT_DTYPE).reshape(-1)["flags"] & 1))
-    rays_per_frame = n + 2 * nhit  # primary + bounce rays of hits (miss slots carry a zero direction)
+        return ph.cpu().numpy().copy(), bh.cpu().numpy().copy()
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    sampler = ClockSampler(local)
-    sampler.start()
+    sampler = ClockSampler(local).start()
+    full_p, full_b = capture(False)
+    if world > 1:
+        dist.barrier()
+    full_ms = events_ms(lambda: batch.launch_frame(stream.cuda_stream), steps, warmup, flush, stream)
+    ref_p, ref_b = capture(True)
+    identical_compact = bool(np.array_equal(ref_p, full_p) and np.array_equal(ref_b, full_b))
+    del full_p, full_b
+    cb, slot = batch.frame_compaction()
+    h2 = int(cb[-1])  # bounce rays of hits in the compacted frame
+    g_p = ref_p.view(vx.HIT_DTYPE).reshape(-1)
+    nhit = int(np.count_nonzero(g_p["flags"] & 1))
+    rays_per_frame = n + 2 * nhit
+    if world > 1:
+        dist.barrier()
+    batched_ms = events_ms(lambda: batch.launch_frame(stream.cuda_stream), steps, warmup, flush, stream)
 
-    def timed(frame_fn, s):
-        with torch.cuda.stream(s):
-            for _ in range(warmup):
-                frame_fn()
-        torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
-        with torch.cuda.stream(s):
-            for a, b in ev:
-                flush.zero_()
-                a.record(s)
-                frame_fn()
-                b.record(s)
-        torch.cuda.synchronize()
-        return [a.elapsed_time(b) for a, b in ev]
+    # Plain arm: one launch per scene and pass over the same rays: the primary rays, then the
+    # compacted bounce rays of hits (left in `bounce` by the batched frame; the plain frame does no
+    # spawning or compaction of its own, which favours it).
+    pbh = torch.zeros((max(h2, 1), 4), dtype=torch.int32, device="cuda")
 
-    plain_ms = timed(plain_frame, stream)
-    full_ms = timed(lambda: batch.launch_frame(stream.cuda_stream), stream)
-    identical = capture(True) and identical_full
-    batched_ms = timed(lambda: batch.launch_frame(stream.cuda_stream), stream)
+    def plain_frame():
+        for i, sc in enumerate(scenes):
+            a, b = int(begin[i]), int(begin[i + 1])
+            if b > a:
+                sc.cast_rays_dev(d_rays[a:b], ph[a:b])
+        for i, sc in enumerate(scenes):
+            a, b = int(cb[i]), int(cb[i + 1])
+            if b > a:
+                sc.cast_rays_dev(bounce[a:b], pbh[a:b])
+
+    if world > 1:
+        dist.barrier()
+    plain_ms = events_ms(plain_frame, steps, warmup, flush, stream)
+    torch.cuda.synchronize()
+    identical_plain = bool(np.array_equal(ph.cpu().numpy(), ref_p)) and \
+        bool(np.array_equal(pbh[:h2].cpu().numpy(), ref_b[slot.astype(np.int64)]))
+
+    # Counting passes and per-pass kernel times (roofline): each pass as its own batched launch
+    # with the frame's tuning for it; the bounce pass over the compacted rays.
+    d_cb = torch.from_numpy(cb.astype(np.int32)).cuda()
+    cnt_p = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+    cnt_b = torch.zeros((max(h2, 1), 4), dtype=torch.int32, device="cuda")
+    batch.cast(d_rays, d_begin, ph, cnt_p)
+    batch.set_tuning(btuning.block, btuning.rays_per_task, btuning.stack_in_shared, btuning.refill)
+    batch.cast(bounce[:h2], d_cb, pbh, cnt_b)
+    torch.cuda.synchronize()
+    tot_p = counter_totals(vx, cnt_p)
+    tot_b = counter_totals(vx, cnt_b[:h2])
+    bounce_pass_ms = events_ms(lambda: batch.cast(bounce[:h2], d_cb, pbh), steps, warmup, flush, stream)
+    batch.set_tuning(tuning.block, tuning.rays_per_task, tuning.stack_in_shared, tuning.refill)
+    primary_pass_ms = events_ms(lambda: batch.cast(d_rays, d_begin, ph), steps, warmup, flush, stream)
+    del cnt_p, cnt_b
     clocks = sampler.stop()
+
+    # e2e: the captured frame from pinned host buffers (rays in; primary and bounce hits out)
+    batch.capture_frame_compact(d_rays, d_begin, ph, bounce, bh, CFG4_SEED, stream.cuda_stream)
+    rays_h = torch.from_numpy(rays_all).pin_memory()
+    ph_h = torch.zeros((n, 4), dtype=torch.int32).pin_memory()
+    bh_h = torch.zeros((2 * n, 4), dtype=torch.int32).pin_memory()
+    e2e_ms = events_ms(lambda: batch.launch_frame_host(rays_h, ph_h, bh_h, stream.cuda_stream), steps, warmup,
+                       flush, stream)
+    e2e_same = bool(np.array_equal(ph_h.numpy(), ref_p) and np.array_equal(bh_h.numpy(), ref_b))
+    del rays_h, ph_h, bh_h
+    batch_total, plain_total, full_total, e2e_total = M.max_over_ranks(
+        [sum(batched_ms), sum(plain_ms), sum(full_ms), sum(e2e_ms)])
+
+    peak, peak_kind = measured_peaks()
+    passes = {}
+    for name, tot, nr, ms, tn, kern in (("primary", tot_p, n, primary_pass_ms, tuning, "primary"),
+                                        ("bounce", tot_b, h2, bounce_pass_ms, btuning, "bounce")):
+        algo = bytes_per_launch(nr, tot["run_iters"], tot["run_grid_reads"], tot["run_dda_steps"], 0, 0)
+        mean_s = statistics.mean(ms) / 1e3
+        kname = "vx::batch_refill_kernel" if tn.refill else "vx::batch_kernel"
+        passes[name] = {"kernel": kname, "rays": nr, "tuning": tn.as_dict(), "kernel_ms_mean": mean_s * 1e3,
+                        "algorithmic_bytes_per_launch": algo, "achieved_gbs": algo / mean_s / 1e9,
+                        "mrays_s": nr / mean_s / 1e6,
+                        "per_ray": {k: v / max(nr, 1) for k, v in tot.items()}}
+    dom = max(passes, key=lambda k: passes[k]["kernel_ms_mean"])
+    d = passes[dom]
+    workload_key = f"cfg4_{dom}_pass"
+    roofline = {"bound": "hbm", "achieved": d["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                "frac": d["achieved_gbs"] / peak, "traffic": profiled_traffic(d["kernel"], workload_key),
+                "peak_source": peak_kind, "kernel": f"{d['kernel']} ({dom} pass of the frame)",
+                "kernel_ms_mean": d["kernel_ms_mean"], "algorithmic_bytes_per_launch": d["algorithmic_bytes_per_launch"],
+                "traffic_source": f"profiles/dram_traffic.json entry '{workload_key}' for the current sources, "
+                                  f"else null", "passes": passes}
+    out = {"config": cfg4_config(specs),
+           "value": world * rays_per_frame * steps / (batch_total / 1e3) / 1e6,
+           "ms_per_frame": batch_total / steps,
+           "frame": {"primary_rays": n, "primary_hits": nhit, "bounce_rays": 2 * nhit, "rays_per_frame": rays_per_frame,
+                     "setup_s": setup_s, "graph": "vx_batch_capture_frame_compact"},
+           "roofline": roofline,
+           "e2e": {"value": world * rays_per_frame * steps / (e2e_total / 1e3) / 1e6, "unit": "Mrays/s",
+                   "h2d_bytes_per_step": world * n * 24, "d2h_bytes_per_step": world * n * (16 + 32),
+                   "call": "vx_batch_launch_frame_host (pinned buffers; primary hits copied out during the bounce "
+                           "pass)", "hits_equal_device_path": e2e_same, "ms_per_frame": e2e_total / steps},
+           "batched": {"mrays_s": world * rays_per_frame * steps / (batch_total / 1e3) / 1e6,
+                       "ms_per_frame": batch_total / steps, "tuning": tuning.as_dict(), "bounce_tuning": btuning.as_dict(),
+                       "autotune_best_ms_primary": tune_ms, "autotune_best_ms_bounce": btune_ms},
+           "plain": {"mrays_s": world * rays_per_frame * steps / (plain_total / 1e3) / 1e6,
+                     "ms_per_frame": plain_total / steps, "launches_per_frame": 2 * len(specs),
+                     "rays": "the same primary rays and compacted bounce rays of hits as the batched frame"},
+           "speedup_batched_vs_plain": plain_total / batch_total,
+           "uncompacted_batched_ms_per_frame": full_total / steps,
+           "compaction_gain": full_total / batch_total,
+           "hits_identical": {"batched_vs_plain": identical_plain, "compacted_vs_uncompacted_frame": identical_compact},
+           "clocks": clocks}
+    if with_cpu:
+        vo = load_oracle()
+        wr = load_oracle_workloads()
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        osc = oracle_scenes(vo, frames)
+        build_s = time.perf_counter() - t0
+        target, spent = 1 << 15, 0.0
+        while True:
+            idx = cfg4_sample(begin, target)
+            prim, brec, _, dt = oracle_cfg4_pass(vo, wr, osc, rays_all, begin, idx, threads)
+            spent += dt
+            if dt >= 2.0 or idx.size >= n or spent > 20.0:
+                break
+            target = int(target * min(16.0, max(2.0, 6.0 / max(dt, 1e-3))))
+        live = np.repeat((prim["flags"] & 1).astype(bool), 2)
+        counted = idx.size + int(live.sum())
+        bslots = (2 * idx[:, None] + np.arange(2)[None, :]).reshape(-1)
+        mp = mismatches(g_p[idx], prim)
+        mb = mismatches(ref_b.view(vx.HIT_DTYPE).reshape(-1)[bslots], brec)
+        out["cpu_baseline"] = {"value": counted / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
+                               "sample": f"every {int(begin[-1]) // max(idx.size, 1)}th primary ray of the frame "
+                                         f"({idx.size} rays over all {len(specs)} scenes) and the 2 bounce rays of "
+                                         f"each of its hits ({int(live.sum())}); {counted} rays in {dt:.2f} s on "
+                                         f"{threads} threads; oracle octree builds {build_s:.1f} s"}
+        out["parity_sample"] = {"primary_rays": int(idx.size), "bounce_rays": int(bslots.size),
+                                "primary_mismatches": mp, "bounce_mismatches": mb,
+                                "fields": "flags, brick, node, voxel, scale, t bits"}
+        it_ref = float(np.mean(prim["iters"]))
+        out["iterations_per_primary_ray"] = {
+            "reference_loop": it_ref, "kernel_executed": passes["primary"]["per_ray"]["run_iters"],
+            "note": "the reference loop runs rays caught in a repeating state to its 500-iteration cap; the kernel "
+                    "detects the repeat exactly and stops, so part of the ratio to the CPU baseline is algorithmic"}
+        del osc
+    batch.close()
+    del scenes, d_rays, ph, bh, bounce, pbh
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_cfg4(args, rank, world):
+    """Prints the headline line: the batched frame (cfg4), with cfg2, cfg3, cfg5 and the next rows
+    attached at N = 1."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    res = measure_cfg4(args, rank, world, args.steps, args.warmup,
+                       with_cpu=(world == 1 and rank == 0 and not args.no_cpu_baseline))
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": res.pop("value"), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": res.pop("ms_per_frame"), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": res.pop("config"),
+            # per timed frame: batched primary cast, octant counts, offsets, compacted scatter, batched bounce cast
+            "gpu_launches": args.steps * 5}
+    line.update(res)
+    if world == 1 and not args.no_extra:
+        extra_steps, extra_warmup = max(3, min(args.steps, 10)), max(3, min(args.warmup, 3))
+        line["cfg2"] = measure_cfg2(args, 0, 1, extra_steps, extra_warmup, with_cpu=not args.no_cpu_baseline)
+        torch.cuda.empty_cache()
+        line["cfg3"] = measure_cfg3(args, extra_steps, extra_warmup, with_oracle=not args.no_cpu_baseline)
+        torch.cuda.empty_cache()
+        line["adjoint"] = measure_cfg5(args, 0, 1, extra_steps, extra_warmup)
+        torch.cuda.empty_cache()
+        line["next_rows"] = measure_next(args, extra_steps, extra_warmup)
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# cfg2: the 1024^3 cave frame, plain cast
+# ---------------------------------------------------------------------------
+
+def cfg2_config(R, width, height, world):
+    return {"workload": f"cfg2_cave{R}_dxt1_{width}x{height}: cave {R}^3 (depth 10), value noise spacing "
+                        f"{64 * R // 1024}, 5 octaves, 50% fill, DXT1 bricks, {width}x{height} FP32 primary rays per "
+                        f"rank, plain cast kernel",
+            "ray_order": "8x4-pixel warp tiles in 32x8 blocks (vx_render's order)",
+            "rays_per_step_per_gpu": width * height, "parallelism": f"replicated scene, {world} camera(s)",
+            "l2": "flushed between timed steps (256 MiB write)"}
+
+
+def measure_cfg2(args, rank, world, steps, warmup, with_cpu):
+    """The cave frame through the plain cast kernel: device Mrays/s, e2e through vx_cast_rays_host,
+    the kernel's roofline, and the oracle on a sample (every field, the texel included)."""
+    import torch
+    import torch.distributed as dist
+    vx = load_pkg()
+    from vx_b200 import workloads as W
     from vx_b200 import multigpu as M
-    plain_total, batched_total, full_total = M.max_over_ranks([sum(plain_ms), sum(batched_ms), sum(full_ms)])
-    value = world * rays_per_frame * steps / (batched_total / 1e3) / 1e6
-    plain_value = world * rays_per_frame * steps / (plain_total / 1e3) / 1e6
-    return {"config": {"workload": f"cfg4: {len(specs)} scenes 64^3..1024^3 (noise 10/50%, urban 90%, half DXT1), "
-                                   f"one camera each 256x256..1920x1080, 2 bounce rays per hit; batched "
-                                   f"persistent kernel in a CUDA graph vs {2 * len(specs)} plain launches",
-                       "primary_rays": n, "rays_per_frame": rays_per_frame, "hits": nhit,
-                       "ray_order": "primary rays in 8x4-pixel warp tiles (workloads.tile_order)",
-                       "scene_R": [sp.R for sp in specs], "setup_s": setup_s,
-                       "l2": "flushed before every timed frame (256 MiB write)"},
-            "batched": {"value": value, "unit": "Mrays/s", "ms_per_frame": batched_total / steps,
-                        "frame": "vx_batch_capture_frame_compact: the bounce pass casts the 2 bounce rays of "
-                                 "each primary hit only, per scene grouped by direction octant",
-                        "ms_per_frame_uncompacted": full_total / steps,
-                        "tuning": tuning.as_dict(), "autotune_best_ms_primary": tune_ms,
-                        "bounce_tuning": btuning.as_dict(), "autotune_best_ms_bounce": btune_ms},
-            "plain": {"value": plain_value, "unit": "Mrays/s", "ms_per_frame": plain_total / steps,
-                      "launches_per_frame": 2 * len(specs) + 1},
-            "speedup_batched_vs_plain": plain_total / batched_total,
-            "hits_identical_batched_vs_plain": identical, "clocks": clocks}
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    R, seed = args.R, args.seed
+    spacing = 64 * R // 1024
+    bits = vx.synth_noise_dev(R, spacing, 5 if R >= 1024 else 3, 0.5, seed, False).cpu().numpy().view(np.uint64)
+    wl = W.config2(R=R, seed=seed, bits=bits)
+    if rank:
+        wl.camera = W.empty_voxel_camera(bits, R, M.rank_seed(seed, rank), 70.0, wl.width, wl.height)
+    scene = vx.Scene(wl.scene)
+    rays_np = wl.rays(order="tiled")
+    n = rays_np.shape[0]
+    rays = torch.from_numpy(rays_np).cuda()
+    hits = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+    color = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+    counters = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+    scene.cast_rays_dev(rays, hits, color, counters)  # counting pass (untimed)
+    torch.cuda.synchronize()
+    tot = counter_totals(vx, counters)
+    cnt = counters.cpu().numpy().view(vx.COUNTER_DTYPE).reshape(-1)
+    g_hits = hits.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1).copy()
+    g_col = color.cpu().numpy().copy()
+    nhit = int(np.count_nonzero(g_hits["flags"] & 1))
+    algo = bytes_per_launch(n, tot["run_iters"], tot["run_grid_reads"], tot["run_dda_steps"], nhit, scene.color_kind)
+    ref_bytes = bytes_per_launch(n, tot["iters"], tot["grid_reads"], tot["dda_steps"], nhit, scene.color_kind)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    sampler = ClockSampler(local).start()
+    t_soak = time.perf_counter()
+    while time.perf_counter() - t_soak < args.soak_seconds:  # clocks to steady state before timing
+        for _ in range(20):
+            scene.cast_rays_dev(rays, hits, color)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    step_ms = events_ms(lambda: scene.cast_rays_dev(rays, hits, color), steps, warmup, flush)
+    rays_h = torch.from_numpy(rays_np).pin_memory()
+    hits_h = torch.zeros((n, 4), dtype=torch.int32).pin_memory()
+    col_h = torch.zeros((n, 3), dtype=torch.float32).pin_memory()
+    L = vx.lib()
+    stream = torch.cuda.current_stream()
+
+    def e2e_call():
+        vx.check(L.vx_cast_rays_host(scene.handle, C.c_void_p(rays_h.data_ptr()), n, 0.0, vx.FLT_MAX,
+                                     C.c_void_p(hits_h.data_ptr()), C.c_void_p(col_h.data_ptr()),
+                                     C.c_void_p(stream.cuda_stream)))
+
+    e2e_ms = events_ms(e2e_call, steps, warmup, flush)
+    clocks = sampler.stop()
+    e2e_same = bool(np.array_equal(hits_h.numpy().view(np.uint8), g_hits.view(np.uint8).reshape(n, 16)))
+    total_ms, e2e_total = M.max_over_ranks([sum(step_ms), sum(e2e_ms)])
+    mean_s = statistics.mean(step_ms) / 1e3
+    peak, peak_kind = measured_peaks()
+    out = {"config": cfg2_config(R, wl.width, wl.height, world),
+           "value": M.aggregate_throughput(n * steps, world, total_ms / 1e3) / 1e6, "unit": "Mrays/s",
+           "ms_per_frame": total_ms / steps, "steps": steps,
+           "bricks": int(wl.scene.brick_count), "nodes": int(wl.scene.node_count), "hit_rate": nhit / n,
+           "e2e": {"value": M.aggregate_throughput(n * steps, world, e2e_total / 1e3) / 1e6, "unit": "Mrays/s",
+                   "h2d_bytes_per_step": world * n * 24, "d2h_bytes_per_step": world * n * (16 + 12),
+                   "hits_equal_device_path": e2e_same},
+           "roofline": {"bound": "hbm", "achieved": algo / mean_s / 1e9, "peak": peak, "unit": "GB/s",
+                        "frac": algo / mean_s / 1e9 / peak,
+                        "traffic": profiled_traffic("vx::cast_kernel", wl.name), "peak_source": peak_kind,
+                        "algorithmic_bytes_per_launch": algo, "reference_loop_bytes_per_launch": ref_bytes,
+                        "per_ray": {k: v / n for k, v in tot.items()}, "kernel": "vx::cast_kernel",
+                        "kernel_ms_mean": mean_s * 1e3},
+           "clocks": clocks}
+    if with_cpu:
+        vo = load_oracle()
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        o = vo.OracleScene.from_dense(bits, R, wl.scene.max_levels)
+        build_s = time.perf_counter() - t0
+        m = min(n, 1 << 16)
+        while True:
+            t0 = time.perf_counter()
+            oh = o.cast_rays(rays_np[:m], threads=threads)
+            dt = time.perf_counter() - t0
+            if dt >= 3.0 or m >= n:
+                break
+            m = min(n, m * 4)
+        o_col = vo.hit_texels_dxt(wl.scene.brick_color, oh)
+        out["cpu_baseline"] = {"value": m / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
+                               "sample": f"first {m} rays of the frame ({m / n:.1%}), {threads} threads, {dt:.2f} s; "
+                                         f"oracle build {build_s:.1f} s"}
+        out["parity_sample"] = {"checked": m, "mismatches": mismatches(g_hits[:m], oh, g_col[:m], o_col, cnt[:m]),
+                                "fields": "flags, brick, node, voxel, scale, t bits, DXT1 texel bits, iteration and "
+                                          "DDA-step counters"}
+    del scene, rays, hits, color, counters
+    torch.cuda.empty_cache()
+    return out
 
 
-def measure_cfg3(args, steps, warmup):
-    """cfg3: 2048^3 urban lattice (32x32 blocks, 8-voxel streets, heights U[64,1800]), DXT1
-    bricks, 3840x2160 primary rays plus one shadow ray per hit toward a seeded light.  One frame =
-    primary cast, shadow spawn, shadow cast (plain kernel)."""
-    import numpy as np
+# ---------------------------------------------------------------------------
+# cfg3: the 2048^3 urban frame with shadow rays
+# ---------------------------------------------------------------------------
+
+def cfg3_config(R, width, height):
+    return {"workload": f"cfg3_urban{R}_dxt1_{width}x{height}: urban {R}^3 (depth 11), 32x32 blocks, 8-voxel "
+                        f"streets, heights U[64,1800], DXT1 bricks; {width}x{height} primary rays + 1 shadow ray per "
+                        f"hit toward a seeded light; one frame = primary cast + compacted shadow pass",
+            "ray_order": "primary rays in 8x4-pixel warp tiles (vx_render's order)",
+            "l2": "flushed before every timed frame (256 MiB write)"}
+
+
+def measure_cfg3(args, steps, warmup, with_oracle):
+    """The urban frame: primary cast (plain kernel, DXT1 texel out), then vx_cast_shadow_rays (the
+    shadow rays of hits, compacted on the device).  ms/frame, Mrays/s, the primary kernel's roofline,
+    and the oracle on a stride sample of the frame (primary record + texel, and the shadow record)."""
     import torch
     vx = load_pkg()
     from vx_b200 import workloads as W
     t0 = time.perf_counter()
-    wl = W.config3(R=args.R if args.R != 1024 else 2048)
+    wl = W.config3(R=args.R3)
     scene = vx.Scene(wl.scene)
     setup_s = time.perf_counter() - t0
-    bricks, nodes, dev_bytes = wl.scene.brick_count, wl.scene.node_count, scene.device_bytes()
-    wl.scene.brick_color = None
     rays_np = wl.rays(order="tiled")
     n = rays_np.shape[0]
     rays = torch.from_numpy(rays_np).cuda()
     hits = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
     col = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
-    shadow = torch.zeros((n, 6), dtype=torch.float32, device="cuda")
+    cnt = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
     sh = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
     L = W.light_dir(3)
+    scene.cast_rays_dev(rays, hits, col, cnt)
+    scene.cast_shadow_rays_dev(rays, hits, L, sh)
+    torch.cuda.synchronize()
+    tot = counter_totals(vx, cnt)
+    g = hits.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1).copy()
+    g_col = col.cpu().numpy().copy()
+    g_sh = sh.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1).copy()
+    del cnt
+    nhit = int(np.count_nonzero(g["flags"] & 1))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
-    def frame_all_slots():  # shadow rays of all n slots, misses included (zero-direction rays)
-        scene.cast_rays_dev(rays, hits, col)
-        vx.spawn_shadow_rays(rays, hits, L, shadow)
-        scene.cast_rays_dev(shadow, sh)
-
-    def frame():  # the shadow rays of the hits only, compacted on the device
+    def frame():
         scene.cast_rays_dev(rays, hits, col)
         scene.cast_shadow_rays_dev(rays, hits, L, sh)
 
-    frame_all_slots()
-    torch.cuda.synchronize()
-    g = hits.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1)
-    nhit = int(np.count_nonzero(g["flags"] & 1))
-    ref_sh = sh.cpu().numpy().copy()
-    shit = int(np.count_nonzero(ref_sh.view(vx.HIT_DTYPE).reshape(-1)["flags"] & 1))
-    sh.fill_(-1)
-    frame()
-    torch.cuda.synchronize()
-    same = bool(np.array_equal(sh.cpu().numpy(), ref_sh))
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    ms = statistics.mean(events_ms(frame, steps, warmup, flush))
+    prim_ms = events_ms(lambda: scene.cast_rays_dev(rays, hits, col), steps, warmup, flush)
+    mean_s = statistics.mean(prim_ms) / 1e3
+    algo = bytes_per_launch(n, tot["run_iters"], tot["run_grid_reads"], tot["run_dda_steps"], nhit, scene.color_kind)
+    peak, peak_kind = measured_peaks()
+    out = {"config": cfg3_config(wl.R, wl.width, wl.height), "mrays_s": (n + nhit) / (ms / 1e3) / 1e6,
+           "ms_per_frame": ms, "steps": steps, "primary_rays": n, "shadow_rays": nhit, "primary_hit_rate": nhit / n,
+           "shadowed_fraction": float(np.count_nonzero(g_sh["flags"] & 1)) / max(nhit, 1),
+           "bricks": int(wl.scene.brick_count), "nodes": int(wl.scene.node_count),
+           "scene_device_bytes": scene.device_bytes(), "setup_s": setup_s,
+           "roofline": {"bound": "hbm", "kernel": "vx::cast_kernel (primary pass)", "kernel_ms_mean": mean_s * 1e3,
+                        "achieved": algo / mean_s / 1e9, "peak": peak, "unit": "GB/s",
+                        "frac": algo / mean_s / 1e9 / peak, "peak_source": peak_kind,
+                        "traffic": profiled_traffic("vx::cast_kernel", wl.name),
+                        "algorithmic_bytes_per_launch": algo, "per_ray": {k: v / n for k, v in tot.items()}}}
+    del scene, rays, hits, col, sh
+    torch.cuda.empty_cache()
+    if with_oracle:
+        vo = load_oracle()
+        wr = load_oracle_workloads()
+        t0 = time.perf_counter()
+        o = vo.OracleScene.from_dense(wl.bits, wl.R, wl.scene.max_levels)
+        build_s = time.perf_counter() - t0
+        idx = np.arange(0, n, max(1, n // 65536), dtype=np.int64)
+        oh = o.cast_rays(rays_np[idx], threads=0)
+        o_col = vo.hit_texels_dxt(wl.scene.brick_color, oh)
+        so = o.cast_rays(wr.spawn_shadow(rays_np[idx], oh, L), threads=0)
+        out["parity_sample"] = {"checked": int(idx.size), "stride": int(n // 65536), "oracle_build_s": build_s,
+                                "primary_mismatches": mismatches(g[idx], oh, g_col[idx], o_col),
+                                "shadow_mismatches": mismatches(g_sh[idx], so),
+                                "fields": "flags, brick, node, voxel, scale, t bits (+ DXT1 texel bits on primaries)"}
+    return out
 
-    def timed(fn):
-        for _ in range(warmup):
-            fn()
-        torch.cuda.synchronize()
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
-        for a, b in ev:
-            flush.zero_()
-            a.record()
-            fn()
-            b.record()
-        torch.cuda.synchronize()
-        return sum(a.elapsed_time(b) for a, b in ev) / steps
 
-    ms_all = timed(frame_all_slots)
-    ms = timed(frame)
-    rays_per_frame = n + nhit
-    return {"workload": f"{wl.name}: urban {wl.R}^3 (depth {wl.scene.max_levels}), 32x32 blocks, heights "
-                        f"U[64,1800], DXT1; {wl.width}x{wl.height} primary + 1 shadow ray per hit",
-            "ray_order": "primary rays in 8x4-pixel warp tiles (workloads.tile_order)",
-            "mrays_s": rays_per_frame / (ms / 1e3) / 1e6, "ms_per_frame": ms,
-            "frame": "primary cast, then vx_cast_shadow_rays (the shadow rays of hits, compacted)",
-            "ms_per_frame_all_slots": ms_all, "shadow_hits_equal_all_slots": same, "primary_rays": n,
-            "shadow_rays": nhit, "primary_hit_rate": nhit / n, "shadowed_fraction": shit / max(nhit, 1),
-            "bricks": bricks, "nodes": nodes, "scene_device_bytes": dev_bytes, "setup_s": setup_s}
+# ---------------------------------------------------------------------------
+# Reference arm: the oracle (CPU restatement of castRay) on this host's cores
+# ---------------------------------------------------------------------------
+
+def run_reference(args, rank, world):
+    """The reference's CPU path over a bounded sample of the same frame, every input built on the
+    oracle side (oracle/workloads_ref.py) without loading the product library.  Under torchrun only
+    rank 0 runs."""
+    if rank != 0:
+        return 0
+    vo = load_oracle()
+    wr = load_oracle_workloads()
+    threads = os.cpu_count() or 1
+    t_setup = time.perf_counter()
+    if args.workload == "cfg2":
+        fr = wr.cfg2(R=args.R, seed=args.seed)
+        rays_all = fr.rays()
+        o = fr.scene()
+        config = cfg2_config(args.R, fr.width, fr.height, world)
+
+        def step(idx):
+            o.cast_rays(rays_all[idx], threads=threads)
+            return idx.size
+        n = rays_all.shape[0]
+        sample_of = lambda m: np.arange(m, dtype=np.int64)  # noqa: E731  (the frame's first m rays)
+        what = "first {m} of {n} rays of the frame per step"
+    else:
+        specs = wr.cfg4_specs(args.scenes, seed=4)
+        frames = [wr.cfg4_frame(sp, threads) for sp in specs]
+        rays = [f.rays() for f in frames]
+        begin = np.concatenate([[0], np.cumsum([r.shape[0] for r in rays])]).astype(np.int64)
+        rays_all = np.concatenate(rays)
+        del rays
+        osc = oracle_scenes(vo, [(f.bits, f.R, f.max_levels) for f in frames])
+        for f in frames:
+            f.bits = None
+        config = cfg4_config(specs)
+        n = int(begin[-1])
+
+        pool = cf.ThreadPoolExecutor(max_workers=threads)
+
+        def step(idx):
+            prim, _, _, _ = oracle_cfg4_pass(vo, wr, osc, rays_all, begin, idx, threads, pool)
+            return idx.size + 2 * int(np.count_nonzero(prim["flags"] & 1))
+        sample_of = lambda m: cfg4_sample(begin, m)  # noqa: E731
+        what = "every (n / {m})th primary ray of the frame over all scenes, and the 2 bounce rays of each hit, per step"
+    setup_s = time.perf_counter() - t_setup
+    m = 1 << 13
+    while True:  # size one step at about 1 s
+        t0 = time.perf_counter()
+        step(sample_of(m))
+        dt = time.perf_counter() - t0
+        if dt >= 0.25 or m >= n:
+            break
+        m = min(n, m * 4)
+    m = min(n, max(1024, int(m * 1.0 / max(dt, 1e-3))))
+    idx = sample_of(m)
+    for _ in range(args.warmup):
+        step(idx)
+    times, units = [], 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        units = step(idx)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    v = units * args.steps / total / 1e6
+    sample = what.format(m=m, n=n) + f"; {units} rays per step, {threads} threads; setup {setup_s:.1f} s"
+    line = {"metric": METRIC, "value": v, "unit": "Mrays/s", "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": config,
+            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 def measure_cfg5(args, rank, world, steps, warmup):
@@ -813,62 +1171,75 @@ def measure_tour(args):
             "ms": out}
 
 
-def config_dict(wl, world):
-    return {"workload": f"{wl.name}: cave {wl.R}^3 (depth {wl.scene.max_levels}), value noise spacing "
-                        f"{64 * wl.R // 1024}, 5 octaves, 50% fill, DXT1 bricks, {wl.width}x{wl.height} FP32 "
-                        f"primary rays per rank, plain cast kernel",
-            "ray_order": "8x4-pixel warp tiles in 32x8 blocks (vx_render's order; workloads.tile_order)",
-            "rays_per_step_per_gpu": wl.width * wl.height, "bricks": int(wl.scene.brick_count),
-            "nodes": int(wl.scene.node_count), "parallelism": f"replicated scene, {world} camera(s)",
-            "l2": "flushed between timed steps (256 MiB write)"}
-
-
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="vx", choices=["vx", "reference"])
-    ap.add_argument("--R", type=int, default=1024)
+    ap.add_argument("--workload", default="cfg4", choices=["cfg4", "cfg2", "cfg3", "cfg5", "next", "tour"],
+                    help="cfg4 (default): the 64-scene batched frame vs plain launches, with cfg2, cfg3, cfg5 and the "
+                         "next rows attached at N=1; cfg2: plain cast of the 1024^3 cave frame; cfg3: the 2048^3 "
+                         "urban frame with shadow rays; cfg5: forward / adjoint ms per view; next: device builder, "
+                         "payload encoders, LOD cut, compressed render, cache file; tour: every kernel once, "
+                         "CUDA-event times per step (the command for ncu captures)")
+    ap.add_argument("--R", type=int, default=1024, help="cfg2 / next: grid side of the cave scene")
+    ap.add_argument("--R3", type=int, default=2048, help="cfg3: grid side of the urban scene")
     ap.add_argument("--seed", type=int, default=2)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg3", "cfg4", "cfg5", "next", "tour"],
-                    help="cfg2: plain cast of the 1024^3 cave frame (with the cfg4, cfg5 and next-row results "
-                         "attached at N=1); cfg4: 64-scene batched frame vs plain; cfg5: forward / adjoint ms per "
-                         "view; next: device builder, payload encoders, LOD cut, compressed render, cache file; "
-                         "tour: every kernel once, CUDA-event times per step (the command for ncu captures)")
-    ap.add_argument("--no-extra", action="store_true",
-                    help="cfg2 only: skip the attached batched (cfg4), adjoint (cfg5) and next-row measurements")
     ap.add_argument("--scenes", type=int, default=64, help="cfg4: number of scenes")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the oracle legs (CPU baseline and parity samples)")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="cfg4 only: skip the attached cfg2, cfg3, adjoint and next-row measurements")
     ap.add_argument("--split-views", action="store_true",
                     help="cfg5: split the views over the ranks and all-reduce the gradient (default when N > 1; "
                          "needs a process group, i.e. torchrun, also for N = 1)")
     ap.add_argument("--soak-seconds", type=float, default=1.5,
-                    help="untimed launches before timing so clocks reach steady state")
+                    help="cfg2: untimed launches before timing so clocks reach steady state")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
+        if args.workload not in ("cfg4", "cfg2"):
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": f"the reference arm times cfg4 (default) or "
+                                                                      f"cfg2, not {args.workload}"}), flush=True)
+            return 0
         return run_reference(args, rank, world)
     if args.workload == "cfg4":
         return run_cfg4(args, rank, world)
+    import torch
+    torch.cuda.set_device(local)
+    if args.workload == "cfg2":
+        import torch.distributed as dist
+        from datetime import timedelta
+        if world > 1:
+            dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+        res = measure_cfg2(args, rank, world, args.steps, args.warmup,
+                           with_cpu=(world == 1 and not args.no_cpu_baseline))
+        if world > 1:
+            dist.destroy_process_group()
+        if rank == 0:
+            line = {"metric": METRIC, "value": res.pop("value"), "unit": res.pop("unit"), "n_gpus": world,
+                    "steps": args.steps, "warmup": args.warmup, "ms_per_step": res.pop("ms_per_frame"),
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                    "data": "synthetic", "config": res.pop("config"), "gpu_launches": args.steps}
+            line.update(res)
+            print(json.dumps(line), flush=True)
+        return 0
     if args.workload == "cfg3":
-        import torch
-        torch.cuda.set_device(local)
-        res = measure_cfg3(args, args.steps, args.warmup)
+        res = measure_cfg3(args, args.steps, args.warmup, with_oracle=not args.no_cpu_baseline)
         if rank == 0:
             line = {"metric": METRIC, "value": res["mrays_s"], "unit": "Mrays/s", "n_gpus": 1, "steps": args.steps,
                     "warmup": args.warmup, "ms_per_step": res["ms_per_frame"], "higher_is_better": True,
                     "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                     # per frame: primary cast, shadow hit count, scan, compacted spawn, shadow cast
-                    "config": {"workload": res.pop("workload")}, "gpu_launches": args.steps * 5}
+                    "config": res.pop("config"), "gpu_launches": args.steps * 5}
             line.update(res)
             print(json.dumps(line), flush=True)
         return 0
     if args.workload == "tour":
-        import torch
-        torch.cuda.set_device(local)
         res = measure_tour(args)
         if rank == 0:
             print(json.dumps({"workload": "tour", "tour": res}), flush=True)
@@ -878,11 +1249,9 @@ def main():
         if rank == 0:
             print(json.dumps({"workload": "next", "next_rows": res}), flush=True)
         return 0
-    if args.workload == "cfg5" and (world > 1 or args.split_views):
-        import torch
+    if world > 1 or args.split_views:
         import torch.distributed as dist
         from datetime import timedelta
-        torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
         res = measure_cfg5_multi(args, rank, world, args.steps, args.warmup)
         dist.destroy_process_group()
@@ -895,163 +1264,15 @@ def main():
                               "config": {"workload": res.pop("workload")}, "adjoint": res,
                               "gpu_launches": args.steps * 2}), flush=True)
         return 0
-    if args.workload == "cfg5":
-        import torch
-        torch.cuda.set_device(local)
-        res = measure_cfg5(args, rank, world, args.steps, args.warmup)
-        if rank == 0:
-            a = res["voxel_rgb"]
-            print(json.dumps({"metric": METRIC, "value": a["fwd_bwd_ms_per_view"], "unit": "ms/view", "n_gpus": 1,
-                              "steps": args.steps, "warmup": args.warmup,
-                              "ms_per_step": a["fwd_bwd_ms_per_view"] * 16, "higher_is_better": False,
-                              "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                              "config": {"workload": res.pop("workload")}, "adjoint": res,
-                              "gpu_launches": args.steps * 2}), flush=True)  # per fwd+bwd step: 1 forward, 1 adjoint
-        return 0
-
-    import numpy as np
-    import torch
-    import torch.distributed as dist
-    from datetime import timedelta
-    torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
-    vx = load_pkg()
-    wl = make_workload(vx, args.R, args.seed, rank, True)
-    scene = vx.Scene(wl.scene)
-    rays_np = wl.rays(order="tiled")
-    n = rays_np.shape[0]
-    rays = torch.from_numpy(rays_np).cuda()
-    hits = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
-    color = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
-    counters = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
-    stream = torch.cuda.current_stream()
-
-    # Counting pass (untimed): per-ray work for the algorithmic-byte count.
-    scene.cast_rays_dev(rays, hits, color, counters)
-    torch.cuda.synchronize()
-    cnt = counters.cpu().numpy().view(vx.COUNTER_DTYPE).reshape(-1)
-    g_hits = hits.cpu().numpy().view(vx.HIT_DTYPE).reshape(-1).copy()
-    nhit = int(np.count_nonzero(g_hits["flags"] & 1))
-    tot = {k: int(cnt[k].astype(np.int64).sum()) for k in cnt.dtype.names}
-    # Bytes the kernel has to move (iterations after a detected cycle repeat
-    # data already read and are not counted) and, for reference, the bytes of
-    # the full 500-iteration reference loop.
-    algo_bytes = bytes_per_launch(n, tot["run_iters"], tot["run_grid_reads"], tot["run_dda_steps"], nhit,
-                                  scene.color_kind)
-    ref_bytes = bytes_per_launch(n, tot["iters"], tot["grid_reads"], tot["dda_steps"], nhit, scene.color_kind)
-
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    sampler = ClockSampler(local)
-    sampler.start()
-    t_soak = time.perf_counter()
-    for _ in range(args.warmup):
-        scene.cast_rays_dev(rays, hits, color)
-    torch.cuda.synchronize()
-    while time.perf_counter() - t_soak < args.soak_seconds:  # clocks to steady state before timing
-        for _ in range(20):
-            scene.cast_rays_dev(rays, hits, color)
-        torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    for k in range(args.steps):
-        flush.zero_()
-        ev0[k].record(stream)
-        scene.cast_rays_dev(rays, hits, color)
-        ev1[k].record(stream)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    step_ms = [a.elapsed_time(b) for a, b in zip(ev0, ev1)]
-    total_ms = sum(step_ms)
-
-    # e2e through the host-buffer entry point: pinned rays in, hits + texels out.
-    rays_h = torch.from_numpy(rays_np).pin_memory()
-    hits_h = torch.zeros((n, 4), dtype=torch.int32).pin_memory()
-    col_h = torch.zeros((n, 3), dtype=torch.float32).pin_memory()
-    L = vx.lib()
-
-    def e2e_call():
-        vx.check(L.vx_cast_rays_host(scene.handle, C.c_void_p(rays_h.data_ptr()), n, 0.0, vx.FLT_MAX,
-                                     C.c_void_p(hits_h.data_ptr()), C.c_void_p(col_h.data_ptr()),
-                                     C.c_void_p(stream.cuda_stream)))
-
-    for _ in range(args.warmup):
-        e2e_call()
-    e0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    e1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    for k in range(args.steps):
-        flush.zero_()
-        e0[k].record(stream)
-        e2e_call()
-        e1[k].record(stream)
-    torch.cuda.synchronize()
-    clocks = sampler.stop()
-    e2e_ms = sum(a.elapsed_time(b) for a, b in zip(e0, e1))
-    e2e_same = bool(np.array_equal(hits_h.numpy().view(np.uint8), g_hits.view(np.uint8).reshape(n, 16)))
-
-    from vx_b200 import multigpu as M
-    total_ms, e2e_ms = M.max_over_ranks([total_ms, e2e_ms])
-    if world > 1:
-        dist.destroy_process_group()
-    if rank != 0:
-        return 0
-
-    value = M.aggregate_throughput(n * args.steps, world, total_ms / 1e3) / 1e6
-    e2e_value = M.aggregate_throughput(n * args.steps, world, e2e_ms / 1e3) / 1e6
-    mean_s = statistics.mean(step_ms) / 1e3
-    peak, peak_kind = measured_peaks()
-    achieved = algo_bytes / mean_s / 1e9
-    traffic = None
-    tf = os.path.join(ROOT, "profiles", "cast_kernel_traffic.json")
-    if os.path.exists(tf):
-        try:
-            with open(tf) as f:
-                d = json.load(f)
-            if d.get("workload") == wl.name:
-                traffic = d.get("dram_bytes_per_launch")
-        except Exception:
-            pass
-    line = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": config_dict(wl, world),
-            "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": world * n * 24,
-                    "d2h_bytes_per_step": world * n * (16 + 12), "hits_equal_device_path": e2e_same},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "algorithmic_bytes_per_launch": algo_bytes,
-                         "reference_loop_bytes_per_launch": ref_bytes,
-                         "per_ray": {k: v / n for k, v in tot.items()},
-                         "kernel": "vx::cast_kernel", "kernel_ms_mean": mean_s * 1e3},
-            "gpu_launches": args.steps, "hit_rate": nhit / n,
-            "clocks": clocks}
-    if world == 1 and not args.no_cpu_baseline:
-        vo = load_oracle()
-        cb, parity = cpu_baseline(vo, wl, rays_np, g_hits)
-        line["cpu_baseline"] = cb
-        line["parity_sample"] = parity
-    if world == 1 and not args.no_extra:
-        del scene
-        torch.cuda.empty_cache()
-        extra_steps, extra_warmup = max(3, min(args.steps, 5)), max(2, min(args.warmup, 3))
-        b = measure_cfg4(args, rank, world, extra_steps, extra_warmup)
-        line["batched"] = {"workload": b["config"]["workload"], "rays_per_frame": b["config"]["rays_per_frame"],
-                           "batched_mrays_s": b["batched"]["value"], "plain_mrays_s": b["plain"]["value"],
-                           "speedup_batched_vs_plain": b["speedup_batched_vs_plain"],
-                           "batched_ms_per_frame": b["batched"]["ms_per_frame"],
-                           "batched_ms_per_frame_uncompacted": b["batched"]["ms_per_frame_uncompacted"],
-                           "hits_identical": b["hits_identical_batched_vs_plain"], "tuning": b["batched"]["tuning"],
-                           "steps": extra_steps}
-        torch.cuda.empty_cache()
-        line["adjoint"] = measure_cfg5(args, rank, world, extra_steps, extra_warmup)
-        torch.cuda.empty_cache()
-        line["next_rows"] = measure_next(args, extra_steps, extra_warmup)
-    print(json.dumps(line), flush=True)
+    res = measure_cfg5(args, rank, world, args.steps, args.warmup)
+    if rank == 0:
+        a = res["voxel_rgb"]
+        print(json.dumps({"metric": METRIC, "value": a["fwd_bwd_ms_per_view"], "unit": "ms/view", "n_gpus": 1,
+                          "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": a["fwd_bwd_ms_per_view"] * 16, "higher_is_better": False,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                          "config": {"workload": res.pop("workload")}, "adjoint": res,
+                          "gpu_launches": args.steps * 2}), flush=True)  # per fwd+bwd step: 1 forward, 1 adjoint
     return 0
 
 

@@ -76,8 +76,14 @@ typedef enum vx_color_kind {
     VX_COLOR_NONE = 0,
     VX_COLOR_RGBA8 = 1,  /* 512 x u32 per brick, voxel z*64+y*8+x (brickData layout,
                             VoxelSceneCacher.cpp:551-578) */
-    VX_COLOR_DXT1 = 2    /* 32 x u64 BC1 blocks per brick, block = voxel >> 4
+    VX_COLOR_DXT1 = 2,   /* 32 x u64 BC1 blocks per brick, block = voxel >> 4
                             (VoxelRayMarch_Compressed.comp:142-158) */
+    VX_COLOR_MATERIAL = 3 /* 512 x u32 material words per brick, voxel z*64+y*8+x:
+                            the reference's brickData (VoxelSceneCacher.cpp:551-587,
+                            material id per voxel, 0 = empty).  A hit is coloured
+                            getMaterialColor(word & 0xFF) (shaders/Materials.glsl:18-60,
+                            VoxelRayMarch.comp:188-192); occupancy (brick_occ) must be
+                            word != 0, the shader's test */
 } vx_color_kind;
 
 /* Host-side description of a scene: the buffers VoxelGridNode publishes
@@ -217,8 +223,11 @@ int vx_scene_download(const vx_scene* scene, uint32_t* nodes, uint32_t* node_bri
  * checksum.  VSCA version 1: the reference's format (one entry written;
  * reading picks entry `entry`): ESVO descriptors in ChildDescriptor layout
  * (child pointers must fit 15 bits), brickData material words (occupied = 1),
- * DXT1 colours, DXT normals, brickGridLookup, OctreeConfig.  A vx_cache holds
- * the host arrays; vx_cache_desc exposes them for vx_scene_create.
+ * DXT1 colours, DXT normals, brickGridLookup, OctreeConfig.  Reading keeps the
+ * brickData material words (occupancy = word != 0); writing stores a
+ * VX_COLOR_MATERIAL scene's words as brickData (otherwise 1 per occupied
+ * voxel).  A vx_cache holds the host arrays; vx_cache_desc exposes them for
+ * vx_scene_create.
  * --------------------------------------------------------------------- */
 typedef struct vx_cache vx_cache;
 int vx_cache_write(const char* path, const vx_scene_desc* desc);
@@ -227,6 +236,12 @@ int vx_cache_write_vsca(const char* path, const vx_scene_desc* desc, uint32_t sc
                         uint32_t resolution, float density, uint32_t seed);
 int vx_cache_read_vsca(const char* path, uint32_t entry, vx_cache** out);
 int vx_cache_desc(const vx_cache* cache, vx_scene_desc* desc);
+/* The same scene with the material words of a VSCA file's brickData as its
+ * colour (VX_COLOR_MATERIAL): the uncompressed shader's colour source
+ * (VoxelRayMarch.comp:188-192).  vx_cache_desc gives the file's DXT1 colours
+ * when it has them and the material words otherwise.  VX_EINVAL when the
+ * cache holds no material words (VXSC files of other colour kinds). */
+int vx_cache_desc_materials(const vx_cache* cache, vx_scene_desc* desc);
 int vx_cache_free(vx_cache* cache);
 /* vx_scene_download + vx_cache_write, and vx_cache_read + vx_scene_create. */
 int vx_scene_save(const vx_scene* scene, const char* path);
@@ -249,7 +264,8 @@ int vx_scene_create_dense_dev(const uint64_t* bits_dev, uint32_t R, int32_t max_
  * SVOBrickDDA.cpp:65-533) for a batch of rays, with identical results.
  * t_min / t_max clip the ray like castRay's tMin / tMax.
  * counters_dev and color_dev may be NULL.  color_dev receives, per ray, the
- * hit voxel's RGBA8 word (u32) for VX_COLOR_RGBA8 scenes or its decoded DXT1
+ * hit voxel's RGBA8 word (u32) for VX_COLOR_RGBA8 scenes, its material word
+ * (u32) for VX_COLOR_MATERIAL scenes, or its decoded DXT1
  * texel (3 floats, DXT1ColorCompressor::decodeColorHead,
  * VoxelData/src/Compression/DXT1Compressor.cpp:14-36) for VX_COLOR_DXT1 scenes;
  * misses leave zeros.
@@ -421,6 +437,21 @@ int vx_batch_capture_frame_compact(vx_batch* batch, const vx_ray* primary_dev, c
                                    uint32_t n, vx_hit* primary_hits_dev, vx_ray* bounce_dev,
                                    vx_hit* bounce_hits_dev, uint64_t seed, void* stream);
 int vx_batch_launch_frame(vx_batch* batch, void* stream);
+/* The captured frame from host buffers: copies n primary rays in (into the
+ * primary buffer the frame was captured with), replays the frame, copies the
+ * n primary hits out while the bounce pass runs and the 2n bounce hits out
+ * after it, and returns when every result is in host memory.  Pinned host
+ * buffers let the copies run at full link speed. */
+int vx_batch_launch_frame_host(vx_batch* batch, const vx_ray* primary_host, vx_hit* primary_hits_host,
+                               vx_hit* bounce_hits_host, void* stream);
+/* Layout of a compacted frame after it has run: the compacted bounce rays of
+ * scene s are bounce_dev[scene_begin[s] .. scene_begin[s + 1]) (count + 1 host
+ * u32), and compacted ray j's record is bounce_hits_dev[map[j]] (map_host:
+ * scene_begin[count] host u32).  Synchronous reads; any pointer may be NULL.
+ * cbegin_dev / map_dev receive the device addresses of those arrays, valid
+ * until the next capture. */
+int vx_batch_frame_compaction(const vx_batch* batch, uint32_t* scene_begin, uint32_t* map_host,
+                              const uint32_t** cbegin_dev, const uint32_t** map_dev);
 /* Tuning of the bounce pass of a captured frame (default, or after a null
  * tuning: the batch's own).  Incoherent bounce rays favour other shapes than
  * camera rays: autotune each pass on its own rays.  Applies to later captures. */
@@ -498,6 +529,15 @@ int vx_build_normals_dev(const uint32_t* brick_occ_dev, uint32_t brick_count, ui
 int vx_build_dxt1(const float* rgb, const uint32_t* brick_occ, uint32_t brick_count, uint64_t* out);
 int vx_build_dxt1_dev(const float* rgb_dev, const uint32_t* brick_occ_dev, uint32_t brick_count,
                       uint64_t* out_dev, void* stream);
+
+/* Per-voxel colours of material words for the DXT1 payload: rgb[3i..3i+2] =
+ * MaterialIdToColor(words[i]) (SVO/src/SVORebuild.cpp:68-120, the colour the
+ * reference's compressed payload is encoded from at :679-700; its ids 33-39
+ * differ from the shader's getMaterialColor).  Feed the result to
+ * vx_build_dxt1 / vx_build_dxt1_dev with the bricks' occupancy.  The host
+ * form uses all host threads; both give identical bits. */
+int vx_material_rgb(const uint32_t* words, uint64_t n, float* rgb);
+int vx_material_rgb_dev(const uint32_t* words_dev, uint64_t n, float* rgb_dev, void* stream);
 
 /* Converts reference-layout descriptors (64-bit ChildDescriptor,
  * SVOTypes.h:36-47: childPointer:15 far:1 valid:8 leaf:8 | brick:24 flags:8)

@@ -100,24 +100,26 @@ int vxo_synth_noise(uint32_t R, uint32_t spacing, uint32_t octaves, float fill, 
             const float wy = fy * fy * (3.0f - 2.0f * fy), wz = fz * fz * (3.0f - 2.0f * fz);
             const uint32_t j = uint32_t(fy0), k = uint32_t(fz0);
             float* v = &value[size_t(row) * R];
+            // the row's y-then-z blend at every lattice column it reaches, then one x blend per voxel
+            const uint32_t cols = R / s + 2;
+            std::vector<float> yz(cols);
+            const float* l = lattice.data();
+            for (uint32_t i = 0; i < cols; ++i) {
+                const float c00 = l[(size_t(k) * L + j) * L + i];
+                const float c10 = l[(size_t(k) * L + j + 1) * L + i];
+                const float c01 = l[(size_t(k + 1) * L + j) * L + i];
+                const float c11 = l[(size_t(k + 1) * L + j + 1) * L + i];
+                const float alongY0 = c00 + wy * (c10 - c00);
+                const float alongY1 = c01 + wy * (c11 - c01);
+                yz[i] = alongY0 + wz * (alongY1 - alongY0);
+            }
             for (uint32_t x = 0; x < R; ++x) {
                 const float px = (float(x) + 0.5f) / fs;
                 const float fx0 = std::floor(px);
                 const float fx = px - fx0;
                 const float wx = fx * fx * (3.0f - 2.0f * fx);
                 const uint32_t i = uint32_t(fx0);
-                float yz[2];
-                for (int di = 0; di < 2; ++di) {  // the two lattice columns i, i + 1
-                    const float* l = lattice.data();
-                    const float c00 = l[(size_t(k) * L + j) * L + i + di];
-                    const float c10 = l[(size_t(k) * L + j + 1) * L + i + di];
-                    const float c01 = l[(size_t(k + 1) * L + j) * L + i + di];
-                    const float c11 = l[(size_t(k + 1) * L + j + 1) * L + i + di];
-                    const float alongY0 = c00 + wy * (c10 - c00);
-                    const float alongY1 = c01 + wy * (c11 - c01);
-                    yz[di] = alongY0 + wz * (alongY1 - alongY0);
-                }
-                v[x] = v[x] + weight * (yz[0] + wx * (yz[1] - yz[0]));
+                v[x] = v[x] + weight * (yz[i] + wx * (yz[i + 1] - yz[i]));
             }
         });
     }

@@ -199,6 +199,23 @@ def test_compacted_frame_equals_eager(vx, cuda, big, bounce_tuning):
         ((rows[:, 5] > 0).astype(np.int64) << 2)
     want = rows[np.lexsort((np.arange(rows.shape[0]), octant, sc))]
     np.testing.assert_array_equal(got[:2 * h].view(np.uint32), want.view(np.uint32))
+    # vx_batch_frame_compaction: per-scene ranges of the compacted rays and their hit slots
+    sb, slot = batch.frame_compaction()
+    assert sb[0] == 0 and sb[-1] == 2 * h and np.all(np.diff(sb.astype(np.int64)) >= 0)
+    np.testing.assert_array_equal(np.diff(sb.astype(np.int64)), np.bincount(sc, minlength=len(begin) - 1))
+    slots = np.flatnonzero(np.repeat(hit, 2))  # slot 2i + k of every bounce ray of a hit
+    np.testing.assert_array_equal(np.sort(slot), slots)
+    np.testing.assert_array_equal(got[:2 * h].view(np.uint32), eager_bounce[slot.astype(np.int64)].view(np.uint32))
+    # vx_batch_launch_frame_host: the same frame from pinned host buffers
+    rays_h = d_rays.cpu().pin_memory()
+    ph_h = torch.full((n, 4), -1, dtype=torch.int32).pin_memory()
+    bh_h = torch.full((2 * n, 4), -1, dtype=torch.int32).pin_memory()
+    d_rays.zero_()  # the call copies the rays in itself
+    for _ in range(2):
+        batch.launch_frame_host(rays_h, ph_h, bh_h, s.cuda_stream)
+        np.testing.assert_array_equal(ph_h.numpy(), eager_ph)
+        np.testing.assert_array_equal(bh_h.numpy(), eager_bh)
+        ph_h.fill_(-1), bh_h.fill_(-1)
 
 
 def test_autotune_keeps_results(vx, cuda):

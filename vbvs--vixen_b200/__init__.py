@@ -27,7 +27,7 @@ VX_HIT_HIT = 0x01
 VX_HIT_NORMAL_NEG = 0x08
 VX_RAY_ITER_CAP = 0x40
 VX_RAY_INVALID = 0x80
-VX_COLOR_NONE, VX_COLOR_RGBA8, VX_COLOR_DXT1 = 0, 1, 2
+VX_COLOR_NONE, VX_COLOR_RGBA8, VX_COLOR_DXT1, VX_COLOR_MATERIAL = 0, 1, 2, 3
 FLT_MAX = 3.4028234663852886e38
 NONE = 0xFFFFFFFF
 
@@ -114,6 +114,9 @@ def lib():
         "vx_cache_write_vsca": (C.c_int, [C.c_char_p, vp, u32, u32, f32, u32]),
         "vx_cache_read_vsca": (C.c_int, [C.c_char_p, u32, vp]),
         "vx_cache_desc": (C.c_int, [vp, vp]),
+        "vx_cache_desc_materials": (C.c_int, [vp, vp]),
+        "vx_material_rgb": (C.c_int, [vp, u64, vp]),
+        "vx_material_rgb_dev": (C.c_int, [vp, u64, vp, vp]),
         "vx_cache_free": (C.c_int, [vp]),
         "vx_scene_save": (C.c_int, [vp, C.c_char_p]),
         "vx_scene_load": (C.c_int, [C.c_char_p, vp]),
@@ -142,6 +145,8 @@ def lib():
         "vx_batch_capture_frame_compact": (C.c_int, [vp, vp, vp, u32, vp, vp, vp, u64, vp]),
         "vx_cast_shadow_rays": (C.c_int, [vp, vp, vp, u32, vp, C.c_float, C.c_float, vp, vp]),
         "vx_batch_launch_frame": (C.c_int, [vp, vp]),
+        "vx_batch_launch_frame_host": (C.c_int, [vp, vp, vp, vp, vp]),
+        "vx_batch_frame_compaction": (C.c_int, [vp, vp, vp, vp, vp]),
         "vx_batch_set_bounce_tuning": (C.c_int, [vp, vp]),
         "vx_cast_batch_noalloc": (C.c_int, [vp, u32, vp, vp, u32, f32, f32, vp, vp]),
         "vx_diff_forward": (C.c_int, [vp, vp, u32, u32, i32, vp, vp, vp, vp, vp]),
@@ -283,6 +288,19 @@ def build_dxt1(rgb: np.ndarray, brick_occ: np.ndarray) -> np.ndarray:
     return out
 
 
+def material_rgb(words: np.ndarray) -> np.ndarray:
+    """vx_material_rgb: MaterialIdToColor of every material word, (n, 3) float32 (host)."""
+    w = np.ascontiguousarray(words, np.uint32).reshape(-1)
+    out = np.zeros((w.size, 3), np.float32)
+    check(lib().vx_material_rgb(_p(w), w.size, _p(out)))
+    return out
+
+
+def material_rgb_dev(words, out, stream=None):
+    """vx_material_rgb_dev: words (n) 32-bit CUDA tensor -> out (n*3) float32 CUDA tensor."""
+    check(lib().vx_material_rgb_dev(_p(words), words.numel(), _p(out), _stream(stream)))
+
+
 def build_dxt1_dev(rgb, occ, out, stream=None):
     """vx_build_dxt1_dev: rgb (bricks*512*3) float32, occ (bricks*16) 32-bit, out (bricks*32) 8-byte CUDA tensors."""
     check(lib().vx_build_dxt1_dev(_p(rgb), _p(occ), occ.numel() // 16, _p(out), _stream(stream)))
@@ -345,9 +363,9 @@ def _desc_of(a: SceneArrays):
     return d, keep
 
 
-def _arrays_of_cache(h) -> SceneArrays:
+def _arrays_of_cache(h, materials=False) -> SceneArrays:
     d = _SceneDesc()
-    check(lib().vx_cache_desc(h, C.byref(d)))
+    check((lib().vx_cache_desc_materials if materials else lib().vx_cache_desc)(h, C.byref(d)))
     bpa, B, D = d.config.bricks_per_axis, d.brick_count, d.node_count
 
     def take(ptr, n, dt):
@@ -357,7 +375,7 @@ def _arrays_of_cache(h) -> SceneArrays:
         return np.frombuffer(buf, dtype=dt, count=n).copy()
 
     color = None
-    if d.color_kind == VX_COLOR_RGBA8:
+    if d.color_kind in (VX_COLOR_RGBA8, VX_COLOR_MATERIAL):
         color = take(d.brick_color, 512 * B, np.uint32)
     elif d.color_kind == VX_COLOR_DXT1:
         color = take(d.brick_color, 32 * B, np.uint64)
@@ -391,11 +409,13 @@ def cache_write_vsca(path: str, arrays: SceneArrays, scene_type: int, resolution
     check(lib().vx_cache_write_vsca(os.fsencode(path), C.byref(d), scene_type, resolution, float(density), seed))
 
 
-def cache_read_vsca(path: str, entry: int = 0) -> SceneArrays:
+def cache_read_vsca(path: str, entry: int = 0, materials: bool = False) -> SceneArrays:
+    """vx_cache_read_vsca -> host arrays; colour = the file's DXT1 colours (vx_cache_desc), or its
+    brickData material words with materials=True (vx_cache_desc_materials)."""
     h = C.c_void_p()
     check(lib().vx_cache_read_vsca(os.fsencode(path), entry, C.byref(h)))
     try:
-        return _arrays_of_cache(h)
+        return _arrays_of_cache(h, materials)
     finally:
         lib().vx_cache_free(h)
 
@@ -435,7 +455,7 @@ class Scene:
         nodes, nb = np.zeros(2 * D, np.uint32), np.zeros(D, np.uint32)
         grid, coord, occ = np.zeros(bpa ** 3, np.uint32), np.zeros(B, np.uint32), np.zeros(16 * B, np.uint32)
         color = None
-        if i.color_kind == VX_COLOR_RGBA8:
+        if i.color_kind in (VX_COLOR_RGBA8, VX_COLOR_MATERIAL):
             color = np.zeros(512 * B, np.uint32)
         elif i.color_kind == VX_COLOR_DXT1:
             color = np.zeros(32 * B, np.uint64)
@@ -489,7 +509,7 @@ class Scene:
 
     # -- device-buffer calls (torch tensors) --------------------------------
     def color_width(self) -> int:
-        return {VX_COLOR_NONE: 0, VX_COLOR_RGBA8: 1, VX_COLOR_DXT1: 3}[self.color_kind]
+        return {VX_COLOR_NONE: 0, VX_COLOR_RGBA8: 1, VX_COLOR_DXT1: 3, VX_COLOR_MATERIAL: 1}[self.color_kind]
 
     def cast_rays_dev(self, rays, hits, color=None, counters=None, t_min=0.0, t_max=FLT_MAX, stream=None, lod=None):
         """rays: (n,6) float32 CUDA tensor; hits: (n,4) int32/uint32 CUDA tensor (16 B per ray).
@@ -715,6 +735,21 @@ class Batch:
 
     def launch_frame(self, stream=None):
         check(lib().vx_batch_launch_frame(self._h, _stream(stream)))
+
+    def launch_frame_host(self, primary_host, primary_hits_host, bounce_hits_host, stream=None):
+        """vx_batch_launch_frame_host: the captured frame from host buffers (rays in, both hit
+        buffers out); returns when the results are in host memory."""
+        check(lib().vx_batch_launch_frame_host(self._h, _p(primary_host), _p(primary_hits_host),
+                                               _p(bounce_hits_host), _stream(stream)))
+
+    def frame_compaction(self):
+        """vx_batch_frame_compaction after a compacted frame has run: (scene offsets of the
+        compacted bounce rays, count + 1 entries; hit slot of every compacted ray)."""
+        sb = np.zeros(len(self.scenes) + 1, np.uint32)
+        check(lib().vx_batch_frame_compaction(self._h, _p(sb), None, None, None))
+        mp = np.zeros(int(sb[-1]), np.uint32)
+        check(lib().vx_batch_frame_compaction(self._h, None, _p(mp), None, None))
+        return sb, mp
 
 
 def spawn_bounce_rays(rays, hits, seed, out, stream=None):

@@ -99,7 +99,7 @@ int scene_alloc(const vx_octree_config& c, uint32_t node_count, uint32_t brick_c
     q.sz_grid = bpa * bpa * bpa * 4;
     q.sz_coord = uint64_t(brick_count) * 4;
     q.sz_occ = uint64_t(brick_count) * 64;
-    if (color_kind == VX_COLOR_RGBA8) q.sz_color = uint64_t(brick_count) * 512 * 4;
+    if (color_kind == VX_COLOR_RGBA8 || color_kind == VX_COLOR_MATERIAL) q.sz_color = uint64_t(brick_count) * 512 * 4;
     if (color_kind == VX_COLOR_DXT1) q.sz_color = uint64_t(brick_count) * 32 * 8;
     q.sz_nrm = normals ? uint64_t(brick_count) * 32 * 16 : 0;
     const uint64_t o_nodes = 0;
@@ -152,7 +152,8 @@ int scene_alloc(const vx_octree_config& c, uint32_t node_count, uint32_t brick_c
     ds.coord = reinterpret_cast<const uint32_t*>(q.coord);
     ds.occ = reinterpret_cast<const uint4*>(q.occ);
     ds.color_kind = color_kind;
-    ds.rgba = color_kind == VX_COLOR_RGBA8 ? reinterpret_cast<const uint32_t*>(q.color) : nullptr;
+    ds.rgba = (color_kind == VX_COLOR_RGBA8 || color_kind == VX_COLOR_MATERIAL) ? reinterpret_cast<const uint32_t*>(q.color)
+                                                                                : nullptr;
     ds.dxt = color_kind == VX_COLOR_DXT1 ? reinterpret_cast<const uint2*>(q.color) : nullptr;
     ds.nrm = reinterpret_cast<const uint4*>(q.nrm);
     s->cfg = c;
@@ -190,7 +191,8 @@ int validate(const vx_scene_desc* d) {
     if (!d->grid_lookup) return fail(VX_EINVAL, "vx_scene_create: grid_lookup missing");
     if (d->brick_count && (!d->brick_coord || !d->brick_occ))
         return fail(VX_EINVAL, "vx_scene_create: brick buffers missing");
-    if (d->color_kind != VX_COLOR_NONE && d->color_kind != VX_COLOR_RGBA8 && d->color_kind != VX_COLOR_DXT1)
+    if (d->color_kind != VX_COLOR_NONE && d->color_kind != VX_COLOR_RGBA8 && d->color_kind != VX_COLOR_DXT1 &&
+        d->color_kind != VX_COLOR_MATERIAL)
         return fail(VX_EINVAL, "vx_scene_create: unknown color_kind");
     if (d->color_kind != VX_COLOR_NONE && d->brick_count && !d->brick_color)
         return fail(VX_EINVAL, "vx_scene_create: brick_color missing");
@@ -295,7 +297,9 @@ int vx_scene_download(const vx_scene* s, uint32_t* nodes, uint32_t* node_brick, 
     if (!s) return fail(VX_EINVAL, "vx_scene_download: null scene");
     const vx::DevScene& d = s->dev;
     const uint64_t bpa = uint64_t(d.bpa), B = d.brick_count;
-    const uint64_t colw = d.color_kind == VX_COLOR_RGBA8 ? 512 * 4 : d.color_kind == VX_COLOR_DXT1 ? 32 * 8 : 0;
+    const uint64_t colw = (d.color_kind == VX_COLOR_RGBA8 || d.color_kind == VX_COLOR_MATERIAL) ? 512 * 4
+                          : d.color_kind == VX_COLOR_DXT1                                   ? 32 * 8
+                                                                                            : 0;
     const void* color_src = d.rgba ? static_cast<const void*>(d.rgba) : static_cast<const void*>(d.dxt);
     struct Copy { void* dst; const void* src; uint64_t n; };
     const Copy copies[] = {{nodes, d.nodes, uint64_t(d.node_count) * 8}, {node_brick, d.node_brick, uint64_t(d.node_count) * 4},

@@ -620,6 +620,17 @@ struct vx_batch {
     cudaGraph_t frame_graph = nullptr;
     void* fscratch = nullptr;  // compacted frame: chunk counts and offsets, scene offsets, hit slots
     uint64_t fscratch_bytes = 0;
+    // Buffers of the captured frame, for vx_batch_launch_frame_host and
+    // vx_batch_frame_compaction.
+    const vx_ray* f_primary = nullptr;
+    vx_hit* f_primary_hits = nullptr;
+    vx_hit* f_bounce_hits = nullptr;
+    uint32_t f_n = 0;
+    const uint32_t* f_cbegin = nullptr;  // compacted frame: S + 1 scene offsets of the compacted rays
+    const uint32_t* f_map = nullptr;     // compacted frame: hit slot of each compacted ray
+    cudaEvent_t ev_primary = nullptr;    // recorded inside the frame once the primary pass is done
+    cudaEvent_t ev_copied = nullptr;
+    cudaStream_t side = nullptr;         // copies the primary hits out while the bounce pass runs
 };
 
 namespace {
@@ -750,6 +761,9 @@ int vx_batch_destroy(vx_batch* b) {
     if (!b) return VX_OK;
     if (b->frame) cudaGraphExecDestroy(b->frame);
     if (b->frame_graph) cudaGraphDestroy(b->frame_graph);
+    if (b->ev_primary) cudaEventDestroy(b->ev_primary);
+    if (b->ev_copied) cudaEventDestroy(b->ev_copied);
+    if (b->side) cudaStreamDestroy(b->side);
     cudaFree(b->scenes);
     cudaFree(b->work);
     cudaFree(b->fscratch);
@@ -917,6 +931,36 @@ int launch_shadow_compact(const vx_ray* rays, const vx_hit* hits, uint32_t n, co
 
 }  // namespace vx
 
+namespace {
+
+// The frame's events and side stream, created once per batch outside any capture.
+int ensure_frame_events(vx_batch* b) {
+    cudaError_t e = cudaSuccess;
+    if (!b->ev_primary) e = cudaEventCreateWithFlags(&b->ev_primary, cudaEventDisableTiming);
+    if (e == cudaSuccess && !b->ev_copied) e = cudaEventCreateWithFlags(&b->ev_copied, cudaEventDisableTiming);
+    if (e == cudaSuccess && !b->side) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
+    return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_batch: frame events");
+}
+
+// Inside a capture: an external event node that marks the end of the primary
+// pass, so vx_batch_launch_frame_host can copy the primary hits out while the
+// bounce pass runs.
+int record_primary_done(vx_batch* b, cudaStream_t st) {
+    cudaError_t e = cudaEventRecordWithFlags(b->ev_primary, st, cudaEventRecordExternal);
+    return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_batch: primary-pass event");
+}
+
+void forget_frame(vx_batch* b) {
+    if (b->frame) { cudaGraphExecDestroy(b->frame); b->frame = nullptr; }
+    if (b->frame_graph) { cudaGraphDestroy(b->frame_graph); b->frame_graph = nullptr; }
+    b->f_primary = nullptr;
+    b->f_primary_hits = b->f_bounce_hits = nullptr;
+    b->f_n = 0;
+    b->f_cbegin = b->f_map = nullptr;
+}
+
+}  // namespace
+
 extern "C" {
 
 int vx_batch_capture_frame(vx_batch* b, const vx_ray* primary, const uint32_t* primary_begin, uint32_t n,
@@ -928,14 +972,15 @@ int vx_batch_capture_frame(vx_batch* b, const vx_ray* primary, const uint32_t* p
     if (int r = vx::ensure_bounce_table()) return r;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (!st) return fail(VX_EINVAL, "vx_batch_capture_frame: capture needs a non-default stream");
-    if (b->frame) { cudaGraphExecDestroy(b->frame); b->frame = nullptr; }
-    if (b->frame_graph) { cudaGraphDestroy(b->frame_graph); b->frame_graph = nullptr; }
+    forget_frame(b);
     // Resolve shared-memory attributes and occupancy outside the capture.
     if (int r = prepare_batch(b, b->tuning)) return r;
     if (int r = prepare_batch(b, bounce_tuning_of(b))) return r;
+    if (int r = ensure_frame_events(b)) return r;
     cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_err(e, "vx_batch_capture_frame: begin capture");
     int r = vx_cast_batch(b, primary, primary_begin, n, 0.0f, 3.402823466e+38f, primary_hits, nullptr, stream);
+    if (r == VX_OK) r = record_primary_done(b, st);
     if (r == VX_OK) r = vx_spawn_bounce_rays(primary, primary_hits, n, seed, bounce, stream);
     if (r == VX_OK)
         r = cast_batch_with(b, bounce_tuning_of(b), bounce, bounce_begin, 2 * n, 0.0f, 3.402823466e+38f, bounce_hits,
@@ -947,6 +992,10 @@ int vx_batch_capture_frame(vx_batch* b, const vx_ray* primary, const uint32_t* p
     e = cudaGraphInstantiate(&b->frame, g, 0);
     if (e != cudaSuccess) { cudaGraphDestroy(g); return cuda_err(e, "vx_batch_capture_frame: instantiate"); }
     b->frame_graph = g;
+    b->f_primary = primary;
+    b->f_primary_hits = primary_hits;
+    b->f_bounce_hits = bounce_hits;
+    b->f_n = n;
     return VX_OK;
 }
 
@@ -961,10 +1010,10 @@ static int vx_batch_capture_frame_compact_body(vx_batch* b, const vx_ray* primar
     if (int r = vx::ensure_bounce_table()) return r;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (!st) return fail(VX_EINVAL, "vx_batch_capture_frame_compact: capture needs a non-default stream");
-    if (b->frame) { cudaGraphExecDestroy(b->frame); b->frame = nullptr; }
-    if (b->frame_graph) { cudaGraphDestroy(b->frame_graph); b->frame_graph = nullptr; }
+    forget_frame(b);
     if (int r = prepare_batch(b, b->tuning)) return r;
     if (int r = prepare_batch(b, bounce_tuning_of(b))) return r;
+    if (int r = ensure_frame_events(b)) return r;
     // The chunk table follows the scene offsets, read once here: primary rays
     // of scene s are [begin[s], begin[s + 1]), split into chunks of at most
     // COMPACT_CHUNK rays.
@@ -1015,6 +1064,7 @@ static int vx_batch_capture_frame_compact_body(vx_batch* b, const vx_ray* primar
     e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_err(e, "vx_batch_capture_frame_compact: begin capture");
     int r = vx_cast_batch(b, primary, primary_begin, n, 0.0f, 3.402823466e+38f, primary_hits, nullptr, stream);
+    if (r == VX_OK) r = record_primary_done(b, st);
     if (r == VX_OK) {
         vx::compact_count_kernel<<<nc, 256, 0, st>>>(chunk_dev, primary, primary_hits, seed, counts);
         vx::compact_offsets_kernel<<<1, 1024, 0, st>>>(counts, first_dev, b->S, offs, tot, cbegin);
@@ -1033,6 +1083,12 @@ static int vx_batch_capture_frame_compact_body(vx_batch* b, const vx_ray* primar
     e = cudaGraphInstantiate(&b->frame, g, 0);
     if (e != cudaSuccess) { cudaGraphDestroy(g); return cuda_err(e, "vx_batch_capture_frame_compact: instantiate"); }
     b->frame_graph = g;
+    b->f_primary = primary;
+    b->f_primary_hits = primary_hits;
+    b->f_bounce_hits = bounce_hits;
+    b->f_n = n;
+    b->f_cbegin = cbegin;
+    b->f_map = map;
     return VX_OK;
 }
 
@@ -1049,6 +1105,50 @@ int vx_batch_launch_frame(vx_batch* b, void* stream) {
     if (!b || !b->frame) return fail(VX_EINVAL, "vx_batch_launch_frame: no captured frame");
     cudaError_t e = cudaGraphLaunch(b->frame, static_cast<cudaStream_t>(stream));
     return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_batch_launch_frame");
+}
+
+int vx_batch_launch_frame_host(vx_batch* b, const vx_ray* primary_host, vx_hit* primary_hits_host,
+                               vx_hit* bounce_hits_host, void* stream) {
+    if (!b || !b->frame) return fail(VX_EINVAL, "vx_batch_launch_frame_host: no captured frame");
+    if (!primary_host || !primary_hits_host || !bounce_hits_host)
+        return fail(VX_EINVAL, "vx_batch_launch_frame_host: null argument");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t n = b->f_n;
+    // rays in; the frame; the primary hits out on the side stream as soon as
+    // the frame's primary pass is done (while the bounce pass runs); the
+    // bounce hits out after the frame; return when both copies are done.
+    cudaError_t e = cudaMemcpyAsync(const_cast<vx_ray*>(b->f_primary), primary_host, n * sizeof(vx_ray),
+                                    cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaGraphLaunch(b->frame, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->side, b->ev_primary, 0);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(primary_hits_host, b->f_primary_hits, n * sizeof(vx_hit), cudaMemcpyDeviceToHost, b->side);
+    if (e == cudaSuccess) e = cudaEventRecord(b->ev_copied, b->side);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(bounce_hits_host, b->f_bounce_hits, 2 * n * sizeof(vx_hit), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, b->ev_copied, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_batch_launch_frame_host");
+}
+
+int vx_batch_frame_compaction(const vx_batch* b, uint32_t* scene_begin, uint32_t* map_host,
+                              const uint32_t** cbegin_dev, const uint32_t** map_dev) {
+    if (!b || !b->frame || !b->f_cbegin)
+        return fail(VX_EINVAL, "vx_batch_frame_compaction: no compacted frame captured");
+    if (cbegin_dev) *cbegin_dev = b->f_cbegin;
+    if (map_dev) *map_dev = b->f_map;
+    if (scene_begin || map_host) {
+        std::vector<uint32_t> sb(size_t(b->S) + 1);
+        cudaError_t e = cudaMemcpy(sb.data(), b->f_cbegin, sb.size() * 4, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_err(e, "vx_batch_frame_compaction: read offsets");
+        if (sb[b->S] > 2 * uint64_t(b->f_n)) return fail(VX_EINVAL, "vx_batch_frame_compaction: frame has not run");
+        if (scene_begin) std::copy(sb.begin(), sb.end(), scene_begin);
+        if (map_host && sb[b->S]) {
+            e = cudaMemcpy(map_host, b->f_map, size_t(sb[b->S]) * 4, cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) return cuda_err(e, "vx_batch_frame_compaction: read slot map");
+        }
+    }
+    return VX_OK;
 }
 
 }  // extern "C"

@@ -16,6 +16,7 @@ struct vx_cache {
     std::vector<uint32_t> nodes, node_brick, grid, coord, occ;
     int32_t color_kind = VX_COLOR_NONE;
     std::vector<uint8_t> color, normal;
+    std::vector<uint32_t> materials;  // a VSCA file's brickData words (512 per brick), or empty
 };
 
 namespace {
@@ -66,7 +67,7 @@ template <class T>
 bool get_v(FILE* f, T& v) { return get(f, &v, sizeof(T)); }
 
 uint64_t color_bytes_per_brick(int32_t kind) {
-    return kind == VX_COLOR_RGBA8 ? 512 * 4 : kind == VX_COLOR_DXT1 ? 32 * 8 : 0;
+    return (kind == VX_COLOR_RGBA8 || kind == VX_COLOR_MATERIAL) ? 512 * 4 : kind == VX_COLOR_DXT1 ? 32 * 8 : 0;
 }
 
 // Host copies of a vx_scene_desc's arrays, after the checks vx_scene_create
@@ -205,8 +206,9 @@ int vx_cache_read(const char* path, vx_cache** out) {
 // VoxelSceneCacher::SerializeToFile (VoxelSceneCacher.cpp:209-265) for one
 // entry.  The reference's ChildDescriptor holds a 15-bit child pointer and no
 // far pointers, so scenes whose child pointers reach 2^15 cannot be written
-// (VX_EOVERFLOW) rather than truncated.  brickData holds material 1 for every
-// occupied voxel; the material table is written empty.
+// (VX_EOVERFLOW) rather than truncated.  brickData holds the material words of
+// a VX_COLOR_MATERIAL scene, else material 1 for every occupied voxel; the
+// material table is written empty.
 static int vx_cache_write_vsca_body(const char* path, const vx_scene_desc* d, uint32_t scene_type, uint32_t resolution,
                         float density, uint32_t seed) {
     if (!path) return fail(VX_EINVAL, "vx_cache_write_vsca: null path");
@@ -226,12 +228,17 @@ static int vx_cache_write_vsca_body(const char* path, const vx_scene_desc* d, ui
     }
     std::vector<uint32_t> brick_data(B * 512, 0u);
     uint32_t solid = 0;
+    const uint32_t* words = c.color_kind == VX_COLOR_MATERIAL ? reinterpret_cast<const uint32_t*>(c.color.data())
+                                                              : nullptr;
     for (uint64_t b = 0; b < B; ++b)
         for (uint32_t v = 0; v < 512; ++v)
             if ((c.occ[b * 16 + (v >> 5)] >> (v & 31)) & 1u) {
-                brick_data[b * 512 + v] = 1u;
+                brick_data[b * 512 + v] = words ? words[b * 512 + v] : 1u;
+                if (brick_data[b * 512 + v] == 0u)
+                    return fail(VX_EINVAL, "vx_cache_write_vsca: an occupied voxel has material word 0");
                 ++solid;
             }
+    if (words) c.color.clear();  // the words went into brickData; the file's colour section stays empty
     RefOctreeConfig oc;
     std::memset(&oc, 0, sizeof(oc));
     const int32_t L = c.cfg.max_levels;
@@ -348,6 +355,7 @@ static int vx_cache_read_vsca_body(const char* path, uint32_t entry, vx_cache** 
         for (uint64_t b = 0; b < bc; ++b)
             for (uint32_t v = 0; v < 512; ++v)
                 if (bd[b * 512 + v]) c->occ[b * 16 + (v >> 5)] |= 1u << (v & 31);
+        c->materials.assign(bd, bd + uint64_t(bc) * 512);
         if (!colors.empty()) {
             c->color_kind = VX_COLOR_DXT1;
             c->color = std::move(colors);
@@ -376,7 +384,22 @@ int vx_cache_desc(const vx_cache* c, vx_scene_desc* d) {
     d->brick_occ = c->occ.data();
     d->color_kind = c->color.empty() ? VX_COLOR_NONE : c->color_kind;
     d->brick_color = c->color.empty() ? nullptr : c->color.data();
+    if (c->color.empty() && !c->materials.empty()) {
+        d->color_kind = VX_COLOR_MATERIAL;
+        d->brick_color = c->materials.data();
+    }
     d->brick_normal = c->normal.empty() ? nullptr : c->normal.data();
+    return VX_OK;
+}
+
+int vx_cache_desc_materials(const vx_cache* c, vx_scene_desc* d) {
+    if (int r = vx_cache_desc(c, d)) return r;
+    if (!c->materials.empty()) {
+        d->color_kind = VX_COLOR_MATERIAL;
+        d->brick_color = c->materials.data();
+    } else if (c->color_kind != VX_COLOR_MATERIAL || c->color.empty()) {
+        return fail(VX_EINVAL, "vx_cache_desc_materials: the cache holds no material words");
+    }
     return VX_OK;
 }
 

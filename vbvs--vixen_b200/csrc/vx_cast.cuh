@@ -41,9 +41,8 @@ constexpr int MAX_ITER = 500;       // SVOTraversal.cpp:588
 #ifndef VX_CYCLE_START
 #define VX_CYCLE_START 3
 #endif
-constexpr int CYCLE_START = VX_CYCLE_START;  // iteration from which loop states are recorded
-constexpr int CYC_SLOT = 9;                   // words of one recorded state: 8 + their sum
-constexpr int CYC_WORDS = 2 * CYC_SLOT;       // cycle-detection words per ray
+constexpr int CYCLE_START = VX_CYCLE_START;  // iteration from which loop states are compared
+constexpr int CYC_WORDS = 8;                  // words of the one loop state a ray may hold for confirmation
 constexpr float FLT_MAX_ = 3.402823466e+38f;
 constexpr uint32_t NONE = 0xFFFFFFFFu;
 
@@ -225,8 +224,10 @@ struct CastState {
     uint32_t pushed;       // stack slots written by PUSH (bit scale - minScale)
     float t_root;          // t_max of the unwritten slots
     // cycle detection
-    uint32_t d1g, d1d;
-    int nrec;
+    uint32_t d1g, d1d;     // grid reads / DDA steps of the previous iteration
+    uint32_t sig1, sig2;   // signatures of the loop states one and two iterations back
+    int nsig;              // signatures recorded (saturates at 2)
+    int cand_p, cand_at;   // pending candidate: period, iteration whose state must equal the stored one
 };
 
 __device__ __forceinline__ void cast_finish(CastState& st) {
@@ -406,7 +407,9 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
     st.hh = t_max;
     st.mValid = st.mLeaf = st.pChild = st.pValid = st.pLeaf = 0;
     st.d1g = st.d1d = 0;
-    st.nrec = 0;
+    st.sig1 = st.sig2 = 0;
+    st.nsig = 0;
+    st.cand_p = st.cand_at = 0;
     return false;
 }
 
@@ -418,10 +421,16 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
 // rewrites stack slots with the values they already hold.  So once the state
 // repeats after one or two iterations the ray can neither hit nor leave before
 // the 500-iteration cap: the result is the capped miss and the remaining
-// iterations' counters repeat the cycle's.  The two previous states are kept
-// in shared memory (cyc[(p * CYC_SLOT + k) * stride], slot p = iteration
-// parity) from iteration CYCLE_START on.  With LOD the cut test reads only the
-// loop state and per-ray constants, so a repeating state still cannot end.
+// iterations' counters repeat the cycle's.  From iteration CYCLE_START on,
+// every state gets a 32-bit signature, and the signatures of the two previous
+// states stay in registers.  A signature equal to the one p iterations back
+// (p = 1 or 2) makes the state a candidate: it is stored (cyc[k * stride],
+// shared memory) and the state p iterations later is compared with it word
+// by word.  Equal states prove the repeat; unequal ones drop the candidate.
+// Equal states always have equal signatures, so every repeat is caught, at
+// most p iterations after the first state that repeats.  With LOD the cut
+// test reads only the loop state and per-ray constants, so a repeating state
+// still cannot end.
 //
 // LOD: castRayWithLOD (SVOTraversal.cpp:198-232) with LODParameters `lod`
 // (enabled, lod.dir > 0): the termination test of :613-651 runs on every
@@ -675,42 +684,43 @@ next_iter:
         cur[2] = __float_as_uint(st.px); cur[3] = __float_as_uint(st.py); cur[4] = __float_as_uint(st.pz);
         cur[5] = __float_as_uint(st.t_min); cur[6] = __float_as_uint(st.t_max); cur[7] = __float_as_uint(st.hh);
         const uint32_t dg = h.grid_reads - g0, ddd = h.dda_steps - dd0;
-        // two slots by parity: the other parity holds the state one iteration
-        // back, this parity two back; this state replaces the latter.  Each
-        // slot also keeps a sum of its words: states are compared word by
-        // word only when the sums agree (a repeat always has equal sums).
-        uint32_t* back2 = cyc + ((st.iter & 1) * CYC_SLOT) * stride;
-        const uint32_t* back1 = cyc + (((st.iter & 1) ^ 1) * CYC_SLOT) * stride;
-        const uint32_t sum = ((cur[0] + cur[1] + cur[2]) + (cur[3] + cur[4] + cur[5])) + (cur[6] + cur[7]);
-        bool eq1 = st.nrec >= 1 && back1[8 * stride] == sum;
-        bool eq2 = st.nrec >= 2 && back2[8 * stride] == sum;
-        if (eq1 || eq2) {
+        if (st.cand_p && st.iter == st.cand_at) {
+            bool eq = true;
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                eq1 = eq1 && (cur[k] == back1[k * stride]);
-                eq2 = eq2 && (cur[k] == back2[k * stride]);
+            for (int k = 0; k < 8; ++k) eq = eq && (cur[k] == cyc[k * stride]);
+            if (eq) {  // state(iter) == state(iter - cand_p): the cycle is proven
+                const uint32_t rem = uint32_t(MAX_ITER - st.iter);
+                h.run_iters = uint32_t(st.iter);
+                h.run_grid_reads = h.grid_reads;
+                h.run_dda_steps = h.dda_steps;
+                if (st.cand_p == 1) {
+                    h.grid_reads += rem * dg;
+                    h.dda_steps += rem * ddd;
+                } else {
+                    h.grid_reads += ((rem + 1) / 2) * st.d1g + (rem / 2) * dg;
+                    h.dda_steps += ((rem + 1) / 2) * st.d1d + (rem / 2) * ddd;
+                }
+                h.iters = uint32_t(MAX_ITER);
+                h.flags |= F_ITER_CAP;
+                return true;
+            }
+            st.cand_p = 0;
+        }
+        // signature: a mix of the eight words (odd multipliers, so one word's change always changes it)
+        const uint32_t sig = ((cur[0] + cur[1] * 0x9E3779B1u) ^ (cur[2] * 0x85EBCA77u + cur[3])) +
+                             ((cur[4] * 0xC2B2AE3Du + cur[5]) ^ (cur[6] * 0x27D4EB2Fu + cur[7] * 0x165667B1u));
+        if (!st.cand_p) {
+            const int p = (st.nsig >= 1 && sig == st.sig1) ? 1 : ((st.nsig >= 2 && sig == st.sig2) ? 2 : 0);
+            if (p) {
+#pragma unroll
+                for (int k = 0; k < 8; ++k) cyc[k * stride] = cur[k];
+                st.cand_p = p;
+                st.cand_at = st.iter + p;
             }
         }
-#pragma unroll
-        for (int k = 0; k < 8; ++k) back2[k * stride] = cur[k];
-        back2[8 * stride] = sum;
-        if (eq1 || eq2) {
-            const uint32_t rem = uint32_t(MAX_ITER - st.iter);
-            h.run_iters = uint32_t(st.iter);
-            h.run_grid_reads = h.grid_reads;
-            h.run_dda_steps = h.dda_steps;
-            if (eq1) {
-                h.grid_reads += rem * dg;
-                h.dda_steps += rem * ddd;
-            } else {
-                h.grid_reads += ((rem + 1) / 2) * st.d1g + (rem / 2) * dg;
-                h.dda_steps += ((rem + 1) / 2) * st.d1d + (rem / 2) * ddd;
-            }
-            h.iters = uint32_t(MAX_ITER);
-            h.flags |= F_ITER_CAP;
-            return true;
-        }
-        ++st.nrec;
+        st.sig2 = st.sig1;
+        st.sig1 = sig;
+        st.nsig = st.nsig < 2 ? st.nsig + 1 : 2;
         st.d1g = dg;
         st.d1d = ddd;
     }
@@ -773,10 +783,11 @@ __device__ __forceinline__ void store_hit(vx_hit* hits, uint32_t i, const Hit& h
     reinterpret_cast<uint4*>(hits)[i] = v;
 }
 
-// Colour of the hit voxel; 0 on a miss and on an LOD hit (no voxel).
+// Colour of the hit voxel (the RGBA8 or material word, or the decoded DXT1
+// texel); 0 on a miss and on an LOD hit (no voxel).
 __device__ __forceinline__ void store_color(const DevScene& s, void* color, uint32_t i, const Hit& h) {
     const bool hit = (h.flags & F_HIT) && h.brick != NONE;
-    if (s.color_kind == VX_COLOR_RGBA8) {
+    if (s.color_kind == VX_COLOR_RGBA8 || s.color_kind == VX_COLOR_MATERIAL) {
         reinterpret_cast<uint32_t*>(color)[i] =
             hit ? __ldg(s.rgba + size_t(bounded(h.brick, s.brick_count, V_BRICK)) * 512 +
                         bounded(h.voxel, 512u, V_VOXEL))

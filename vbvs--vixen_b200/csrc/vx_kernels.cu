@@ -1,5 +1,6 @@
 // vx_kernels.cu - plain (one launch per scene) cast and render kernels.
 #include "vx_cast.cuh"
+#include "vx_palette.h"
 
 namespace vx {
 namespace {
@@ -103,6 +104,10 @@ __global__ void __launch_bounds__(RENDER_THREADS, 768 / RENDER_THREADS) render_k
                 bb = float((c >> 16) & 0xFFu) / 255.0f;
             } else if (s.color_kind == VX_COLOR_DXT1) {
                 dxt_texel(s.dxt, h.brick, h.voxel, br, bg, bb);
+            } else if (s.color_kind == VX_COLOR_MATERIAL) {
+                // getMaterialColor(voxelData & 0xFF) (VoxelRayMarch.comp:188-192)
+                const Rgb m = material_color_shader(__ldg(s.rgba + size_t(h.brick) * 512 + h.voxel) & 0xFFu);
+                br = m.r; bg = m.g; bb = m.b;
             }
             const float Ld = (1.0f * 1.0f + 1.0f * 1.0f) + (-1.0f) * (-1.0f);
             const float Linv = 1.0f / sqrtf(Ld);

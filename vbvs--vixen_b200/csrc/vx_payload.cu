@@ -11,9 +11,20 @@
 #include "vx_cast.cuh"
 #include "vx_dxt1.h"
 #include "vx_dxtn.h"
+#include "vx_palette.h"
 
 namespace vx {
 namespace {
+
+// MaterialIdToColor of every material word (grid-stride).
+__global__ void material_rgb_kernel(const uint32_t* __restrict__ words, uint64_t n, float* __restrict__ rgb) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        const Rgb c = material_color_payload(words[i]);
+        rgb[3 * i] = c.r;
+        rgb[3 * i + 1] = c.g;
+        rgb[3 * i + 2] = c.b;
+    }
+}
 
 // Thread i encodes block i & 31 of brick i >> 5.  The 32 threads of a warp
 // share one brick, so the occupancy words a thread reads (at most 6 of the
@@ -194,6 +205,48 @@ static int vx_build_dxt1_body(const float* rgb, const uint32_t* occ, uint32_t br
 
 extern "C" int vx_build_dxt1(const float* rgb, const uint32_t* occ, uint32_t brick_count, uint64_t* out) {
     return vx::guarded("vx_build_dxt1", [&] { return vx_build_dxt1_body(rgb, occ, brick_count, out); });
+}
+
+static int vx_material_rgb_body(const uint32_t* words, uint64_t n, float* rgb) {
+    if (n && (!words || !rgb)) return vx::fail(VX_EINVAL, "vx_material_rgb: null argument");
+    const unsigned T = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    auto work = [&](uint64_t a, uint64_t b) {
+        for (uint64_t i = a; i < b; ++i) {
+            const vx::Rgb c = vx::material_color_payload(words[i]);
+            rgb[3 * i] = c.r;
+            rgb[3 * i + 1] = c.g;
+            rgb[3 * i + 2] = c.b;
+        }
+    };
+    if (T == 1 || n < (uint64_t(1) << 16)) {
+        work(0, n);
+        return VX_OK;
+    }
+    std::vector<std::thread> th;
+    const uint64_t chunk = (n + T - 1) / T;
+    for (unsigned t = 0; t < T; ++t) {
+        const uint64_t a = uint64_t(t) * chunk, b = std::min(n, a + chunk);
+        if (a >= b) break;
+        th.emplace_back(work, a, b);
+    }
+    for (auto& x : th) x.join();
+    return VX_OK;
+}
+
+extern "C" int vx_material_rgb(const uint32_t* words, uint64_t n, float* rgb) {
+    return vx::guarded("vx_material_rgb", [&] { return vx_material_rgb_body(words, n, rgb); });
+}
+
+extern "C" int vx_material_rgb_dev(const uint32_t* words, uint64_t n, float* rgb, void* stream) {
+    using namespace vx;
+    if (n && (!words || !rgb)) return fail(VX_EINVAL, "vx_material_rgb_dev: null argument");
+    if (reinterpret_cast<uintptr_t>(words) % 4 || reinterpret_cast<uintptr_t>(rgb) % 4)
+        return fail(VX_EINVAL, "vx_material_rgb_dev: misaligned buffer");
+    if (n == 0) return VX_OK;
+    const uint64_t blocks = std::min<uint64_t>((n + 255) / 256, 148 * 16);
+    material_rgb_kernel<<<unsigned(blocks), 256, 0, static_cast<cudaStream_t>(stream)>>>(words, n, rgb);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_material_rgb_dev");
 }
 
 extern "C" int vx_hit_normals(const vx_scene* scene, const vx_hit* hits_dev, uint32_t n, float* normals_dev,
