@@ -117,6 +117,11 @@ int vxo_synth_noise(uint32_t R, uint32_t spacing, uint32_t octaves, float fill, 
                     uint64_t* out, int threads);
 int vxo_synth_urban(uint32_t R, uint32_t hmin, uint32_t hmax, uint64_t seed, uint64_t* out);
 void vxo_bounce_table(float* out /* 4096 x 3 */);
+/* Material colours: MaterialIdToColor (SVORebuild.cpp:68-120, the compressed
+ * payload's source) and getMaterialColor (shaders/Materials.glsl:18-60, the
+ * uncompressed shader's). */
+void vxo_material_color_cpu(uint32_t id, float out[3]);
+void vxo_material_color_shader(uint32_t id, float out[3]);
 /* kind 0: 2 bounce rays per ray (out 2n x 6); kind 1: a shadow ray toward
  * light (out n x 6).  index: each ray's position in its frame (NULL: i). */
 void vxo_spawn_rays(const float* rays, const vxo_hit* hits, const uint64_t* index, uint64_t n, int kind,

@@ -68,6 +68,8 @@ def lib():
         L.vxo_synth_urban.restype = C.c_int
         L.vxo_synth_urban.argtypes = [u32, u32, u32, u64, vp]
         L.vxo_bounce_table.argtypes = [vp]
+        L.vxo_material_color_cpu.argtypes = [u32, vp]
+        L.vxo_material_color_shader.argtypes = [u32, vp]
         L.vxo_spawn_rays.argtypes = [vp, vp, vp, u64, C.c_int, u64, vp, vp]
         L.vxo_hit_texels_dxt.argtypes = [vp, u64, vp, vp, vp]
         L.vxo_shade.restype = u32
@@ -304,6 +306,13 @@ def camera_rays(pc, width: int, height: int, with_uv_y: bool = False):
     uv = np.zeros(width * height, np.float32) if with_uv_y else None
     lib().vxo_camera_rays(_ptr(words), width, height, _ptr(out), _ptr(uv))
     return (out, uv) if with_uv_y else out
+
+
+def material_color(material_id: int, shader: bool = False) -> np.ndarray:
+    """MaterialIdToColor (shader=False) or getMaterialColor (shader=True) of one id, 3 float32."""
+    out = np.zeros(3, np.float32)
+    (lib().vxo_material_color_shader if shader else lib().vxo_material_color_cpu)(int(material_id), _ptr(out))
+    return out
 
 
 def hit_texels_dxt(brick_dxt: np.ndarray, hits: np.ndarray) -> np.ndarray:

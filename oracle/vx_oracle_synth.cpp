@@ -206,6 +206,62 @@ int vxo_synth_urban(uint32_t R, uint32_t hmin, uint32_t hmax, uint64_t seed, uin
     return 0;
 }
 
+// Material colours.  vxo_material_color_cpu: MaterialIdToColor
+// (SVO/src/SVORebuild.cpp:68-120), the colour the compressed payload is
+// encoded from.  vxo_material_color_shader: getMaterialColor
+// (shaders/Materials.glsl:18-60) of the uncompressed compute shader, whose
+// ids 33-39 are mix(stone0, stone1, (id - 33) / 6) with GLSL's
+// mix(x, y, a) = x * (1 - a) + y * a.  Both end in the same HSV wheel.
+namespace {
+struct Entry { uint32_t id; float r, g, b; };
+const Entry kListed[] = {
+    {1, 1.0f, 0.0f, 0.0f},     {2, 0.0f, 1.0f, 0.0f},     {3, 0.9f, 0.9f, 0.9f},     {4, 0.85f, 0.85f, 0.85f},
+    {5, 0.95f, 0.95f, 0.95f},  {6, 0.8f, 0.8f, 0.8f},     {7, 0.4f, 0.4f, 0.4f},     {10, 0.8f, 0.6f, 0.2f},
+    {11, 0.6f, 0.8f, 0.9f},    {20, 1.0f, 0.98f, 0.9f},   {30, 0.5f, 0.45f, 0.4f},   {31, 0.6f, 0.55f, 0.5f},
+    {32, 0.55f, 0.5f, 0.45f},  {40, 0.8f, 0.6f, 0.2f},    {50, 0.2f, 0.2f, 0.22f},   {60, 0.6f, 0.58f, 0.55f},
+    {61, 0.7f, 0.85f, 0.95f}};
+const Entry kStoneCpu[] = {
+    {33, 0.52f, 0.48f, 0.42f}, {34, 0.48f, 0.44f, 0.38f}, {35, 0.45f, 0.42f, 0.36f}, {36, 0.58f, 0.52f, 0.46f},
+    {37, 0.62f, 0.56f, 0.48f}, {38, 0.65f, 0.58f, 0.5f},  {39, 0.68f, 0.6f, 0.52f}};
+
+bool lookup(const Entry* t, size_t n, uint32_t id, float out[3]) {
+    for (size_t k = 0; k < n; ++k)
+        if (t[k].id == id) {
+            out[0] = t[k].r; out[1] = t[k].g; out[2] = t[k].b;
+            return true;
+        }
+    return false;
+}
+
+void hsv_wheel(uint32_t id, float out[3]) {
+    const float hue = static_cast<float>(id % 256) / 256.0f;
+    const float h = hue * 6.0f;
+    const int i = static_cast<int>(h);
+    const float f = h - static_cast<float>(i);
+    const float p = 0.8f * 0.3f, q = 0.8f * (1.0f - 0.7f * f), t = 0.8f * (1.0f - 0.7f * (1.0f - f));
+    const float rows[6][3] = {{0.8f, t, p}, {q, 0.8f, p}, {p, 0.8f, t}, {p, q, 0.8f}, {t, p, 0.8f}, {0.8f, p, q}};
+    const int r = i < 5 ? i : 5;
+    out[0] = rows[r][0]; out[1] = rows[r][1]; out[2] = rows[r][2];
+}
+}  // namespace
+
+void vxo_material_color_cpu(uint32_t id, float out[3]) {
+    if (lookup(kListed, sizeof(kListed) / sizeof(kListed[0]), id, out)) return;
+    if (lookup(kStoneCpu, sizeof(kStoneCpu) / sizeof(kStoneCpu[0]), id, out)) return;
+    hsv_wheel(id, out);
+}
+
+void vxo_material_color_shader(uint32_t id, float out[3]) {
+    if (lookup(kListed, sizeof(kListed) / sizeof(kListed[0]), id, out)) return;
+    if (id >= 33 && id <= 39) {
+        const float a = static_cast<float>(id - 33) / 6.0f;
+        const float lo[3] = {0.52f, 0.48f, 0.42f}, hi[3] = {0.68f, 0.6f, 0.52f};
+        for (int c = 0; c < 3; ++c) out[c] = lo[c] * (1.0f - a) + hi[c] * a;
+        return;
+    }
+    hsv_wheel(id, out);
+}
+
 void vxo_bounce_table(float* out) {
     for (uint32_t k = 0; k < 4096; ++k) {
         const uint64_t a = sm64(0xB0C0E5EEDULL + k), b = sm64(a);

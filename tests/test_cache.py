@@ -84,9 +84,12 @@ def _pack_vsca(entries):
         esvo = _ref_descriptors(a).tobytes()
         B = a.brick_count
         occ_bits = np.unpackbits(a.brick_occ.reshape(B, 16).view(np.uint8), axis=1, bitorder="little")
-        brick_data = np.where(occ_bits == 1, e.get("material", 1), 0).astype(np.uint32).tobytes()
+        if "words" in e:  # per-voxel material words (0 for empty voxels)
+            brick_data = np.ascontiguousarray(e["words"], np.uint32).tobytes()
+        else:
+            brick_data = np.where(occ_bits == 1, e.get("material", 1), 0).astype(np.uint32).tobytes()
         materials = np.zeros((e.get("n_materials", 64), 8), np.float32).tobytes()
-        colors = a.brick_color.tobytes() if a.brick_color is not None else b""
+        colors = a.brick_color.tobytes() if a.brick_color is not None and a.color_kind == 2 else b""
         normals = a.brick_normal.tobytes() if a.brick_normal is not None else b""
         grid = a.grid_lookup.astype(np.uint32).tobytes()
         for blob, elem in ((esvo, 1), (brick_data, 1), (materials, 32), (colors, 1), (normals, 1), (grid, 4)):
