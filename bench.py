@@ -474,6 +474,66 @@ def measure_cfg4(args, rank, world, steps, warmup, with_cpu):
     return out
 
 
+def run_cfg4_pass(args):
+    """One launch of each pass of the batched frame over the first `--scenes` scenes of the frame,
+    with the tunings the default run's autotuner picks (primary: block 256, 32 rays per task,
+    shared-memory stack; bounce: block 256, 256 rays per task, local stack, refill 16).  The
+    command for ncu captures of the frame's kernels on a small case: after the frame's graph, each
+    of --steps steps launches the primary pass, then the bounce pass over the compacted bounce
+    rays."""
+    import torch
+    vx = load_pkg()
+    from vx_b200 import workloads as W
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    specs = W.config4_specs(64, seed=4)[:args.scenes]
+    scenes, rays = [], []
+    for sp in specs:
+        bits = None
+        if sp.kind == "noise" and sp.R >= 256:
+            spacing = max(4, 64 * sp.R // 1024)
+            bits = vx.synth_noise_dev(sp.R, spacing, 5 if spacing >= 64 else 3, sp.fill, sp.seed,
+                                      False).cpu().numpy().view(np.uint64)
+        wl = W.build_spec(sp, bits)
+        scenes.append(vx.Scene(wl.scene))
+        rays.append(wl.rays(order="tiled"))
+    begin = np.concatenate([[0], np.cumsum([r.shape[0] for r in rays])]).astype(np.int64)
+    n = int(begin[-1])
+    d_rays = torch.from_numpy(np.concatenate(rays)).cuda()
+    d_begin = torch.from_numpy(begin.astype(np.int32)).cuda()
+    ph = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+    bh = torch.zeros((2 * n, 4), dtype=torch.int32, device="cuda")
+    bounce = torch.zeros((2 * n, 6), dtype=torch.float32, device="cuda")
+    batch = vx.Batch(scenes)
+    batch.set_tuning(256, 32, 1, 0)
+    batch.set_bounce_tuning(vx.BatchTuning(256, 256, 0, 16))
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        batch.capture_frame_compact(d_rays, d_begin, ph, bounce, bh, CFG4_SEED, s.cuda_stream)
+        batch.launch_frame(s.cuda_stream)
+    torch.cuda.synchronize()
+    cb, _ = batch.frame_compaction()
+    h2 = int(cb[-1])
+    d_cb = torch.from_numpy(cb.astype(np.int32)).cuda()
+    pbh = torch.zeros((max(h2, 1), 4), dtype=torch.int32, device="cuda")
+    times = []
+    for _ in range(max(1, args.steps)):  # each step: the primary pass, then the bounce pass
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        batch.set_tuning(256, 32, 1, 0)
+        ev[0].record()
+        batch.cast(d_rays, d_begin, ph)
+        ev[1].record()
+        batch.set_tuning(256, 256, 0, 16)
+        ev[2].record()
+        batch.cast(bounce[:h2], d_cb, pbh)
+        ev[3].record()
+        torch.cuda.synchronize()
+        times.append((ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3])))
+    print(json.dumps({"workload": "cfg4-passes", "scenes": len(specs), "primary_rays": n, "bounce_rays": h2,
+                      "primary_ms": [t[0] for t in times], "bounce_ms": [t[1] for t in times],
+                      "source_sha256": source_hash()}), flush=True)
+    return 0
+
+
 def run_cfg4(args, rank, world):
     """Prints the headline line: the batched frame (cfg4), with cfg2, cfg3, cfg5 and the next rows
     attached at N = 1."""
@@ -1185,12 +1245,14 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="vx", choices=["vx", "reference"])
-    ap.add_argument("--workload", default="cfg4", choices=["cfg4", "cfg2", "cfg3", "cfg5", "next", "tour"],
+    ap.add_argument("--workload", default="cfg4",
+                    choices=["cfg4", "cfg2", "cfg3", "cfg5", "next", "tour", "cfg4-passes"],
                     help="cfg4 (default): the 64-scene batched frame vs plain launches, with cfg2, cfg3, cfg5 and the "
                          "next rows attached at N=1; cfg2: plain cast of the 1024^3 cave frame; cfg3: the 2048^3 "
                          "urban frame with shadow rays; cfg5: forward / adjoint ms per view; next: device builder, "
                          "payload encoders, LOD cut, compressed render, cache file; tour: every kernel once, "
-                         "CUDA-event times per step (the command for ncu captures)")
+                         "CUDA-event times per step (the command for ncu captures); cfg4-passes: one launch of "
+                         "each pass of the batched frame over --scenes scenes (ncu captures of its kernels)")
     ap.add_argument("--R", type=int, default=1024, help="cfg2 / next: grid side of the cave scene")
     ap.add_argument("--R3", type=int, default=2048, help="cfg3: grid side of the urban scene")
     ap.add_argument("--seed", type=int, default=2)
@@ -1217,6 +1279,8 @@ def main():
         return run_reference(args, rank, world)
     if args.workload == "cfg4":
         return run_cfg4(args, rank, world)
+    if args.workload == "cfg4-passes":
+        return run_cfg4_pass(args)
     import torch
     torch.cuda.set_device(local)
     if args.workload == "cfg2":

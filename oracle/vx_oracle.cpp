@@ -6,7 +6,9 @@
  * this file.  Every function cites the reference file:line it restates; paths
  * are relative to the reference project's VIXEN/ directory.
  *
- * Substitutions (the reference cannot be built here):
+ * Substitutions (the reference's dependencies glm and gaia-ecs are not
+ * installed here; oracle/ref_shim/ compiles the reference itself against
+ * stand-ins for them, and tests/test_ref_pin.py holds this file to it):
  *  (1) glm -> V3 below, with glm's operation order: dot = (x*x + y*y) + z*z,
  *      normalize = v * (1 / sqrt(dot)), min(x,y) = (y < x) ? y : x,
  *      max(x,y) = (x < y) ? y : x, clamp = min(max(x, lo), hi).

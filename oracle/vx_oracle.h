@@ -8,11 +8,13 @@
  * Only tests, the smoke check and the CPU-baseline leg of the benchmark may
  * load it; the product library never links or calls it.
  *
- * Parity status: the reference cannot be compiled here (it needs glm,
- * gaia-ecs and TBB, none of which is available), and its own tests pin only
- * tolerances, so bit-level parity with the reference binary is UNPINNED.  The
- * restatement is pinned to the reference's behavioural tests (ported as KATs
- * in tests/test_oracle_kat.py) and to golden vectors it generated itself.
+ * Parity status: pinned to the reference's own code.  `make -C oracle ref`
+ * compiles the reference's rebuild, castRay / castRayWithLOD, brick DDA and
+ * rebuild payload encoders from its sources, with stand-ins for glm and
+ * gaia-ecs (not installed here; oracle/ref_shim/), and tests/test_ref_pin.py
+ * requires this restatement to give the same bits on the same voxels and
+ * rays.  It is also held to the reference's behavioural tests (KATs in
+ * tests/test_oracle_kat.py) and to golden vectors it generated itself.
  */
 #ifndef VX_ORACLE_H
 #define VX_ORACLE_H

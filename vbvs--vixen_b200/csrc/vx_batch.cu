@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_refill_kernel(BatchArgs a) 
             if (!tasks_left && next >= end) break;
             continue;
         }
-        if (active && cast_step(sc[sid], st, stkN, stkT, cyc, stride)) {
+        if (active && cast_step<false, !SMEM_STACK>(sc[sid], st, stkN, stkT, cyc, stride)) {
             store_hit(a.hits, out_slot(a, ray), st.h);
             store_counters(a.counters, out_slot(a, ray), st.h);
             active = false;
@@ -215,7 +215,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
             const float2* r2 = reinterpret_cast<const float2*>(a.rays + r);
             const float2 p = __ldg(r2), q = __ldg(r2 + 1), w = __ldg(r2 + 2);
             Hit h;
-            cast_ray(sc[lo], p.x, p.y, q.x, q.y, w.x, w.y, a.tmin, a.tmax, stkN, stkT, cyc, stride, h);
+            cast_ray<false, !SMEM_STACK>(sc[lo], p.x, p.y, q.x, q.y, w.x, w.y, a.tmin, a.tmax, stkN, stkT, cyc,
+                                         stride, h);
             store_hit(a.hits, out_slot(a, r), h);
             store_counters(a.counters, out_slot(a, r), h);
         }

@@ -42,7 +42,7 @@ constexpr int MAX_ITER = 500;       // SVOTraversal.cpp:588
 #define VX_CYCLE_START 3
 #endif
 constexpr int CYCLE_START = VX_CYCLE_START;  // iteration from which loop states are compared
-constexpr int CYC_WORDS = 8;                  // words of the one loop state a ray may hold for confirmation
+constexpr int CYC_WORDS = 16;                 // cycle-detection words per ray: two stored loop states
 constexpr float FLT_MAX_ = 3.402823466e+38f;
 constexpr uint32_t NONE = 0xFFFFFFFFu;
 
@@ -227,7 +227,7 @@ struct CastState {
     uint32_t d1g, d1d;     // grid reads / DDA steps of the previous iteration
     uint32_t sig1, sig2;   // signatures of the loop states one and two iterations back
     int nsig;              // signatures recorded (saturates at 2)
-    int cand_p, cand_at;   // pending candidate: period, iteration whose state must equal the stored one
+    int cand_p, cand_at;   // deferred check: pending candidate's period, iteration it is confirmed at
 };
 
 __device__ __forceinline__ void cast_finish(CastState& st) {
@@ -413,8 +413,10 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
     return false;
 }
 
-// One iteration of castRayImpl's loop (SVOTraversal.cpp:597-688), its loop
-// condition first.  Returns true when the ray is finished (hit, exit, cap).
+// One iteration of castRayImpl's loop (SVOTraversal.cpp:597-688) is built
+// from the parts below: the corner t values, the leaf stage (handleLeafHit and
+// the brick DDA), ADVANCE + POP, and the end-of-iteration cycle check; each
+// reads and writes only CastState.
 //
 // Cycle detection: the loop state (scale, idx, fetched, parent, pos, t_min,
 // t_max, h) with the stack determines every later iteration, and a cycle only
@@ -423,19 +425,282 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
 // the 500-iteration cap: the result is the capped miss and the remaining
 // iterations' counters repeat the cycle's.  From iteration CYCLE_START on,
 // every state gets a 32-bit signature, and the signatures of the two previous
-// states stay in registers.  A signature equal to the one p iterations back
-// (p = 1 or 2) makes the state a candidate: it is stored (cyc[k * stride],
-// shared memory) and the state p iterations later is compared with it word
-// by word.  Equal states prove the repeat; unequal ones drop the candidate.
-// Equal states always have equal signatures, so every repeat is caught, at
-// most p iterations after the first state that repeats.  With LOD the cut
-// test reads only the loop state and per-ray constants, so a repeating state
-// still cannot end.
+// states stay in registers; equal states always have equal signatures.  Two
+// policies, the same results:
+//  - immediate (DEFER = false; the stack in shared memory): every state is
+//    stored in one of two parity slots (cyc[(p * 8 + k) * stride]), and a
+//    signature equal to the one 1 or 2 iterations back compares the stored
+//    state word by word, so the repeat ends the ray on the iteration it occurs;
+//  - deferred (DEFER = true; the stack in local memory, where a store per
+//    iteration costs more): a signature match makes the state a candidate,
+//    stored once, and the state p iterations later is compared with it;
+//    equal states prove the repeat, unequal ones drop the candidate, so a
+//    repeat ends the ray at most p iterations later.
+// With LOD the cut test reads only the loop state and per-ray constants, so a
+// repeating state still cannot end.
 //
 // LOD: castRayWithLOD (SVOTraversal.cpp:198-232) with LODParameters `lod`
 // (enabled, lod.dir > 0): the termination test of :613-651 runs on every
 // processed child before the leaf test.
-template <bool LOD = false>
+
+// Voxel corners at the iteration's position (computeVoxelCorners, :786-794)
+// and the corrected tc_max (:768-784); checkChildValidity, PUSH and ADVANCE
+// all evaluate them at this position and t_max.
+struct Corners {
+    float tx, ty, tz, tcc;
+};
+__device__ __forceinline__ Corners corners_of(const CastState& st, bool csx, bool csy, bool csz) {
+    const Coef& c = st.c;
+    Corners k;
+    k.tx = st.px * c.tx_coef - c.tx_bias;
+    k.ty = st.py * c.ty_coef - c.ty_bias;
+    k.tz = st.pz * c.tz_coef - c.tz_bias;
+    k.tcc = min3((csx && fabsf(k.tx) < 1000.0f) ? k.tx : st.t_max, (csy && fabsf(k.ty) < 1000.0f) ? k.ty : st.t_max,
+                 (csz && fabsf(k.tz) < 1000.0f) ? k.tz : st.t_max);
+    return k;
+}
+
+// handleLeafHit (SVOBrickDDA.cpp:65-181) and traverseBrickAndReturnHit
+// (:187-225) at the iteration's leaf child; true (and the hit record
+// complete) when the brick DDA hits.
+__device__ __forceinline__ bool leaf_stage(const DevScene& s, CastState& st, bool csx, bool csy, bool csz) {
+    Hit& h = st.h;
+    const Coef& c = st.c;
+    float lx = st.px, ly = st.py, lz = st.pz;
+    if ((c.octant_mask & 1) == 0) lx = 3.0f - st.scale_exp2 - lx;
+    if ((c.octant_mask & 2) == 0) ly = 3.0f - st.scale_exp2 - ly;
+    if ((c.octant_mask & 4) == 0) lz = 3.0f - st.scale_exp2 - lz;
+    const float ix = fclamp(csx ? (lx - 1.0f) + ((st.dx > 0) ? 0.001f : -0.001f) : st.rlx, 0.001f, 0.999f);
+    const float iy = fclamp(csy ? (ly - 1.0f) + ((st.dy > 0) ? 0.001f : -0.001f) : st.rly, 0.001f, 0.999f);
+    const float iz = fclamp(csz ? (lz - 1.0f) + ((st.dz > 0) ? 0.001f : -0.001f) : st.rlz, 0.001f, 0.999f);
+    const int bmax = s.bpa - 1;
+    // Method 1: ESVO state position (x / 8 == x * 0.125 exactly)
+    const float hx = fclamp(ix * s.wsize[0], 0.0f, s.wsm[0]);
+    const float hy = fclamp(iy * s.wsize[1], 0.0f, s.wsm[1]);
+    const float hz = fclamp(iz * s.wsize[2], 0.0f, s.wsm[2]);
+    uint32_t brick = grid_lookup(s, iclamp(f2i(hx * 0.125f), 0, bmax), iclamp(f2i(hy * 0.125f), 0, bmax),
+                                 iclamp(f2i(hz * 0.125f), 0, bmax));
+    ++h.grid_reads;
+    uint32_t method = 1;
+    if (brick == NONE) {
+        // Method 2: ray entry position (the same brick for the whole ray)
+        if (!st.have_brick2) {
+            const float te0 = gmax(st.tEntry, 0.0f);
+            const float ex = fclamp(((st.ox + st.dx * te0) - s.wmin[0]) + st.dx * 0.01f, 0.0f, s.wsm[0]);
+            const float ey = fclamp(((st.oy + st.dy * te0) - s.wmin[1]) + st.dy * 0.01f, 0.0f, s.wsm[1]);
+            const float ez = fclamp(((st.oz + st.dz * te0) - s.wmin[2]) + st.dz * 0.01f, 0.0f, s.wsm[2]);
+            st.brick2 = grid_lookup(s, iclamp(f2i(ex * 0.125f), 0, bmax), iclamp(f2i(ey * 0.125f), 0, bmax),
+                                    iclamp(f2i(ez * 0.125f), 0, bmax));
+            st.have_brick2 = true;
+        }
+        brick = st.brick2;
+        ++h.grid_reads;
+        method = 2;
+    }
+    if (brick == NONE) {
+        // Fallback 3: leaf child of the parent at the local octant
+        // (leafToBrickView, SVORebuild.cpp:569-574)
+        method = 3;
+        const uint32_t lo = uint32_t(st.idx ^ (~c.octant_mask & 7));
+        const uint32_t leafs = st.pValid & st.pLeaf;
+        if ((leafs >> lo) & 1u) {
+            const uint32_t ci =
+                st.pChild + __popc(st.pValid & ~st.pLeaf & 0xFFu) + __popc(leafs & ((1u << lo) - 1u));
+            if (ci < s.node_count) {
+                const uint32_t b = __ldg(s.node_brick + ci);
+                if (b < s.brick_count) brick = b;
+            }
+        }
+    }
+    if (brick != NONE) {
+        // traverseBrickAndReturnHit (SVOBrickDDA.cpp:187-225)
+        const uint32_t bc = __ldg(s.coord + bounded(brick, s.brick_count, V_BRICK));
+        const float bmn[3] = {float(int(bc & 0x3FFu) * 8), float(int((bc >> 10) & 0x3FFu) * 8),
+                              float(int((bc >> 20) & 0x3FFu) * 8)};
+        float tn[3], tf[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const float t0 = (bmn[i] - st.rb.lo[i]) * st.rb.inv[i];
+            const float t1 = ((bmn[i] + 8.0f) - st.rb.lo[i]) * st.rb.inv[i];
+            tn[i] = gmin(t0, t1);
+            tf[i] = gmax(t0, t1);
+        }
+        const float btmin = gmax(gmax(gmax(tn[0], tn[1]), tn[2]), st.tEntry);
+        const float btmax = gmin(gmin(tf[0], tf[1]), tf[2]);
+        if (brick_dda(s, brick, bmn, st.rb, btmin, btmax, h)) {
+            h.brick = brick;
+            h.node = st.parent;
+            h.flags |= method << 4;
+            h.scale = uint32_t(s.max_levels - 1);  // SVOBrickDDA.cpp:509
+            h.iters = uint32_t(st.iter);
+            h.run_iters = h.iters;
+            h.run_grid_reads = h.grid_reads;
+            h.run_dda_steps = h.dda_steps;
+            return true;
+        }
+    }
+    return false;
+}
+
+// executeAdvancePhase (:380-416) and, when the step leaves the parent,
+// executePopPhase (:418-510).  Returns 1 when the ray is finished (it left
+// the octree or the quantised position ends the traversal), else 0.
+__device__ __forceinline__ bool advance_pop(const DevScene& s, CastState& st, const Corners& k, bool csx, bool csy,
+                                            bool csz, uint32_t* stkN, float* stkT, int stride) {
+    const Coef& c = st.c;
+    const int minScale = s.min_scale;
+    {
+        float tca = k.tcc;
+        if (tca == FLT_MAX_) tca = max3(csx ? k.tx : -FLT_MAX_, csy ? k.ty : -FLT_MAX_, csz ? k.tz : -FLT_MAX_);
+        int step_mask = 0;
+        if (csx && k.tx <= tca) { step_mask ^= 1; st.px -= st.scale_exp2; }
+        if (csy && k.ty <= tca) { step_mask ^= 2; st.py -= st.scale_exp2; }
+        if (csz && k.tz <= tca) { step_mask ^= 4; st.pz -= st.scale_exp2; }
+        st.t_min = gmax(tca, 0.0f);
+        st.idx ^= step_mask;
+        if ((st.idx & step_mask) == 0) return false;
+    }
+    // POP: step mask recomputed at the new position (:672-681)
+    int step_mask = 0;
+    {
+        const float ux = st.px * c.tx_coef - c.tx_bias;
+        const float uy = st.py * c.ty_coef - c.ty_bias;
+        const float uz = st.pz * c.tz_coef - c.tz_bias;
+        const float ucc = min3((csx && fabsf(ux) < 1000.0f) ? ux : st.t_max,
+                               (csy && fabsf(uy) < 1000.0f) ? uy : st.t_max,
+                               (csz && fabsf(uz) < 1000.0f) ? uz : st.t_max);
+        if (csx && ux <= ucc) step_mask ^= 1;
+        if (csy && uy <= ucc) step_mask ^= 2;
+        if (csz && uz <= ucc) step_mask ^= 4;
+    }
+    if (st.scale == ESVO_MAX_SCALE) {
+        if (st.t_min > st.t_max || st.px < 1.0f || st.px >= 2.0f || st.py < 1.0f || st.py >= 2.0f || st.pz < 1.0f ||
+            st.pz >= 2.0f) {
+            cast_finish(st);
+            return true;
+        }
+        st.fetched = false;
+        return false;
+    }
+    // floatToInt: std::max(0, std::min(f, 1)), * 2^22, std::min(., 2^22-1),
+    // std::max(0, .), truncate (SVOTraversal.cpp:439-442)
+    auto f2q = [](float f) -> uint32_t {
+        const float m1 = (1.0f < f) ? 1.0f : f;
+        const float cl = (0.0f < m1) ? m1 : 0.0f;
+        const float sc = cl * 4194304.0f;
+        const float m2 = (4194303.0f < sc) ? 4194303.0f : sc;
+        return uint32_t((0.0f < m2) ? m2 : 0.0f);
+    };
+    uint32_t qx = f2q(gmax(0.0f, st.px - 1.0f));
+    uint32_t qy = f2q(gmax(0.0f, st.py - 1.0f));
+    uint32_t qz = f2q(gmax(0.0f, st.pz - 1.0f));
+    uint32_t diff = 0;
+    if (step_mask & 1) diff |= qx ^ f2q(gmax(0.0f, st.px + st.scale_exp2 - 1.0f));
+    if (step_mask & 2) diff |= qy ^ f2q(gmax(0.0f, st.py + st.scale_exp2 - 1.0f));
+    if (step_mask & 4) diff |= qz ^ f2q(gmax(0.0f, st.pz + st.scale_exp2 - 1.0f));
+    if (diff == 0) { cast_finish(st); return true; }
+    st.scale = 31 - __clz(diff);
+    if (st.scale < minScale || st.scale > ESVO_MAX_SCALE) { cast_finish(st); return true; }
+    st.scale_exp2 = __int_as_float((st.scale - ESVO_MAX_SCALE + 127) << 23);
+    if ((st.pushed >> (st.scale - minScale)) & 1u) {
+        const uint32_t kk = bounded(uint32_t(st.scale - minScale), uint32_t(s.max_levels), V_STACK);
+        st.parent = stkN[kk * stride];
+        st.t_max = stkT[kk * stride];
+    } else {
+        st.parent = 0u;
+        st.t_max = st.t_root;
+    }
+    const uint32_t mask = ~((1u << (ESVO_MAX_SCALE - st.scale)) - 1u);
+    qx &= mask; qy &= mask; qz &= mask;
+    st.px = 1.0f + float(qx) * (1.0f / 4194304.0f);  // / 2^22, exact as a product
+    st.py = 1.0f + float(qy) * (1.0f / 4194304.0f);
+    st.pz = 1.0f + float(qz) * (1.0f / 4194304.0f);
+    const int sh = ESVO_MAX_SCALE - st.scale - 1;
+    if (sh < 0 || sh >= 32) st.idx = 0;
+    else st.idx = int(((qx >> sh) & 1u) | (((qy >> sh) & 1u) << 1) | (((qz >> sh) & 1u) << 2));
+    st.hh = 0.0f;
+    st.fetched = false;
+    return false;
+}
+
+// The end of an iteration: the cycle check (see above).  g0 / dd0: the grid
+// reads and DDA steps counted when the iteration began.  True when a proven
+// repeat ends the ray.
+template <bool DEFER>
+__device__ __forceinline__ bool cycle_check(CastState& st, uint32_t g0, uint32_t dd0, uint32_t* cyc, int stride) {
+    Hit& h = st.h;
+    if (st.iter < CYCLE_START) return false;
+    uint32_t cur[8];
+    cur[0] = uint32_t(st.scale) | (uint32_t(st.idx) << 8) | (uint32_t(st.fetched) << 16);
+    cur[1] = st.parent;
+    cur[2] = __float_as_uint(st.px); cur[3] = __float_as_uint(st.py); cur[4] = __float_as_uint(st.pz);
+    cur[5] = __float_as_uint(st.t_min); cur[6] = __float_as_uint(st.t_max); cur[7] = __float_as_uint(st.hh);
+    const uint32_t dg = h.grid_reads - g0, ddd = h.dda_steps - dd0;
+    // signature: the words' sum (a repeat always has an equal sum)
+    const uint32_t sig = ((cur[0] + cur[1] + cur[2]) + (cur[3] + cur[4] + cur[5])) + (cur[6] + cur[7]);
+    int period = 0;  // 1 or 2 once state(iter) == state(iter - period) is proven
+    if constexpr (!DEFER) {
+        uint32_t* back2 = cyc + ((st.iter & 1) * 8) * stride;
+        const uint32_t* back1 = cyc + (((st.iter & 1) ^ 1) * 8) * stride;
+        bool eq1 = st.nsig >= 1 && st.sig1 == sig;
+        bool eq2 = st.nsig >= 2 && st.sig2 == sig;
+        if (eq1 || eq2) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                eq1 = eq1 && (cur[k] == back1[k * stride]);
+                eq2 = eq2 && (cur[k] == back2[k * stride]);
+            }
+        }
+        period = eq1 ? 1 : (eq2 ? 2 : 0);
+        if (!period) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) back2[k * stride] = cur[k];
+        }
+    } else {
+        if (st.cand_p && st.iter == st.cand_at) {
+            bool eq = true;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) eq = eq && (cur[k] == cyc[k * stride]);
+            if (eq) period = st.cand_p;
+            st.cand_p = 0;
+        }
+        if (!period && !st.cand_p) {
+            const int p = (st.nsig >= 1 && sig == st.sig1) ? 1 : ((st.nsig >= 2 && sig == st.sig2) ? 2 : 0);
+            if (p) {
+#pragma unroll
+                for (int k = 0; k < 8; ++k) cyc[k * stride] = cur[k];
+                st.cand_p = p;
+                st.cand_at = st.iter + p;
+            }
+        }
+    }
+    if (period) {  // the rest of the 500 iterations repeat the cycle: the capped miss
+        const uint32_t rem = uint32_t(MAX_ITER - st.iter);
+        h.run_iters = uint32_t(st.iter);
+        h.run_grid_reads = h.grid_reads;
+        h.run_dda_steps = h.dda_steps;
+        if (period == 1) {
+            h.grid_reads += rem * dg;
+            h.dda_steps += rem * ddd;
+        } else {
+            h.grid_reads += ((rem + 1) / 2) * st.d1g + (rem / 2) * dg;
+            h.dda_steps += ((rem + 1) / 2) * st.d1d + (rem / 2) * ddd;
+        }
+        h.iters = uint32_t(MAX_ITER);
+        h.flags |= F_ITER_CAP;
+        return true;
+    }
+    st.sig2 = st.sig1;
+    st.sig1 = sig;
+    st.nsig = st.nsig < 2 ? st.nsig + 1 : 2;
+    st.d1g = dg;
+    st.d1d = ddd;
+    return false;
+}
+
+// One iteration, its loop condition first.  Returns true when the ray is
+// finished (hit, exit, cap).
+template <bool LOD = false, bool DEFER = false>
 __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint32_t* stkN, float* stkT,
                                           uint32_t* cyc, int stride, LodCone lod = LodCone{0.0f, 0.0f}) {
     Hit& h = st.h;
@@ -448,146 +713,64 @@ __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint
     const bool csx = fabsf(st.dx) >= 1e-5f, csy = fabsf(st.dy) >= 1e-5f, csz = fabsf(st.dz) >= 1e-5f;
     ++st.iter;
     const uint32_t g0 = h.grid_reads, dd0 = h.dda_steps;
-    {  // one iteration; `goto next_iter` is the reference's `continue`
-        // fetchChildDescriptor (:282-293)
-        if (!st.fetched) {
-            const uint2 nd = __ldg(s.nodes + bounded(st.parent, s.node_count, V_NODE));
-            st.pChild = nd.x;
-            st.pValid = nd.y & 0xFFu;
-            st.pLeaf = (nd.y >> 8) & 0xFFu;
-            const uint32_t mm = mirror_masks(nd.y & 0xFFFFu, c.octant_mask);
-            st.mValid = mm & 0xFFu;
-            st.mLeaf = mm >> 8;
-            const uint32_t nonLeaf = ~st.mLeaf & 0xFFu;
-            st.fetched = (nonLeaf | (st.mValid << 8) | st.pChild) != 0u;
-        }
-        // Voxel corners at the iteration's position (computeVoxelCorners,
-        // :786-794) and the corrected tc_max (:768-784); checkChildValidity,
-        // PUSH and ADVANCE all evaluate them at this position and t_max.
-        const float tx = st.px * c.tx_coef - c.tx_bias;
-        const float ty = st.py * c.ty_coef - c.ty_bias;
-        const float tz = st.pz * c.tz_coef - c.tz_bias;
-        const float tcc = min3((csx && fabsf(tx) < 1000.0f) ? tx : st.t_max,
-                               (csy && fabsf(ty) < 1000.0f) ? ty : st.t_max,
-                               (csz && fabsf(tz) < 1000.0f) ? tz : st.t_max);
-        // checkChildValidity (:295-326)
-        const bool child_valid = (st.mValid >> st.idx) & 1u;
-        bool isLeaf = (st.mLeaf >> st.idx) & 1u;
-        if (st.scale - minScale == s.brick_user_scale && child_valid) isLeaf = true;
-        float tv_max = 0.0f;
-        if (child_valid && !(st.t_min > st.t_max) && st.t_min <= (tv_max = gmin(st.t_max, tcc))) {
-            if constexpr (LOD) {
-                // worldDistance = tRayStart + t_min * |worldSize| (:627);
-                // esvoScaleToWorldSize = 2^(scale - 23) * worldSize.x (SVOLOD.h:189-195),
-                // an exact power of two for scale in [0, 22];
-                // shouldTerminate: distance * rayDirSize + rayOrigSize >= size (SVOLOD.h:129-146).
-                const float wd = st.tRayStart + st.t_min * s.wrl;
-                const float vs = __int_as_float((st.scale - ESVO_MAX_SCALE - 1 + 127) << 23) * s.wsize[0];
-                if (wd * lod.dir + lod.orig >= vs) {
-                    // The LOD hit (:639-649): tMin = distance, normal (0,1,0), no entity.
-                    h.t = wd;
-                    h.node = st.parent;
-                    h.flags = F_HIT | (1u << 1);
-                    h.scale = uint32_t(st.scale - minScale);  // esvoToUserScale
-                    cast_finish(st);
-                    return true;
-                }
+    // fetchChildDescriptor (:282-293)
+    if (!st.fetched) {
+        const uint2 nd = __ldg(s.nodes + bounded(st.parent, s.node_count, V_NODE));
+        st.pChild = nd.x;
+        st.pValid = nd.y & 0xFFu;
+        st.pLeaf = (nd.y >> 8) & 0xFFu;
+        const uint32_t mm = mirror_masks(nd.y & 0xFFFFu, c.octant_mask);
+        st.mValid = mm & 0xFFu;
+        st.mLeaf = mm >> 8;
+        const uint32_t nonLeaf = ~st.mLeaf & 0xFFu;
+        st.fetched = (nonLeaf | (st.mValid << 8) | st.pChild) != 0u;
+    }
+    const Corners k = corners_of(st, csx, csy, csz);
+    // checkChildValidity (:295-326)
+    const bool child_valid = (st.mValid >> st.idx) & 1u;
+    bool isLeaf = (st.mLeaf >> st.idx) & 1u;
+    if (st.scale - minScale == s.brick_user_scale && child_valid) isLeaf = true;
+    float tv_max = 0.0f;
+    if (child_valid && !(st.t_min > st.t_max) && st.t_min <= (tv_max = gmin(st.t_max, k.tcc))) {
+        if constexpr (LOD) {
+            // worldDistance = tRayStart + t_min * |worldSize| (:627);
+            // esvoScaleToWorldSize = 2^(scale - 23) * worldSize.x (SVOLOD.h:189-195),
+            // an exact power of two for scale in [0, 22];
+            // shouldTerminate: distance * rayDirSize + rayOrigSize >= size (SVOLOD.h:129-146).
+            const float wd = st.tRayStart + st.t_min * s.wrl;
+            const float vs = __int_as_float((st.scale - ESVO_MAX_SCALE - 1 + 127) << 23) * s.wsize[0];
+            if (wd * lod.dir + lod.orig >= vs) {
+                // The LOD hit (:639-649): tMin = distance, normal (0,1,0), no entity.
+                h.t = wd;
+                h.node = st.parent;
+                h.flags = F_HIT | (1u << 1);
+                h.scale = uint32_t(st.scale - minScale);  // esvoToUserScale
+                cast_finish(st);
+                return true;
             }
-            if (isLeaf) {
-                // handleLeafHit (SVOBrickDDA.cpp:65-181)
-                float lx = st.px, ly = st.py, lz = st.pz;
-                if ((c.octant_mask & 1) == 0) lx = 3.0f - st.scale_exp2 - lx;
-                if ((c.octant_mask & 2) == 0) ly = 3.0f - st.scale_exp2 - ly;
-                if ((c.octant_mask & 4) == 0) lz = 3.0f - st.scale_exp2 - lz;
-                const float ix = fclamp(csx ? (lx - 1.0f) + ((st.dx > 0) ? 0.001f : -0.001f) : st.rlx, 0.001f, 0.999f);
-                const float iy = fclamp(csy ? (ly - 1.0f) + ((st.dy > 0) ? 0.001f : -0.001f) : st.rly, 0.001f, 0.999f);
-                const float iz = fclamp(csz ? (lz - 1.0f) + ((st.dz > 0) ? 0.001f : -0.001f) : st.rlz, 0.001f, 0.999f);
-                const int bmax = s.bpa - 1;
-                // Method 1: ESVO state position (x / 8 == x * 0.125 exactly)
-                const float hx = fclamp(ix * s.wsize[0], 0.0f, s.wsm[0]);
-                const float hy = fclamp(iy * s.wsize[1], 0.0f, s.wsm[1]);
-                const float hz = fclamp(iz * s.wsize[2], 0.0f, s.wsm[2]);
-                uint32_t brick = grid_lookup(s, iclamp(f2i(hx * 0.125f), 0, bmax), iclamp(f2i(hy * 0.125f), 0, bmax),
-                                             iclamp(f2i(hz * 0.125f), 0, bmax));
-                ++h.grid_reads;
-                uint32_t method = 1;
-                if (brick == NONE) {
-                    // Method 2: ray entry position (the same brick for the whole ray)
-                    if (!st.have_brick2) {
-                        const float te0 = gmax(st.tEntry, 0.0f);
-                        const float ex = fclamp(((st.ox + st.dx * te0) - s.wmin[0]) + st.dx * 0.01f, 0.0f, s.wsm[0]);
-                        const float ey = fclamp(((st.oy + st.dy * te0) - s.wmin[1]) + st.dy * 0.01f, 0.0f, s.wsm[1]);
-                        const float ez = fclamp(((st.oz + st.dz * te0) - s.wmin[2]) + st.dz * 0.01f, 0.0f, s.wsm[2]);
-                        st.brick2 = grid_lookup(s, iclamp(f2i(ex * 0.125f), 0, bmax), iclamp(f2i(ey * 0.125f), 0, bmax),
-                                                iclamp(f2i(ez * 0.125f), 0, bmax));
-                        st.have_brick2 = true;
-                    }
-                    brick = st.brick2;
-                    ++h.grid_reads;
-                    method = 2;
-                }
-                if (brick == NONE) {
-                    // Fallback 3: leaf child of the parent at the local octant
-                    // (leafToBrickView, SVORebuild.cpp:569-574)
-                    method = 3;
-                    const uint32_t lo = uint32_t(st.idx ^ (~c.octant_mask & 7));
-                    const uint32_t leafs = st.pValid & st.pLeaf;
-                    if ((leafs >> lo) & 1u) {
-                        const uint32_t ci = st.pChild + __popc(st.pValid & ~st.pLeaf & 0xFFu) +
-                                            __popc(leafs & ((1u << lo) - 1u));
-                        if (ci < s.node_count) {
-                            const uint32_t b = __ldg(s.node_brick + ci);
-                            if (b < s.brick_count) brick = b;
-                        }
-                    }
-                }
-                if (brick != NONE) {
-                    // traverseBrickAndReturnHit (SVOBrickDDA.cpp:187-225)
-                    const uint32_t bc = __ldg(s.coord + bounded(brick, s.brick_count, V_BRICK));
-                    const float bmn[3] = {float(int(bc & 0x3FFu) * 8), float(int((bc >> 10) & 0x3FFu) * 8),
-                                          float(int((bc >> 20) & 0x3FFu) * 8)};
-                    float tn[3], tf[3];
-#pragma unroll
-                    for (int i = 0; i < 3; ++i) {
-                        const float t0 = (bmn[i] - st.rb.lo[i]) * st.rb.inv[i];
-                        const float t1 = ((bmn[i] + 8.0f) - st.rb.lo[i]) * st.rb.inv[i];
-                        tn[i] = gmin(t0, t1);
-                        tf[i] = gmax(t0, t1);
-                    }
-                    const float btmin = gmax(gmax(gmax(tn[0], tn[1]), tn[2]), st.tEntry);
-                    const float btmax = gmin(gmin(tf[0], tf[1]), tf[2]);
-                    if (brick_dda(s, brick, bmn, st.rb, btmin, btmax, h)) {
-                        h.brick = brick;
-                        h.node = st.parent;
-                        h.flags |= method << 4;
-                        h.scale = uint32_t(s.max_levels - 1);  // SVOBrickDDA.cpp:509
-                        h.iters = uint32_t(st.iter);
-                        h.run_iters = h.iters;
-                        h.run_grid_reads = h.grid_reads;
-                        h.run_dda_steps = h.dda_steps;
-                        return true;
-                    }
-                }
-                st.t_min = tv_max;
-                // fall through to ADVANCE
-            } else {
-                // executePushPhase (:328-378); tx_center etc. of checkChildValidity
-                const float half = st.scale_exp2 * 0.5f;
-                const float tx_center = half * c.tx_coef + tx;
-                const float ty_center = half * c.ty_coef + ty;
-                const float tz_center = half * c.tz_coef + tz;
-                const float tc_max = min3(tx, ty, tz);
-                if (tc_max < st.hh) {
-                    const uint32_t k = bounded(uint32_t(st.scale - minScale), uint32_t(s.max_levels), V_STACK);
-                    stkN[k * stride] = st.parent;
-                    stkT[k * stride] = st.t_max;
-                    st.pushed |= 1u << (st.scale - minScale);
-                }
-                st.hh = tc_max;
-                const int worldIdx = st.idx ^ (~c.octant_mask & 7);
-                const uint32_t nonLeafMask = ~st.pLeaf & st.pValid & 0xFFu;
-                const uint32_t child_index = st.pChild + __popc(nonLeafMask & ((1u << worldIdx) - 1u));
-                if (child_index >= s.node_count) goto next_iter;
+        }
+        if (isLeaf) {
+            if (leaf_stage(s, st, csx, csy, csz)) return true;
+            st.t_min = tv_max;
+            if (advance_pop(s, st, k, csx, csy, csz, stkN, stkT, stride)) return true;
+        } else {
+            // executePushPhase (:328-378); tx_center etc. of checkChildValidity
+            const float half = st.scale_exp2 * 0.5f;
+            const float tx_center = half * c.tx_coef + k.tx;
+            const float ty_center = half * c.ty_coef + k.ty;
+            const float tz_center = half * c.tz_coef + k.tz;
+            const float tc_max = min3(k.tx, k.ty, k.tz);
+            if (tc_max < st.hh) {
+                const uint32_t kk = bounded(uint32_t(st.scale - minScale), uint32_t(s.max_levels), V_STACK);
+                stkN[kk * stride] = st.parent;
+                stkT[kk * stride] = st.t_max;
+                st.pushed |= 1u << (st.scale - minScale);
+            }
+            st.hh = tc_max;
+            const int worldIdx = st.idx ^ (~c.octant_mask & 7);
+            const uint32_t nonLeafMask = ~st.pLeaf & st.pValid & 0xFFu;
+            const uint32_t child_index = st.pChild + __popc(nonLeafMask & ((1u << worldIdx) - 1u));
+            if (child_index < s.node_count) {
                 st.parent = child_index;
                 st.idx = 0;
                 st.scale--;
@@ -597,145 +780,23 @@ __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint
                 if (tz_center > st.t_min) { st.idx ^= 4; st.pz += st.scale_exp2; }
                 st.t_max = tv_max;
                 st.fetched = false;
-                goto next_iter;
             }
         }
-        // executeAdvancePhase (:380-416)
-        {
-            float tca = tcc;
-            if (tca == FLT_MAX_) tca = max3(csx ? tx : -FLT_MAX_, csy ? ty : -FLT_MAX_, csz ? tz : -FLT_MAX_);
-            int step_mask = 0;
-            if (csx && tx <= tca) { step_mask ^= 1; st.px -= st.scale_exp2; }
-            if (csy && ty <= tca) { step_mask ^= 2; st.py -= st.scale_exp2; }
-            if (csz && tz <= tca) { step_mask ^= 4; st.pz -= st.scale_exp2; }
-            st.t_min = gmax(tca, 0.0f);
-            st.idx ^= step_mask;
-            if ((st.idx & step_mask) == 0) goto next_iter;
-        }
-        // POP: step mask recomputed at the new position (:672-681)
-        int step_mask = 0;
-        {
-            const float ux = st.px * c.tx_coef - c.tx_bias;
-            const float uy = st.py * c.ty_coef - c.ty_bias;
-            const float uz = st.pz * c.tz_coef - c.tz_bias;
-            const float ucc = min3((csx && fabsf(ux) < 1000.0f) ? ux : st.t_max,
-                                   (csy && fabsf(uy) < 1000.0f) ? uy : st.t_max,
-                                   (csz && fabsf(uz) < 1000.0f) ? uz : st.t_max);
-            if (csx && ux <= ucc) step_mask ^= 1;
-            if (csy && uy <= ucc) step_mask ^= 2;
-            if (csz && uz <= ucc) step_mask ^= 4;
-        }
-        // executePopPhase (:418-510)
-        if (st.scale == ESVO_MAX_SCALE) {
-            if (st.t_min > st.t_max || st.px < 1.0f || st.px >= 2.0f || st.py < 1.0f || st.py >= 2.0f ||
-                st.pz < 1.0f || st.pz >= 2.0f) {
-                cast_finish(st);
-                return true;
-            }
-            st.fetched = false;
-            goto next_iter;
-        }
-        {
-            // floatToInt: std::max(0, std::min(f, 1)), * 2^22, std::min(., 2^22-1),
-            // std::max(0, .), truncate (SVOTraversal.cpp:439-442)
-            auto f2q = [](float f) -> uint32_t {
-                const float m1 = (1.0f < f) ? 1.0f : f;
-                const float cl = (0.0f < m1) ? m1 : 0.0f;
-                const float sc = cl * 4194304.0f;
-                const float m2 = (4194303.0f < sc) ? 4194303.0f : sc;
-                return uint32_t((0.0f < m2) ? m2 : 0.0f);
-            };
-            uint32_t qx = f2q(gmax(0.0f, st.px - 1.0f));
-            uint32_t qy = f2q(gmax(0.0f, st.py - 1.0f));
-            uint32_t qz = f2q(gmax(0.0f, st.pz - 1.0f));
-            uint32_t diff = 0;
-            if (step_mask & 1) diff |= qx ^ f2q(gmax(0.0f, st.px + st.scale_exp2 - 1.0f));
-            if (step_mask & 2) diff |= qy ^ f2q(gmax(0.0f, st.py + st.scale_exp2 - 1.0f));
-            if (step_mask & 4) diff |= qz ^ f2q(gmax(0.0f, st.pz + st.scale_exp2 - 1.0f));
-            if (diff == 0) { cast_finish(st); return true; }
-            st.scale = 31 - __clz(diff);
-            if (st.scale < minScale || st.scale > ESVO_MAX_SCALE) { cast_finish(st); return true; }
-            st.scale_exp2 = __int_as_float((st.scale - ESVO_MAX_SCALE + 127) << 23);
-            if ((st.pushed >> (st.scale - minScale)) & 1u) {
-                const uint32_t k = bounded(uint32_t(st.scale - minScale), uint32_t(s.max_levels), V_STACK);
-                st.parent = stkN[k * stride];
-                st.t_max = stkT[k * stride];
-            } else {
-                st.parent = 0u;
-                st.t_max = st.t_root;
-            }
-            const uint32_t mask = ~((1u << (ESVO_MAX_SCALE - st.scale)) - 1u);
-            qx &= mask; qy &= mask; qz &= mask;
-            st.px = 1.0f + float(qx) * (1.0f / 4194304.0f);  // / 2^22, exact as a product
-            st.py = 1.0f + float(qy) * (1.0f / 4194304.0f);
-            st.pz = 1.0f + float(qz) * (1.0f / 4194304.0f);
-            const int sh = ESVO_MAX_SCALE - st.scale - 1;
-            if (sh < 0 || sh >= 32) st.idx = 0;
-            else st.idx = int(((qx >> sh) & 1u) | (((qy >> sh) & 1u) << 1) | (((qz >> sh) & 1u) << 2));
-            st.hh = 0.0f;
-            st.fetched = false;
-        }
+    } else {
+        if (advance_pop(s, st, k, csx, csy, csz, stkN, stkT, stride)) return true;
     }
-next_iter:
-    if (st.iter >= CYCLE_START) {
-        uint32_t cur[8];
-        cur[0] = uint32_t(st.scale) | (uint32_t(st.idx) << 8) | (uint32_t(st.fetched) << 16);
-        cur[1] = st.parent;
-        cur[2] = __float_as_uint(st.px); cur[3] = __float_as_uint(st.py); cur[4] = __float_as_uint(st.pz);
-        cur[5] = __float_as_uint(st.t_min); cur[6] = __float_as_uint(st.t_max); cur[7] = __float_as_uint(st.hh);
-        const uint32_t dg = h.grid_reads - g0, ddd = h.dda_steps - dd0;
-        if (st.cand_p && st.iter == st.cand_at) {
-            bool eq = true;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) eq = eq && (cur[k] == cyc[k * stride]);
-            if (eq) {  // state(iter) == state(iter - cand_p): the cycle is proven
-                const uint32_t rem = uint32_t(MAX_ITER - st.iter);
-                h.run_iters = uint32_t(st.iter);
-                h.run_grid_reads = h.grid_reads;
-                h.run_dda_steps = h.dda_steps;
-                if (st.cand_p == 1) {
-                    h.grid_reads += rem * dg;
-                    h.dda_steps += rem * ddd;
-                } else {
-                    h.grid_reads += ((rem + 1) / 2) * st.d1g + (rem / 2) * dg;
-                    h.dda_steps += ((rem + 1) / 2) * st.d1d + (rem / 2) * ddd;
-                }
-                h.iters = uint32_t(MAX_ITER);
-                h.flags |= F_ITER_CAP;
-                return true;
-            }
-            st.cand_p = 0;
-        }
-        // signature: a mix of the eight words (odd multipliers, so one word's change always changes it)
-        const uint32_t sig = ((cur[0] + cur[1] * 0x9E3779B1u) ^ (cur[2] * 0x85EBCA77u + cur[3])) +
-                             ((cur[4] * 0xC2B2AE3Du + cur[5]) ^ (cur[6] * 0x27D4EB2Fu + cur[7] * 0x165667B1u));
-        if (!st.cand_p) {
-            const int p = (st.nsig >= 1 && sig == st.sig1) ? 1 : ((st.nsig >= 2 && sig == st.sig2) ? 2 : 0);
-            if (p) {
-#pragma unroll
-                for (int k = 0; k < 8; ++k) cyc[k * stride] = cur[k];
-                st.cand_p = p;
-                st.cand_at = st.iter + p;
-            }
-        }
-        st.sig2 = st.sig1;
-        st.sig1 = sig;
-        st.nsig = st.nsig < 2 ? st.nsig + 1 : 2;
-        st.d1g = dg;
-        st.d1d = ddd;
-    }
-    return false;
+    return cycle_check<DEFER>(st, g0, dd0, cyc, stride);
 }
 
 // castRayImpl (SVOTraversal.cpp:516-691): setup, then the loop.  LOD = false
 // is castRay, LOD = true castRayWithLOD with an enabled `lod`.
-template <bool LOD = false>
+template <bool LOD = false, bool DEFER = false>
 __device__ __forceinline__ void cast_ray(const DevScene& s, float ox, float oy, float oz, float ddx, float ddy,
                                          float ddz, float tMinArg, float tMaxArg, uint32_t* stkN, float* stkT,
                                          uint32_t* cyc, int stride, Hit& h, LodCone lod = LodCone{0.0f, 0.0f}) {
     CastState st;
     if (!cast_init(s, ox, oy, oz, ddx, ddy, ddz, tMinArg, tMaxArg, stkN, stkT, stride, st))
-        while (!cast_step<LOD>(s, st, stkN, stkT, cyc, stride, lod)) {
+        while (!cast_step<LOD, DEFER>(s, st, stkN, stkT, cyc, stride, lod)) {
         }
     h = st.h;
 }
