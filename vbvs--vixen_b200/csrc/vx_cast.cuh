@@ -85,22 +85,20 @@ __device__ __forceinline__ int iclamp(int v, int lo, int hi) { return imin(imax(
 __device__ __forceinline__ float fclamp(float v, float lo, float hi) { return gmin(gmax(v, lo), hi); }
 __device__ __forceinline__ float min3(float a, float b, float c) { return gmin(gmin(a, b), c); }
 __device__ __forceinline__ float max3(float a, float b, float c) { return gmax(gmax(a, b), c); }
+// The same min / max where no operand is NaN or -0 (the octree loop's
+// parametric t values and positions: finite, and every zero among them comes
+// from x - x or a product of +0, so it is +0).  There glm's selections give
+// the number the hardware min / max gives, in one instruction instead of a
+// compare and a select.
+__device__ __forceinline__ float nmin(float x, float y) { return fminf(x, y); }
+__device__ __forceinline__ float nmax(float x, float y) { return fmaxf(x, y); }
+__device__ __forceinline__ float nmin3(float a, float b, float c) { return fminf(fminf(a, b), c); }
+__device__ __forceinline__ float nmax3(float a, float b, float c) { return fmaxf(fmaxf(a, b), c); }
+__device__ __forceinline__ float nclamp(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
 // static_cast<int>(float) as x86-64 evaluates it (cvttss2si: INT_MIN when
 // the value is outside the int range or NaN).
 __device__ __forceinline__ int f2i(float f) {
     return (f >= -2147483648.0f && f < 2147483648.0f) ? __float2int_rz(f) : INT_MIN;
-}
-
-// mirrorMask (SVOTypes.h:343-364): bit i moves to i ^ flip, here on the valid
-// mask (bits 0-7) and the leaf mask (bits 8-15) at once.
-__device__ __forceinline__ uint32_t mirror_masks(uint32_t m, int octant_mask) {
-    const int flip = (~octant_mask) & 7;
-    const uint32_t a = ((m & 0x5555u) << 1) | ((m & 0xAAAAu) >> 1);
-    m = (flip & 1) ? a : m;
-    const uint32_t b = ((m & 0x3333u) << 2) | ((m & 0xCCCCu) >> 2);
-    m = (flip & 2) ? b : m;
-    const uint32_t c = ((m & 0x0F0Fu) << 4) | ((m & 0xF0F0u) >> 4);
-    return (flip & 4) ? c : m;
 }
 
 __device__ __forceinline__ uint32_t grid_lookup(const DevScene& s, int bx, int by, int bz) {
@@ -162,10 +160,13 @@ __device__ __forceinline__ bool brick_dda(const DevScene& s, uint32_t brick, con
                 if (fabsf(rb.d[a]) < 1e-8f) {
                     tn[a] = -__int_as_float(0x7f800000);
                 } else {
+                    // glm::min(t0, t1) of t0 = (vmn - lo) / d, t1 = ((vmn + 1) - lo) / d:
+                    // rounded division by one divisor is monotone in the
+                    // numerator, so the smaller is the near plane's quotient
+                    // (t0 for d > 0, t1 for d < 0), and when the two round equal
+                    // they are the same number.  No operand is NaN.
                     const float vmn = bmn[a] + float(cur[a]);
-                    const float t0 = (vmn - rb.lo[a]) / rb.d[a];
-                    const float t1 = ((vmn + 1.0f) - rb.lo[a]) / rb.d[a];
-                    tn[a] = gmin(t0, t1);
+                    tn[a] = ((rb.d[a] > 0.0f ? vmn : vmn + 1.0f) - rb.lo[a]) / rb.d[a];
                 }
             }
             float hitT = gmax(gmax(tn[0], tn[1]), tn[2]);
@@ -220,7 +221,11 @@ struct CastState {
     uint32_t parent;
     bool fetched;
     float px, py, pz, scale_exp2, t_min, t_max, hh;
-    uint32_t mValid, mLeaf, pChild, pValid, pLeaf;
+    // the parent's descriptor: child pointer and valid | leaf << 8 in world
+    // octant order.  The reference tests the mirrored masks (mirrorMask,
+    // SVOTypes.h:343-364, moves bit i to i ^ flip, flip = ~octant_mask & 7) at
+    // the ray-space octant idx; that is bit idx ^ flip of the unmirrored mask.
+    uint32_t pChild, pMask;
     uint32_t pushed;       // stack slots written by PUSH (bit scale - minScale)
     float t_root;          // t_max of the unwritten slots
     // cycle detection
@@ -405,7 +410,7 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
     st.t_min = t_min;
     st.t_max = t_max;
     st.hh = t_max;
-    st.mValid = st.mLeaf = st.pChild = st.pValid = st.pLeaf = 0;
+    st.pChild = st.pMask = 0;
     st.d1g = st.d1d = 0;
     st.sig1 = st.sig2 = 0;
     st.nsig = 0;
@@ -455,8 +460,8 @@ __device__ __forceinline__ Corners corners_of(const CastState& st, bool csx, boo
     k.tx = st.px * c.tx_coef - c.tx_bias;
     k.ty = st.py * c.ty_coef - c.ty_bias;
     k.tz = st.pz * c.tz_coef - c.tz_bias;
-    k.tcc = min3((csx && fabsf(k.tx) < 1000.0f) ? k.tx : st.t_max, (csy && fabsf(k.ty) < 1000.0f) ? k.ty : st.t_max,
-                 (csz && fabsf(k.tz) < 1000.0f) ? k.tz : st.t_max);
+    k.tcc = nmin3((csx && fabsf(k.tx) < 1000.0f) ? k.tx : st.t_max, (csy && fabsf(k.ty) < 1000.0f) ? k.ty : st.t_max,
+                  (csz && fabsf(k.tz) < 1000.0f) ? k.tz : st.t_max);
     return k;
 }
 
@@ -470,14 +475,14 @@ __device__ __forceinline__ bool leaf_stage(const DevScene& s, CastState& st, boo
     if ((c.octant_mask & 1) == 0) lx = 3.0f - st.scale_exp2 - lx;
     if ((c.octant_mask & 2) == 0) ly = 3.0f - st.scale_exp2 - ly;
     if ((c.octant_mask & 4) == 0) lz = 3.0f - st.scale_exp2 - lz;
-    const float ix = fclamp(csx ? (lx - 1.0f) + ((st.dx > 0) ? 0.001f : -0.001f) : st.rlx, 0.001f, 0.999f);
-    const float iy = fclamp(csy ? (ly - 1.0f) + ((st.dy > 0) ? 0.001f : -0.001f) : st.rly, 0.001f, 0.999f);
-    const float iz = fclamp(csz ? (lz - 1.0f) + ((st.dz > 0) ? 0.001f : -0.001f) : st.rlz, 0.001f, 0.999f);
+    const float ix = nclamp(csx ? (lx - 1.0f) + ((st.dx > 0) ? 0.001f : -0.001f) : st.rlx, 0.001f, 0.999f);
+    const float iy = nclamp(csy ? (ly - 1.0f) + ((st.dy > 0) ? 0.001f : -0.001f) : st.rly, 0.001f, 0.999f);
+    const float iz = nclamp(csz ? (lz - 1.0f) + ((st.dz > 0) ? 0.001f : -0.001f) : st.rlz, 0.001f, 0.999f);
     const int bmax = s.bpa - 1;
     // Method 1: ESVO state position (x / 8 == x * 0.125 exactly)
-    const float hx = fclamp(ix * s.wsize[0], 0.0f, s.wsm[0]);
-    const float hy = fclamp(iy * s.wsize[1], 0.0f, s.wsm[1]);
-    const float hz = fclamp(iz * s.wsize[2], 0.0f, s.wsm[2]);
+    const float hx = nclamp(ix * s.wsize[0], 0.0f, s.wsm[0]);
+    const float hy = nclamp(iy * s.wsize[1], 0.0f, s.wsm[1]);
+    const float hz = nclamp(iz * s.wsize[2], 0.0f, s.wsm[2]);
     uint32_t brick = grid_lookup(s, iclamp(f2i(hx * 0.125f), 0, bmax), iclamp(f2i(hy * 0.125f), 0, bmax),
                                  iclamp(f2i(hz * 0.125f), 0, bmax));
     ++h.grid_reads;
@@ -502,10 +507,9 @@ __device__ __forceinline__ bool leaf_stage(const DevScene& s, CastState& st, boo
         // (leafToBrickView, SVORebuild.cpp:569-574)
         method = 3;
         const uint32_t lo = uint32_t(st.idx ^ (~c.octant_mask & 7));
-        const uint32_t leafs = st.pValid & st.pLeaf;
+        const uint32_t valid = st.pMask & 0xFFu, leafs = valid & (st.pMask >> 8);
         if ((leafs >> lo) & 1u) {
-            const uint32_t ci =
-                st.pChild + __popc(st.pValid & ~st.pLeaf & 0xFFu) + __popc(leafs & ((1u << lo) - 1u));
+            const uint32_t ci = st.pChild + __popc(valid & ~leafs) + __popc(leafs & ((1u << lo) - 1u));
             if (ci < s.node_count) {
                 const uint32_t b = __ldg(s.node_brick + ci);
                 if (b < s.brick_count) brick = b;
@@ -520,10 +524,15 @@ __device__ __forceinline__ bool leaf_stage(const DevScene& s, CastState& st, boo
         float tn[3], tf[3];
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
+            // min / max of t0 = (bmn - lo) * inv, t1 = ((bmn + 8) - lo) * inv:
+            // rounded multiplication by one factor is monotone, so the order
+            // of t0 and t1 is the sign of inv (equal values are the same
+            // number, a -0 among them included).  No operand is NaN.
             const float t0 = (bmn[i] - st.rb.lo[i]) * st.rb.inv[i];
             const float t1 = ((bmn[i] + 8.0f) - st.rb.lo[i]) * st.rb.inv[i];
-            tn[i] = gmin(t0, t1);
-            tf[i] = gmax(t0, t1);
+            const bool pos = st.rb.inv[i] > 0.0f;
+            tn[i] = pos ? t0 : t1;
+            tf[i] = pos ? t1 : t0;
         }
         const float btmin = gmax(gmax(gmax(tn[0], tn[1]), tn[2]), st.tEntry);
         const float btmax = gmin(gmin(tf[0], tf[1]), tf[2]);
@@ -551,12 +560,12 @@ __device__ __forceinline__ bool advance_pop(const DevScene& s, CastState& st, co
     const int minScale = s.min_scale;
     {
         float tca = k.tcc;
-        if (tca == FLT_MAX_) tca = max3(csx ? k.tx : -FLT_MAX_, csy ? k.ty : -FLT_MAX_, csz ? k.tz : -FLT_MAX_);
+        if (tca == FLT_MAX_) tca = nmax3(csx ? k.tx : -FLT_MAX_, csy ? k.ty : -FLT_MAX_, csz ? k.tz : -FLT_MAX_);
         int step_mask = 0;
         if (csx && k.tx <= tca) { step_mask ^= 1; st.px -= st.scale_exp2; }
         if (csy && k.ty <= tca) { step_mask ^= 2; st.py -= st.scale_exp2; }
         if (csz && k.tz <= tca) { step_mask ^= 4; st.pz -= st.scale_exp2; }
-        st.t_min = gmax(tca, 0.0f);
+        st.t_min = nmax(tca, 0.0f);
         st.idx ^= step_mask;
         if ((st.idx & step_mask) == 0) return false;
     }
@@ -566,9 +575,9 @@ __device__ __forceinline__ bool advance_pop(const DevScene& s, CastState& st, co
         const float ux = st.px * c.tx_coef - c.tx_bias;
         const float uy = st.py * c.ty_coef - c.ty_bias;
         const float uz = st.pz * c.tz_coef - c.tz_bias;
-        const float ucc = min3((csx && fabsf(ux) < 1000.0f) ? ux : st.t_max,
-                               (csy && fabsf(uy) < 1000.0f) ? uy : st.t_max,
-                               (csz && fabsf(uz) < 1000.0f) ? uz : st.t_max);
+        const float ucc = nmin3((csx && fabsf(ux) < 1000.0f) ? ux : st.t_max,
+                                (csy && fabsf(uy) < 1000.0f) ? uy : st.t_max,
+                                (csz && fabsf(uz) < 1000.0f) ? uz : st.t_max);
         if (csx && ux <= ucc) step_mask ^= 1;
         if (csy && uy <= ucc) step_mask ^= 2;
         if (csz && uz <= ucc) step_mask ^= 4;
@@ -583,21 +592,17 @@ __device__ __forceinline__ bool advance_pop(const DevScene& s, CastState& st, co
         return false;
     }
     // floatToInt: std::max(0, std::min(f, 1)), * 2^22, std::min(., 2^22-1),
-    // std::max(0, .), truncate (SVOTraversal.cpp:439-442)
-    auto f2q = [](float f) -> uint32_t {
-        const float m1 = (1.0f < f) ? 1.0f : f;
-        const float cl = (0.0f < m1) ? m1 : 0.0f;
-        const float sc = cl * 4194304.0f;
-        const float m2 = (4194303.0f < sc) ? 4194303.0f : sc;
-        return uint32_t((0.0f < m2) ? m2 : 0.0f);
-    };
-    uint32_t qx = f2q(gmax(0.0f, st.px - 1.0f));
-    uint32_t qy = f2q(gmax(0.0f, st.py - 1.0f));
-    uint32_t qz = f2q(gmax(0.0f, st.pz - 1.0f));
+    // std::max(0, .), truncate (SVOTraversal.cpp:439-442).  Every argument
+    // here is max(0, .) of a finite value, so f >= +0 and both std::max
+    // calls return their other operand.
+    auto f2q = [](float f) -> uint32_t { return uint32_t(nmin(nmin(f, 1.0f) * 4194304.0f, 4194303.0f)); };
+    uint32_t qx = f2q(nmax(0.0f, st.px - 1.0f));
+    uint32_t qy = f2q(nmax(0.0f, st.py - 1.0f));
+    uint32_t qz = f2q(nmax(0.0f, st.pz - 1.0f));
     uint32_t diff = 0;
-    if (step_mask & 1) diff |= qx ^ f2q(gmax(0.0f, st.px + st.scale_exp2 - 1.0f));
-    if (step_mask & 2) diff |= qy ^ f2q(gmax(0.0f, st.py + st.scale_exp2 - 1.0f));
-    if (step_mask & 4) diff |= qz ^ f2q(gmax(0.0f, st.pz + st.scale_exp2 - 1.0f));
+    if (step_mask & 1) diff |= qx ^ f2q(nmax(0.0f, st.px + st.scale_exp2 - 1.0f));
+    if (step_mask & 2) diff |= qy ^ f2q(nmax(0.0f, st.py + st.scale_exp2 - 1.0f));
+    if (step_mask & 4) diff |= qz ^ f2q(nmax(0.0f, st.pz + st.scale_exp2 - 1.0f));
     if (diff == 0) { cast_finish(st); return true; }
     st.scale = 31 - __clz(diff);
     if (st.scale < minScale || st.scale > ESVO_MAX_SCALE) { cast_finish(st); return true; }
@@ -717,21 +722,20 @@ __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint
     if (!st.fetched) {
         const uint2 nd = __ldg(s.nodes + bounded(st.parent, s.node_count, V_NODE));
         st.pChild = nd.x;
-        st.pValid = nd.y & 0xFFu;
-        st.pLeaf = (nd.y >> 8) & 0xFFu;
-        const uint32_t mm = mirror_masks(nd.y & 0xFFFFu, c.octant_mask);
-        st.mValid = mm & 0xFFu;
-        st.mLeaf = mm >> 8;
-        const uint32_t nonLeaf = ~st.mLeaf & 0xFFu;
-        st.fetched = (nonLeaf | (st.mValid << 8) | st.pChild) != 0u;
+        st.pMask = nd.y & 0xFFFFu;
+        // a descriptor reads as fetched unless it is all zero (child pointer 0,
+        // no valid child, all eight leaf bits clear); mirroring keeps a mask's
+        // zeroness
+        st.fetched = ((st.pMask & 0xFFu) | (~st.pMask & 0xFF00u) | st.pChild) != 0u;
     }
     const Corners k = corners_of(st, csx, csy, csz);
     // checkChildValidity (:295-326)
-    const bool child_valid = (st.mValid >> st.idx) & 1u;
-    bool isLeaf = (st.mLeaf >> st.idx) & 1u;
+    const int worldIdx = st.idx ^ (~c.octant_mask & 7);
+    const bool child_valid = (st.pMask >> worldIdx) & 1u;
+    bool isLeaf = (st.pMask >> (worldIdx + 8)) & 1u;
     if (st.scale - minScale == s.brick_user_scale && child_valid) isLeaf = true;
     float tv_max = 0.0f;
-    if (child_valid && !(st.t_min > st.t_max) && st.t_min <= (tv_max = gmin(st.t_max, k.tcc))) {
+    if (child_valid && !(st.t_min > st.t_max) && st.t_min <= (tv_max = nmin(st.t_max, k.tcc))) {
         if constexpr (LOD) {
             // worldDistance = tRayStart + t_min * |worldSize| (:627);
             // esvoScaleToWorldSize = 2^(scale - 23) * worldSize.x (SVOLOD.h:189-195),
@@ -759,7 +763,7 @@ __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint
             const float tx_center = half * c.tx_coef + k.tx;
             const float ty_center = half * c.ty_coef + k.ty;
             const float tz_center = half * c.tz_coef + k.tz;
-            const float tc_max = min3(k.tx, k.ty, k.tz);
+            const float tc_max = nmin3(k.tx, k.ty, k.tz);
             if (tc_max < st.hh) {
                 const uint32_t kk = bounded(uint32_t(st.scale - minScale), uint32_t(s.max_levels), V_STACK);
                 stkN[kk * stride] = st.parent;
@@ -767,8 +771,7 @@ __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint
                 st.pushed |= 1u << (st.scale - minScale);
             }
             st.hh = tc_max;
-            const int worldIdx = st.idx ^ (~c.octant_mask & 7);
-            const uint32_t nonLeafMask = ~st.pLeaf & st.pValid & 0xFFu;
+            const uint32_t nonLeafMask = ~(st.pMask >> 8) & st.pMask & 0xFFu;
             const uint32_t child_index = st.pChild + __popc(nonLeafMask & ((1u << worldIdx) - 1u));
             if (child_index < s.node_count) {
                 st.parent = child_index;

@@ -58,12 +58,12 @@ __device__ __forceinline__ void forward_pixel(const DevScene& s, const CameraDev
                                               uint32_t w, uint32_t hgt, uint32_t i, int kind,
                                               const float* __restrict__ attr, const uint32_t* __restrict__ idx,
                                               float* __restrict__ image, vx_hit* __restrict__ record,
-                                              uint32_t* stkN, float* stkT, uint32_t* cyc) {
+                                              uint32_t* stkN, float* stkT, uint32_t* cyc, uint32_t stride) {
     vx_ray r;
     float uv_y;
     camera_ray(cam, px, py, w, hgt, r, &uv_y);
     Hit h;
-    cast_ray(s, r.ox, r.oy, r.oz, r.dx, r.dy, r.dz, 0.0f, FLT_MAX_, stkN, stkT, cyc, blockDim.x, h);
+    cast_ray(s, r.ox, r.oy, r.oz, r.dx, r.dy, r.dz, 0.0f, FLT_MAX_, stkN, stkT, cyc, stride, h);
     store_hit(record, i, h);
     float c[3];
     if (h.flags & F_HIT) {
@@ -106,8 +106,8 @@ __global__ void __launch_bounds__(FWD_THREADS, 768 / FWD_THREADS) diff_forward_k
     const uint32_t* __restrict__ idx, float* __restrict__ image, vx_hit* __restrict__ record) {
     extern __shared__ uint32_t smem[];
     uint32_t* stkN = smem + threadIdx.x;
-    float* stkT = reinterpret_cast<float*>(smem + s.max_levels * blockDim.x) + threadIdx.x;
-    uint32_t* cyc = smem + 2 * s.max_levels * blockDim.x + threadIdx.x;
+    float* stkT = reinterpret_cast<float*>(smem + s.max_levels * FWD_THREADS) + threadIdx.x;
+    uint32_t* cyc = smem + 2 * s.max_levels * FWD_THREADS + threadIdx.x;
     const uint32_t per_view = w * hgt;
 #if VX_DIFF_TILED
     const uint32_t tw = (w + 31) / 32, tiles = tw * ((hgt + 7) / 8);
@@ -120,12 +120,12 @@ __global__ void __launch_bounds__(FWD_THREADS, 768 / FWD_THREADS) diff_forward_k
     const uint32_t py = (tl / tw) * 8 + (piece >> 2) * 4 + (lane >> 3);
     if (px >= w || py >= hgt) return;
     forward_pixel(s, views.cam[v], px, py, w, hgt, v * per_view + py * w + px, kind, attr, idx, image, record, stkN,
-                  stkT, cyc);
+                  stkT, cyc, FWD_THREADS);
 #else
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nviews * per_view) return;
     const uint32_t v = i / per_view, p = i - v * per_view;
-    forward_pixel(s, views.cam[v], p % w, p / w, w, hgt, i, kind, attr, idx, image, record, stkN, stkT, cyc);
+    forward_pixel(s, views.cam[v], p % w, p / w, w, hgt, i, kind, attr, idx, image, record, stkN, stkT, cyc, FWD_THREADS);
 #endif
 }
 

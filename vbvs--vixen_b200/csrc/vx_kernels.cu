@@ -24,14 +24,14 @@ __global__ void __launch_bounds__(BLOCK, 768 / BLOCK) cast_kernel(DevScene s, co
                                                       vx_ray_counters* __restrict__ counters, LodCone lod) {
     extern __shared__ uint32_t smem[];
     uint32_t* stkN = smem + threadIdx.x;
-    float* stkT = reinterpret_cast<float*>(smem + s.max_levels * blockDim.x) + threadIdx.x;
-    uint32_t* cyc = smem + 2 * s.max_levels * blockDim.x + threadIdx.x;
+    float* stkT = reinterpret_cast<float*>(smem + s.max_levels * BLOCK) + threadIdx.x;
+    uint32_t* cyc = smem + 2 * s.max_levels * BLOCK + threadIdx.x;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float2* r2 = reinterpret_cast<const float2*>(rays + i);
     const float2 a = __ldg(r2), b = __ldg(r2 + 1), c = __ldg(r2 + 2);
     Hit h;
-    cast_ray<LOD>(s, a.x, a.y, b.x, b.y, c.x, c.y, tmin, tmax, stkN, stkT, cyc, blockDim.x, h, lod);
+    cast_ray<LOD>(s, a.x, a.y, b.x, b.y, c.x, c.y, tmin, tmax, stkN, stkT, cyc, BLOCK, h, lod);
     store_hit(hits, i, h);
     if (color) store_color(s, color, i, h);
     if (counters) {
@@ -53,14 +53,14 @@ __global__ void __launch_bounds__(BLOCK, 768 / BLOCK) cast_mapped_kernel(DevScen
                                                                         float tmax, vx_hit* __restrict__ hits) {
     extern __shared__ uint32_t smem[];
     uint32_t* stkN = smem + threadIdx.x;
-    float* stkT = reinterpret_cast<float*>(smem + s.max_levels * blockDim.x) + threadIdx.x;
-    uint32_t* cyc = smem + 2 * s.max_levels * blockDim.x + threadIdx.x;
+    float* stkT = reinterpret_cast<float*>(smem + s.max_levels * BLOCK) + threadIdx.x;
+    uint32_t* cyc = smem + 2 * s.max_levels * BLOCK + threadIdx.x;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= min(n_max, __ldg(count))) return;
     const float2* r2 = reinterpret_cast<const float2*>(rays + i);
     const float2 a = __ldg(r2), b = __ldg(r2 + 1), c = __ldg(r2 + 2);
     Hit h;
-    cast_ray(s, a.x, a.y, b.x, b.y, c.x, c.y, tmin, tmax, stkN, stkT, cyc, blockDim.x, h);
+    cast_ray(s, a.x, a.y, b.x, b.y, c.x, c.y, tmin, tmax, stkN, stkT, cyc, BLOCK, h);
     store_hit(hits, __ldg(map + i), h);
 }
 
@@ -74,8 +74,8 @@ __global__ void __launch_bounds__(RENDER_THREADS, 768 / RENDER_THREADS) render_k
     void* __restrict__ color) {
     extern __shared__ uint32_t smem[];
     uint32_t* stkN = smem + threadIdx.x;
-    float* stkT = reinterpret_cast<float*>(smem + s.max_levels * blockDim.x) + threadIdx.x;
-    uint32_t* cyc = smem + 2 * s.max_levels * blockDim.x + threadIdx.x;
+    float* stkT = reinterpret_cast<float*>(smem + s.max_levels * RENDER_THREADS) + threadIdx.x;
+    uint32_t* cyc = smem + 2 * s.max_levels * RENDER_THREADS + threadIdx.x;
     const uint32_t tw = (w + 31) / 32;
     const uint32_t lane = threadIdx.x & 31u;
     const uint64_t t = uint64_t(blockIdx.x) * RENDER_WARPS + (threadIdx.x >> 5);
@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(RENDER_THREADS, 768 / RENDER_THREADS) render_k
     float uv_y;
     camera_ray(cam, px, py, w, hgt, r, &uv_y);
     Hit h;
-    cast_ray(s, r.ox, r.oy, r.oz, r.dx, r.dy, r.dz, 0.0f, FLT_MAX_, stkN, stkT, cyc, blockDim.x, h);
+    cast_ray(s, r.ox, r.oy, r.oz, r.dx, r.dy, r.dz, 0.0f, FLT_MAX_, stkN, stkT, cyc, RENDER_THREADS, h);
     if (hits) store_hit(hits, i, h);
     if (color) store_color(s, color, i, h);
     if (image) {
