@@ -381,17 +381,27 @@ def measure_cfg4(args, rank, world, steps, warmup, with_cpu):
     del cnt_p, cnt_b
     clocks = sampler.stop()
 
-    # e2e: the captured frame from pinned host buffers (rays in; primary and bounce hits out)
-    batch.capture_frame_compact(d_rays, d_begin, ph, bounce, bh, CFG4_SEED, stream.cuda_stream)
+    # e2e: the frame from pinned host buffers (rays in; primary and bounce hits out) through
+    # vx_batch_launch_frame_host, the frame captured in parts so that the copies of each part
+    # overlap the casts of its neighbours; the whole frame's host call for comparison.
     rays_h = torch.from_numpy(rays_all).pin_memory()
     ph_h = torch.zeros((n, 4), dtype=torch.int32).pin_memory()
     bh_h = torch.zeros((2 * n, 4), dtype=torch.int32).pin_memory()
+    with torch.cuda.stream(stream):
+        batch.capture_frame_compact(d_rays, d_begin, ph, bounce, bh, CFG4_SEED, stream.cuda_stream)
+    whole_ms = events_ms(lambda: batch.launch_frame_host(rays_h, ph_h, bh_h, stream.cuda_stream), steps, warmup,
+                         flush, stream)
+    whole_same = bool(np.array_equal(ph_h.numpy(), ref_p) and np.array_equal(bh_h.numpy(), ref_b))
+    ph_h.zero_(), bh_h.zero_()
+    with torch.cuda.stream(stream):
+        batch.capture_frame_parts(d_rays, d_begin, ph, bounce, bh, CFG4_SEED, args.e2e_parts, stream.cuda_stream)
+    torch.cuda.synchronize()
     e2e_ms = events_ms(lambda: batch.launch_frame_host(rays_h, ph_h, bh_h, stream.cuda_stream), steps, warmup,
                        flush, stream)
     e2e_same = bool(np.array_equal(ph_h.numpy(), ref_p) and np.array_equal(bh_h.numpy(), ref_b))
     del rays_h, ph_h, bh_h
-    batch_total, plain_total, full_total, e2e_total = M.max_over_ranks(
-        [sum(batched_ms), sum(plain_ms), sum(full_ms), sum(e2e_ms)])
+    batch_total, plain_total, full_total, e2e_total, whole_total = M.max_over_ranks(
+        [sum(batched_ms), sum(plain_ms), sum(full_ms), sum(e2e_ms), sum(whole_ms)])
 
     peak, peak_kind = measured_peaks()
     passes = {}
@@ -421,8 +431,14 @@ def measure_cfg4(args, rank, world, steps, warmup, with_cpu):
            "roofline": roofline,
            "e2e": {"value": world * rays_per_frame * steps / (e2e_total / 1e3) / 1e6, "unit": "Mrays/s",
                    "h2d_bytes_per_step": world * n * 24, "d2h_bytes_per_step": world * n * (16 + 32),
-                   "call": "vx_batch_launch_frame_host (pinned buffers; primary hits copied out during the bounce "
-                           "pass)", "hits_equal_device_path": e2e_same, "ms_per_frame": e2e_total / steps},
+                   "call": f"vx_batch_launch_frame_host on the frame captured in {args.e2e_parts} parts "
+                           f"(vx_batch_capture_frame_parts; pinned buffers; rays in, primary and bounce hits out, "
+                           f"overlapped with the other parts' casts)", "hits_equal_device_path": e2e_same,
+                   "ms_per_frame": e2e_total / steps,
+                   "whole_frame": {"value": world * rays_per_frame * steps / (whole_total / 1e3) / 1e6,
+                                   "ms_per_frame": whole_total / steps, "hits_equal_device_path": whole_same,
+                                   "call": "vx_batch_launch_frame_host on the frame of vx_batch_capture_frame_compact "
+                                           "(primary hits copied out during the bounce pass)"}},
            "batched": {"mrays_s": world * rays_per_frame * steps / (batch_total / 1e3) / 1e6,
                        "ms_per_frame": batch_total / steps, "tuning": tuning.as_dict(), "bounce_tuning": btuning.as_dict(),
                        "autotune_best_ms_primary": tune_ms, "autotune_best_ms_bounce": btune_ms},
@@ -1257,6 +1273,8 @@ def main():
     ap.add_argument("--R3", type=int, default=2048, help="cfg3: grid side of the urban scene")
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--scenes", type=int, default=64, help="cfg4: number of scenes")
+    ap.add_argument("--e2e-parts", type=int, default=16,
+                    help="cfg4: parts of the frame whose host copies overlap the other parts' casts (e2e)")
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the oracle legs (CPU baseline and parity samples)")
     ap.add_argument("--no-extra", action="store_true",

@@ -444,6 +444,22 @@ int vx_batch_launch_frame(vx_batch* batch, void* stream);
  * buffers let the copies run at full link speed. */
 int vx_batch_launch_frame_host(vx_batch* batch, const vx_ray* primary_host, vx_hit* primary_hits_host,
                                vx_hit* bounce_hits_host, void* stream);
+/* The frame of vx_batch_capture_frame_compact, captured as `parts` pieces
+ * with a graph each: piece k casts the primary rays [k n / parts,
+ * (k + 1) n / parts) of the frame (a piece may begin or end inside a scene)
+ * and the bounce rays of their hits.  primary_hits_dev and bounce_hits_dev
+ * end up exactly as with the whole frame (bounce directions follow the frame's
+ * ray index); each piece compacts its bounce rays into its own range
+ * bounce_dev[2 r0 .. 2 r1).  vx_batch_launch_frame replays the pieces in order
+ * on its stream; vx_batch_launch_frame_host overlaps them with the copies:
+ * the rays of every piece go in on a copy stream, piece k casts once its rays
+ * are in, and its primary and bounce hits go out on a second copy stream once
+ * it is done, while the next pieces cast.  vx_batch_frame_compaction returns
+ * VX_EINVAL for such a frame.  Scratch: that of the compacted frame, per
+ * piece. */
+int vx_batch_capture_frame_parts(vx_batch* batch, const vx_ray* primary_dev, const uint32_t* primary_begin_dev,
+                                 uint32_t n, vx_hit* primary_hits_dev, vx_ray* bounce_dev, vx_hit* bounce_hits_dev,
+                                 uint64_t seed, uint32_t parts, void* stream);
 /* Layout of a compacted frame after it has run: the compacted bounce rays of
  * scene s are bounce_dev[scene_begin[s] .. scene_begin[s + 1]) (count + 1 host
  * u32), and compacted ray j's record is bounce_hits_dev[map[j]] (map_host:

@@ -211,10 +211,54 @@ def test_compacted_frame_equals_eager(vx, cuda, big, bounce_tuning):
     ph_h = torch.full((n, 4), -1, dtype=torch.int32).pin_memory()
     bh_h = torch.full((2 * n, 4), -1, dtype=torch.int32).pin_memory()
     d_rays.zero_()  # the call copies the rays in itself
+    torch.cuda.synchronize()  # the zeroing ran on another stream than the call's
     for _ in range(2):
         batch.launch_frame_host(rays_h, ph_h, bh_h, s.cuda_stream)
         np.testing.assert_array_equal(ph_h.numpy(), eager_ph)
         np.testing.assert_array_equal(bh_h.numpy(), eager_bh)
+        ph_h.fill_(-1), bh_h.fill_(-1)
+
+
+@pytest.mark.parametrize("parts", [1, 3, 7, 40])
+def test_frame_in_parts_equals_whole_frame(vx, cuda, parts):
+    """vx_batch_capture_frame_parts: pieces of consecutive primary rays (they begin and end
+    inside scenes) give the whole compacted frame's primary and bounce records, replayed on the
+    device and through vx_batch_launch_frame_host's pipelined copies; frame_compaction refuses
+    a frame in parts."""
+    import torch
+    from vx_b200 import workloads as W
+    wls, scenes, rays, begin, allr, d_rays, d_begin = _setup(vx, W, n=8, seed=31)
+    n = d_rays.shape[0]
+    batch = vx.Batch(scenes)
+    batch.set_bounce_tuning(vx.BatchTuning(256, 256, 0, 16))
+    s = torch.cuda.Stream()
+    ph = torch.full((n, 4), -1, dtype=torch.int32, device="cuda")
+    bh = torch.full((2 * n, 4), -1, dtype=torch.int32, device="cuda")
+    bounce = torch.zeros((2 * n, 6), dtype=torch.float32, device="cuda")
+    with torch.cuda.stream(s):
+        batch.capture_frame_compact(d_rays, d_begin, ph, bounce, bh, 9, s.cuda_stream)
+        batch.launch_frame(s.cuda_stream)
+    torch.cuda.synchronize()
+    whole_ph, whole_bh = ph.cpu().numpy().copy(), bh.cpu().numpy().copy()
+    ph.fill_(-1), bh.fill_(-1), bounce.zero_()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(s):
+        batch.capture_frame_parts(d_rays, d_begin, ph, bounce, bh, 9, parts, s.cuda_stream)
+        batch.launch_frame(s.cuda_stream)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(ph.cpu().numpy(), whole_ph)
+    np.testing.assert_array_equal(bh.cpu().numpy(), whole_bh)
+    with pytest.raises(vx.VxError):
+        batch.frame_compaction()
+    rays_h = d_rays.cpu().pin_memory()
+    ph_h = torch.full((n, 4), -1, dtype=torch.int32).pin_memory()
+    bh_h = torch.full((2 * n, 4), -1, dtype=torch.int32).pin_memory()
+    d_rays.zero_()  # the call copies the rays in itself
+    torch.cuda.synchronize()
+    for _ in range(2):
+        batch.launch_frame_host(rays_h, ph_h, bh_h, s.cuda_stream)
+        np.testing.assert_array_equal(ph_h.numpy(), whole_ph)
+        np.testing.assert_array_equal(bh_h.numpy(), whole_bh)
         ph_h.fill_(-1), bh_h.fill_(-1)
 
 

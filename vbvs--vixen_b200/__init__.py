@@ -143,6 +143,7 @@ def lib():
         "vx_bounce_table": (C.c_int, [vp]),
         "vx_batch_capture_frame": (C.c_int, [vp, vp, vp, u32, vp, vp, vp, vp, u64, vp]),
         "vx_batch_capture_frame_compact": (C.c_int, [vp, vp, vp, u32, vp, vp, vp, u64, vp]),
+        "vx_batch_capture_frame_parts": (C.c_int, [vp, vp, vp, u32, vp, vp, vp, u64, u32, vp]),
         "vx_cast_shadow_rays": (C.c_int, [vp, vp, vp, u32, vp, C.c_float, C.c_float, vp, vp]),
         "vx_batch_launch_frame": (C.c_int, [vp, vp]),
         "vx_batch_launch_frame_host": (C.c_int, [vp, vp, vp, vp, vp]),
@@ -732,6 +733,14 @@ class Batch:
         check(lib().vx_batch_capture_frame_compact(self._h, _p(primary), _p(primary_begin), primary.shape[0],
                                                    _p(primary_hits), _p(bounce), _p(bounce_hits), seed,
                                                    C.c_void_p(stream)))
+
+    def capture_frame_parts(self, primary, primary_begin, primary_hits, bounce, bounce_hits, seed, parts, stream):
+        """vx_batch_capture_frame_parts: the compacted frame as `parts` pieces of consecutive primary
+        rays, each with its own graph; launch_frame_host overlaps each piece's copies with the casts
+        of the others.  Results as with capture_frame_compact."""
+        check(lib().vx_batch_capture_frame_parts(self._h, _p(primary), _p(primary_begin), primary.shape[0],
+                                                 _p(primary_hits), _p(bounce), _p(bounce_hits), seed, int(parts),
+                                                 C.c_void_p(stream)))
 
     def launch_frame(self, stream=None):
         check(lib().vx_batch_launch_frame(self._h, _stream(stream)))

@@ -632,11 +632,24 @@ struct vx_batch {
     cudaEvent_t ev_primary = nullptr;    // recorded inside the frame once the primary pass is done
     cudaEvent_t ev_copied = nullptr;
     cudaStream_t side = nullptr;         // copies the primary hits out while the bounce pass runs
+    // A frame captured in parts (vx_batch_capture_frame_parts): part k is a
+    // batch over the scenes of the frame's primary rays [r0, r1), with its own
+    // compacted frame graph; `in` / `done` order its copies in and out.
+    struct Part {
+        vx_batch* sub;
+        uint32_t r0, r1;
+        cudaEvent_t in, done;
+    };
+    std::vector<Part> parts;
+    uint32_t* part_begin = nullptr;  // device: the parts' scene offsets, relative to r0
+    cudaStream_t in_stream = nullptr;  // copies the rays of the parts in
 };
 
 namespace {
 
 using vx::fail;
+
+void forget_parts(vx_batch* b);
 
 int cuda_err(cudaError_t e, const char* what) {
     return fail(VX_ECUDA, std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
@@ -760,6 +773,8 @@ int vx_batch_create(const vx_scene* const* scenes, uint32_t count, vx_batch** ou
 
 int vx_batch_destroy(vx_batch* b) {
     if (!b) return VX_OK;
+    forget_parts(b);
+    if (b->in_stream) cudaStreamDestroy(b->in_stream);
     if (b->frame) cudaGraphExecDestroy(b->frame);
     if (b->frame_graph) cudaGraphDestroy(b->frame_graph);
     if (b->ev_primary) cudaEventDestroy(b->ev_primary);
@@ -951,6 +966,17 @@ int record_primary_done(vx_batch* b, cudaStream_t st) {
     return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_batch: primary-pass event");
 }
 
+void forget_parts(vx_batch* b) {
+    for (auto& p : b->parts) {
+        vx_batch_destroy(p.sub);
+        if (p.in) cudaEventDestroy(p.in);
+        if (p.done) cudaEventDestroy(p.done);
+    }
+    b->parts.clear();
+    cudaFree(b->part_begin);
+    b->part_begin = nullptr;
+}
+
 void forget_frame(vx_batch* b) {
     if (b->frame) { cudaGraphExecDestroy(b->frame); b->frame = nullptr; }
     if (b->frame_graph) { cudaGraphDestroy(b->frame_graph); b->frame_graph = nullptr; }
@@ -973,6 +999,7 @@ int vx_batch_capture_frame(vx_batch* b, const vx_ray* primary, const uint32_t* p
     if (int r = vx::ensure_bounce_table()) return r;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (!st) return fail(VX_EINVAL, "vx_batch_capture_frame: capture needs a non-default stream");
+    forget_parts(b);
     forget_frame(b);
     // Resolve shared-memory attributes and occupancy outside the capture.
     if (int r = prepare_batch(b, b->tuning)) return r;
@@ -1000,10 +1027,17 @@ int vx_batch_capture_frame(vx_batch* b, const vx_ray* primary, const uint32_t* p
     return VX_OK;
 }
 
-static int vx_batch_capture_frame_compact_body(vx_batch* b, const vx_ray* primary, const uint32_t* primary_begin,
-                                               uint32_t n, vx_hit* primary_hits, vx_ray* bounce, vx_hit* bounce_hits,
-                                               uint64_t seed, void* stream) {
-    if (!b || !primary || !primary_begin || !primary_hits || !bounce || !bounce_hits || n == 0 || n > 0x7FFFFFFFu)
+// The compacted frame of batch b over primary rays [ray0, ray0 + n) of a
+// frame: primary / primary_hits / bounce_hits are the frame's buffers (ray i
+// of the frame at index i, its bounce slots at 2i, 2i + 1), primary_begin the
+// S + 1 offsets of b's scenes relative to ray0, and bounce the part's own 2n
+// rays of compaction output.  Bounce directions follow the frame index i, so
+// a frame captured in parts casts the rays of the whole frame.
+static int capture_compact(vx_batch* b, const vx_ray* primary, const uint32_t* primary_begin, uint32_t n,
+                           vx_hit* primary_hits, vx_ray* bounce, vx_hit* bounce_hits, uint64_t seed, void* stream,
+                           uint32_t ray0) {
+    if (!b || !primary || !primary_begin || !primary_hits || !bounce || !bounce_hits || n == 0 || n > 0x7FFFFFFFu ||
+        uint64_t(ray0) + n > 0x7FFFFFFFu)
         return fail(VX_EINVAL, "vx_batch_capture_frame_compact: bad argument");
     if (reinterpret_cast<uintptr_t>(bounce) % 8 || reinterpret_cast<uintptr_t>(bounce_hits) % 16 ||
         reinterpret_cast<uintptr_t>(primary_hits) % 16)
@@ -1030,7 +1064,8 @@ static int vx_batch_capture_frame_compact_body(vx_batch* b, const vx_ray* primar
         if (hb[sc + 1] < hb[sc]) return fail(VX_EINVAL, "vx_batch_capture_frame_compact: primary_begin decreases");
         first[sc] = uint32_t(chunks.size());
         for (uint32_t a = hb[sc]; a < hb[sc + 1]; a += std::min(vx::COMPACT_CHUNK, hb[sc + 1] - a))
-            chunks.push_back(vx::CompactChunk{a, a + std::min(vx::COMPACT_CHUNK, hb[sc + 1] - a), sc, 0u});
+            chunks.push_back(
+                vx::CompactChunk{ray0 + a, ray0 + a + std::min(vx::COMPACT_CHUNK, hb[sc + 1] - a), sc, 0u});
     }
     first[b->S] = uint32_t(chunks.size());
     const uint32_t nc = uint32_t(chunks.size());
@@ -1064,7 +1099,8 @@ static int vx_batch_capture_frame_compact_body(vx_batch* b, const vx_ray* primar
     if (e != cudaSuccess) return cuda_err(e, "vx_batch_capture_frame_compact: chunk table");
     e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_err(e, "vx_batch_capture_frame_compact: begin capture");
-    int r = vx_cast_batch(b, primary, primary_begin, n, 0.0f, 3.402823466e+38f, primary_hits, nullptr, stream);
+    int r = vx_cast_batch(b, primary + ray0, primary_begin, n, 0.0f, 3.402823466e+38f, primary_hits + ray0, nullptr,
+                          stream);
     if (r == VX_OK) r = record_primary_done(b, st);
     if (r == VX_OK) {
         vx::compact_count_kernel<<<nc, 256, 0, st>>>(chunk_dev, primary, primary_hits, seed, counts);
@@ -1084,9 +1120,9 @@ static int vx_batch_capture_frame_compact_body(vx_batch* b, const vx_ray* primar
     e = cudaGraphInstantiate(&b->frame, g, 0);
     if (e != cudaSuccess) { cudaGraphDestroy(g); return cuda_err(e, "vx_batch_capture_frame_compact: instantiate"); }
     b->frame_graph = g;
-    b->f_primary = primary;
-    b->f_primary_hits = primary_hits;
-    b->f_bounce_hits = bounce_hits;
+    b->f_primary = primary + ray0;
+    b->f_primary_hits = primary_hits + ray0;
+    b->f_bounce_hits = bounce_hits + 2 * size_t(ray0);
     b->f_n = n;
     b->f_cbegin = cbegin;
     b->f_map = map;
@@ -1097,12 +1133,159 @@ int vx_batch_capture_frame_compact(vx_batch* b, const vx_ray* primary, const uin
                                    vx_hit* primary_hits, vx_ray* bounce, vx_hit* bounce_hits, uint64_t seed,
                                    void* stream) {
     return vx::guarded("vx_batch_capture_frame_compact", [&] {
-        return vx_batch_capture_frame_compact_body(b, primary, primary_begin, n, primary_hits, bounce, bounce_hits,
-                                                   seed, stream);
+        if (b) forget_parts(b);
+        return capture_compact(b, primary, primary_begin, n, primary_hits, bounce, bounce_hits, seed, stream, 0u);
+    });
+}
+
+}  // extern "C"
+
+namespace {
+
+// Batch over scenes [s0, s0 + count) of b, with b's tunings.
+int make_part(const vx_batch* b, uint32_t s0, uint32_t count, vx_batch** out) {
+    *out = nullptr;
+    auto* p = new (std::nothrow) vx_batch();
+    if (!p) return fail(VX_ENOMEM, "vx_batch_capture_frame_parts: out of host memory");
+    p->device = b->device;
+    p->S = count;
+    p->maxL = b->maxL;
+    p->tuning = b->tuning;
+    p->bounce_tuning = b->bounce_tuning;
+    p->num_sms = b->num_sms;
+    cudaError_t e = cudaMalloc(&p->scenes, sizeof(vx::DevScene) * count);
+    if (e == cudaSuccess) e = cudaMalloc(&p->work, 256);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(p->scenes, b->scenes + s0, sizeof(vx::DevScene) * count, cudaMemcpyDeviceToDevice);
+    if (e != cudaSuccess) {
+        vx_batch_destroy(p);
+        return cuda_err(e, "vx_batch_capture_frame_parts: part");
+    }
+    *out = p;
+    return VX_OK;
+}
+
+int capture_parts(vx_batch* b, const vx_ray* primary, const uint32_t* primary_begin, uint32_t n,
+                  vx_hit* primary_hits, vx_ray* bounce, vx_hit* bounce_hits, uint64_t seed, uint32_t parts,
+                  void* stream) {
+    if (!b || !primary || !primary_begin || !primary_hits || !bounce || !bounce_hits || n == 0 || n > 0x7FFFFFFFu ||
+        parts == 0)
+        return fail(VX_EINVAL, "vx_batch_capture_frame_parts: bad argument");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (!st) return fail(VX_EINVAL, "vx_batch_capture_frame_parts: capture needs a non-default stream");
+    forget_parts(b);
+    forget_frame(b);
+    std::vector<uint32_t> hb(size_t(b->S) + 1);
+    cudaError_t e = cudaMemcpyAsync(hb.data(), primary_begin, hb.size() * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_err(e, "vx_batch_capture_frame_parts: read scene offsets");
+    if (hb[0] != 0 || hb[b->S] != n) return fail(VX_EINVAL, "vx_batch_capture_frame_parts: primary_begin must run from 0 to n");
+    for (uint32_t sc = 0; sc < b->S; ++sc)
+        if (hb[sc + 1] < hb[sc]) return fail(VX_EINVAL, "vx_batch_capture_frame_parts: primary_begin decreases");
+    if (!b->in_stream) {
+        e = cudaStreamCreateWithFlags(&b->in_stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cuda_err(e, "vx_batch_capture_frame_parts: copy stream");
+    }
+    if (int r = ensure_frame_events(b)) return r;
+    // Part k: primary rays [k n / P, (k + 1) n / P) and the scenes they fall
+    // in; its scene offsets are the frame's clamped to the part, relative to
+    // its first ray.
+    const uint32_t P = std::min(parts, n);
+    std::vector<uint32_t> lb;
+    struct Span { uint32_t r0, r1, s0, count, lb0; };
+    std::vector<Span> spans;
+    for (uint32_t k = 0; k < P; ++k) {
+        const uint32_t r0 = uint32_t(uint64_t(n) * k / P), r1 = uint32_t(uint64_t(n) * (k + 1) / P);
+        if (r1 == r0) continue;
+        // scene of ray r: the last s with hb[s] <= r (hb[s + 1] > r)
+        const uint32_t s0 = uint32_t(std::upper_bound(hb.begin(), hb.end(), r0) - hb.begin()) - 1;
+        const uint32_t s1 = uint32_t(std::upper_bound(hb.begin(), hb.end(), r1 - 1) - hb.begin());
+        spans.push_back(Span{r0, r1, s0, s1 - s0, uint32_t(lb.size())});
+        for (uint32_t j = 0; j <= s1 - s0; ++j) lb.push_back(std::min(std::max(hb[s0 + j], r0), r1) - r0);
+    }
+    e = cudaMalloc(&b->part_begin, lb.size() * 4);
+    if (e == cudaSuccess) e = cudaMemcpy(b->part_begin, lb.data(), lb.size() * 4, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_err(e, "vx_batch_capture_frame_parts: part offsets");
+    for (const Span& sp : spans) {
+        vx_batch::Part part{nullptr, sp.r0, sp.r1, nullptr, nullptr};
+        int r = make_part(b, sp.s0, sp.count, &part.sub);
+        if (r == VX_OK) {
+            e = cudaEventCreateWithFlags(&part.in, cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&part.done, cudaEventDisableTiming);
+            if (e != cudaSuccess) r = cuda_err(e, "vx_batch_capture_frame_parts: part events");
+        }
+        if (r == VX_OK)
+            r = capture_compact(part.sub, primary, b->part_begin + sp.lb0, sp.r1 - sp.r0, primary_hits,
+                                bounce + 2 * size_t(sp.r0), bounce_hits, seed, stream, sp.r0);
+        b->parts.push_back(part);  // forget_parts releases whatever was made
+        if (r != VX_OK) {
+            forget_parts(b);
+            return r;
+        }
+    }
+    b->f_primary = primary;
+    b->f_primary_hits = primary_hits;
+    b->f_bounce_hits = bounce_hits;
+    b->f_n = n;
+    return VX_OK;
+}
+
+// vx_batch_launch_frame_host for a frame captured in parts: the rays of
+// every part go in on the copy stream, part k's frame runs on `st` once its
+// rays are in, and its primary and bounce hits go out on the side stream once
+// it is done, so the copies of one part overlap the casts of its neighbours.
+int launch_parts_host(vx_batch* b, const vx_ray* primary_host, vx_hit* primary_hits_host, vx_hit* bounce_hits_host,
+                      cudaStream_t st) {
+    cudaError_t e = cudaSuccess;
+    // the copy stream starts after whatever was queued on st before the call
+    e = cudaEventRecord(b->ev_copied, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->in_stream, b->ev_copied, 0);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->side, b->ev_copied, 0);
+    for (size_t k = 0; e == cudaSuccess && k < b->parts.size(); ++k) {
+        const auto& p = b->parts[k];
+        e = cudaMemcpyAsync(const_cast<vx_ray*>(b->f_primary) + p.r0, primary_host + p.r0,
+                            size_t(p.r1 - p.r0) * sizeof(vx_ray), cudaMemcpyHostToDevice, b->in_stream);
+        if (e == cudaSuccess) e = cudaEventRecord(p.in, b->in_stream);
+    }
+    for (size_t k = 0; e == cudaSuccess && k < b->parts.size(); ++k) {
+        const auto& p = b->parts[k];
+        e = cudaStreamWaitEvent(st, p.in, 0);
+        if (e == cudaSuccess) e = cudaGraphLaunch(p.sub->frame, st);
+        if (e == cudaSuccess) e = cudaEventRecord(p.done, st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->side, p.done, 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(primary_hits_host + p.r0, b->f_primary_hits + p.r0,
+                                size_t(p.r1 - p.r0) * sizeof(vx_hit), cudaMemcpyDeviceToHost, b->side);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(bounce_hits_host + 2 * size_t(p.r0), b->f_bounce_hits + 2 * size_t(p.r0),
+                                2 * size_t(p.r1 - p.r0) * sizeof(vx_hit), cudaMemcpyDeviceToHost, b->side);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(b->ev_copied, b->side);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, b->ev_copied, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_batch_launch_frame_host");
+}
+
+}  // namespace
+
+extern "C" {
+
+int vx_batch_capture_frame_parts(vx_batch* b, const vx_ray* primary, const uint32_t* primary_begin, uint32_t n,
+                                 vx_hit* primary_hits, vx_ray* bounce, vx_hit* bounce_hits, uint64_t seed,
+                                 uint32_t parts, void* stream) {
+    return vx::guarded("vx_batch_capture_frame_parts", [&] {
+        return capture_parts(b, primary, primary_begin, n, primary_hits, bounce, bounce_hits, seed, parts, stream);
     });
 }
 
 int vx_batch_launch_frame(vx_batch* b, void* stream) {
+    if (b && !b->parts.empty()) {
+        for (const auto& p : b->parts) {
+            const cudaError_t e = cudaGraphLaunch(p.sub->frame, static_cast<cudaStream_t>(stream));
+            if (e != cudaSuccess) return cuda_err(e, "vx_batch_launch_frame");
+        }
+        return VX_OK;
+    }
     if (!b || !b->frame) return fail(VX_EINVAL, "vx_batch_launch_frame: no captured frame");
     cudaError_t e = cudaGraphLaunch(b->frame, static_cast<cudaStream_t>(stream));
     return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_batch_launch_frame");
@@ -1110,6 +1293,11 @@ int vx_batch_launch_frame(vx_batch* b, void* stream) {
 
 int vx_batch_launch_frame_host(vx_batch* b, const vx_ray* primary_host, vx_hit* primary_hits_host,
                                vx_hit* bounce_hits_host, void* stream) {
+    if (b && !b->parts.empty()) {
+        if (!primary_host || !primary_hits_host || !bounce_hits_host)
+            return fail(VX_EINVAL, "vx_batch_launch_frame_host: null argument");
+        return launch_parts_host(b, primary_host, primary_hits_host, bounce_hits_host, static_cast<cudaStream_t>(stream));
+    }
     if (!b || !b->frame) return fail(VX_EINVAL, "vx_batch_launch_frame_host: no captured frame");
     if (!primary_host || !primary_hits_host || !bounce_hits_host)
         return fail(VX_EINVAL, "vx_batch_launch_frame_host: null argument");
@@ -1134,6 +1322,8 @@ int vx_batch_launch_frame_host(vx_batch* b, const vx_ray* primary_host, vx_hit* 
 
 int vx_batch_frame_compaction(const vx_batch* b, uint32_t* scene_begin, uint32_t* map_host,
                               const uint32_t** cbegin_dev, const uint32_t** map_dev) {
+    if (b && !b->parts.empty())
+        return fail(VX_EINVAL, "vx_batch_frame_compaction: the frame was captured in parts (each part compacts its own rays)");
     if (!b || !b->frame || !b->f_cbegin)
         return fail(VX_EINVAL, "vx_batch_frame_compaction: no compacted frame captured");
     if (cbegin_dev) *cbegin_dev = b->f_cbegin;

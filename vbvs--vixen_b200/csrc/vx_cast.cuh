@@ -231,7 +231,6 @@ struct CastState {
     // cycle detection
     uint32_t d1g, d1d;     // grid reads / DDA steps of the previous iteration
     uint32_t sig1, sig2;   // signatures of the loop states one and two iterations back
-    int nsig;              // signatures recorded (saturates at 2)
     int cand_p, cand_at;   // deferred check: pending candidate's period, iteration it is confirmed at
 };
 
@@ -311,10 +310,14 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
             } else {
                 inv = rcp[i];
             }
+            // glm::min / max of the two plane t values: multiplication by one
+            // factor is monotone, so their order is the sign of inv (equal
+            // values are the same number); neither is NaN
             const float t0 = (s.wmin[i] - o[i]) * inv;
             const float t1 = (s.wmax[i] - o[i]) * inv;
-            tnear[i] = gmin(t0, t1);
-            tfar[i] = gmax(t0, t1);
+            const bool pos = inv > 0.0f;
+            tnear[i] = pos ? t0 : t1;
+            tfar[i] = pos ? t1 : t0;
         }
         tEntry = max3(tnear[0], tnear[1], tnear[2]);
         tExit = min3(tfar[0], tfar[1], tfar[2]);
@@ -413,7 +416,6 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
     st.pChild = st.pMask = 0;
     st.d1g = st.d1d = 0;
     st.sig1 = st.sig2 = 0;
-    st.nsig = 0;
     st.cand_p = st.cand_at = 0;
     return false;
 }
@@ -430,7 +432,10 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
 // the 500-iteration cap: the result is the capped miss and the remaining
 // iterations' counters repeat the cycle's.  From iteration CYCLE_START on,
 // every state gets a 32-bit signature, and the signatures of the two previous
-// states stay in registers; equal states always have equal signatures.  Two
+// states stay in registers; equal states always have equal signatures.  Every
+// iteration from CYCLE_START that does not end the ray records one, so at
+// iteration i the signature one back exists from CYCLE_START + 1 and the one
+// two back from CYCLE_START + 2.  Two
 // policies, the same results:
 //  - immediate (DEFER = false; the stack in shared memory): every state is
 //    stored in one of two parity slots (cyc[(p * 8 + k) * stride]), and a
@@ -647,8 +652,8 @@ __device__ __forceinline__ bool cycle_check(CastState& st, uint32_t g0, uint32_t
     if constexpr (!DEFER) {
         uint32_t* back2 = cyc + ((st.iter & 1) * 8) * stride;
         const uint32_t* back1 = cyc + (((st.iter & 1) ^ 1) * 8) * stride;
-        bool eq1 = st.nsig >= 1 && st.sig1 == sig;
-        bool eq2 = st.nsig >= 2 && st.sig2 == sig;
+        bool eq1 = st.iter >= CYCLE_START + 1 && st.sig1 == sig;
+        bool eq2 = st.iter >= CYCLE_START + 2 && st.sig2 == sig;
         if (eq1 || eq2) {
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
@@ -670,7 +675,9 @@ __device__ __forceinline__ bool cycle_check(CastState& st, uint32_t g0, uint32_t
             st.cand_p = 0;
         }
         if (!period && !st.cand_p) {
-            const int p = (st.nsig >= 1 && sig == st.sig1) ? 1 : ((st.nsig >= 2 && sig == st.sig2) ? 2 : 0);
+            const int p = (st.iter >= CYCLE_START + 1 && sig == st.sig1)
+                              ? 1
+                              : ((st.iter >= CYCLE_START + 2 && sig == st.sig2) ? 2 : 0);
             if (p) {
 #pragma unroll
                 for (int k = 0; k < 8; ++k) cyc[k * stride] = cur[k];
@@ -697,7 +704,6 @@ __device__ __forceinline__ bool cycle_check(CastState& st, uint32_t g0, uint32_t
     }
     st.sig2 = st.sig1;
     st.sig1 = sig;
-    st.nsig = st.nsig < 2 ? st.nsig + 1 : 2;
     st.d1g = dg;
     st.d1d = ddd;
     return false;
@@ -735,7 +741,9 @@ __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint
     bool isLeaf = (st.pMask >> (worldIdx + 8)) & 1u;
     if (st.scale - minScale == s.brick_user_scale && child_valid) isLeaf = true;
     float tv_max = 0.0f;
-    if (child_valid && !(st.t_min > st.t_max) && st.t_min <= (tv_max = nmin(st.t_max, k.tcc))) {
+    // !(t_min > t_max) && t_min <= min(t_max, tc_max): the first test follows
+    // from the second, the loop's t values being NaN-free
+    if (child_valid && st.t_min <= (tv_max = nmin(st.t_max, k.tcc))) {
         if constexpr (LOD) {
             // worldDistance = tRayStart + t_min * |worldSize| (:627);
             // esvoScaleToWorldSize = 2^(scale - 23) * worldSize.x (SVOLOD.h:189-195),
