@@ -307,7 +307,7 @@ def measure_cfg4(args, rank, world, steps, warmup, with_cpu):
     tuning, tune_ms = batch.autotune(d_rays, d_begin, ph)
     vx.spawn_bounce_rays(d_rays, ph, CFG4_SEED, bounce)
     btuning, btune_ms = batch.autotune(bounce, d_bbegin, bh)
-    batch.set_tuning(tuning.block, tuning.rays_per_task, tuning.stack_in_shared, tuning.refill)
+    batch.set_tuning(**tuning.as_dict())
     batch.set_bounce_tuning(btuning)
     stream = torch.cuda.Stream()
 
@@ -370,13 +370,13 @@ def measure_cfg4(args, rank, world, steps, warmup, with_cpu):
     cnt_p = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
     cnt_b = torch.zeros((max(h2, 1), 4), dtype=torch.int32, device="cuda")
     batch.cast(d_rays, d_begin, ph, cnt_p)
-    batch.set_tuning(btuning.block, btuning.rays_per_task, btuning.stack_in_shared, btuning.refill)
+    batch.set_tuning(**btuning.as_dict())
     batch.cast(bounce[:h2], d_cb, pbh, cnt_b)
     torch.cuda.synchronize()
     tot_p = counter_totals(vx, cnt_p)
     tot_b = counter_totals(vx, cnt_b[:h2])
     bounce_pass_ms = events_ms(lambda: batch.cast(bounce[:h2], d_cb, pbh), steps, warmup, flush, stream)
-    batch.set_tuning(tuning.block, tuning.rays_per_task, tuning.stack_in_shared, tuning.refill)
+    batch.set_tuning(**tuning.as_dict())
     primary_pass_ms = events_ms(lambda: batch.cast(d_rays, d_begin, ph), steps, warmup, flush, stream)
     del cnt_p, cnt_b
     clocks = sampler.stop()
@@ -411,6 +411,7 @@ def measure_cfg4(args, rank, world, steps, warmup, with_cpu):
         mean_s = statistics.mean(ms) / 1e3
         kname = "vx::batch_refill_kernel" if tn.refill else "vx::batch_kernel"
         passes[name] = {"kernel": kname, "rays": nr, "tuning": tn.as_dict(), "kernel_ms_mean": mean_s * 1e3,
+                        "launches": 2 if tn.budget else 1,  # a budgeted pass: all rays, then the set-aside ones
                         "algorithmic_bytes_per_launch": algo, "achieved_gbs": algo / mean_s / 1e9,
                         "mrays_s": nr / mean_s / 1e6,
                         "per_ray": {k: v / max(nr, 1) for k, v in tot.items()}}
@@ -445,6 +446,7 @@ def measure_cfg4(args, rank, world, steps, warmup, with_cpu):
            "plain": {"mrays_s": world * rays_per_frame * steps / (plain_total / 1e3) / 1e6,
                      "ms_per_frame": plain_total / steps, "launches_per_frame": 2 * len(specs),
                      "rays": "the same primary rays and compacted bounce rays of hits as the batched frame"},
+           "launches_per_frame": 5 + int(tuning.budget > 0) + int(btuning.budget > 0),
            "speedup_batched_vs_plain": plain_total / batch_total,
            "uncompacted_batched_ms_per_frame": full_total / steps,
            "compaction_gain": full_total / batch_total,
@@ -570,8 +572,9 @@ def run_cfg4(args, rank, world):
             "warmup": args.warmup, "ms_per_step": res.pop("ms_per_frame"), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": res.pop("config"),
-            # per timed frame: batched primary cast, octant counts, offsets, compacted scatter, batched bounce cast
-            "gpu_launches": args.steps * 5}
+            # per timed frame: batched primary cast, octant counts, offsets, compacted scatter, batched bounce
+            # cast, and the second launch of each pass whose tuning has an iteration budget
+            "gpu_launches": args.steps * res.pop("launches_per_frame")}
     line.update(res)
     if world == 1 and not args.no_extra:
         extra_steps, extra_warmup = max(3, min(args.steps, 10)), max(3, min(args.warmup, 3))
@@ -1273,7 +1276,7 @@ def main():
     ap.add_argument("--R3", type=int, default=2048, help="cfg3: grid side of the urban scene")
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--scenes", type=int, default=64, help="cfg4: number of scenes")
-    ap.add_argument("--e2e-parts", type=int, default=16,
+    ap.add_argument("--e2e-parts", type=int, default=32,
                     help="cfg4: parts of the frame whose host copies overlap the other parts' casts (e2e)")
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the oracle legs (CPU baseline and parity samples)")

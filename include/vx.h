@@ -353,6 +353,12 @@ typedef struct vx_batch_tuning {
     int32_t refill;           /* 0: each lane casts its rays of a task start to end;
                                  1..32: lanes advance one ESVO iteration per round and the
                                  warp deals new rays to idle lanes once this many are idle */
+    int32_t budget;           /* refill 0 only.  0: none; 1..500: a ray still running after this
+                                 many ESVO iterations is set aside, and a second launch casts the
+                                 set-aside rays from the start (a warp otherwise waits for its
+                                 longest ray).  Same results; the batch holds a list of n u32,
+                                 allocated on the first call with a larger n (outside a capture:
+                                 cast once before capturing by hand) */
 } vx_batch_tuning;
 
 int vx_batch_create(const vx_scene* const* scenes, uint32_t count, vx_batch** out);
@@ -362,9 +368,9 @@ int vx_batch_get_tuning(const vx_batch* batch, vx_batch_tuning* tuning);
 int vx_cast_batch(vx_batch* batch, const vx_ray* rays_dev, const uint32_t* begin_dev, uint32_t n,
                   float t_min, float t_max, vx_hit* hits_dev, vx_ray_counters* counters_dev,
                   void* stream);
-/* Times every (block, rays_per_task, stack placement, refill) candidate on
- * the given rays (3 launches each, best of the last 2), keeps the fastest in
- * the batch and returns it.  Writes hits_dev. */
+/* Times every (block, rays_per_task, stack placement, refill, budget)
+ * candidate on the given rays (3 calls each, best of the last 2), keeps the
+ * fastest in the batch and returns it.  Writes hits_dev. */
 int vx_batch_autotune(vx_batch* batch, const vx_ray* rays_dev, const uint32_t* begin_dev, uint32_t n,
                       vx_hit* hits_dev, void* stream, vx_batch_tuning* best, float* best_ms);
 
@@ -450,11 +456,14 @@ int vx_batch_launch_frame_host(vx_batch* batch, const vx_ray* primary_host, vx_h
  * and the bounce rays of their hits.  primary_hits_dev and bounce_hits_dev
  * end up exactly as with the whole frame (bounce directions follow the frame's
  * ray index); each piece compacts its bounce rays into its own range
- * bounce_dev[2 r0 .. 2 r1).  vx_batch_launch_frame replays the pieces in order
- * on its stream; vx_batch_launch_frame_host overlaps them with the copies:
- * the rays of every piece go in on a copy stream, piece k casts once its rays
- * are in, and its primary and bounce hits go out on a second copy stream once
- * it is done, while the next pieces cast.  vx_batch_frame_compaction returns
+ * bounce_dev[2 r0 .. 2 r1).  vx_batch_launch_frame replays the pieces in order,
+ * the even ones on its stream and the odd ones on a stream of the batch, so
+ * that one piece's kernels start while the previous piece's drain, and makes
+ * its stream wait for both; vx_batch_launch_frame_host does the same and
+ * overlaps the pieces with the copies: the rays of every piece go in on a
+ * copy stream, piece k casts once its rays are in, and its primary and bounce
+ * hits go out on a second copy stream once it is done, while the next pieces
+ * cast.  vx_batch_frame_compaction returns
  * VX_EINVAL for such a frame.  Scratch: that of the compacted frame, per
  * piece. */
 int vx_batch_capture_frame_parts(vx_batch* batch, const vx_ray* primary_dev, const uint32_t* primary_begin_dev,

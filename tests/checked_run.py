@@ -57,7 +57,7 @@ def main(out_path):
     br = torch.from_numpy(np.concatenate(rl)).cuda()
     bb = torch.from_numpy(begin).cuda()
     batch = vx.Batch(scenes)
-    for tune in ((256, 32, 1, 0), (128, 64, 0, 16)):
+    for tune in ((256, 32, 1, 0, 3), (128, 64, 0, 16, 0)):
         batch.set_tuning(*tune)
         bh = torch.zeros((br.shape[0], 4), dtype=torch.int32, device="cuda")
         batch.cast(br, bb, bh)

@@ -32,16 +32,18 @@ def _plain(vx, scenes, rays, begin, d_rays):
     return hits
 
 
-@pytest.mark.parametrize("block,k,smem,refill", [(256, 128, 1, 0), (128, 32, 1, 0), (256, 64, 0, 0), (128, 512, 0, 0),
-                                                 (256, 32, 1, 16), (128, 64, 1, 8), (256, 128, 0, 24),
-                                                 (256, 32, 1, 32), (128, 32, 0, 1)])
-def test_batch_equals_plain_and_oracle(vx, vo, cuda, block, k, smem, refill):
+@pytest.mark.parametrize("block,k,smem,refill,budget", [
+    (256, 128, 1, 0, 0), (128, 32, 1, 0, 0), (256, 64, 0, 0, 0), (128, 512, 0, 0, 0),
+    (256, 32, 1, 16, 0), (128, 64, 1, 8, 0), (256, 128, 0, 24, 0), (256, 32, 1, 32, 0), (128, 32, 0, 1, 0),
+    # iteration budgets: every ray still running after 1, 3 or 8 iterations is cast again
+    (256, 32, 1, 0, 1), (128, 64, 0, 0, 3), (256, 32, 1, 0, 8)])
+def test_batch_equals_plain_and_oracle(vx, vo, cuda, block, k, smem, refill, budget):
     import torch
     from vx_b200 import workloads as W
     wls, scenes, rays, begin, allr, d_rays, d_begin = _setup(vx, W)
     plain = _plain(vx, scenes, rays, begin, d_rays)
     batch = vx.Batch(scenes)
-    batch.set_tuning(block, k, smem, refill)
+    batch.set_tuning(block, k, smem, refill, budget)
     hits = torch.full_like(plain, -1)
     cnt = torch.zeros((allr.shape[0], 4), dtype=torch.int32, device="cuda")
     batch.cast(d_rays, d_begin, hits, cnt)
@@ -104,7 +106,7 @@ def test_shadow_spawn_matches_reference(vx, cuda):
     assert np.all(got[hit, 3:] == L) and np.all(got[~hit, 3:] == 0)
 
 
-@pytest.mark.parametrize("bounce_tuning", [None, (128, 64, 0, 16), (256, 256, 0, 24)])
+@pytest.mark.parametrize("bounce_tuning", [None, (128, 64, 0, 16), (256, 256, 0, 24), (256, 32, 1, 0, 4)])
 def test_frame_graph_equals_eager(vx, cuda, bounce_tuning):
     import torch
     from vx_b200 import workloads as W
@@ -134,7 +136,8 @@ def test_frame_graph_equals_eager(vx, cuda, bounce_tuning):
     np.testing.assert_array_equal(bh.cpu().numpy(), eager[1])
 
 
-@pytest.mark.parametrize("big,bounce_tuning", [(False, None), (False, (256, 256, 0, 24)), (True, (128, 64, 0, 16))])
+@pytest.mark.parametrize("big,bounce_tuning", [(False, None), (False, (256, 256, 0, 24)), (True, (128, 64, 0, 16)),
+                                                (True, (256, 32, 1, 0, 6))])
 def test_compacted_frame_equals_eager(vx, cuda, big, bounce_tuning):
     """vx_batch_capture_frame_compact: primary and bounce hit records equal the eager frame's
     (whose bounce pass casts all 2n slots, zero-direction rays included); the compacted bounce
@@ -230,7 +233,7 @@ def test_frame_in_parts_equals_whole_frame(vx, cuda, parts):
     wls, scenes, rays, begin, allr, d_rays, d_begin = _setup(vx, W, n=8, seed=31)
     n = d_rays.shape[0]
     batch = vx.Batch(scenes)
-    batch.set_bounce_tuning(vx.BatchTuning(256, 256, 0, 16))
+    batch.set_bounce_tuning(vx.BatchTuning(256, 32, 1, 0, 5))
     s = torch.cuda.Stream()
     ph = torch.full((n, 4), -1, dtype=torch.int32, device="cuda")
     bh = torch.full((2 * n, 4), -1, dtype=torch.int32, device="cuda")
@@ -287,6 +290,10 @@ def test_batch_rejects_bad_tuning(vx, cuda):
         b.set_tuning(rays_per_task=40)
     with pytest.raises(vx.VxError):
         b.set_tuning(refill=33)
+    with pytest.raises(vx.VxError):
+        b.set_tuning(refill=8, budget=24)  # a budget applies to static lanes only
+    with pytest.raises(vx.VxError):
+        b.set_tuning(budget=501)
     with pytest.raises(vx.VxError):
         b.set_bounce_tuning(vx.BatchTuning(256, 48, 1, 0))
     b.set_bounce_tuning(None)

@@ -664,11 +664,11 @@ class CudaOctree:
 
 class BatchTuning(C.Structure):
     _fields_ = [("block", C.c_int32), ("rays_per_task", C.c_int32), ("stack_in_shared", C.c_int32),
-                ("refill", C.c_int32)]
+                ("refill", C.c_int32), ("budget", C.c_int32)]
 
     def as_dict(self):
         return {"block": self.block, "rays_per_task": self.rays_per_task, "stack_in_shared": self.stack_in_shared,
-                "refill": self.refill}
+                "refill": self.refill, "budget": self.budget}
 
 
 def _stream(stream):
@@ -702,8 +702,8 @@ class Batch:
         check(lib().vx_batch_get_tuning(self._h, C.byref(t)))
         return t
 
-    def set_tuning(self, block=256, rays_per_task=32, stack_in_shared=1, refill=0):
-        t = BatchTuning(block, rays_per_task, stack_in_shared, refill)
+    def set_tuning(self, block=256, rays_per_task=32, stack_in_shared=1, refill=0, budget=0):
+        t = BatchTuning(block, rays_per_task, stack_in_shared, refill, budget)
         check(lib().vx_batch_set_tuning(self._h, C.byref(t)))
 
     def set_bounce_tuning(self, tuning=None):

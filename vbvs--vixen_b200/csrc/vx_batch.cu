@@ -43,6 +43,14 @@ struct BatchArgs {
     int refill;      // refill idle lanes once this many are idle (refilling kernels)
     const uint32_t* map = nullptr;    // hit / counter slot of ray r (null: slot r)
     const uint32_t* n_dev = nullptr;  // ray count known on the device only (null: n)
+    // Static lanes with an iteration budget: a ray still running after
+    // `budget` iterations is appended to retry[0 .. *retry_n) instead of being
+    // finished.  A second launch with gather = retry casts exactly those rays
+    // (task ray j is ray gather[j]).
+    int budget = 0;
+    uint32_t* retry = nullptr;
+    uint32_t* retry_n = nullptr;
+    const uint32_t* gather = nullptr;
 };
 
 // Rays of the launch: n, or the device-side count when the rays were
@@ -210,13 +218,18 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
         const uint64_t r0 = uint64_t(t) * a.K;
         if (r0 >= n) break;
         const uint32_t r1 = uint32_t(min(r0 + a.K, uint64_t(n)));
-        for (uint32_t r = uint32_t(r0) + lane; r < r1; r += 32) {
+        for (uint32_t j = uint32_t(r0) + lane; j < r1; j += 32) {
+            const uint32_t r = a.gather ? __ldg(a.gather + j) : j;
             const int lo = scene_of(beg, a.S, r);
             const float2* r2 = reinterpret_cast<const float2*>(a.rays + r);
             const float2 p = __ldg(r2), q = __ldg(r2 + 1), w = __ldg(r2 + 2);
             Hit h;
-            cast_ray<false, !SMEM_STACK>(sc[lo], p.x, p.y, q.x, q.y, w.x, w.y, a.tmin, a.tmax, stkN, stkT, cyc,
-                                         stride, h);
+            // no budget: MAX_ITER + 1, which no cast reaches (the loop stops at MAX_ITER)
+            if (!cast_ray_budget<false, !SMEM_STACK>(sc[lo], p.x, p.y, q.x, q.y, w.x, w.y, a.tmin, a.tmax, stkN, stkT,
+                                                     cyc, stride, a.budget > 0 ? a.budget : MAX_ITER + 1, h)) {
+                a.retry[atomicAdd(a.retry_n, 1u)] = r;
+                continue;
+            }
             store_hit(a.hits, out_slot(a, r), h);
             store_counters(a.counters, out_slot(a, r), h);
         }
@@ -614,8 +627,10 @@ struct vx_batch {
     int maxL = 1;
     vx::DevScene* scenes = nullptr;  // device copy of the scene table
     uint32_t* work = nullptr;        // task counter (device scratch)
-    vx_batch_tuning tuning{256, 32, 1, 0};
-    vx_batch_tuning bounce_tuning{0, 0, 0, 0};  // block 0: the bounce pass of a frame uses `tuning`
+    uint32_t* retry = nullptr;       // budgeted tunings: set-aside count at [0], ray list from [64]
+    uint64_t retry_cap = 0;          // rays the list holds
+    vx_batch_tuning tuning{256, 32, 1, 0, 0};
+    vx_batch_tuning bounce_tuning{0, 0, 0, 0, 0};  // block 0: the bounce pass of a frame uses `tuning`
     int num_sms = 148;
     cudaGraphExec_t frame = nullptr;
     cudaGraph_t frame_graph = nullptr;
@@ -643,6 +658,8 @@ struct vx_batch {
     std::vector<Part> parts;
     uint32_t* part_begin = nullptr;  // device: the parts' scene offsets, relative to r0
     cudaStream_t in_stream = nullptr;  // copies the rays of the parts in
+    cudaStream_t alt = nullptr;        // casts the odd parts (the even ones run on the caller's stream)
+    cudaEvent_t ev_alt = nullptr;
 };
 
 namespace {
@@ -725,9 +742,28 @@ int prepare_batch(vx_batch* b, const vx_batch_tuning& t) { return dispatch_batch
 
 int check_tuning(const vx_batch_tuning* t) {
     if (!t || (t->block != 128 && t->block != 256) || t->rays_per_task < 32 || t->rays_per_task > 65536 ||
-        (t->rays_per_task % 32) != 0 || t->refill < 0 || t->refill > 32)
+        (t->rays_per_task % 32) != 0 || t->refill < 0 || t->refill > 32 || t->budget < 0 || t->budget > 500 ||
+        (t->budget && t->refill))
         return fail(VX_EINVAL, "batch tuning: block must be 128 or 256, rays_per_task a multiple of 32 in "
-                               "[32, 65536], refill in [0, 32]");
+                               "[32, 65536], refill in [0, 32], budget in [0, 500] and 0 with refill");
+    return VX_OK;
+}
+
+// The set-aside list of a budgeted tuning, for n rays.  Allocates (outside a
+// stream capture only) when n grows.
+int ensure_retry(vx_batch* b, uint64_t n, cudaStream_t st) {
+    if (b->retry_cap >= n) return VX_OK;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (st) cudaStreamIsCapturing(st, &cs);
+    if (cs != cudaStreamCaptureStatusNone)
+        return fail(VX_EINVAL, "vx_cast_batch: a budgeted tuning needs its set-aside list before a capture "
+                               "(cast once with at least this many rays first)");
+    cudaFree(b->retry);
+    b->retry = nullptr;
+    b->retry_cap = 0;
+    cudaError_t e = cudaMalloc(&b->retry, 256 + n * 4);
+    if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch: set-aside list");
+    b->retry_cap = n;
     return VX_OK;
 }
 
@@ -775,6 +811,8 @@ int vx_batch_destroy(vx_batch* b) {
     if (!b) return VX_OK;
     forget_parts(b);
     if (b->in_stream) cudaStreamDestroy(b->in_stream);
+    if (b->alt) cudaStreamDestroy(b->alt);
+    if (b->ev_alt) cudaEventDestroy(b->ev_alt);
     if (b->frame) cudaGraphExecDestroy(b->frame);
     if (b->frame_graph) cudaGraphDestroy(b->frame_graph);
     if (b->ev_primary) cudaEventDestroy(b->ev_primary);
@@ -783,6 +821,7 @@ int vx_batch_destroy(vx_batch* b) {
     cudaFree(b->scenes);
     cudaFree(b->work);
     cudaFree(b->fscratch);
+    cudaFree(b->retry);
     delete b;
     return VX_OK;
 }
@@ -815,7 +854,25 @@ int cast_batch_with(vx_batch* b, const vx_batch_tuning& t, const vx_ray* rays, c
     if (n == 0) return VX_OK;
     vx::BatchArgs a{b->scenes, b->S, begin, rays, n, tmin, tmax, hits, counters, b->work,
                     uint32_t(t.rays_per_task), b->maxL, t.refill, map, n_dev};
-    return launch_batch(b, t, a, st);
+    if (t.budget <= 0) return launch_batch(b, t, a, st);
+    // Budgeted: the rays still running after t.budget iterations are set
+    // aside, then a second launch casts them from the start.
+    if (int r = ensure_retry(b, n, st)) return r;
+    e = cudaMemsetAsync(b->retry, 0, 4, st);
+    if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch: reset set-aside count");
+    a.budget = t.budget;
+    a.retry = b->retry + 64;
+    a.retry_n = b->retry;
+    if (int r = launch_batch(b, t, a, st)) return r;
+    e = cudaMemsetAsync(b->work, 0, 4, st);
+    if (e != cudaSuccess) return cuda_err(e, "vx_cast_batch: reset work counter");
+    vx::BatchArgs a2 = a;
+    a2.budget = 0;
+    a2.retry = nullptr;
+    a2.retry_n = nullptr;
+    a2.gather = b->retry + 64;
+    a2.n_dev = b->retry;
+    return launch_batch(b, t, a2, st);
 }
 
 const vx_batch_tuning& bounce_tuning_of(const vx_batch* b) {
@@ -832,7 +889,7 @@ int vx_cast_batch(vx_batch* b, const vx_ray* rays, const uint32_t* begin, uint32
 
 int vx_batch_set_bounce_tuning(vx_batch* b, const vx_batch_tuning* t) {
     if (!b) return fail(VX_EINVAL, "vx_batch_set_bounce_tuning: null batch");
-    if (!t) { b->bounce_tuning = vx_batch_tuning{0, 0, 0, 0}; return VX_OK; }
+    if (!t) { b->bounce_tuning = vx_batch_tuning{0, 0, 0, 0, 0}; return VX_OK; }
     if (int r = check_tuning(t)) return r;
     b->bounce_tuning = *t;
     return VX_OK;
@@ -850,33 +907,33 @@ static int vx_batch_autotune_body(vx_batch* b, const vx_ray* rays, const uint32_
     const int blocks[] = {128, 256};
     const int ks[] = {32, 64, 128, 256, 512, 1024};
     const int refills[] = {0, 8, 16, 24};
+    const int budgets[] = {0, 24, 48};
+    if (int r = ensure_retry(b, n, st)) { cudaEventDestroy(e0); cudaEventDestroy(e1); return r; }
     for (int blk : blocks)
         for (int sm = 1; sm >= 0; --sm)
             for (int rf : refills)
-                for (int k : ks) {
-                    if (rf && k > 256) continue;  // refilling warps draw rays one round at a time
-                    vx_batch_tuning t{blk, k, sm, rf};
-                    vx::BatchArgs a{b->scenes, b->S, begin, rays, n, 0.0f, 3.402823466e+38f, hits, nullptr, b->work,
-                                    uint32_t(k), b->maxL, rf};
-                    float ms_min = 1e30f;
-                    for (int rep = 0; rep < 3; ++rep) {
-                        cudaMemsetAsync(b->work, 0, 4, st);
-                        cudaEventRecord(e0, st);
-                        int r = launch_batch(b, t, a, st);
-                        cudaEventRecord(e1, st);
-                        if (r != VX_OK) { cudaEventDestroy(e0); cudaEventDestroy(e1); return r; }
-                        cudaError_t e = cudaEventSynchronize(e1);
-                        if (e != cudaSuccess) {
-                            cudaEventDestroy(e0);
-                            cudaEventDestroy(e1);
-                            return cuda_err(e, "autotune");
+                for (int bud : budgets)
+                    for (int k : ks) {
+                        if (rf && (k > 256 || bud)) continue;  // refilling warps draw rays one round at a time
+                        vx_batch_tuning t{blk, k, sm, rf, bud};
+                        float ms_min = 1e30f;
+                        for (int rep = 0; rep < 3; ++rep) {
+                            cudaEventRecord(e0, st);
+                            int r = cast_batch_with(b, t, rays, begin, n, 0.0f, 3.402823466e+38f, hits, nullptr, st);
+                            cudaEventRecord(e1, st);
+                            if (r != VX_OK) { cudaEventDestroy(e0); cudaEventDestroy(e1); return r; }
+                            cudaError_t e = cudaEventSynchronize(e1);
+                            if (e != cudaSuccess) {
+                                cudaEventDestroy(e0);
+                                cudaEventDestroy(e1);
+                                return cuda_err(e, "autotune");
+                            }
+                            float ms = 0;
+                            cudaEventElapsedTime(&ms, e0, e1);
+                            if (rep > 0) ms_min = std::min(ms_min, ms);
                         }
-                        float ms = 0;
-                        cudaEventElapsedTime(&ms, e0, e1);
-                        if (rep > 0) ms_min = std::min(ms_min, ms);
+                        if (ms_min < best) { best = ms_min; bt = t; }
                     }
-                    if (ms_min < best) { best = ms_min; bt = t; }
-                }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     b->tuning = bt;
@@ -1004,6 +1061,8 @@ int vx_batch_capture_frame(vx_batch* b, const vx_ray* primary, const uint32_t* p
     // Resolve shared-memory attributes and occupancy outside the capture.
     if (int r = prepare_batch(b, b->tuning)) return r;
     if (int r = prepare_batch(b, bounce_tuning_of(b))) return r;
+    if (b->tuning.budget || bounce_tuning_of(b).budget)
+        if (int r = ensure_retry(b, 2 * uint64_t(n), nullptr)) return r;
     if (int r = ensure_frame_events(b)) return r;
     cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_err(e, "vx_batch_capture_frame: begin capture");
@@ -1048,6 +1107,8 @@ static int capture_compact(vx_batch* b, const vx_ray* primary, const uint32_t* p
     forget_frame(b);
     if (int r = prepare_batch(b, b->tuning)) return r;
     if (int r = prepare_batch(b, bounce_tuning_of(b))) return r;
+    if (b->tuning.budget || bounce_tuning_of(b).budget)
+        if (int r = ensure_retry(b, 2 * uint64_t(n), nullptr)) return r;
     if (int r = ensure_frame_events(b)) return r;
     // The chunk table follows the scene offsets, read once here: primary rays
     // of scene s are [begin[s], begin[s + 1]), split into chunks of at most
@@ -1182,10 +1243,10 @@ int capture_parts(vx_batch* b, const vx_ray* primary, const uint32_t* primary_be
     if (hb[0] != 0 || hb[b->S] != n) return fail(VX_EINVAL, "vx_batch_capture_frame_parts: primary_begin must run from 0 to n");
     for (uint32_t sc = 0; sc < b->S; ++sc)
         if (hb[sc + 1] < hb[sc]) return fail(VX_EINVAL, "vx_batch_capture_frame_parts: primary_begin decreases");
-    if (!b->in_stream) {
-        e = cudaStreamCreateWithFlags(&b->in_stream, cudaStreamNonBlocking);
-        if (e != cudaSuccess) return cuda_err(e, "vx_batch_capture_frame_parts: copy stream");
-    }
+    if (!b->in_stream) e = cudaStreamCreateWithFlags(&b->in_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !b->alt) e = cudaStreamCreateWithFlags(&b->alt, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !b->ev_alt) e = cudaEventCreateWithFlags(&b->ev_alt, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_err(e, "vx_batch_capture_frame_parts: streams");
     if (int r = ensure_frame_events(b)) return r;
     // Part k: primary rays [k n / P, (k + 1) n / P) and the scenes they fall
     // in; its scene offsets are the frame's clamped to the part, relative to
@@ -1230,18 +1291,23 @@ int capture_parts(vx_batch* b, const vx_ray* primary, const uint32_t* primary_be
     return VX_OK;
 }
 
-// vx_batch_launch_frame_host for a frame captured in parts: the rays of
-// every part go in on the copy stream, part k's frame runs on `st` once its
-// rays are in, and its primary and bounce hits go out on the side stream once
-// it is done, so the copies of one part overlap the casts of its neighbours.
-int launch_parts_host(vx_batch* b, const vx_ray* primary_host, vx_hit* primary_hits_host, vx_hit* bounce_hits_host,
-                      cudaStream_t st) {
-    cudaError_t e = cudaSuccess;
-    // the copy stream starts after whatever was queued on st before the call
-    e = cudaEventRecord(b->ev_copied, st);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->in_stream, b->ev_copied, 0);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->side, b->ev_copied, 0);
-    for (size_t k = 0; e == cudaSuccess && k < b->parts.size(); ++k) {
+// The parts of a frame in order, part k on `st` for even k and on b->alt for
+// odd k, so that the persistent kernels of one part fill the SMs the tail of
+// the previous part leaves idle (the parts share no buffer or counter).  With
+// host buffers (primary_host != null) the rays of every part first go in on
+// the copy stream, part k casts once its rays are in, and its primary and
+// bounce hits go out on the side stream once it is done, so that the copies
+// of one part overlap the casts of its neighbours.  Returns after `st` has
+// been made to wait for all of it (and, with host buffers, synchronised).
+int run_parts(vx_batch* b, const vx_ray* primary_host, vx_hit* primary_hits_host, vx_hit* bounce_hits_host,
+              cudaStream_t st) {
+    const bool host = primary_host != nullptr;
+    // every stream starts after whatever was queued on st before the call
+    cudaError_t e = cudaEventRecord(b->ev_copied, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->alt, b->ev_copied, 0);
+    if (host && e == cudaSuccess) e = cudaStreamWaitEvent(b->in_stream, b->ev_copied, 0);
+    if (host && e == cudaSuccess) e = cudaStreamWaitEvent(b->side, b->ev_copied, 0);
+    for (size_t k = 0; host && e == cudaSuccess && k < b->parts.size(); ++k) {
         const auto& p = b->parts[k];
         e = cudaMemcpyAsync(const_cast<vx_ray*>(b->f_primary) + p.r0, primary_host + p.r0,
                             size_t(p.r1 - p.r0) * sizeof(vx_ray), cudaMemcpyHostToDevice, b->in_stream);
@@ -1249,9 +1315,11 @@ int launch_parts_host(vx_batch* b, const vx_ray* primary_host, vx_hit* primary_h
     }
     for (size_t k = 0; e == cudaSuccess && k < b->parts.size(); ++k) {
         const auto& p = b->parts[k];
-        e = cudaStreamWaitEvent(st, p.in, 0);
-        if (e == cudaSuccess) e = cudaGraphLaunch(p.sub->frame, st);
-        if (e == cudaSuccess) e = cudaEventRecord(p.done, st);
+        cudaStream_t cs = (k & 1) ? b->alt : st;
+        if (host) e = cudaStreamWaitEvent(cs, p.in, 0);
+        if (e == cudaSuccess) e = cudaGraphLaunch(p.sub->frame, cs);
+        if (e == cudaSuccess) e = cudaEventRecord(p.done, cs);
+        if (!host) continue;
         if (e == cudaSuccess) e = cudaStreamWaitEvent(b->side, p.done, 0);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(primary_hits_host + p.r0, b->f_primary_hits + p.r0,
@@ -1260,10 +1328,14 @@ int launch_parts_host(vx_batch* b, const vx_ray* primary_host, vx_hit* primary_h
             e = cudaMemcpyAsync(bounce_hits_host + 2 * size_t(p.r0), b->f_bounce_hits + 2 * size_t(p.r0),
                                 2 * size_t(p.r1 - p.r0) * sizeof(vx_hit), cudaMemcpyDeviceToHost, b->side);
     }
-    if (e == cudaSuccess) e = cudaEventRecord(b->ev_copied, b->side);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, b->ev_copied, 0);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_batch_launch_frame_host");
+    if (e == cudaSuccess) e = cudaEventRecord(b->ev_alt, b->alt);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, b->ev_alt, 0);
+    if (host) {
+        if (e == cudaSuccess) e = cudaEventRecord(b->ev_copied, b->side);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(st, b->ev_copied, 0);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    return e == cudaSuccess ? VX_OK : cuda_err(e, host ? "vx_batch_launch_frame_host" : "vx_batch_launch_frame");
 }
 
 }  // namespace
@@ -1279,13 +1351,7 @@ int vx_batch_capture_frame_parts(vx_batch* b, const vx_ray* primary, const uint3
 }
 
 int vx_batch_launch_frame(vx_batch* b, void* stream) {
-    if (b && !b->parts.empty()) {
-        for (const auto& p : b->parts) {
-            const cudaError_t e = cudaGraphLaunch(p.sub->frame, static_cast<cudaStream_t>(stream));
-            if (e != cudaSuccess) return cuda_err(e, "vx_batch_launch_frame");
-        }
-        return VX_OK;
-    }
+    if (b && !b->parts.empty()) return run_parts(b, nullptr, nullptr, nullptr, static_cast<cudaStream_t>(stream));
     if (!b || !b->frame) return fail(VX_EINVAL, "vx_batch_launch_frame: no captured frame");
     cudaError_t e = cudaGraphLaunch(b->frame, static_cast<cudaStream_t>(stream));
     return e == cudaSuccess ? VX_OK : cuda_err(e, "vx_batch_launch_frame");
@@ -1296,7 +1362,7 @@ int vx_batch_launch_frame_host(vx_batch* b, const vx_ray* primary_host, vx_hit* 
     if (b && !b->parts.empty()) {
         if (!primary_host || !primary_hits_host || !bounce_hits_host)
             return fail(VX_EINVAL, "vx_batch_launch_frame_host: null argument");
-        return launch_parts_host(b, primary_host, primary_hits_host, bounce_hits_host, static_cast<cudaStream_t>(stream));
+        return run_parts(b, primary_host, primary_hits_host, bounce_hits_host, static_cast<cudaStream_t>(stream));
     }
     if (!b || !b->frame) return fail(VX_EINVAL, "vx_batch_launch_frame_host: no captured frame");
     if (!primary_host || !primary_hits_host || !bounce_hits_host)

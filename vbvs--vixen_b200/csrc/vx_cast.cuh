@@ -743,7 +743,8 @@ __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint
     float tv_max = 0.0f;
     // !(t_min > t_max) && t_min <= min(t_max, tc_max): the first test follows
     // from the second, the loop's t values being NaN-free
-    if (child_valid && st.t_min <= (tv_max = nmin(st.t_max, k.tcc))) {
+    const bool in_range = child_valid && st.t_min <= (tv_max = nmin(st.t_max, k.tcc));
+    if (in_range) {
         if constexpr (LOD) {
             // worldDistance = tRayStart + t_min * |worldSize| (:627);
             // esvoScaleToWorldSize = 2^(scale - 23) * worldSize.x (SVOLOD.h:189-195),
@@ -761,37 +762,41 @@ __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint
                 return true;
             }
         }
-        if (isLeaf) {
-            if (leaf_stage(s, st, csx, csy, csz)) return true;
-            st.t_min = tv_max;
-            if (advance_pop(s, st, k, csx, csy, csz, stkN, stkT, stride)) return true;
-        } else {
-            // executePushPhase (:328-378); tx_center etc. of checkChildValidity
-            const float half = st.scale_exp2 * 0.5f;
-            const float tx_center = half * c.tx_coef + k.tx;
-            const float ty_center = half * c.ty_coef + k.ty;
-            const float tz_center = half * c.tz_coef + k.tz;
-            const float tc_max = nmin3(k.tx, k.ty, k.tz);
-            if (tc_max < st.hh) {
-                const uint32_t kk = bounded(uint32_t(st.scale - minScale), uint32_t(s.max_levels), V_STACK);
-                stkN[kk * stride] = st.parent;
-                stkT[kk * stride] = st.t_max;
-                st.pushed |= 1u << (st.scale - minScale);
-            }
-            st.hh = tc_max;
-            const uint32_t nonLeafMask = ~(st.pMask >> 8) & st.pMask & 0xFFu;
-            const uint32_t child_index = st.pChild + __popc(nonLeafMask & ((1u << worldIdx) - 1u));
-            if (child_index < s.node_count) {
-                st.parent = child_index;
-                st.idx = 0;
-                st.scale--;
-                st.scale_exp2 = half;
-                if (tx_center > st.t_min) { st.idx ^= 1; st.px += st.scale_exp2; }
-                if (ty_center > st.t_min) { st.idx ^= 2; st.py += st.scale_exp2; }
-                if (tz_center > st.t_min) { st.idx ^= 4; st.pz += st.scale_exp2; }
-                st.t_max = tv_max;
-                st.fetched = false;
-            }
+    }
+    // A leaf child in range: the leaf stage; when its brick is not hit the
+    // iteration continues with ADVANCE from tv_max, like a child out of range,
+    // so both run the one ADVANCE below together (lanes of a warp that took
+    // either way stay converged there).
+    if (in_range && isLeaf) {
+        if (leaf_stage(s, st, csx, csy, csz)) return true;
+        st.t_min = tv_max;
+    }
+    if (in_range && !isLeaf) {
+        // executePushPhase (:328-378); tx_center etc. of checkChildValidity
+        const float half = st.scale_exp2 * 0.5f;
+        const float tx_center = half * c.tx_coef + k.tx;
+        const float ty_center = half * c.ty_coef + k.ty;
+        const float tz_center = half * c.tz_coef + k.tz;
+        const float tc_max = nmin3(k.tx, k.ty, k.tz);
+        if (tc_max < st.hh) {
+            const uint32_t kk = bounded(uint32_t(st.scale - minScale), uint32_t(s.max_levels), V_STACK);
+            stkN[kk * stride] = st.parent;
+            stkT[kk * stride] = st.t_max;
+            st.pushed |= 1u << (st.scale - minScale);
+        }
+        st.hh = tc_max;
+        const uint32_t nonLeafMask = ~(st.pMask >> 8) & st.pMask & 0xFFu;
+        const uint32_t child_index = st.pChild + __popc(nonLeafMask & ((1u << worldIdx) - 1u));
+        if (child_index < s.node_count) {
+            st.parent = child_index;
+            st.idx = 0;
+            st.scale--;
+            st.scale_exp2 = half;
+            if (tx_center > st.t_min) { st.idx ^= 1; st.px += st.scale_exp2; }
+            if (ty_center > st.t_min) { st.idx ^= 2; st.py += st.scale_exp2; }
+            if (tz_center > st.t_min) { st.idx ^= 4; st.pz += st.scale_exp2; }
+            st.t_max = tv_max;
+            st.fetched = false;
         }
     } else {
         if (advance_pop(s, st, k, csx, csy, csz, stkN, stkT, stride)) return true;
@@ -810,6 +815,24 @@ __device__ __forceinline__ void cast_ray(const DevScene& s, float ox, float oy, 
         while (!cast_step<LOD, DEFER>(s, st, stkN, stkT, cyc, stride, lod)) {
         }
     h = st.h;
+}
+
+// cast_ray that gives up once `budget` iterations have run without ending the
+// ray: false then, and h is not written.  The cast is deterministic, so the
+// caller can cast the ray again from the start for its result.
+template <bool LOD = false, bool DEFER = false>
+__device__ __forceinline__ bool cast_ray_budget(const DevScene& s, float ox, float oy, float oz, float ddx, float ddy,
+                                                float ddz, float tMinArg, float tMaxArg, uint32_t* stkN, float* stkT,
+                                                uint32_t* cyc, int stride, int budget, Hit& h) {
+    CastState st;
+    if (!cast_init(s, ox, oy, oz, ddx, ddy, ddz, tMinArg, tMaxArg, stkN, stkT, stride, st)) {
+        // every cast_step that returns false has counted one iteration in st.iter
+        while (!cast_step<LOD, DEFER>(s, st, stkN, stkT, cyc, stride)) {
+            if (st.iter >= budget) return false;
+        }
+    }
+    h = st.h;
+    return true;
 }
 
 // DXT1 texel of the hit voxel: decodeColorHead (DXT1Compressor.cpp:14-36)
