@@ -446,7 +446,7 @@ def measure_cfg4(args, rank, world, steps, warmup, with_cpu):
            "plain": {"mrays_s": world * rays_per_frame * steps / (plain_total / 1e3) / 1e6,
                      "ms_per_frame": plain_total / steps, "launches_per_frame": 2 * len(specs),
                      "rays": "the same primary rays and compacted bounce rays of hits as the batched frame"},
-           "launches_per_frame": 5 + int(tuning.budget > 0) + int(btuning.budget > 0),
+           "launches_per_frame": 6 + int(tuning.budget > 0) + int(btuning.budget > 0),
            "speedup_batched_vs_plain": plain_total / batch_total,
            "uncompacted_batched_ms_per_frame": full_total / steps,
            "compaction_gain": full_total / batch_total,
@@ -572,8 +572,8 @@ def run_cfg4(args, rank, world):
             "warmup": args.warmup, "ms_per_step": res.pop("ms_per_frame"), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": res.pop("config"),
-            # per timed frame: batched primary cast, octant counts, offsets, compacted scatter, batched bounce
-            # cast, and the second launch of each pass whose tuning has an iteration budget
+            # per timed frame: batched primary cast, bin counts, per-scene scans, bases, compacted scatter,
+            # batched bounce cast, and the second launch of each pass whose tuning has an iteration budget
             "gpu_launches": args.steps * res.pop("launches_per_frame")}
     line.update(res)
     if world == 1 and not args.no_extra:

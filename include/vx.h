@@ -431,9 +431,11 @@ int vx_batch_capture_frame(vx_batch* batch, const vx_ray* primary_dev, const uin
                            void* stream);
 /* The same frame with the bounce rays compacted: the bounce pass casts only
  * the 2 rays of every primary hit.  bounce_dev (2n rays of scratch) receives
- * them, 2h of them for h primary hits, per scene grouped by direction octant
- * (primary order inside a group, the same order on every launch); the frame
- * computes the per-scene offsets itself.  primary_begin_dev is read once, at
+ * them, 2h of them for h primary hits, per scene grouped by direction bin
+ * (the octant and the order of the three axes by |d|: 48 bins); inside a
+ * group chunk by chunk of 1024 primary rays of the scene, inside a chunk the
+ * first bounce rays in primary order, then the second ones (the same order on
+ * every launch).  The frame computes the per-scene offsets itself.  primary_begin_dev is read once, at
  * capture (it must run from 0 to n and not decrease).  bounce_hits_dev (2n records) ends up exactly as
  * with vx_batch_capture_frame: slot 2i + k holds bounce k of primary ray i,
  * and the slots of primary misses hold the invalid-ray record a cast writes

@@ -21,6 +21,19 @@ def _setup(vx, W, n=10, seed=11):
     return wls, scenes, rays, begin, allr, torch.from_numpy(allr).cuda(), torch.from_numpy(begin.astype(np.int32)).cuda()
 
 
+def _direction_bin(rows):
+    """The compaction's direction bin of rays {o, d}: octant * 6 + the order of the axes by |d|
+    (major axis, then whether the minor one follows it cyclically)."""
+    d = rows[:, 3:6]
+    ax, ay, az = np.abs(d).T
+    octant = (d[:, 0] > 0).astype(np.int64) | ((d[:, 1] > 0).astype(np.int64) << 1) | \
+        ((d[:, 2] > 0).astype(np.int64) << 2)
+    major = np.where((ax >= ay) & (ax >= az), 0, np.where(ay >= az, 1, 2))
+    minor = np.where((ax < ay) & (ax < az), 0, np.where(ay < az, 1, 2))
+    assert np.all(major != minor)
+    return octant * 6 + major * 2 + (minor != (major + 1) % 3).astype(np.int64)
+
+
 def _plain(vx, scenes, rays, begin, d_rays):
     import torch
     n = d_rays.shape[0]
@@ -141,8 +154,8 @@ def test_frame_graph_equals_eager(vx, cuda, bounce_tuning):
 def test_compacted_frame_equals_eager(vx, cuda, big, bounce_tuning):
     """vx_batch_capture_frame_compact: primary and bounce hit records equal the eager frame's
     (whose bounce pass casts all 2n slots, zero-direction rays included); the compacted bounce
-    rays are the eager bounce rays of the primary hits, per scene grouped by direction octant
-    in primary order, the same on every launch.  `big` (more than 2^20 primary rays) gives
+    rays are the eager bounce rays of the primary hits, per scene grouped by direction bin, then
+    by chunk of 1024 primary rays, bounce k and primary order, the same on every launch.  `big` (more than 2^20 primary rays) gives
     scenes of many chunks with a partial last chunk."""
     import torch
     from vx_b200 import workloads as W
@@ -192,15 +205,16 @@ def test_compacted_frame_equals_eager(vx, cuda, big, bounce_tuning):
     hit = (eager_ph.view(vx.HIT_DTYPE).reshape(-1)["flags"] & 1).astype(bool)
     h = int(hit.sum())
     assert 0 < h < n
-    # expected order: scene, then octant of the direction, then (primary ray, k)
+    # expected order: scene, direction bin, chunk of 1024 primary rays of the scene, k, primary ray
     pair = eager_bounce.reshape(n, 2, 6)
     scene = np.repeat(np.arange(len(begin) - 1), np.diff(begin.astype(np.int64)))
     idx = np.flatnonzero(hit)
     rows = pair[idx].reshape(-1, 6)
     sc = np.repeat(scene[idx], 2)
-    octant = (rows[:, 3] > 0).astype(np.int64) | ((rows[:, 4] > 0).astype(np.int64) << 1) | \
-        ((rows[:, 5] > 0).astype(np.int64) << 2)
-    want = rows[np.lexsort((np.arange(rows.shape[0]), octant, sc))]
+    prim = np.repeat(idx, 2)
+    kk = np.tile(np.arange(2), idx.size)
+    chunk = (prim - begin.astype(np.int64)[sc]) // 1024
+    want = rows[np.lexsort((prim, kk, chunk, _direction_bin(rows), sc))]
     np.testing.assert_array_equal(got[:2 * h].view(np.uint32), want.view(np.uint32))
     # vx_batch_frame_compaction: per-scene ranges of the compacted rays and their hit slots
     sb, slot = batch.frame_compaction()

@@ -728,7 +728,7 @@ class Batch:
 
     def capture_frame_compact(self, primary, primary_begin, primary_hits, bounce, bounce_hits, seed, stream):
         """vx_batch_capture_frame_compact: the bounce pass casts only the bounce rays of primary hits
-        (compacted into `bounce`, 2 * hits of its 2n rows, per scene grouped by direction octant);
+        (compacted into `bounce`, 2 * hits of its 2n rows, per scene grouped by direction bin);
         `bounce_hits` ends up as with capture_frame."""
         check(lib().vx_batch_capture_frame_compact(self._h, _p(primary), _p(primary_begin), primary.shape[0],
                                                    _p(primary_hits), _p(bounce), _p(bounce_hits), seed,

@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_refill_kernel(BatchArgs a) 
             if (!tasks_left && next >= end) break;
             continue;
         }
-        if (active && cast_step<false, !SMEM_STACK>(sc[sid], st, stkN, stkT, cyc, stride)) {
+        if (active && cast_step<false, !SMEM_STACK, true>(sc[sid], st, stkN, stkT, cyc, stride)) {
             store_hit(a.hits, out_slot(a, ray), st.h);
             store_counters(a.counters, out_slot(a, ray), st.h);
             active = false;
@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
             const float2 p = __ldg(r2), q = __ldg(r2 + 1), w = __ldg(r2 + 2);
             Hit h;
             // no budget: MAX_ITER + 1, which no cast reaches (the loop stops at MAX_ITER)
-            if (!cast_ray_budget<false, !SMEM_STACK>(sc[lo], p.x, p.y, q.x, q.y, w.x, w.y, a.tmin, a.tmax, stkN, stkT,
+            if (!cast_ray_budget<false, !SMEM_STACK, true>(sc[lo], p.x, p.y, q.x, q.y, w.x, w.y, a.tmin, a.tmax, stkN, stkT,
                                                      cyc, stride, a.budget > 0 ? a.budget : MAX_ITER + 1, h)) {
                 a.retry[atomicAdd(a.retry_n, 1u)] = r;
                 continue;
@@ -311,101 +311,125 @@ __global__ void spawn_shadow_kernel(const vx_ray* __restrict__ rays, const vx_hi
 }
 
 // Bounce-ray compaction of a frame: the bounce pass casts only the 2 rays of
-// every primary hit, grouped per scene by direction octant (rays that head the
-// same way through the same scene take similar paths through the octree), in
-// primary order inside a group.  The primary rays are split into chunks of at
+// every primary hit, grouped per scene by direction bin (rays that head the
+// same way through the same scene take similar paths through the octree).
+// A direction's bin is its octant and the order of its three axes by
+// magnitude (8 x 6 = 48 bins).  The primary rays are split into chunks of at
 // most COMPACT_CHUNK rays that never straddle a scene (chunk c: rays
-// [start, end) of scene `scene`).  Per chunk and octant the bounce rays are
-// counted, the counts turned into offsets per scene and octant, and each chunk
-// writes its bounce rays at their place with the hit slot (2i + k) of each in
-// `map`.  Every position follows from the counts alone, so the order is the
+// [start, end) of scene `scene`).  Per chunk and bin the bounce rays are
+// counted; the counts become offsets per scene and bin; each chunk writes its
+// bounce rays at their place with the hit slot (2i + k) of each in `map`.
+// Order inside a (scene, bin) group: chunk by chunk, inside a chunk the first
+// bounce rays (k = 0) of its primary rays in primary order, then the second
+// ones.  Every position follows from the counts alone, so the order is the
 // same on every run.
 constexpr uint32_t COMPACT_CHUNK = 1024;
+constexpr uint32_t NB = 48;  // direction bins
 
 struct CompactChunk {
     uint32_t start, end, scene, pad;
 };
 
-__device__ __forceinline__ uint32_t octant_of(const vx_ray& r) {
-    return uint32_t(r.dx > 0.0f) | (uint32_t(r.dy > 0.0f) << 1) | (uint32_t(r.dz > 0.0f) << 2);
+__device__ __forceinline__ uint32_t bin_of(const vx_ray& r) {
+    const uint32_t octant = uint32_t(r.dx > 0.0f) | (uint32_t(r.dy > 0.0f) << 1) | (uint32_t(r.dz > 0.0f) << 2);
+    const float ax = fabsf(r.dx), ay = fabsf(r.dy), az = fabsf(r.dz);
+    const uint32_t major = (ax >= ay && ax >= az) ? 0u : (ay >= az ? 1u : 2u);
+    const uint32_t minor = (ax < ay && ax < az) ? 0u : (ay < az ? 1u : 2u);  // never equal to major
+    const uint32_t next = major == 2u ? 0u : major + 1u;
+    return octant * 6u + major * 2u + (minor == next ? 0u : 1u);
 }
 
-// The 2 bounce rays of primary ray i, or false on a miss.
-__device__ __forceinline__ bool bounce_pair(const vx_ray* __restrict__ rays, const vx_hit* __restrict__ hits,
-                                            uint64_t i, uint64_t seed, vx_ray out[2]) {
+// Secondary origin of primary ray i, or false on a miss.
+__device__ __forceinline__ bool bounce_origin(const vx_ray* __restrict__ rays, const vx_hit* __restrict__ hits,
+                                              uint64_t i, float org[3], int& axis, float& sgn) {
     const vx_ray r = rays[i];
     const vx_hit h = hits[i];
-    float org[3];
-    int axis;
-    float sgn;
-    if (!secondary_origin(r, h, org, axis, sgn)) return false;
-    out[0] = bounce_ray(org, axis, sgn, i, 0, seed);
-    out[1] = bounce_ray(org, axis, sgn, i, 1, seed);
-    return true;
+    return secondary_origin(r, h, org, axis, sgn);
 }
 
-// counts[c * 8 + o]: bounce rays of chunk c heading into octant o.
+// counts[c * NB + b]: bounce rays of chunk c in bin b.
 __global__ void __launch_bounds__(256) compact_count_kernel(const CompactChunk* __restrict__ chunks,
                                                             const vx_ray* __restrict__ rays,
                                                             const vx_hit* __restrict__ hits, uint64_t seed,
                                                             uint32_t* __restrict__ counts) {
-    __shared__ uint32_t hist[8];
-    if (threadIdx.x < 8) hist[threadIdx.x] = 0;
+    __shared__ uint32_t hist[NB];
+    if (threadIdx.x < NB) hist[threadIdx.x] = 0;
     __syncthreads();
     const CompactChunk ch = chunks[blockIdx.x];
     for (uint32_t i = ch.start + threadIdx.x; i < ch.end; i += blockDim.x) {
-        vx_ray b[2];
-        if (bounce_pair(rays, hits, i, seed, b)) {
-            atomicAdd(&hist[octant_of(b[0])], 1u);
-            atomicAdd(&hist[octant_of(b[1])], 1u);
+        float org[3];
+        int axis;
+        float sgn;
+        if (bounce_origin(rays, hits, i, org, axis, sgn)) {
+            atomicAdd(&hist[bin_of(bounce_ray(org, axis, sgn, i, 0, seed))], 1u);
+            atomicAdd(&hist[bin_of(bounce_ray(org, axis, sgn, i, 1, seed))], 1u);
         }
     }
     __syncthreads();
-    if (threadIdx.x < 8) counts[blockIdx.x * 8 + threadIdx.x] = hist[threadIdx.x];
+    if (threadIdx.x < NB) counts[blockIdx.x * NB + threadIdx.x] = hist[threadIdx.x];
 }
 
-// One block: offs[c * 8 + o] = bounce rays of scene s = chunk c's scene that
-// come before chunk c's octant-o rays in the compacted order, i.e. the rays of
-// the scenes before s, of s's octants below o, and of s's earlier chunks in
-// octant o.  cbegin[s] is scene s's first compacted ray, cbegin[S] the count.
-// tot (S * 8 words of scratch) holds the per-scene, per-octant totals.
-__global__ void __launch_bounds__(1024) compact_offsets_kernel(const uint32_t* __restrict__ counts,
-                                                               const uint32_t* __restrict__ first_chunk, uint32_t S,
-                                                               uint32_t* __restrict__ offs, uint32_t* __restrict__ tot,
-                                                               uint32_t* __restrict__ cbegin) {
-    // one warp per (scene, octant): exclusive scan over the scene's chunks, 32 at a time
-    const uint32_t lane = threadIdx.x & 31u, nwarps = blockDim.x >> 5;
-    for (uint32_t t = threadIdx.x >> 5; t < S * 8; t += nwarps) {
-        const uint32_t sc = t >> 3, o = t & 7u, end = first_chunk[sc + 1];
+// Block s: offs[c * NB + b] = bounce rays of scene s's bin b in its chunks
+// before chunk c (an exclusive scan over the scene's chunks, one warp per
+// bin, 32 chunks at a time); tot[s * NB + b] = the bin's total.
+__global__ void __launch_bounds__(512) compact_scan_kernel(const uint32_t* __restrict__ counts,
+                                                           const uint32_t* __restrict__ first_chunk,
+                                                           uint32_t* __restrict__ offs, uint32_t* __restrict__ tot) {
+    const uint32_t sc = blockIdx.x, lane = threadIdx.x & 31u, nwarps = blockDim.x >> 5;
+    const uint32_t begin = first_chunk[sc], end = first_chunk[sc + 1];
+    for (uint32_t b = threadIdx.x >> 5; b < NB; b += nwarps) {
         uint32_t run = 0;
-        for (uint32_t c0 = first_chunk[sc]; c0 < end; c0 += 32) {
+        for (uint32_t c0 = begin; c0 < end; c0 += 32) {
             const uint32_t c = c0 + lane;
-            const uint32_t v = c < end ? counts[c * 8 + o] : 0u;
+            const uint32_t v = c < end ? counts[c * NB + b] : 0u;
             uint32_t x = v;
             for (int d = 1; d < 32; d <<= 1) {
                 const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
                 if (lane >= uint32_t(d)) x += y;
             }
-            if (c < end) offs[c * 8 + o] = run + (x - v);
+            if (c < end) offs[c * NB + b] = run + (x - v);
             run += __shfl_sync(0xFFFFFFFFu, x, 31);
         }
-        if (lane == 0) tot[t] = run;
+        if (lane == 0) tot[sc * NB + b] = run;
     }
+}
+
+// One block: tot (S * NB totals in (scene, bin) order) becomes the exclusive
+// prefix, the first compacted ray of each (scene, bin) group; cbegin[s] is
+// scene s's first compacted ray and cbegin[S] the count.
+__global__ void __launch_bounds__(1024) compact_base_kernel(uint32_t* __restrict__ tot, uint32_t S,
+                                                            uint32_t* __restrict__ cbegin) {
+    __shared__ uint32_t wsum[32];
+    const uint32_t items = S * NB, per = (items + blockDim.x - 1) / blockDim.x;
+    const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+    const uint32_t lo = min(items, t * per), hi = min(items, lo + per);
+    uint32_t mine = 0;
+    for (uint32_t j = lo; j < hi; ++j) mine += tot[j];
+    uint32_t x = mine;  // inclusive scan over the block: warps, then warp totals
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+        if (lane >= uint32_t(d)) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t run = 0;
-        for (uint32_t t = 0; t < S * 8; ++t) {
-            if ((t & 7u) == 0) cbegin[t >> 3] = run;
-            const uint32_t v = tot[t];
-            tot[t] = run;  // now the base of (scene, octant)
-            run += v;
+    if (warp == 0) {
+        const uint32_t nw = blockDim.x >> 5;
+        uint32_t w = lane < nw ? wsum[lane] : 0u;
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, d);
+            if (lane >= uint32_t(d)) w += y;
         }
-        cbegin[S] = run;
+        wsum[lane] = w;  // inclusive over warps
     }
     __syncthreads();
-    for (uint32_t sc = 0; sc < S; ++sc)
-        for (uint32_t c = first_chunk[sc] + threadIdx.x / 8; c < first_chunk[sc + 1]; c += blockDim.x / 8)
-            offs[c * 8 + (threadIdx.x & 7u)] += tot[sc * 8 + (threadIdx.x & 7u)];
+    uint32_t run = (warp ? wsum[warp - 1] : 0u) + (x - mine);
+    for (uint32_t j = lo; j < hi; ++j) {
+        const uint32_t v = tot[j];
+        tot[j] = run;
+        if (j % NB == 0) cbegin[j / NB] = run;
+        run += v;
+    }
+    if (t == blockDim.x - 1) cbegin[S] = wsum[(blockDim.x >> 5) - 1];
 }
 
 // The record a cast writes for a zero-direction ray (cast_init: the ray fails
@@ -414,59 +438,60 @@ __device__ __forceinline__ void store_invalid(vx_hit* hits, uint64_t slot) {
     reinterpret_cast<uint4*>(hits)[slot] = make_uint4(0u, NONE, NONE, 0xFFFFu | (uint32_t(F_INVALID) << 16));
 }
 
-// Writes chunk c's bounce rays at offs[c * 8 + o] + their rank among the
-// chunk's octant-o rays in (i, k) order; the slots of misses get the invalid
-// record.  256 primary rays per round: lane ranks by ballot per octant, warp
-// totals through shared memory, a running count per octant across rounds.
+// Writes chunk c's bounce rays at base[scene * NB + b] + offs[c * NB + b] +
+// their rank in the chunk's order (k = 0 rays in primary order, then k = 1);
+// the slots of misses get the invalid record.  256 primary rays per round:
+// lanes of one bin find each other with __match_any_sync and rank by lane,
+// warp totals go through shared memory, a running count per bin crosses the
+// rounds and the two k passes.
 __global__ void __launch_bounds__(256) compact_scatter_kernel(const CompactChunk* __restrict__ chunks,
                                                               const vx_ray* __restrict__ rays,
                                                               const vx_hit* __restrict__ hits, uint64_t seed,
                                                               const uint32_t* __restrict__ offs,
+                                                              const uint32_t* __restrict__ base,
                                                               vx_ray* __restrict__ out, uint32_t* __restrict__ map,
                                                               vx_hit* __restrict__ bounce_hits) {
-    __shared__ uint32_t wcnt[8][8];  // [warp][octant]
-    __shared__ uint32_t run[8];
+    __shared__ uint32_t wcnt[8][NB];  // [warp][bin]
+    __shared__ uint32_t run[NB];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t below = (1u << lane) - 1u;
     const CompactChunk ch = chunks[blockIdx.x];
-    if (threadIdx.x < 8) run[threadIdx.x] = offs[blockIdx.x * 8 + threadIdx.x];
-    __syncthreads();
-    for (uint32_t base = ch.start; base < ch.end; base += 256) {
-        const uint32_t i = base + threadIdx.x;
-        vx_ray b[2];
-        const bool hit = i < ch.end && bounce_pair(rays, hits, i, seed, b);
-        const uint32_t o0 = hit ? octant_of(b[0]) : 8u, o1 = hit ? octant_of(b[1]) : 8u;
-        uint32_t r0 = 0, r1 = 0;
-#pragma unroll
-        for (uint32_t o = 0; o < 8; ++o) {
-            const uint32_t m0 = __ballot_sync(0xFFFFFFFFu, o0 == o), m1 = __ballot_sync(0xFFFFFFFFu, o1 == o);
-            const uint32_t before = __popc(m0 & below) + __popc(m1 & below);
-            if (o0 == o) r0 = before;
-            if (o1 == o) r1 = before + (o0 == o ? 1u : 0u);
-            if (lane == 0) wcnt[warp][o] = __popc(m0) + __popc(m1);
-        }
-        __syncthreads();
-        if (hit) {
-            uint32_t p0 = run[o0] + r0, p1 = run[o1] + r1;
-            for (uint32_t w = 0; w < warp; ++w) {
-                p0 += wcnt[w][o0];
-                p1 += wcnt[w][o1];
+    if (threadIdx.x < NB) run[threadIdx.x] = base[ch.scene * NB + threadIdx.x] + offs[blockIdx.x * NB + threadIdx.x];
+    for (uint32_t k = 0; k < 2; ++k) {
+        for (uint32_t r0 = ch.start; r0 < ch.end; r0 += 256) {
+            for (uint32_t j = threadIdx.x; j < 8 * NB; j += blockDim.x) (&wcnt[0][0])[j] = 0u;
+            __syncthreads();
+            const uint32_t i = r0 + threadIdx.x;
+            float org[3];
+            int axis;
+            float sgn;
+            const bool hit = i < ch.end && bounce_origin(rays, hits, i, org, axis, sgn);
+            vx_ray b{};
+            uint32_t bin = NB;  // none
+            if (hit) {
+                b = bounce_ray(org, axis, sgn, i, k, seed);
+                bin = bin_of(b);
             }
-            out[p0] = b[0];
-            map[p0] = 2 * i;
-            out[p1] = b[1];
-            map[p1] = 2 * i + 1;
-        } else if (i < ch.end) {
-            store_invalid(bounce_hits, 2 * uint64_t(i));
-            store_invalid(bounce_hits, 2 * uint64_t(i) + 1);
+            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, bin);
+            if (hit && (peers & below) == 0) wcnt[warp][bin] = __popc(peers);  // the group's first lane
+            __syncthreads();
+            if (hit) {
+                uint32_t p = run[bin] + __popc(peers & below);
+                for (uint32_t w = 0; w < warp; ++w) p += wcnt[w][bin];
+                out[p] = b;
+                map[p] = 2 * i + k;
+            } else if (k == 0 && i < ch.end) {
+                store_invalid(bounce_hits, 2 * uint64_t(i));
+                store_invalid(bounce_hits, 2 * uint64_t(i) + 1);
+            }
+            __syncthreads();
+            if (threadIdx.x < NB) {
+                uint32_t add = 0;
+                for (uint32_t w = 0; w < 8; ++w) add += wcnt[w][threadIdx.x];
+                run[threadIdx.x] += add;
+            }
+            __syncthreads();  // the next round clears wcnt
         }
-        __syncthreads();
-        if (threadIdx.x < 8) {
-            uint32_t add = 0;
-            for (uint32_t w = 0; w < 8; ++w) add += wcnt[w][threadIdx.x];
-            run[threadIdx.x] += add;
-        }
-        __syncthreads();
     }
 }
 
@@ -907,7 +932,7 @@ static int vx_batch_autotune_body(vx_batch* b, const vx_ray* rays, const uint32_
     const int blocks[] = {128, 256};
     const int ks[] = {32, 64, 128, 256, 512, 1024};
     const int refills[] = {0, 8, 16, 24};
-    const int budgets[] = {0, 24, 48};
+    const int budgets[] = {0, 32};
     if (int r = ensure_retry(b, n, st)) { cudaEventDestroy(e0); cudaEventDestroy(e1); return r; }
     for (int blk : blocks)
         for (int sm = 1; sm >= 0; --sm)
@@ -1130,13 +1155,14 @@ static int capture_compact(vx_batch* b, const vx_ray* primary, const uint32_t* p
     }
     first[b->S] = uint32_t(chunks.size());
     const uint32_t nc = uint32_t(chunks.size());
-    // Scratch (allocated outside the capture): chunk table, per-chunk octant
-    // counts and offsets, first chunk of each scene, per-scene octant bases,
-    // the S + 1 scene offsets of the compacted rays and their 2n hit slots.
+    // Scratch (allocated outside the capture): chunk table, per-chunk bin
+    // counts and offsets, first chunk of each scene, (scene, bin) totals and
+    // then bases, the S + 1 scene offsets of the compacted rays and their 2n
+    // hit slots.
     auto a256 = [](uint64_t x) { return (x + 255) & ~uint64_t(255); };
     const uint64_t o_cnt = a256(uint64_t(nc) * sizeof(vx::CompactChunk));
-    const uint64_t o_offs = o_cnt + a256(uint64_t(nc) * 32), o_first = o_offs + a256(uint64_t(nc) * 32);
-    const uint64_t o_tot = o_first + a256((uint64_t(b->S) + 1) * 4), o_cbeg = o_tot + a256(uint64_t(b->S) * 32);
+    const uint64_t o_offs = o_cnt + a256(uint64_t(nc) * vx::NB * 4), o_first = o_offs + a256(uint64_t(nc) * vx::NB * 4);
+    const uint64_t o_tot = o_first + a256((uint64_t(b->S) + 1) * 4), o_cbeg = o_tot + a256(uint64_t(b->S) * vx::NB * 4);
     const uint64_t o_map = o_cbeg + a256((uint64_t(b->S) + 1) * 4), need = o_map + a256(uint64_t(n) * 8);
     if (need > b->fscratch_bytes) {
         cudaFree(b->fscratch);
@@ -1165,8 +1191,9 @@ static int capture_compact(vx_batch* b, const vx_ray* primary, const uint32_t* p
     if (r == VX_OK) r = record_primary_done(b, st);
     if (r == VX_OK) {
         vx::compact_count_kernel<<<nc, 256, 0, st>>>(chunk_dev, primary, primary_hits, seed, counts);
-        vx::compact_offsets_kernel<<<1, 1024, 0, st>>>(counts, first_dev, b->S, offs, tot, cbegin);
-        vx::compact_scatter_kernel<<<nc, 256, 0, st>>>(chunk_dev, primary, primary_hits, seed, offs, bounce, map,
+        vx::compact_scan_kernel<<<b->S, 512, 0, st>>>(counts, first_dev, offs, tot);
+        vx::compact_base_kernel<<<1, 1024, 0, st>>>(tot, b->S, cbegin);
+        vx::compact_scatter_kernel<<<nc, 256, 0, st>>>(chunk_dev, primary, primary_hits, seed, offs, tot, bounce, map,
                                                        bounce_hits);
         const cudaError_t le = cudaGetLastError();
         if (le != cudaSuccess) r = cuda_err(le, "vx_batch_capture_frame_compact: compaction launch");

@@ -633,6 +633,39 @@ __device__ __forceinline__ bool advance_pop(const DevScene& s, CastState& st, co
     return false;
 }
 
+// executePushPhase (:328-378) into the iteration's child (tx_center etc. of
+// checkChildValidity): the parent goes on the stack when tc_max < h.
+__device__ __forceinline__ void push_child(const DevScene& s, CastState& st, const Corners& k, int worldIdx,
+                                           float tv_max, uint32_t* stkN, float* stkT, int stride) {
+    const Coef& c = st.c;
+    const int minScale = s.min_scale;
+    const float half = st.scale_exp2 * 0.5f;
+    const float tx_center = half * c.tx_coef + k.tx;
+    const float ty_center = half * c.ty_coef + k.ty;
+    const float tz_center = half * c.tz_coef + k.tz;
+    const float tc_max = nmin3(k.tx, k.ty, k.tz);
+    if (tc_max < st.hh) {
+        const uint32_t kk = bounded(uint32_t(st.scale - minScale), uint32_t(s.max_levels), V_STACK);
+        stkN[kk * stride] = st.parent;
+        stkT[kk * stride] = st.t_max;
+        st.pushed |= 1u << (st.scale - minScale);
+    }
+    st.hh = tc_max;
+    const uint32_t nonLeafMask = ~(st.pMask >> 8) & st.pMask & 0xFFu;
+    const uint32_t child_index = st.pChild + __popc(nonLeafMask & ((1u << worldIdx) - 1u));
+    if (child_index < s.node_count) {
+        st.parent = child_index;
+        st.idx = 0;
+        st.scale--;
+        st.scale_exp2 = half;
+        if (tx_center > st.t_min) { st.idx ^= 1; st.px += st.scale_exp2; }
+        if (ty_center > st.t_min) { st.idx ^= 2; st.py += st.scale_exp2; }
+        if (tz_center > st.t_min) { st.idx ^= 4; st.pz += st.scale_exp2; }
+        st.t_max = tv_max;
+        st.fetched = false;
+    }
+}
+
 // The end of an iteration: the cycle check (see above).  g0 / dd0: the grid
 // reads and DDA steps counted when the iteration began.  True when a proven
 // repeat ends the ray.
@@ -710,8 +743,9 @@ __device__ __forceinline__ bool cycle_check(CastState& st, uint32_t g0, uint32_t
 }
 
 // One iteration, its loop condition first.  Returns true when the ray is
-// finished (hit, exit, cap).
-template <bool LOD = false, bool DEFER = false>
+// finished (hit, exit, cap).  MERGE: how the branches after the child test are
+// laid out (same operations and results either way).
+template <bool LOD = false, bool DEFER = false, bool MERGE = false>
 __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint32_t* stkN, float* stkT,
                                           uint32_t* cyc, int stride, LodCone lod = LodCone{0.0f, 0.0f}) {
     Hit& h = st.h;
@@ -763,43 +797,31 @@ __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint
             }
         }
     }
-    // A leaf child in range: the leaf stage; when its brick is not hit the
-    // iteration continues with ADVANCE from tv_max, like a child out of range,
-    // so both run the one ADVANCE below together (lanes of a warp that took
-    // either way stay converged there).
-    if (in_range && isLeaf) {
-        if (leaf_stage(s, st, csx, csy, csz)) return true;
-        st.t_min = tv_max;
-    }
-    if (in_range && !isLeaf) {
-        // executePushPhase (:328-378); tx_center etc. of checkChildValidity
-        const float half = st.scale_exp2 * 0.5f;
-        const float tx_center = half * c.tx_coef + k.tx;
-        const float ty_center = half * c.ty_coef + k.ty;
-        const float tz_center = half * c.tz_coef + k.tz;
-        const float tc_max = nmin3(k.tx, k.ty, k.tz);
-        if (tc_max < st.hh) {
-            const uint32_t kk = bounded(uint32_t(st.scale - minScale), uint32_t(s.max_levels), V_STACK);
-            stkN[kk * stride] = st.parent;
-            stkT[kk * stride] = st.t_max;
-            st.pushed |= 1u << (st.scale - minScale);
+    if constexpr (MERGE) {
+        // A leaf child in range: the leaf stage; when its brick is not hit the
+        // iteration continues with ADVANCE from tv_max, like a child out of
+        // range, and both run the one ADVANCE below (lanes of a warp that took
+        // either way stay converged there: incoherent rays).
+        if (in_range && isLeaf) {
+            if (leaf_stage(s, st, csx, csy, csz)) return true;
+            st.t_min = tv_max;
         }
-        st.hh = tc_max;
-        const uint32_t nonLeafMask = ~(st.pMask >> 8) & st.pMask & 0xFFu;
-        const uint32_t child_index = st.pChild + __popc(nonLeafMask & ((1u << worldIdx) - 1u));
-        if (child_index < s.node_count) {
-            st.parent = child_index;
-            st.idx = 0;
-            st.scale--;
-            st.scale_exp2 = half;
-            if (tx_center > st.t_min) { st.idx ^= 1; st.px += st.scale_exp2; }
-            if (ty_center > st.t_min) { st.idx ^= 2; st.py += st.scale_exp2; }
-            if (tz_center > st.t_min) { st.idx ^= 4; st.pz += st.scale_exp2; }
-            st.t_max = tv_max;
-            st.fetched = false;
-        }
+        if (in_range && !isLeaf) push_child(s, st, k, worldIdx, tv_max, stkN, stkT, stride);
+        else if (advance_pop(s, st, k, csx, csy, csz, stkN, stkT, stride)) return true;
     } else {
-        if (advance_pop(s, st, k, csx, csy, csz, stkN, stkT, stride)) return true;
+        // The same iteration as the reference writes its branches (coherent
+        // rays, whose warps take one way at a time).
+        if (in_range) {
+            if (isLeaf) {
+                if (leaf_stage(s, st, csx, csy, csz)) return true;
+                st.t_min = tv_max;
+                if (advance_pop(s, st, k, csx, csy, csz, stkN, stkT, stride)) return true;
+            } else {
+                push_child(s, st, k, worldIdx, tv_max, stkN, stkT, stride);
+            }
+        } else if (advance_pop(s, st, k, csx, csy, csz, stkN, stkT, stride)) {
+            return true;
+        }
     }
     return cycle_check<DEFER>(st, g0, dd0, cyc, stride);
 }
@@ -820,14 +842,14 @@ __device__ __forceinline__ void cast_ray(const DevScene& s, float ox, float oy, 
 // cast_ray that gives up once `budget` iterations have run without ending the
 // ray: false then, and h is not written.  The cast is deterministic, so the
 // caller can cast the ray again from the start for its result.
-template <bool LOD = false, bool DEFER = false>
+template <bool LOD = false, bool DEFER = false, bool MERGE = false>
 __device__ __forceinline__ bool cast_ray_budget(const DevScene& s, float ox, float oy, float oz, float ddx, float ddy,
                                                 float ddz, float tMinArg, float tMaxArg, uint32_t* stkN, float* stkT,
                                                 uint32_t* cyc, int stride, int budget, Hit& h) {
     CastState st;
     if (!cast_init(s, ox, oy, oz, ddx, ddy, ddz, tMinArg, tMaxArg, stkN, stkT, stride, st)) {
         // every cast_step that returns false has counted one iteration in st.iter
-        while (!cast_step<LOD, DEFER>(s, st, stkN, stkT, cyc, stride)) {
+        while (!cast_step<LOD, DEFER, MERGE>(s, st, stkN, stkT, cyc, stride)) {
             if (st.iter >= budget) return false;
         }
     }
