@@ -132,6 +132,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_refill_kernel(BatchArgs a) 
     uint32_t ray = 0;
     int sid = 0;
     CastState st;
+    uint32_t ck[CK_WORDS];
     for (;;) {
         uint32_t idle = __ballot_sync(FULL, !active);
         if (__popc(idle) >= a.refill || idle == FULL) {
@@ -169,7 +170,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_refill_kernel(BatchArgs a) 
             if (!tasks_left && next >= end) break;
             continue;
         }
-        if (active && cast_step<false, !SMEM_STACK, true>(sc[sid], st, stkN, stkT, cyc, stride)) {
+        if (active && cast_step<false, !SMEM_STACK, true>(sc[sid], st, stkN, stkT, cyc, stride, ck)) {
+            finish_skipped(st, ck);
             store_hit(a.hits, out_slot(a, ray), st.h);
             store_counters(a.counters, out_slot(a, ray), st.h);
             active = false;

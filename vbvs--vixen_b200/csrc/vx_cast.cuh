@@ -43,6 +43,9 @@ constexpr int MAX_ITER = 500;       // SVOTraversal.cpp:588
 #endif
 constexpr int CYCLE_START = VX_CYCLE_START;  // iteration from which loop states are compared
 constexpr int CYC_WORDS = 16;                 // cycle-detection words per ray: two stored loop states
+constexpr int LONG_FIRST = 16;                // first checkpoint of the long-cycle check (then 32, 64, ...)
+constexpr int CK_WORDS = 16 + 2 * 23;         // long-cycle checkpoint: state, counters, stack (23 slots at most)
+constexpr uint32_t SKIPPED = 1u << 31;        // in CastState::pushed: whole cycles were skipped
 constexpr float FLT_MAX_ = 3.402823466e+38f;
 constexpr uint32_t NONE = 0xFFFFFFFFu;
 
@@ -231,6 +234,7 @@ struct CastState {
     // cycle detection
     uint32_t d1g, d1d;     // grid reads / DDA steps of the previous iteration
     uint32_t sig1, sig2;   // signatures of the loop states one and two iterations back
+    uint32_t ck_sig;       // signature of the long-cycle checkpoint
     int cand_p, cand_at;   // deferred check: pending candidate's period, iteration it is confirmed at
 };
 
@@ -415,7 +419,7 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
     st.hh = t_max;
     st.pChild = st.pMask = 0;
     st.d1g = st.d1d = 0;
-    st.sig1 = st.sig2 = 0;
+    st.sig1 = st.sig2 = st.ck_sig = 0;
     st.cand_p = st.cand_at = 0;
     return false;
 }
@@ -666,11 +670,90 @@ __device__ __forceinline__ void push_child(const DevScene& s, CastState& st, con
     }
 }
 
+// Long cycles (Brent's method).  A state can also repeat after p > 2
+// iterations; then the stack matters too, since a POP inside the cycle may
+// read a slot that the cycle only writes after it.  At iterations 16, 32, 64,
+// 128 and 256 the loop state, the pushed mask, the pushed stack slots and the
+// counters are copied to the checkpoint `ck` (per-thread local memory, only
+// touched there); a later state whose signature equals the checkpoint's is
+// compared in full, stack included.  Equal means that every later iteration
+// repeats the p = iter - iter(ck) iterations since the checkpoint, with the
+// same counter increments, and that no hit or exit can come.  The whole
+// cycles the 500-iteration cap leaves room for are then skipped (an even
+// number when p is odd, so the short check's parity slots stay in step):
+// iter and the counters advance by whole cycles and the loop goes on for the
+// rest, fewer than 2p iterations, which ends at the cap with the reference's
+// counters.  ck[12..14] keep the skipped iterations, grid reads and DDA steps
+// so that the executed counts (run_*) can be restored (finish_skipped).
+//   ck: [0..7] state words, [8] pushed mask, [9] iter, [10] grid reads,
+//       [11] DDA steps, [12..14] skipped, [16 + 2j], [17 + 2j] stack slot j
+__device__ __forceinline__ void long_cycle_checkpoint(const CastState& st, const uint32_t* cur, const uint32_t* stkN,
+                                                      const float* stkT, int stride, uint32_t* ck) {
+    const uint32_t pm = st.pushed & ~SKIPPED;
+    for (int k = 0; k < 8; ++k) ck[k] = cur[k];
+    ck[8] = pm;
+    ck[9] = uint32_t(st.iter);
+    ck[10] = st.h.grid_reads;
+    ck[11] = st.h.dda_steps;
+    for (uint32_t m = pm; m; m &= m - 1u) {
+        const int j = __ffs(int(m)) - 1;
+        ck[16 + 2 * j] = stkN[j * stride];
+        ck[17 + 2 * j] = __float_as_uint(stkT[j * stride]);
+    }
+}
+
+__device__ __forceinline__ bool long_cycle_equal(const CastState& st, const uint32_t* cur, const uint32_t* stkN,
+                                                 const float* stkT, int stride, const uint32_t* ck) {
+    bool eq = (st.pushed & ~SKIPPED) == ck[8];
+    for (int k = 0; k < 8; ++k) eq = eq && cur[k] == ck[k];
+    for (uint32_t m = ck[8]; eq && m; m &= m - 1u) {
+        const int j = __ffs(int(m)) - 1;
+        eq = stkN[j * stride] == ck[16 + 2 * j] && __float_as_uint(stkT[j * stride]) == ck[17 + 2 * j];
+    }
+    return eq;
+}
+
+__device__ __forceinline__ void long_cycle(CastState& st, uint32_t sig, const uint32_t* cur, const uint32_t* stkN,
+                                           const float* stkT, int stride, uint32_t* ck) {
+    Hit& h = st.h;
+    if ((st.iter & (st.iter - 1)) == 0) {
+        long_cycle_checkpoint(st, cur, stkN, stkT, stride, ck);
+        st.ck_sig = sig;
+    } else if (sig == st.ck_sig && long_cycle_equal(st, cur, stkN, stkT, stride, ck)) {
+        const uint32_t p = uint32_t(st.iter) - ck[9];
+        uint32_t m = uint32_t(MAX_ITER - st.iter) / p;
+        if (p & 1u) m &= ~1u;
+        if (m) {
+            const uint32_t si = m * p, sg = m * (h.grid_reads - ck[10]), sd = m * (h.dda_steps - ck[11]);
+            if (!(st.pushed & SKIPPED)) {
+                ck[12] = ck[13] = ck[14] = 0u;
+                st.pushed |= SKIPPED;
+            }
+            ck[12] += si;
+            ck[13] += sg;
+            ck[14] += sd;
+            st.iter += int(si);
+            h.grid_reads += sg;
+            h.dda_steps += sd;
+        }
+    }
+}
+
+// After the ray has finished: run_* count what was executed, not the skipped cycles.
+__device__ __forceinline__ void finish_skipped(CastState& st, const uint32_t* ck) {
+    if (st.pushed & SKIPPED) {
+        st.h.run_iters -= ck[12];
+        st.h.run_grid_reads -= ck[13];
+        st.h.run_dda_steps -= ck[14];
+    }
+}
+
 // The end of an iteration: the cycle check (see above).  g0 / dd0: the grid
 // reads and DDA steps counted when the iteration began.  True when a proven
 // repeat ends the ray.
 template <bool DEFER>
-__device__ __forceinline__ bool cycle_check(CastState& st, uint32_t g0, uint32_t dd0, uint32_t* cyc, int stride) {
+__device__ __forceinline__ bool cycle_check(CastState& st, uint32_t g0, uint32_t dd0, uint32_t* cyc, int stride,
+                                            const uint32_t* stkN, const float* stkT, uint32_t* ck) {
     Hit& h = st.h;
     if (st.iter < CYCLE_START) return false;
     uint32_t cur[8];
@@ -735,6 +818,7 @@ __device__ __forceinline__ bool cycle_check(CastState& st, uint32_t g0, uint32_t
         h.flags |= F_ITER_CAP;
         return true;
     }
+    if (st.iter >= LONG_FIRST) long_cycle(st, sig, cur, stkN, stkT, stride, ck);
     st.sig2 = st.sig1;
     st.sig1 = sig;
     st.d1g = dg;
@@ -747,7 +831,8 @@ __device__ __forceinline__ bool cycle_check(CastState& st, uint32_t g0, uint32_t
 // laid out (same operations and results either way).
 template <bool LOD = false, bool DEFER = false, bool MERGE = false>
 __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint32_t* stkN, float* stkT,
-                                          uint32_t* cyc, int stride, LodCone lod = LodCone{0.0f, 0.0f}) {
+                                          uint32_t* cyc, int stride, uint32_t* ck,
+                                          LodCone lod = LodCone{0.0f, 0.0f}) {
     Hit& h = st.h;
     const Coef& c = st.c;
     const int minScale = s.min_scale;
@@ -823,7 +908,7 @@ __device__ __forceinline__ bool cast_step(const DevScene& s, CastState& st, uint
             return true;
         }
     }
-    return cycle_check<DEFER>(st, g0, dd0, cyc, stride);
+    return cycle_check<DEFER>(st, g0, dd0, cyc, stride, stkN, stkT, ck);
 }
 
 // castRayImpl (SVOTraversal.cpp:516-691): setup, then the loop.  LOD = false
@@ -833,9 +918,12 @@ __device__ __forceinline__ void cast_ray(const DevScene& s, float ox, float oy, 
                                          float ddz, float tMinArg, float tMaxArg, uint32_t* stkN, float* stkT,
                                          uint32_t* cyc, int stride, Hit& h, LodCone lod = LodCone{0.0f, 0.0f}) {
     CastState st;
-    if (!cast_init(s, ox, oy, oz, ddx, ddy, ddz, tMinArg, tMaxArg, stkN, stkT, stride, st))
-        while (!cast_step<LOD, DEFER>(s, st, stkN, stkT, cyc, stride, lod)) {
+    uint32_t ck[CK_WORDS];
+    if (!cast_init(s, ox, oy, oz, ddx, ddy, ddz, tMinArg, tMaxArg, stkN, stkT, stride, st)) {
+        while (!cast_step<LOD, DEFER>(s, st, stkN, stkT, cyc, stride, ck, lod)) {
         }
+        finish_skipped(st, ck);
+    }
     h = st.h;
 }
 
@@ -847,11 +935,13 @@ __device__ __forceinline__ bool cast_ray_budget(const DevScene& s, float ox, flo
                                                 float ddz, float tMinArg, float tMaxArg, uint32_t* stkN, float* stkT,
                                                 uint32_t* cyc, int stride, int budget, Hit& h) {
     CastState st;
+    uint32_t ck[CK_WORDS];
     if (!cast_init(s, ox, oy, oz, ddx, ddy, ddz, tMinArg, tMaxArg, stkN, stkT, stride, st)) {
         // every cast_step that returns false has counted one iteration in st.iter
-        while (!cast_step<LOD, DEFER, MERGE>(s, st, stkN, stkT, cyc, stride)) {
+        while (!cast_step<LOD, DEFER, MERGE>(s, st, stkN, stkT, cyc, stride, ck)) {
             if (st.iter >= budget) return false;
         }
+        finish_skipped(st, ck);
     }
     h = st.h;
     return true;
