@@ -494,8 +494,8 @@ def measure_cfg4(args, rank, world, steps, warmup, with_cpu):
 
 def run_cfg4_pass(args):
     """One launch of each pass of the batched frame over the first `--scenes` scenes of the frame,
-    with the tunings the default run's autotuner picks (primary: block 256, 32 rays per task,
-    shared-memory stack; bounce: block 256, 256 rays per task, local stack, refill 16).  The
+    with fixed tunings (both passes: block 256, 32 rays per task, shared-memory stack, static
+    lanes, no iteration budget; what the default run's autotuner picks on this frame).  The
     command for ncu captures of the frame's kernels on a small case: after the frame's graph, each
     of --steps steps launches the primary pass, then the bounce pass over the compacted bounce
     rays."""
@@ -523,7 +523,7 @@ def run_cfg4_pass(args):
     bounce = torch.zeros((2 * n, 6), dtype=torch.float32, device="cuda")
     batch = vx.Batch(scenes)
     batch.set_tuning(256, 32, 1, 0)
-    batch.set_bounce_tuning(vx.BatchTuning(256, 256, 0, 16))
+    batch.set_bounce_tuning(vx.BatchTuning(256, 32, 1, 0, 0))
     s = torch.cuda.Stream()
     with torch.cuda.stream(s):
         batch.capture_frame_compact(d_rays, d_begin, ph, bounce, bh, CFG4_SEED, s.cuda_stream)
@@ -540,7 +540,7 @@ def run_cfg4_pass(args):
         ev[0].record()
         batch.cast(d_rays, d_begin, ph)
         ev[1].record()
-        batch.set_tuning(256, 256, 0, 16)
+        batch.set_tuning(256, 32, 1, 0, 0)
         ev[2].record()
         batch.cast(bounce[:h2], d_cb, pbh)
         ev[3].record()
