@@ -16,9 +16,14 @@ namespace {
 constexpr int BLOCK = VX_CAST_BLOCK;
 constexpr int RENDER_WARPS = VX_RENDER_WARPS;
 constexpr int RENDER_THREADS = RENDER_WARPS * 32;
+// Resident blocks per SM the cast kernel is compiled for: 14 blocks of 64
+// threads leave 72 registers a thread (cfg2 frame 0.1208 -> 0.1188 ms against
+// 12 blocks at 80 registers; 16 blocks at 64 registers spill and measure
+// 0.1249 ms).
+constexpr int CAST_MIN_BLOCKS = 896 / BLOCK;
 
 template <bool LOD>
-__global__ void __launch_bounds__(BLOCK, 768 / BLOCK) cast_kernel(DevScene s, const vx_ray* __restrict__ rays, uint32_t n,
+__global__ void __launch_bounds__(BLOCK, CAST_MIN_BLOCKS) cast_kernel(DevScene s, const vx_ray* __restrict__ rays, uint32_t n,
                                                       float tmin, float tmax, vx_hit* __restrict__ hits,
                                                       void* __restrict__ color,
                                                       vx_ray_counters* __restrict__ counters, LodCone lod) {
