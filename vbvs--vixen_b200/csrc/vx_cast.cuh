@@ -103,6 +103,8 @@ __device__ __forceinline__ float nclamp(float v, float lo, float hi) { return fm
 __device__ __forceinline__ int f2i(float f) {
     return (f >= -2147483648.0f && f < 2147483648.0f) ? __float2int_rz(f) : INT_MIN;
 }
+// The same for a value known to lie in [0, 2^31): the truncation alone.
+__device__ __forceinline__ int f2i_in_range(float f) { return __float2int_rz(f); }
 
 __device__ __forceinline__ uint32_t grid_lookup(const DevScene& s, int bx, int by, int bz) {
     // getBrickViewByGrid (SVOBuilder.h:107-116) over the dense table
@@ -492,8 +494,9 @@ __device__ __forceinline__ bool leaf_stage(const DevScene& s, CastState& st, boo
     const float hx = nclamp(ix * s.wsize[0], 0.0f, s.wsm[0]);
     const float hy = nclamp(iy * s.wsize[1], 0.0f, s.wsm[1]);
     const float hz = nclamp(iz * s.wsize[2], 0.0f, s.wsm[2]);
-    uint32_t brick = grid_lookup(s, iclamp(f2i(hx * 0.125f), 0, bmax), iclamp(f2i(hy * 0.125f), 0, bmax),
-                                 iclamp(f2i(hz * 0.125f), 0, bmax));
+    // hx, hy, hz are clamped to [0, wsize - 0.001]: the conversions are in range
+    uint32_t brick = grid_lookup(s, iclamp(f2i_in_range(hx * 0.125f), 0, bmax),
+                                 iclamp(f2i_in_range(hy * 0.125f), 0, bmax), iclamp(f2i_in_range(hz * 0.125f), 0, bmax));
     ++h.grid_reads;
     uint32_t method = 1;
     if (brick == NONE) {
@@ -503,8 +506,9 @@ __device__ __forceinline__ bool leaf_stage(const DevScene& s, CastState& st, boo
             const float ex = fclamp(((st.ox + st.dx * te0) - s.wmin[0]) + st.dx * 0.01f, 0.0f, s.wsm[0]);
             const float ey = fclamp(((st.oy + st.dy * te0) - s.wmin[1]) + st.dy * 0.01f, 0.0f, s.wsm[1]);
             const float ez = fclamp(((st.oz + st.dz * te0) - s.wmin[2]) + st.dz * 0.01f, 0.0f, s.wsm[2]);
-            st.brick2 = grid_lookup(s, iclamp(f2i(ex * 0.125f), 0, bmax), iclamp(f2i(ey * 0.125f), 0, bmax),
-                                    iclamp(f2i(ez * 0.125f), 0, bmax));
+            st.brick2 = grid_lookup(s, iclamp(f2i_in_range(ex * 0.125f), 0, bmax),
+                                    iclamp(f2i_in_range(ey * 0.125f), 0, bmax),
+                                    iclamp(f2i_in_range(ez * 0.125f), 0, bmax));
             st.have_brick2 = true;
         }
         brick = st.brick2;
@@ -957,17 +961,15 @@ __device__ __forceinline__ void dxt_texel(const uint2* dxt, uint32_t brick, uint
     const float scale = 1.0f / 4294967296.0f;
     const float r0x = float(head << 16) * scale, r0y = float(head << 21) * scale, r0z = float(head << 27) * scale;
     const float r1x = float(head) * scale, r1y = float(head << 5) * scale, r1z = float(head << 11) * scale;
-    if (sel == 0) { r = r0x; g = r0y; b = r0z; }
-    else if (sel == 1) { r = r1x; g = r1y; b = r1z; }
-    else if (sel == 2) {
-        r = r0x * (2.0f / 3.0f) + r1x * (1.0f / 3.0f);
-        g = r0y * (2.0f / 3.0f) + r1y * (1.0f / 3.0f);
-        b = r0z * (2.0f / 3.0f) + r1z * (1.0f / 3.0f);
-    } else {
-        r = r0x * (1.0f / 3.0f) + r1x * (2.0f / 3.0f);
-        g = r0y * (1.0f / 3.0f) + r1y * (2.0f / 3.0f);
-        b = r0z * (1.0f / 3.0f) + r1z * (2.0f / 3.0f);
-    }
+    // The shader's four cases as one blend r0 * w0 + r1 * w1, (w0, w1) = (1, 0), (0, 1),
+    // (2/3, 1/3), (1/3, 2/3) for selectors 0..3: the same roundings (the endpoints are finite
+    // and non-negative, so x * 1 = x and x * 0 + y = y exactly), without a branch per selector
+    // (neighbouring voxels of a warp have different selectors).
+    const float w0 = sel == 0u ? 1.0f : (sel == 1u ? 0.0f : (sel == 2u ? 2.0f / 3.0f : 1.0f / 3.0f));
+    const float w1 = sel == 0u ? 0.0f : (sel == 1u ? 1.0f : (sel == 2u ? 1.0f / 3.0f : 2.0f / 3.0f));
+    r = r0x * w0 + r1x * w1;
+    g = r0y * w0 + r1y * w1;
+    b = r0z * w0 + r1z * w1;
 }
 
 // getCompressedVoxelNormal (VoxelRayMarch_Compressed.comp:160-165):
