@@ -349,15 +349,13 @@ __device__ __forceinline__ bool bounce_origin(const vx_ray* __restrict__ rays, c
     return secondary_origin(r, h, org, axis, sgn);
 }
 
-// counts[c * NB + b]: bounce rays of chunk c in bin b; first[c * NB + b]:
-// those of them that are first bounce rays (k = 0).
+// counts[c * NB + b]: bounce rays of chunk c in bin b.
 __global__ void __launch_bounds__(256) compact_count_kernel(const CompactChunk* __restrict__ chunks,
                                                             const vx_ray* __restrict__ rays,
                                                             const vx_hit* __restrict__ hits, uint64_t seed,
-                                                            uint32_t* __restrict__ counts,
-                                                            uint32_t* __restrict__ first) {
-    __shared__ uint32_t hist[2][NB];
-    if (threadIdx.x < 2 * NB) (&hist[0][0])[threadIdx.x] = 0;
+                                                            uint32_t* __restrict__ counts) {
+    __shared__ uint32_t hist[NB];
+    if (threadIdx.x < NB) hist[threadIdx.x] = 0;
     __syncthreads();
     const CompactChunk ch = chunks[blockIdx.x];
     for (uint32_t i = ch.start + threadIdx.x; i < ch.end; i += blockDim.x) {
@@ -365,15 +363,12 @@ __global__ void __launch_bounds__(256) compact_count_kernel(const CompactChunk* 
         int axis;
         float sgn;
         if (bounce_origin(rays, hits, i, org, axis, sgn)) {
-            atomicAdd(&hist[0][bin_of(bounce_ray(org, axis, sgn, i, 0, seed))], 1u);
-            atomicAdd(&hist[1][bin_of(bounce_ray(org, axis, sgn, i, 1, seed))], 1u);
+            atomicAdd(&hist[bin_of(bounce_ray(org, axis, sgn, i, 0, seed))], 1u);
+            atomicAdd(&hist[bin_of(bounce_ray(org, axis, sgn, i, 1, seed))], 1u);
         }
     }
     __syncthreads();
-    if (threadIdx.x < NB) {
-        counts[blockIdx.x * NB + threadIdx.x] = hist[0][threadIdx.x] + hist[1][threadIdx.x];
-        first[blockIdx.x * NB + threadIdx.x] = hist[0][threadIdx.x];
-    }
+    if (threadIdx.x < NB) counts[blockIdx.x * NB + threadIdx.x] = hist[threadIdx.x];
 }
 
 // Block s: offs[c * NB + b] = bounce rays of scene s's bin b in its chunks
@@ -446,73 +441,59 @@ __device__ __forceinline__ void store_invalid(vx_hit* hits, uint64_t slot) {
 }
 
 // Writes chunk c's bounce rays at base[scene * NB + b] + offs[c * NB + b] +
-// their rank in the chunk's order (the k = 0 rays of bin b in primary order,
-// then its k = 1 rays, which start first[c * NB + b] later); the slots of
-// misses get the invalid record.  256 primary rays per round, both bounce
-// rays of each: lanes of one bin find each other with __match_any_sync and
-// rank by lane, warp totals go through shared memory, a running count per
-// (k, bin) crosses the rounds.
+// their rank in the chunk's order (k = 0 rays in primary order, then k = 1);
+// the slots of misses get the invalid record.  256 primary rays per round:
+// lanes of one bin find each other with __match_any_sync and rank by lane,
+// warp totals go through shared memory, a running count per bin crosses the
+// rounds and the two k passes.
 __global__ void __launch_bounds__(256) compact_scatter_kernel(const CompactChunk* __restrict__ chunks,
                                                               const vx_ray* __restrict__ rays,
                                                               const vx_hit* __restrict__ hits, uint64_t seed,
                                                               const uint32_t* __restrict__ offs,
-                                                              const uint32_t* __restrict__ first,
                                                               const uint32_t* __restrict__ base,
                                                               vx_ray* __restrict__ out, uint32_t* __restrict__ map,
                                                               vx_hit* __restrict__ bounce_hits) {
-    __shared__ uint32_t wcnt[2][8][NB];  // [k][warp][bin]
-    __shared__ uint32_t run[2][NB];
+    __shared__ uint32_t wcnt[8][NB];  // [warp][bin]
+    __shared__ uint32_t run[NB];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t below = (1u << lane) - 1u;
     const CompactChunk ch = chunks[blockIdx.x];
-    if (threadIdx.x < NB) {
-        const uint32_t r0 = base[ch.scene * NB + threadIdx.x] + offs[blockIdx.x * NB + threadIdx.x];
-        run[0][threadIdx.x] = r0;
-        run[1][threadIdx.x] = r0 + first[blockIdx.x * NB + threadIdx.x];
-    }
-    for (uint32_t r0 = ch.start; r0 < ch.end; r0 += 256) {
-        for (uint32_t j = threadIdx.x; j < 2 * 8 * NB; j += blockDim.x) (&wcnt[0][0][0])[j] = 0u;
-        __syncthreads();
-        const uint32_t i = r0 + threadIdx.x;
-        float org[3];
-        int axis;
-        float sgn;
-        const bool hit = i < ch.end && bounce_origin(rays, hits, i, org, axis, sgn);
-        vx_ray b[2] = {};
-        uint32_t bin[2] = {NB, NB};  // NB: none
-        if (hit) {
-            b[0] = bounce_ray(org, axis, sgn, i, 0, seed);
-            b[1] = bounce_ray(org, axis, sgn, i, 1, seed);
-            bin[0] = bin_of(b[0]);
-            bin[1] = bin_of(b[1]);
-        }
-        const uint32_t peers0 = __match_any_sync(0xFFFFFFFFu, bin[0]);
-        const uint32_t peers1 = __match_any_sync(0xFFFFFFFFu, bin[1]);
-        if (hit && (peers0 & below) == 0) wcnt[0][warp][bin[0]] = __popc(peers0);  // the group's first lane
-        if (hit && (peers1 & below) == 0) wcnt[1][warp][bin[1]] = __popc(peers1);
-        __syncthreads();
-        if (hit) {
-            uint32_t p0 = run[0][bin[0]] + __popc(peers0 & below), p1 = run[1][bin[1]] + __popc(peers1 & below);
-            for (uint32_t w = 0; w < warp; ++w) {
-                p0 += wcnt[0][w][bin[0]];
-                p1 += wcnt[1][w][bin[1]];
+    if (threadIdx.x < NB) run[threadIdx.x] = base[ch.scene * NB + threadIdx.x] + offs[blockIdx.x * NB + threadIdx.x];
+    for (uint32_t k = 0; k < 2; ++k) {
+        for (uint32_t r0 = ch.start; r0 < ch.end; r0 += 256) {
+            for (uint32_t j = threadIdx.x; j < 8 * NB; j += blockDim.x) (&wcnt[0][0])[j] = 0u;
+            __syncthreads();
+            const uint32_t i = r0 + threadIdx.x;
+            float org[3];
+            int axis;
+            float sgn;
+            const bool hit = i < ch.end && bounce_origin(rays, hits, i, org, axis, sgn);
+            vx_ray b{};
+            uint32_t bin = NB;  // none
+            if (hit) {
+                b = bounce_ray(org, axis, sgn, i, k, seed);
+                bin = bin_of(b);
             }
-            out[p0] = b[0];
-            map[p0] = 2 * i;
-            out[p1] = b[1];
-            map[p1] = 2 * i + 1;
-        } else if (i < ch.end) {
-            store_invalid(bounce_hits, 2 * uint64_t(i));
-            store_invalid(bounce_hits, 2 * uint64_t(i) + 1);
+            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, bin);
+            if (hit && (peers & below) == 0) wcnt[warp][bin] = __popc(peers);  // the group's first lane
+            __syncthreads();
+            if (hit) {
+                uint32_t p = run[bin] + __popc(peers & below);
+                for (uint32_t w = 0; w < warp; ++w) p += wcnt[w][bin];
+                out[p] = b;
+                map[p] = 2 * i + k;
+            } else if (k == 0 && i < ch.end) {
+                store_invalid(bounce_hits, 2 * uint64_t(i));
+                store_invalid(bounce_hits, 2 * uint64_t(i) + 1);
+            }
+            __syncthreads();
+            if (threadIdx.x < NB) {
+                uint32_t add = 0;
+                for (uint32_t w = 0; w < 8; ++w) add += wcnt[w][threadIdx.x];
+                run[threadIdx.x] += add;
+            }
+            __syncthreads();  // the next round clears wcnt
         }
-        __syncthreads();
-        if (threadIdx.x < 2 * NB) {
-            const uint32_t kk = threadIdx.x / NB, bb = threadIdx.x - kk * NB;
-            uint32_t add = 0;
-            for (uint32_t w = 0; w < 8; ++w) add += wcnt[kk][w][bb];
-            run[kk][bb] += add;
-        }
-        __syncthreads();  // the next round clears wcnt
     }
 }
 
@@ -1177,13 +1158,12 @@ static int capture_compact(vx_batch* b, const vx_ray* primary, const uint32_t* p
     first[b->S] = uint32_t(chunks.size());
     const uint32_t nc = uint32_t(chunks.size());
     // Scratch (allocated outside the capture): chunk table, per-chunk bin
-    // counts (all and first bounce rays) and offsets, first chunk of each
-    // scene, (scene, bin) totals and then bases, the S + 1 scene offsets of
-    // the compacted rays and their 2n hit slots.
+    // counts and offsets, first chunk of each scene, (scene, bin) totals and
+    // then bases, the S + 1 scene offsets of the compacted rays and their 2n
+    // hit slots.
     auto a256 = [](uint64_t x) { return (x + 255) & ~uint64_t(255); };
     const uint64_t o_cnt = a256(uint64_t(nc) * sizeof(vx::CompactChunk));
-    const uint64_t o_k0 = o_cnt + a256(uint64_t(nc) * vx::NB * 4);
-    const uint64_t o_offs = o_k0 + a256(uint64_t(nc) * vx::NB * 4), o_first = o_offs + a256(uint64_t(nc) * vx::NB * 4);
+    const uint64_t o_offs = o_cnt + a256(uint64_t(nc) * vx::NB * 4), o_first = o_offs + a256(uint64_t(nc) * vx::NB * 4);
     const uint64_t o_tot = o_first + a256((uint64_t(b->S) + 1) * 4), o_cbeg = o_tot + a256(uint64_t(b->S) * vx::NB * 4);
     const uint64_t o_map = o_cbeg + a256((uint64_t(b->S) + 1) * 4), need = o_map + a256(uint64_t(n) * 8);
     if (need > b->fscratch_bytes) {
@@ -1197,7 +1177,6 @@ static int capture_compact(vx_batch* b, const vx_ray* primary, const uint32_t* p
     char* base = static_cast<char*>(b->fscratch);
     auto* chunk_dev = reinterpret_cast<vx::CompactChunk*>(base);
     uint32_t* counts = reinterpret_cast<uint32_t*>(base + o_cnt);
-    uint32_t* counts0 = reinterpret_cast<uint32_t*>(base + o_k0);
     uint32_t* offs = reinterpret_cast<uint32_t*>(base + o_offs);
     uint32_t* first_dev = reinterpret_cast<uint32_t*>(base + o_first);
     uint32_t* tot = reinterpret_cast<uint32_t*>(base + o_tot);
@@ -1213,11 +1192,10 @@ static int capture_compact(vx_batch* b, const vx_ray* primary, const uint32_t* p
                           stream);
     if (r == VX_OK) r = record_primary_done(b, st);
     if (r == VX_OK) {
-        vx::compact_count_kernel<<<nc, 256, 0, st>>>(chunk_dev, primary, primary_hits, seed, counts, counts0);
+        vx::compact_count_kernel<<<nc, 256, 0, st>>>(chunk_dev, primary, primary_hits, seed, counts);
         vx::compact_scan_kernel<<<b->S, 512, 0, st>>>(counts, first_dev, offs, tot);
         vx::compact_base_kernel<<<1, 1024, 0, st>>>(tot, b->S, cbegin);
-        vx::compact_scatter_kernel<<<nc, 256, 0, st>>>(chunk_dev, primary, primary_hits, seed, offs, counts0, tot,
-                                                       bounce, map,
+        vx::compact_scatter_kernel<<<nc, 256, 0, st>>>(chunk_dev, primary, primary_hits, seed, offs, tot, bounce, map,
                                                        bounce_hits);
         const cudaError_t le = cudaGetLastError();
         if (le != cudaSuccess) r = cuda_err(le, "vx_batch_capture_frame_compact: compaction launch");
