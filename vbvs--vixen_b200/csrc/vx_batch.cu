@@ -11,6 +11,11 @@
 // that finish early take their next ray while others are still traversing);
 // the warp re-converges at the next task fetch.  The per-ray traversal is the
 // one of the plain kernel (vx_cast.cuh), so hits are identical bit for bit.
+// Static lanes may take an iteration budget: rays still running after it are
+// listed and cast again from the start by a second launch over the list.
+// The frame (vx_batch_capture_frame_compact) casts only the bounce rays of
+// primary hits, grouped per scene by direction bin; vx_batch_capture_frame_parts
+// captures it in parts whose host copies overlap the other parts' casts.
 #include <algorithm>
 #include <cmath>
 #include <mutex>

@@ -231,7 +231,7 @@ struct CastState {
     // SVOTypes.h:343-364, moves bit i to i ^ flip, flip = ~octant_mask & 7) at
     // the ray-space octant idx; that is bit idx ^ flip of the unmirrored mask.
     uint32_t pChild, pMask;
-    uint32_t pushed;       // stack slots written by PUSH (bit scale - minScale)
+    uint32_t pushed;       // stack slots written by PUSH (bit scale - minScale); bit 31: SKIPPED
     float t_root;          // t_max of the unwritten slots
     // cycle detection
     uint32_t d1g, d1d;     // grid reads / DDA steps of the previous iteration
