@@ -108,8 +108,9 @@ __device__ __forceinline__ int f2i_in_range(float f) { return __float2int_rz(f);
 
 __device__ __forceinline__ uint32_t grid_lookup(const DevScene& s, int bx, int by, int bz) {
     // getBrickViewByGrid (SVOBuilder.h:107-116) over the dense table
-    // (VoxelSceneCacher.cpp:670-713).
-    size_t li = size_t(bx) + size_t(by) * size_t(s.bpa) + size_t(bz) * size_t(s.bpa) * size_t(s.bpa);
+    // (VoxelSceneCacher.cpp:670-713).  Every scene constructor keeps
+    // bricks_per_axis <= 1024, so the index fits 32 bits.
+    size_t li = uint32_t(bx) + uint32_t(s.bpa) * (uint32_t(by) + uint32_t(s.bpa) * uint32_t(bz));
 #if VX_CHECKED
     const size_t slots = size_t(s.bpa) * size_t(s.bpa) * size_t(s.bpa);
     if (li >= slots || bx < 0 || by < 0 || bz < 0) { atomicOr(&vx_violation, V_GRID); li = 0; }
@@ -281,15 +282,20 @@ __device__ __forceinline__ bool cast_init(const DevScene& s, float ox, float oy,
         dx = ddx * inv; dy = ddy * inv; dz = ddz * inv;
         // length(normalize(d)) < 1e-6: for dd in [1e-30, 1e30] every component is
         // finite and the normalised length is 1 within a few ulp, so the check
-        // can only fail outside that range.
+        // can only fail outside that range.  In that range |d_i| <= sqrt(dd),
+        // so the normalised components are finite as well and only the origin
+        // needs the isnan || isinf test; outside it (an infinite or NaN input
+        // lands there too) the components are tested.
+        // isnan || isinf of a value: !(|x| < inf) is both tests at once
+        const float inf = __int_as_float(0x7F800000);
         if (!(dd >= 1e-30f && dd <= 1e30f)) {
             const float len = sqrtf((dx * dx + dy * dy) + dz * dz);
-            if (len < 1e-6f) { h.flags = F_INVALID; return true; }
+            if (len < 1e-6f || !(fabsf(dx) < inf) || !(fabsf(dy) < inf) || !(fabsf(dz) < inf)) {
+                h.flags = F_INVALID;
+                return true;
+            }
         }
-        // isnan || isinf of any component: !(|x| < inf) is both tests at once
-        const float inf = __int_as_float(0x7F800000);
-        if (!(fabsf(ox) < inf) || !(fabsf(oy) < inf) || !(fabsf(oz) < inf) || !(fabsf(dx) < inf) ||
-            !(fabsf(dy) < inf) || !(fabsf(dz) < inf)) {
+        if (!(fabsf(ox) < inf) || !(fabsf(oy) < inf) || !(fabsf(oz) < inf)) {
             h.flags = F_INVALID;
             return true;
         }
